@@ -1,0 +1,261 @@
+/*
+ * rav2d_gpu.h - C ABI of the B200 in-loop filter + film-grain library.
+ *
+ * This is the drop-in boundary for the post-reconstruction stage of the rav2d
+ * AV2 decoder. A host decoder (the rav2d Rust crate through an `extern "C"`
+ * FFI crate, or any C/C++/Python caller) keeps entropy decoding, prediction
+ * and reconstruction on the CPU and hands each reconstructed frame plus its
+ * filter side-info to this library, which runs deblocking, CDEF+CCSO, loop
+ * restoration (NS-Wiener, PC-Wiener, GDF) and film grain on one GPU.
+ *
+ * Every struct below is a fixed-layout mirror of the reference's Rust types;
+ * the citation on each gives the file:line (paths inside the rav2d project)
+ * of the type it mirrors. Plain pointers and sizes only: no CUDA or torch
+ * types appear in any signature.
+ *
+ * Sample storage: 8-bit frames are uint8_t samples, 10-bit frames uint16_t.
+ * Strides are in BYTES, as in the reference's Picture (picture.rs:79-97).
+ * Supported layout: 4:2:0, sb128 = 0, one tile row, width and height
+ * multiples of 8 (every workload the library is specified for); anything else
+ * is rejected with R2G_E_INVALID rather than filtered differently.
+ *
+ * Threading: a context is used by one host thread at a time. Calls enqueue
+ * work on the context's streams and return; r2g_wait / r2g_sync block.
+ */
+#ifndef RAV2D_GPU_H
+#define RAV2D_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference filters are infallible; these report
+ * boundary misuse and device problems instead of aborting) ---- */
+#define R2G_OK 0
+#define R2G_E_INVALID (-1)  /* bad argument or unsupported configuration */
+#define R2G_E_OOM (-2)      /* device-memory budget or allocation exhausted */
+#define R2G_E_TIMEOUT (-3)  /* r2g_wait deadline passed; work still queued */
+#define R2G_E_DEVICE (-4)   /* CUDA error or device-side watchdog tripped */
+#define R2G_E_NOTREADY (-5) /* ticket not complete (non-blocking poll) */
+
+/* ---- inloop filter bitmask (looprestoration.rs:1697-1706) ---- */
+#define R2G_INLOOP_DEBLOCK (1u << 0)
+#define R2G_INLOOP_CDEF (1u << 1)
+#define R2G_INLOOP_CCSO (1u << 2)
+#define R2G_INLOOP_WIENER (1u << 3)
+#define R2G_INLOOP_GDF (1u << 4)
+#define R2G_INLOOP_ALL 0x1fu
+
+/* ---- restoration types (looprestoration.rs:1671-1677) ---- */
+#define R2G_RESTORE_NONE 0
+#define R2G_RESTORE_PC_WIENER 1
+#define R2G_RESTORE_NS_WIENER 2
+#define R2G_RESTORE_SWITCHABLE 3
+
+/* Per-SB256 filter side-info; mirrors `Av2Filter` (lf_mask.rs:8-19).
+ * filter_y[dir][pos][k][i]: dir 0 = vertical edges (pos = x4 in the SB256,
+ * i = sb64 row, bit = y4 in the sb64), dir 1 = horizontal edges (pos = y4,
+ * i = sb64 column, bit = x4); k = edge class 0..3, k = 4 marks sub-PU edges.
+ * filter_uv: the same for 4:2:0 chroma (pos = chroma x4/y4 in the SB256,
+ * i = pair index, low/high byte for even/odd sb64).  sizeof == 12100. */
+typedef struct R2gAv2Filter {
+    uint16_t filter_y[2][64][5][4];
+    uint16_t filter_uv[2][64][5][4];
+    uint16_t qidx[16];
+    uint8_t gdf[16];
+    int8_t cdef_idx[16];
+    uint8_t ccso[3];
+    uint8_t _pad0;
+    uint16_t noskip_mask[32][4];
+    uint16_t lr_noskip_mask[64][4];
+    uint16_t lossless_mask_y[64][4];
+    uint16_t lossless_mask_uv[64][4];
+} R2gAv2Filter;
+
+/* Mirrors `Av2RestorationUnit` (lf_mask.rs:2-5).  sizeof == 513. */
+typedef struct R2gAv2RestorationUnit {
+    uint8_t restoration_type;
+    int8_t ns_filter[16][32];
+} R2gAv2RestorationUnit;
+
+/* Mirrors `Av2Restoration` (lf_mask.rs:39-41): [plane][unit in SB256]. */
+typedef struct R2gAv2Restoration {
+    R2gAv2RestorationUnit lr[3][16];
+} R2gAv2Restoration;
+
+/* Mirrors `FhCcsoPlane` (headers.rs:640-652). */
+typedef struct R2gCcsoPlane {
+    uint8_t enabled;
+    uint8_t bo_only;
+    uint8_t scale_idx;
+    uint8_t quant_idx;
+    uint8_t ext_filter_support;
+    uint8_t edge_clf;
+    uint8_t max_band_log2;
+    uint8_t _pad0;
+    uint8_t filter_off[64];
+} R2gCcsoPlane;
+
+/* Mirrors `NSWienerPlane` + `FhRestorationPlane` (headers.rs:618-632). */
+typedef struct R2gRestorationPlane {
+    uint8_t restoration_type;
+    uint8_t frame_filters_on;
+    uint8_t num_classes_idx;
+    uint8_t num_classes;
+    int8_t filter[16][18];
+} R2gRestorationPlane;
+
+/* Frame-constant parameters of the filter path: the parts of the sequence
+ * and frame headers that `FilterFrameParams::new` (decode.rs:3645-3710),
+ * `init_wiener` (decode.rs:27), `compute_restore_planes` (decode.rs:59) and
+ * `compute_gdf_ref_dst_idx` (decode.rs:67) read. */
+typedef struct R2gFrameParams {
+    int32_t width;  /* luma samples */
+    int32_t height; /* luma samples */
+    int32_t bitdepth; /* 8 or 10 */
+    int32_t layout;   /* 1 = 4:2:0 (the only supported value) */
+    int32_t sb128;    /* must be 0 */
+    int32_t cfl_ds_filter_index; /* SequenceHeader.cfl_ds_filter_index */
+    /* FhDeblock (headers.rs:590-598) */
+    uint8_t deblock_level_y[2];
+    uint8_t deblock_level_u;
+    uint8_t deblock_level_v;
+    int8_t deblock_delta_q_y[2];
+    int8_t deblock_delta_q_u;
+    int8_t deblock_delta_q_v;
+    /* FhQuant (headers.rs:556-564): yac and the AC deltas */
+    int32_t quant_yac;
+    int8_t quant_uac_delta;
+    int8_t quant_vac_delta;
+    /* FhSegmentation (headers.rs:566-576): enabled, per-segment delta_q and
+     * lossless flags.  segmap pointers may be NULL when disabled. */
+    uint8_t seg_enabled;
+    uint8_t _pad0;
+    int16_t seg_delta_q[8];
+    uint8_t seg_lossless[8];
+    /* SequenceHeader.cdef + FhCdef (headers.rs:608-615) */
+    uint8_t seq_cdef;
+    uint8_t cdef_damping;
+    uint8_t cdef_on_skiptx;
+    uint8_t cdef_n_strengths;
+    uint8_t cdef_y_strength[8];
+    uint8_t cdef_uv_strength[8];
+    /* FhCcso (headers.rs:673-677) */
+    R2gCcsoPlane ccso[3];
+    /* FhRestoration (headers.rs:634-638) */
+    R2gRestorationPlane restoration[3];
+    uint8_t restoration_unit_size[2]; /* log2, luma / chroma */
+    /* FhGdf (headers.rs:601-606): enabled is AdaptiveBoolean (0 = off) */
+    uint8_t gdf_enabled;
+    uint8_t gdf_qp_idx;
+    uint8_t gdf_scale;
+    /* inputs of compute_gdf_ref_dst_idx: frame_type & 1 = inter/switch */
+    uint8_t frame_type;
+    uint8_t n_ref_frames;
+    uint8_t absrefdist[7];
+} R2gFrameParams;
+
+/* Mirrors `FilmGrainData` (headers.rs:509-525). */
+typedef struct R2gFilmGrainData {
+    int32_t chroma_scaling_from_luma;
+    int32_t num_points[3];
+    uint8_t points[3][14][2];
+    int32_t scaling_shift;
+    int32_t ar_coeff_lag;
+    int8_t ar_coeffs[3][28];
+    int32_t ar_coeff_shift;
+    int32_t grain_scale_shift;
+    int32_t uv_mult[2];
+    int32_t uv_luma_mult[2];
+    int32_t uv_offset[2];
+    int32_t overlap_flag;
+    int32_t clip_to_restricted_range;
+    int32_t mc_identity;
+    int32_t block_size;
+} R2gFilmGrainData;
+
+/* Opaque handles. */
+typedef struct R2gCtx R2gCtx;
+typedef struct R2gFrame R2gFrame;
+
+/* Frame side-info as the reference keeps it in `LoopFilterState`
+ * (internal.rs:152-167) after Phase A: n_sb256 = sb256w * sb256h masks in
+ * raster order, the same count of restoration records, and the optional
+ * segment maps (b4 granularity; NULL = all segment 0). */
+typedef struct R2gSideInfo {
+    const R2gAv2Filter *masks;
+    const R2gAv2Restoration *lr;
+    int32_t n_sb256;
+    const uint8_t *segmap;
+    int32_t segmap_stride;
+    const uint8_t *segmap_uv;
+    int32_t segmap_uv_stride;
+} R2gSideInfo;
+
+/* ---- version / capability ---- */
+int r2g_version(void);
+/* Plane geometry of the reference's DefaultPicAllocator (picture.rs:79-97):
+ * width/height aligned to 128, stride in bytes, bumped by 64 when it is a
+ * multiple of 1024.  Pure host function. */
+int r2g_plane_geometry(int width, int height, int bitdepth, int64_t *y_stride,
+                       int64_t *uv_stride, int64_t *y_rows, int64_t *uv_rows);
+/* Bytes of `sizeof` for each ABI struct, so a binding can check its mirror. */
+int r2g_struct_sizes(int32_t *sizes, int n);
+
+/* ---- context: one per host thread; `device` is the CUDA ordinal,
+ * `mem_budget` the device bytes the context may hold (0 = no limit). ---- */
+int r2g_ctx_create(int device, int64_t mem_budget, R2gCtx **out);
+int r2g_ctx_destroy(R2gCtx *ctx);
+const char *r2g_last_error(R2gCtx *ctx);
+
+/* ---- device-resident frames (frame buffers live in the context) ---- */
+int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth, R2gFrame **out);
+int r2g_frame_free(R2gCtx *ctx, R2gFrame *f);
+/* Upload the reconstructed planes (host pointers, byte strides). */
+int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, int64_t y_stride,
+                           const void *u, const void *v, int64_t uv_stride);
+/* Run every enabled stage for the whole frame.  Equivalent to calling the
+ * reference's `filter_sbrow` (decode.rs:3718-4058) for every sby of the frame
+ * in order; replaces the Phase-B loop at decode.rs:3597-3625. */
+int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp,
+                     const R2gSideInfo *side, uint32_t inloop_mask);
+/* Film grain on the filtered frame into the frame's display copy; replaces
+ * `apply_grain_to_picture_mt` (decode.rs:4672). */
+int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed);
+/* Copy the filtered planes (which = 0) or the grained display copy
+ * (which = 1) into host memory; enqueued, complete after r2g_sync. */
+int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_t y_stride, void *u,
+                 void *v, int64_t uv_stride);
+/* Block until every call enqueued on the context has finished. */
+int r2g_sync(R2gCtx *ctx);
+
+/* ---- one-call convenience: host recon in, host filtered/grained out ---- */
+int r2g_filter_frame_host(R2gCtx *ctx, const R2gFrameParams *fp, const R2gSideInfo *side,
+                          uint32_t inloop_mask, const R2gFilmGrainData *fgd, uint32_t grain_seed,
+                          const void *src_y, const void *src_u, const void *src_v,
+                          int64_t y_stride, int64_t uv_stride, void *dst_y, void *dst_u,
+                          void *dst_v, void *grain_y, void *grain_u, void *grain_v);
+
+/* ---- batching: one persistent launch per stage over many frames ---- */
+typedef struct R2gBatchItem {
+    R2gFrame *frame;
+    const R2gFrameParams *fp;
+    const R2gSideInfo *side;
+    uint32_t inloop_mask;
+    const R2gFilmGrainData *fgd; /* NULL = no grain */
+    uint32_t grain_seed;
+} R2gBatchItem;
+/* Enqueue the whole batch; returns a ticket for r2g_wait. */
+int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ticket);
+/* Wait for a ticket; R2G_E_TIMEOUT after timeout_ms (<0 = forever),
+ * timeout_ms == 0 polls (R2G_E_NOTREADY when pending). */
+int r2g_wait(R2gCtx *ctx, uint64_t ticket, int timeout_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RAV2D_GPU_H */

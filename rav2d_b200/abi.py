@@ -1,0 +1,196 @@
+"""ctypes / numpy mirrors of the C ABI in include/rav2d_gpu.h.
+
+The per-SB256 side-info records are numpy structured dtypes (so whole frames
+of masks are one contiguous array); the frame-constant parameter blocks are
+ctypes structures.  Both reproduce the C layout byte for byte; `check_sizes`
+compares them against the library's own `sizeof` values.
+"""
+import ctypes as C
+
+import numpy as np
+
+R2G_OK = 0
+R2G_E_INVALID = -1
+R2G_E_OOM = -2
+R2G_E_TIMEOUT = -3
+R2G_E_DEVICE = -4
+R2G_E_NOTREADY = -5
+
+INLOOP_DEBLOCK = 1 << 0
+INLOOP_CDEF = 1 << 1
+INLOOP_CCSO = 1 << 2
+INLOOP_WIENER = 1 << 3
+INLOOP_GDF = 1 << 4
+INLOOP_ALL = 0x1F
+
+RESTORE_NONE = 0
+RESTORE_PC_WIENER = 1
+RESTORE_NS_WIENER = 2
+RESTORE_SWITCHABLE = 3
+
+# R2gAv2Filter (mirrors Av2Filter, lf_mask.rs:8-19)
+AV2_FILTER_DTYPE = np.dtype([
+    ("filter_y", "<u2", (2, 64, 5, 4)),
+    ("filter_uv", "<u2", (2, 64, 5, 4)),
+    ("qidx", "<u2", (16,)),
+    ("gdf", "u1", (16,)),
+    ("cdef_idx", "i1", (16,)),
+    ("ccso", "u1", (3,)),
+    ("_pad0", "u1"),
+    ("noskip_mask", "<u2", (32, 4)),
+    ("lr_noskip_mask", "<u2", (64, 4)),
+    ("lossless_mask_y", "<u2", (64, 4)),
+    ("lossless_mask_uv", "<u2", (64, 4)),
+])
+assert AV2_FILTER_DTYPE.itemsize == 12100
+
+# R2gAv2RestorationUnit / R2gAv2Restoration (lf_mask.rs:2-5, :39-41)
+LR_UNIT_DTYPE = np.dtype([("restoration_type", "u1"), ("ns_filter", "i1", (16, 32))])
+assert LR_UNIT_DTYPE.itemsize == 513
+AV2_RESTORATION_DTYPE = np.dtype([("lr", LR_UNIT_DTYPE, (3, 16))])
+assert AV2_RESTORATION_DTYPE.itemsize == 513 * 48
+
+
+class CcsoPlane(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_uint8),
+        ("bo_only", C.c_uint8),
+        ("scale_idx", C.c_uint8),
+        ("quant_idx", C.c_uint8),
+        ("ext_filter_support", C.c_uint8),
+        ("edge_clf", C.c_uint8),
+        ("max_band_log2", C.c_uint8),
+        ("_pad0", C.c_uint8),
+        ("filter_off", C.c_uint8 * 64),
+    ]
+
+
+class RestorationPlane(C.Structure):
+    _fields_ = [
+        ("restoration_type", C.c_uint8),
+        ("frame_filters_on", C.c_uint8),
+        ("num_classes_idx", C.c_uint8),
+        ("num_classes", C.c_uint8),
+        ("filter", (C.c_int8 * 18) * 16),
+    ]
+
+
+class FrameParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("bitdepth", C.c_int32),
+        ("layout", C.c_int32),
+        ("sb128", C.c_int32),
+        ("cfl_ds_filter_index", C.c_int32),
+        ("deblock_level_y", C.c_uint8 * 2),
+        ("deblock_level_u", C.c_uint8),
+        ("deblock_level_v", C.c_uint8),
+        ("deblock_delta_q_y", C.c_int8 * 2),
+        ("deblock_delta_q_u", C.c_int8),
+        ("deblock_delta_q_v", C.c_int8),
+        ("quant_yac", C.c_int32),
+        ("quant_uac_delta", C.c_int8),
+        ("quant_vac_delta", C.c_int8),
+        ("seg_enabled", C.c_uint8),
+        ("_pad0", C.c_uint8),
+        ("seg_delta_q", C.c_int16 * 8),
+        ("seg_lossless", C.c_uint8 * 8),
+        ("seq_cdef", C.c_uint8),
+        ("cdef_damping", C.c_uint8),
+        ("cdef_on_skiptx", C.c_uint8),
+        ("cdef_n_strengths", C.c_uint8),
+        ("cdef_y_strength", C.c_uint8 * 8),
+        ("cdef_uv_strength", C.c_uint8 * 8),
+        ("ccso", CcsoPlane * 3),
+        ("restoration", RestorationPlane * 3),
+        ("restoration_unit_size", C.c_uint8 * 2),
+        ("gdf_enabled", C.c_uint8),
+        ("gdf_qp_idx", C.c_uint8),
+        ("gdf_scale", C.c_uint8),
+        ("frame_type", C.c_uint8),
+        ("n_ref_frames", C.c_uint8),
+        ("absrefdist", C.c_uint8 * 7),
+    ]
+
+
+class FilmGrainData(C.Structure):
+    _fields_ = [
+        ("chroma_scaling_from_luma", C.c_int32),
+        ("num_points", C.c_int32 * 3),
+        ("points", ((C.c_uint8 * 2) * 14) * 3),
+        ("scaling_shift", C.c_int32),
+        ("ar_coeff_lag", C.c_int32),
+        ("ar_coeffs", (C.c_int8 * 28) * 3),
+        ("ar_coeff_shift", C.c_int32),
+        ("grain_scale_shift", C.c_int32),
+        ("uv_mult", C.c_int32 * 2),
+        ("uv_luma_mult", C.c_int32 * 2),
+        ("uv_offset", C.c_int32 * 2),
+        ("overlap_flag", C.c_int32),
+        ("clip_to_restricted_range", C.c_int32),
+        ("mc_identity", C.c_int32),
+        ("block_size", C.c_int32),
+    ]
+
+
+class SideInfo(C.Structure):
+    _fields_ = [
+        ("masks", C.c_void_p),
+        ("lr", C.c_void_p),
+        ("n_sb256", C.c_int32),
+        ("segmap", C.c_void_p),
+        ("segmap_stride", C.c_int32),
+        ("segmap_uv", C.c_void_p),
+        ("segmap_uv_stride", C.c_int32),
+    ]
+
+
+class BatchItem(C.Structure):
+    _fields_ = [
+        ("frame", C.c_void_p),
+        ("fp", C.POINTER(FrameParams)),
+        ("side", C.POINTER(SideInfo)),
+        ("inloop_mask", C.c_uint32),
+        ("fgd", C.POINTER(FilmGrainData)),
+        ("grain_seed", C.c_uint32),
+    ]
+
+
+# order of r2g_struct_sizes()
+STRUCT_SIZES = [
+    ("R2gAv2Filter", AV2_FILTER_DTYPE.itemsize),
+    ("R2gAv2RestorationUnit", LR_UNIT_DTYPE.itemsize),
+    ("R2gAv2Restoration", AV2_RESTORATION_DTYPE.itemsize),
+    ("R2gFrameParams", C.sizeof(FrameParams)),
+    ("R2gFilmGrainData", C.sizeof(FilmGrainData)),
+    ("R2gSideInfo", C.sizeof(SideInfo)),
+    ("R2gBatchItem", C.sizeof(BatchItem)),
+]
+
+
+def plane_geometry(width, height, bitdepth):
+    """Reference DefaultPicAllocator geometry (picture.rs:79-97), strides in bytes."""
+    hbd = 1 if bitdepth > 8 else 0
+    aw = (width + 127) & ~127
+    ah = (height + 127) & ~127
+    y_stride = aw << hbd
+    uv_stride = y_stride >> 1
+    if y_stride & 1023 == 0:
+        y_stride += 64
+    if uv_stride & 1023 == 0:
+        uv_stride += 64
+    return y_stride, uv_stride, ah, ah >> 1
+
+
+def side_info(masks, lr, segmap=None, segmap_stride=0, segmap_uv=None, segmap_uv_stride=0):
+    """Build an R2gSideInfo pointing at numpy arrays (caller keeps them alive)."""
+    s = SideInfo()
+    s.masks = masks.ctypes.data
+    s.lr = lr.ctypes.data
+    s.n_sb256 = int(masks.shape[0])
+    s.segmap = segmap.ctypes.data if segmap is not None else None
+    s.segmap_stride = segmap_stride
+    s.segmap_uv = segmap_uv.ctypes.data if segmap_uv is not None else None
+    s.segmap_uv_stride = segmap_uv_stride
+    return s
