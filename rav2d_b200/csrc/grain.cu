@@ -1,0 +1,443 @@
+// Film-grain synthesis and apply on the GPU: filtered frame L -> display
+// copy G.
+//
+// Reference: crates/rav2d/src/filmgrain.rs (get_random_number :11,
+// generate_scaling_* :22/:59, generate_grain_y/uv :115/:160, fgy_32x32xn
+// :248, fguv_32x32xn :409, prep_grain :617, apply_grain_row :688) and
+// decode.rs:4641-4775.
+//
+// The reference's serial parts are re-scheduled, not approximated:
+// * the 16-bit LFSR is linear over GF(2), so the state after k steps is
+//   M^k * s; the host derives M from the LFSR taps and tabulates M^(2^j), and
+//   each thread jumps straight to its first draw;
+// * the auto-regressive filter reads rows y-lag..y-1 at x-lag..x+lag and row
+//   y at x-lag..x-1, so every sample on the line x + 4y = t depends only on
+//   lines < t: the template is filled as a wavefront over t;
+// * block offsets of row band r and block b are draws 8b + 4n + 1 of the
+//   band's seed, evaluated directly by jump-ahead in the apply kernel.
+#include <cstring>
+
+#include "r2g_common.cuh"
+#include "r2g_runtime.h"
+
+namespace {
+
+constexpr int GW = 82, GH = 73, SGW = 44, SGH = 38;
+
+__constant__ uint16_t c_lfsr_pow[14][16];  // columns of M^(2^j)
+
+// one LFSR step (filmgrain.rs:11-16)
+R2G_HD uint32_t lfsr_step(uint32_t r) {
+    uint32_t bit = (r ^ (r >> 1) ^ (r >> 3) ^ (r >> 12)) & 1;
+    return (r >> 1) | (bit << 15);
+}
+
+R2G_D uint32_t apply_mat(const uint16_t *cols, uint32_t s) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        if ((s >> i) & 1) o ^= cols[i];
+    return o;
+}
+
+// state after k steps from s (16-bit state; k < 2^14)
+R2G_D uint32_t lfsr_jump(uint32_t s, uint32_t k) {
+    uint32_t st = s & 0xffff;  // seeds are 16-bit (checked at the boundary)
+    for (int j = 0; j < 14; j++)
+        if ((k >> j) & 1) st = apply_mat(c_lfsr_pow[j], st);
+    return st;
+}
+
+R2G_D int round2(int x, int shift) { return (x + ((1 << shift) >> 1)) >> shift; }
+
+struct GrainParams {
+    R2gFilmGrainData d;
+    uint32_t seed;
+    int bitdepth;
+    int has_y, has_u, has_v;  // which planes are grained
+};
+
+// Templates: luma 73x82, chroma 38x44 (stored in 73x82 arrays as the
+// reference's GrainLut does); scaling LUTs per plane (1 << bitdepth).
+__global__ void __launch_bounds__(256) grain_template_kernel(const GrainParams gp, const DevTables tab,
+                                                             int16_t *lut, uint8_t *scaling) {
+    __shared__ int16_t ly[GH][GW];
+    __shared__ int16_t lc[2][SGH][SGW];
+    const int tid = threadIdx.x;
+    const R2gFilmGrainData &d = gp.d;
+    const int b8 = gp.bitdepth - 8;
+    const int shift = 4 - b8 + d.grain_scale_shift;
+    const int gmin = -(128 << b8), gmax = (128 << b8) - 1;
+    const bool gen_u = d.num_points[1] > 0 || d.chroma_scaling_from_luma;
+    const bool gen_v = d.num_points[2] > 0 || d.chroma_scaling_from_luma;
+
+    // Gaussian fills: value k uses the state after k + 1 steps
+    {
+        const int n = GH * GW;
+        const int chunk = (n + 255) / 256;
+        int k0 = tid * chunk;
+        if (k0 < n) {
+            uint32_t st = lfsr_jump(gp.seed & 0xffff, (uint32_t)k0);
+            for (int k = k0; k < k0 + chunk && k < n; k++) {
+                st = lfsr_step(st);
+                ly[k / GW][k % GW] = (int16_t)round2(tab.GAUSSIAN_SEQUENCE[(st >> 5) & 2047], shift);
+            }
+        }
+        const int nc = SGH * SGW;
+        const int cchunk = (nc + 127) / 128;
+        int uv = tid >> 7, t = tid & 127;
+        int c0 = t * cchunk;
+        if (c0 < nc) {
+            uint32_t s0 = (gp.seed ^ (uv ? 0x49d8 : 0xb524)) & 0xffff;
+            uint32_t st = lfsr_jump(s0, (uint32_t)c0);
+            for (int k = c0; k < c0 + cchunk && k < nc; k++) {
+                st = lfsr_step(st);
+                lc[uv][k / SGW][k % SGW] = (int16_t)round2(tab.GAUSSIAN_SEQUENCE[(st >> 5) & 2047], shift);
+            }
+        }
+    }
+    __syncthreads();
+    const int lag = d.ar_coeff_lag;
+    const int ar_shift = (int)d.ar_coeff_shift;
+    // luma AR wavefront (generate_grain_y :134-157)
+    for (int t = 3 + 4 * 3; t <= (GW - 4) + 4 * (GH - 1); t++) {
+        for (int y = 3 + tid; y < GH; y += 256) {
+            int x = t - 4 * y;
+            if (x < 3 || x >= GW - 3) continue;
+            int sum = 0, ci = 0;
+            for (int dy = y - lag; dy <= y; dy++) {
+                int dx_end = dy == y ? x : x + lag + 1;
+                for (int dx = x - lag; dx < dx_end; dx++) sum += d.ar_coeffs[0][ci++] * ly[dy][dx];
+            }
+            ly[y][x] = (int16_t)iclip_(ly[y][x] + round2(sum, ar_shift), gmin, gmax);
+        }
+        __syncthreads();
+    }
+    // chroma AR wavefront (generate_grain_uv :183-228), both planes
+    for (int t = 3 + 4 * 3; t <= (SGW - 4) + 4 * (SGH - 1); t++) {
+        int uv = tid >> 7;
+        for (int y = 3 + (tid & 127); y < SGH; y += 128) {
+            int x = t - 4 * y;
+            if (x < 3 || x >= SGW - 3) continue;
+            if (!(uv ? gen_v : gen_u)) continue;
+            const int8_t *coeff = d.ar_coeffs[1 + uv];
+            int sum = 0, ci = 0;
+            for (int dy = y - lag; dy < y; dy++)
+                for (int dx = x - lag; dx <= x + lag; dx++) sum += coeff[ci++] * lc[uv][dy][dx];
+            for (int dx = x - lag; dx < x; dx++) sum += coeff[ci++] * lc[uv][y][dx];
+            if (d.num_points[0] > 0) {
+                int lx = ((x - 3) << 1) + 3, lyy = ((y - 3) << 1) + 3;
+                int luma = ly[lyy][lx] + ly[lyy][lx + 1] + ly[lyy + 1][lx] + ly[lyy + 1][lx + 1];
+                sum += round2(luma, 2) * coeff[ci];
+            }
+            lc[uv][y][x] = (int16_t)iclip_(lc[uv][y][x] + round2(sum, ar_shift), gmin, gmax);
+        }
+        __syncthreads();
+    }
+    // write templates (zero where a plane's template is not generated)
+    for (int i = tid; i < GH * GW; i += 256) {
+        int y = i / GW, x = i % GW;
+        lut[i] = ly[y][x];
+        lut[GH * GW + i] = (gen_u && y < SGH && x < SGW) ? lc[0][y][x] : 0;
+        lut[2 * GH * GW + i] = (gen_v && y < SGH && x < SGW) ? lc[1][y][x] : 0;
+    }
+    // scaling LUTs (generate_scaling_8bpc / _hbd), one thread per plane
+    if (tid < 3) {
+        int pl = tid;
+        uint8_t *sc = scaling + pl * 1024;
+        int size = 1 << gp.bitdepth, sx = b8;
+        int num = d.num_points[pl];
+        bool wanted = pl == 0 || !d.chroma_scaling_from_luma;
+        if (!wanted || num == 0) {
+            for (int i = 0; i < size; i++) sc[i] = 0;
+        } else {
+            const uint8_t(*pts)[2] = d.points[pl];
+            for (int i = 0; i < (pts[0][0] << sx); i++) sc[i] = pts[0][1];
+            for (int i = 0; i < num - 1; i++) {
+                int bx = pts[i][0], by = pts[i][1], ex = pts[i + 1][0], ey = pts[i + 1][1];
+                int dx = ex - bx, dyv = ey - by;
+                if (dx <= 0) continue;
+                int delta = dyv * ((0x10000 + (dx >> 1)) / dx);
+                int dd = 0x8000;
+                for (int x = 0; x < dx; x++) {
+                    sc[(bx + x) << sx] = (uint8_t)(by + (dd >> 16));
+                    dd += delta;
+                }
+            }
+            for (int i = pts[num - 1][0] << sx; i < size; i++) sc[i] = pts[num - 1][1];
+            if (sx > 0) {
+                int pad = 1 << sx, rnd = pad >> 1;
+                for (int i = 0; i < num - 1; i++) {
+                    int bx = pts[i][0] << sx, ex = pts[i + 1][0] << sx;
+                    for (int x = 0; x < ex - bx; x += pad) {
+                        int base = sc[bx + x], range = sc[bx + x + pad] - base, r = rnd;
+                        for (int n2 = 1; n2 < pad; n2++) {
+                            r += range;
+                            sc[bx + x + n2] = (uint8_t)(base + (r >> sx));
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Offsets of block b for row band `row` and seed index i (filmgrain.rs:
+// 274-305): draws 8b + 4n + 1 of the band's seed.
+R2G_D int block_offset(uint32_t in_seed, int row, int i, int b, int n, int block_size) {
+    uint32_t s = in_seed;
+    s ^= (uint32_t)((((row - i) * 37 + 178) & 0xFF)) << 8;
+    s ^= (uint32_t)(((row - i) * 173 + 105) & 0xFF);
+    uint32_t st = lfsr_jump(s, (uint32_t)(8 * b + 4 * n + 1));
+    return (int)(((uint32_t)(3 - block_size) * ((st >> 7) & 511)) >> 6);
+}
+
+// One CTA per (row band, 32-px block): luma 32x32 (or the frame remainder)
+// and both chroma 16x16 blocks.
+template <typename P>
+__global__ void __launch_bounds__(256) grain_apply_kernel(const DevFrame f, const GrainParams gp, const int16_t *lut,
+                                                          const uint8_t *scaling) {
+    __shared__ int off[2][2][2];  // [cur/prev block][seed i][n]
+    const int tid = threadIdx.x;
+    const R2gFilmGrainData &d = gp.d;
+    const int bs = 16 << d.block_size;
+    const int row = blockIdx.y, b = blockIdx.x;
+    const int rows = 1 + (d.overlap_flag && row > 0);
+    if (tid < 8) {
+        int which = tid >> 2, i = (tid >> 1) & 1, n = tid & 1;
+        int v = 0;
+        int bb = b - which;
+        if (i < rows && bb >= 0) v = block_offset(gp.seed, row, i, bb, n, d.block_size);
+        off[which][i][n] = v;
+    }
+    __syncthreads();
+    const int b8 = f.bitdepth - 8, bdmax = f.bdmax;
+    const int gmin = -(128 << b8), gmax = (128 << b8) - 1;
+    const int64_t ys = f.stride[0], uvs = f.stride[1];
+    const P *Ly = plane_ptr<const P>(f.L[0]);
+    // ---- luma ----
+    {
+        const int x0 = b * bs, y0 = row * bs;
+        const int bw = imin_(bs, f.w - x0), bh = imin_(bs, f.h - y0);
+        P *Gy = plane_ptr<P>(f.G[0]);
+        const int ystart = (d.overlap_flag && row > 0) ? imin_(2, bh) : 0;
+        const int xstart = (d.overlap_flag && b > 0) ? imin_(2, bw) : 0;
+        int minv, maxv;
+        if (d.clip_to_restricted_range) {
+            minv = 16 << b8;
+            maxv = 235 << b8;
+        } else {
+            minv = 0;
+            maxv = bdmax;
+        }
+        const int w[2][2] = {{27, 17}, {17, 27}};
+        for (int i = tid; i < bs * bs; i += 256) {
+            int y = i / bs, x = i % bs;
+            if (y >= bh || x >= bw) continue;
+            int64_t o = (int64_t)(y0 + y) * ys + x0 + x;
+            int sv = Ly[o];
+            if (!gp.has_y) {
+                Gy[o] = (P)sv;
+                continue;
+            }
+            auto S = [&](int bxs, int bys) -> int {
+                const int *of = off[bxs][bys];
+                int offx = 3 + 2 * (3 + of[1]), offy = 3 + 2 * (3 + of[0]);
+                return lut[(offy + y + bs * bys) * GW + offx + x + bs * bxs];
+            };
+            int grain;
+            if (y >= ystart) {
+                if (x >= xstart)
+                    grain = S(0, 0);
+                else
+                    grain = iclip_(round2(S(1, 0) * w[x][0] + S(0, 0) * w[x][1], 5), gmin, gmax);
+            } else {
+                if (x >= xstart) {
+                    grain = iclip_(round2(S(0, 1) * w[y][0] + S(0, 0) * w[y][1], 5), gmin, gmax);
+                } else {
+                    int top = iclip_(round2(S(1, 1) * w[x][0] + S(0, 1) * w[x][1], 5), gmin, gmax);
+                    int g = iclip_(round2(S(1, 0) * w[x][0] + S(0, 0) * w[x][1], 5), gmin, gmax);
+                    grain = iclip_(round2(top * w[y][0] + g * w[y][1], 5), gmin, gmax);
+                }
+            }
+            int noise = round2(scaling[sv] * grain, d.scaling_shift);
+            Gy[o] = (P)iclip_(sv + noise, minv, maxv);
+        }
+    }
+    // ---- chroma (fguv_32x32xn, 4:2:0) ----
+    {
+        const int cbs = bs >> 1;
+        const int x0 = b * cbs, y0 = row * cbs;
+        const int pw = (f.w + 1) >> 1;
+        const int bw = imin_(cbs, pw - x0);
+        const int bh = (imin_(f.h - row * bs, bs) + 1) >> 1;
+        const int ystart = (d.overlap_flag && row > 0) ? imin_(1, bh) : 0;
+        const int xstart = (d.overlap_flag && b > 0) ? imin_(1, bw) : 0;
+        for (int i = tid; i < 2 * cbs * cbs; i += 256) {
+            int uv = i / (cbs * cbs), j = i % (cbs * cbs);
+            int y = j / cbs, x = j % cbs;
+            if (y >= bh || x >= bw) continue;
+            const P *Lc = plane_ptr<const P>(f.L[1 + uv]);
+            P *Gc = plane_ptr<P>(f.G[1 + uv]);
+            int64_t o = (int64_t)(y0 + y) * uvs + x0 + x;
+            int sv = Lc[o];
+            bool has = uv ? gp.has_v : gp.has_u;
+            if (!has) {
+                Gc[o] = (P)sv;
+                continue;
+            }
+            const int16_t *cl = lut + (1 + uv) * GH * GW;
+            auto S = [&](int bxs, int bys) -> int {
+                const int *of = off[bxs][bys];
+                int offx = 3 + (3 + of[1]), offy = 3 + (3 + of[0]);
+                return cl[(offy + y + cbs * bys) * GW + offx + x + cbs * bxs];
+            };
+            int grain;
+            if (y >= ystart) {
+                if (x >= xstart)
+                    grain = S(0, 0);
+                else
+                    grain = iclip_(round2(S(1, 0) * 23 + S(0, 0) * 22, 5), gmin, gmax);
+            } else {
+                if (x >= xstart) {
+                    grain = iclip_(round2(S(0, 1) * 23 + S(0, 0) * 22, 5), gmin, gmax);
+                } else {
+                    int top = iclip_(round2(S(1, 1) * 23 + S(0, 1) * 22, 5), gmin, gmax);
+                    int g = iclip_(round2(S(1, 0) * 23 + S(0, 0) * 22, 5), gmin, gmax);
+                    grain = iclip_(round2(top * 23 + g * 22, 5), gmin, gmax);
+                }
+            }
+            int lx = (x0 + x) << 1, lyy = (y0 + y) << 1;
+            int luma = Ly[(int64_t)lyy * ys + lx];
+            int avg = (luma + Ly[(int64_t)lyy * ys + lx + 1] + 1) >> 1;
+            int val;
+            if (!d.chroma_scaling_from_luma) {
+                int combined = avg * d.uv_luma_mult[uv] + sv * d.uv_mult[uv];
+                val = iclip_((combined >> 6) + d.uv_offset[uv] * (1 << b8), 0, bdmax);
+            } else {
+                val = avg;
+            }
+            const uint8_t *sc = scaling + (d.chroma_scaling_from_luma ? 0 : (1 + uv)) * 1024;
+            int noise = round2(sc[val] * grain, d.scaling_shift);
+            int minv = 0, maxv = bdmax;
+            if (d.clip_to_restricted_range) {
+                minv = 16 << b8;
+                maxv = (d.mc_identity ? 235 : 240) << b8;
+            }
+            Gc[o] = (P)iclip_(sv + noise, minv, maxv);
+        }
+    }
+}
+
+bool g_pow_ready[64] = {false};
+
+}  // namespace
+
+// Per-context grain scratch: templates (3 x 73 x 82 int16) + scaling LUTs.
+struct GrainCtx {
+    int16_t *lut = nullptr;
+    uint8_t *scaling = nullptr;
+    cudaEvent_t ready = nullptr;  // templates written (side stream)
+    cudaEvent_t freed = nullptr;  // last apply that read them (main stream)
+    bool used = false;
+};
+
+void r2g_grain_ctx_free(R2gCtx *ctx) {
+    if (!ctx->grain) return;
+    r2g_dev_free(ctx, ctx->grain->lut, 3 * GH * GW * sizeof(int16_t));
+    r2g_dev_free(ctx, ctx->grain->scaling, 3 * 1024);
+    if (ctx->grain->ready) cudaEventDestroy(ctx->grain->ready);
+    if (ctx->grain->freed) cudaEventDestroy(ctx->grain->freed);
+    delete ctx->grain;
+    ctx->grain = nullptr;
+}
+
+// Columns of M^(2^j) for the LFSR of filmgrain.rs:11, derived by stepping
+// each basis vector.
+static cudaError_t init_lfsr_pow(int device) {
+    if (device >= 0 && device < 64 && g_pow_ready[device]) return cudaSuccess;
+    uint16_t pw[14][16];
+    for (int i = 0; i < 16; i++) pw[0][i] = (uint16_t)lfsr_step(1u << i);
+    for (int j = 1; j < 14; j++)
+        for (int i = 0; i < 16; i++) {
+            uint32_t v = pw[j - 1][i], o = 0;
+            for (int k = 0; k < 16; k++)
+                if ((v >> k) & 1) o ^= pw[j - 1][k];
+            pw[j][i] = (uint16_t)o;
+        }
+    cudaError_t e = cudaMemcpyToSymbol(c_lfsr_pow, pw, sizeof(pw));
+    if (e == cudaSuccess && device >= 0 && device < 64) g_pow_ready[device] = true;
+    return e;
+}
+
+// decode.rs:4641-4650 picture_has_grain + filmgrain.rs:688-830 plane gating
+static void grain_planes(const R2gFilmGrainData &d, int &has_y, int &has_u, int &has_v, bool &any) {
+    any = d.num_points[0] || d.num_points[1] || d.num_points[2] ||
+          (d.clip_to_restricted_range && d.chroma_scaling_from_luma);
+    has_y = any && d.num_points[0] > 0;
+    bool luma_lut = d.num_points[0] > 0;
+    has_u = any && (d.num_points[1] > 0 || d.chroma_scaling_from_luma) && (!d.chroma_scaling_from_luma || luma_lut);
+    has_v = any && (d.num_points[2] > 0 || d.chroma_scaling_from_luma) && (!d.chroma_scaling_from_luma || luma_lut);
+}
+
+int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed) {
+    if (init_lfsr_pow(ctx->device) != cudaSuccess) return R2G_E_DEVICE;
+    if (!ctx->grain) {
+        ctx->grain = new GrainCtx();
+        int rc = r2g_dev_alloc(ctx, (void **)&ctx->grain->lut, 3 * GH * GW * sizeof(int16_t));
+        if (rc == R2G_OK) rc = r2g_dev_alloc(ctx, (void **)&ctx->grain->scaling, 3 * 1024);
+        if (rc != R2G_OK) return rc;
+        if (cudaEventCreateWithFlags(&ctx->grain->ready, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->grain->freed, cudaEventDisableTiming) != cudaSuccess)
+            return R2G_E_DEVICE;
+    }
+    GrainParams gp;
+    gp.d = *fgd;
+    gp.seed = seed;
+    gp.bitdepth = f->bd;
+    bool any;
+    grain_planes(*fgd, gp.has_y, gp.has_u, gp.has_v, any);
+    DevFrame d = f->desc;
+    void *p[3];
+    char *base = (char *)f->buf[3];
+    p[0] = base;
+    p[1] = base + f->plane_bytes[0];
+    p[2] = base + f->plane_bytes[0] + f->plane_bytes[1];
+    for (int i = 0; i < 3; i++) d.G[i] = p[i];
+    if (any) {
+        // the templates do not depend on the frame: build them on the side
+        // stream (after the previous apply stopped reading them), then join
+        // before this apply
+        if (ctx->grain->used && cudaStreamWaitEvent(ctx->side_stream, ctx->grain->freed, 0) != cudaSuccess)
+            return R2G_E_DEVICE;
+        grain_template_kernel<<<1, 256, 0, ctx->side_stream>>>(gp, ctx->tab, ctx->grain->lut, ctx->grain->scaling);
+        if (cudaEventRecord(ctx->grain->ready, ctx->side_stream) != cudaSuccess) return R2G_E_DEVICE;
+        if (cudaStreamWaitEvent(ctx->stream, ctx->grain->ready, 0) != cudaSuccess) return R2G_E_DEVICE;
+    }
+    int bs = 16 << fgd->block_size;
+    dim3 grid((f->w + bs - 1) / bs, (f->h + bs - 1) / bs);
+    if (f->bd > 8)
+        grain_apply_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
+    else
+        grain_apply_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
+    if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaEventRecord(ctx->grain->freed, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
+    ctx->grain->used = true;
+    f->grain_buf = 3;
+    return R2G_OK;
+}
+
+extern "C" int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed) {
+    if (!ctx || !f || !fgd) return R2G_E_INVALID;
+    if (f->out_buf < 0) {
+        ctx->err = "frame not filtered";
+        return R2G_E_INVALID;
+    }
+    if (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
+        fgd->scaling_shift < 8 || fgd->scaling_shift > 11 || seed > 0xffff) {
+        ctx->err = "film-grain parameters out of range";
+        return R2G_E_INVALID;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return R2G_E_DEVICE;
+    return r2g_grain_enqueue(ctx, f, fgd, seed);
+}

@@ -1,0 +1,535 @@
+// Loop restoration (NS-Wiener single/multi, PC-Wiener, chroma NS-Wiener with
+// cross-component luma taps, GDF) out of place: C (CDEF+CCSO output) and D
+// (deblocked frame) -> L.
+//
+// Reference: crates/rav2d/src/looprestoration.rs (lr_sbrow_apply :2401,
+// lr_sbrow_plane :2276, lr_stripe :1847, ns_wiener_single_y :524,
+// wiener_multi :715, get_class_lut_idx :195, ns_wiener_single_uv :1145,
+// backup_row_luma :408, gdf_prep :1432, compute_gradient_row :114, gdf_add
+// :273) and decode.rs:4003-4056.  The reference filters in place, stripe by
+// stripe, through rings of row buffers; the rows a stripe sees are:
+//   rows inside the stripe: pre-LR samples (C), left context from the saved
+//     pre-LR border of the unit to the left, right context in place (C);
+//   the 2 rows above / below a stripe boundary: deblocked rows saved by
+//     copy_db (D); rows further out repeat the outermost saved row;
+//   at the frame top / bottom: the stripe's first / last row repeated;
+//   at the frame left / right: the row's first / last sample repeated.
+// Each CTA materialises exactly that window for one (plane, stripe, 64-wide
+// unit) in shared memory and evaluates every restoration tap from it.
+#include "r2g_common.cuh"
+
+namespace {
+
+enum { LR_HAVE_LEFT = 1, LR_HAVE_RIGHT = 2, LR_HAVE_TOP = 4, LR_HAVE_BOTTOM = 8 };
+
+constexpr int LW = 76;   // luma window width: -6 .. 69
+constexpr int LH = 76;   // luma window height: -6 .. 69 (stripe <= 64 rows)
+constexpr int CWW = 68;  // chroma window width: -2 .. 65
+constexpr int CWH = 36;  // chroma window height: -2 .. 33 (stripe <= 32 rows)
+
+__constant__ uint16_t c_pcw_norm[4] = {3739, 3273, 3074, 7};
+__constant__ int16_t c_mode_weights[4][3] = {{-527, 15325, 321}, {26436, -17705, 17905}, {366, -147, -194}, {202, -267, -179}};
+__constant__ int16_t c_mode_offsets[4] = {-547, -21565, -573, -680};
+__constant__ int8_t c_gdf_coords[18][2] = {{6, 0}, {5, 0}, {4, 0}, {3, 0}, {2, 1}, {2, 0}, {2, -1}, {1, 2}, {1, 1},
+                                           {1, 0}, {1, -1}, {1, -2}, {0, 6}, {0, 5}, {0, 4}, {0, 3}, {0, 2}, {0, 1}};
+__constant__ int8_t c_cfg_uv[6][2] = {{1, 0}, {0, 1}, {1, 1}, {-1, 1}, {2, 0}, {0, 2}};
+__constant__ int8_t c_cfg_uv_from_y[12][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1},
+                                              {-1, 1}, {1, -1}, {2, 0}, {-2, 0}, {0, 2}, {0, -2}};
+__constant__ int8_t c_cfg_pc[12][2] = {{1, 0}, {0, 1}, {2, 0}, {0, 2}, {1, 1}, {-1, 1},
+                                       {2, 1}, {2, -1}, {1, 2}, {1, -2}, {3, 0}, {0, 3}};
+__constant__ int8_t c_cfg_y[16][2] = {{1, 0}, {0, 1}, {2, 0}, {0, 2}, {1, 1}, {-1, 1}, {2, 1}, {2, -1},
+                                      {1, 2}, {1, -2}, {3, 0}, {0, 3}, {4, 0}, {0, 4}, {3, 3}, {3, -3}};
+
+enum { W_NONE = 0, W_NS_SINGLE = 1, W_NS_MULTI = 2, W_PC = 3 };
+
+struct UnitGeom {
+    int plane, x0, uw, y0, sh, edges, valid;
+    int sb256x, sb64x_idx;
+    const R2gAv2RestorationUnit *unit;
+};
+
+// looprestoration.rs:40-50
+R2G_D int get_qval(int qstep, int tskip, int i, int b8) {
+    qstep = (qstep + ((1 << b8) >> 1)) >> b8;
+    int prod = (tskip * qstep + 128) >> 8;
+    int qval = c_mode_weights[i][0] * (tskip << 5) + c_mode_weights[i][1] * qstep + c_mode_weights[i][2] * prod;
+    int aq = qval < 0 ? -qval : qval;
+    qval = apply_sign_((aq + (1 << 12)) >> 13, qval);
+    return 255 * (c_mode_offsets[i] + qval);
+}
+
+// Work item -> geometry, following lr_sbrow_apply / lr_sbrow_plane /
+// lr_stripe for one tile row (sb128 = 0).  A superblock row's LR call covers
+// [y_call, row_h); its first stripe is 56 (luma) rows high on superblock row
+// 0 and 64 otherwise, so a call holds one stripe, or two when the frame
+// height is a multiple of 64 and this is the last superblock row.
+R2G_D void unit_geom(const DevFrame &f, int plane, int sby, int sub, int ux, UnitGeom &g) {
+    const int chroma = plane != 0;
+    const int ss = chroma;  // 4:2:0: ss_hor = ss_ver = 1 for chroma
+    const int W = chroma ? f.cw : f.w, H = chroma ? f.ch : f.h;
+    const int not_last = sby + 1 < f.sbh;
+    const int next_row_y = (sby + 1) << (6 - ss);
+    const int row_h = imin_(next_row_y - (8 >> ss) * not_last, H);
+    const int y_call = (sby << (6 - ss)) - ((8 * (sby != 0)) >> ss);
+    const int sh0 = imin_((sby == 0 ? 56 : 64) >> ss, row_h - y_call);
+    int y0 = y_call, sh = sh0;
+    if (sub) {
+        y0 = y_call + sh0;
+        sh = imin_(64 >> ss, row_h - y0);
+    }
+    g.plane = plane;
+    g.y0 = y0;
+    g.sh = sh;
+    g.x0 = ux * 64;
+    g.uw = imin_(64, W - g.x0);
+    g.edges = (y0 > 0 ? LR_HAVE_TOP : 0) | (ux > 0 ? LR_HAVE_LEFT : 0) | (g.x0 + 64 < W ? LR_HAVE_RIGHT : 0) |
+              ((not_last || y0 + sh != row_h) ? LR_HAVE_BOTTOM : 0);
+    g.sb256x = (g.x0 << ss) >> 8;
+    g.sb64x_idx = ((g.x0 << ss) >> 6) & 3;
+    // unit selection (looprestoration.rs:2295-2331) from the call's first
+    // row; only sby 0 is the first superblock row of the (single) tile row
+    const int unit_size = 1 << f.fp.restoration_unit_size[chroma];
+    const int half = unit_size >> 1;
+    int row_y = y_call + ((8 >> ss) * (sby == 0));
+    int aligned = row_y & ~(unit_size - 1);
+    if (aligned != 0 && aligned + half > H) aligned -= unit_size;
+    aligned <<= ss;
+    const int sb_idx = (aligned >> 8) * f.sb256w;
+    const int unit_idx_base = ((aligned >> 6) & 3) << 2;
+    int lr_sb = sb_idx, lr_u = unit_idx_base;
+    if (g.x0 > 0) {
+        int start = g.x0 & ~(unit_size - 1);
+        if (start != 0 && W - start < half) start -= unit_size;
+        const int shift_hor = 8 - ss;
+        lr_u = unit_idx_base + ((start >> (shift_hor - 2)) & 3);
+        lr_sb = sb_idx + (start >> shift_hor);
+    }
+    g.valid = sh > 0 && lr_sb < f.sb256w * f.sb256h && lr_u < 16;
+    g.unit = g.valid ? &f.lr[lr_sb].lr[plane][lr_u] : nullptr;
+}
+
+// Source row of window row r (stripe-relative) and whether it is deblocked.
+R2G_D void row_src(const UnitGeom &g, int r, int &row, bool &from_d) {
+    if (r >= 0 && r < g.sh) {
+        row = g.y0 + r;
+        from_d = false;
+    } else if (r < 0) {
+        if (g.edges & LR_HAVE_TOP) {
+            row = g.y0 + (r < -2 ? -2 : r);
+            from_d = true;
+        } else {
+            row = g.y0;
+            from_d = false;
+        }
+    } else {
+        if (g.edges & LR_HAVE_BOTTOM) {
+            row = g.y0 + g.sh + (r - g.sh > 1 ? 1 : r - g.sh);
+            from_d = true;
+        } else {
+            row = g.y0 + g.sh - 1;
+            from_d = false;
+        }
+    }
+}
+
+R2G_D int col_src(const UnitGeom &g, int c) {
+    if (c < 0 && !(g.edges & LR_HAVE_LEFT)) return g.x0;
+    if (c >= g.uw && !(g.edges & LR_HAVE_RIGHT)) return g.x0 + g.uw - 1;
+    return g.x0 + c;
+}
+
+template <typename P>
+__global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_units, int nux_l, int nux_c) {
+    __shared__ int16_t win[LH * LW];  // luma window, or chroma window
+    __shared__ int16_t lwin[CWH * CWW];  // chroma: downsampled luma window
+    __shared__ int8_t gerr[64 * 64];
+    __shared__ uint8_t classes[16][16];
+    __shared__ uint16_t noskip[18];
+    __shared__ uint16_t llm[17];
+    __shared__ uint16_t s_alpha[88];
+    __shared__ int16_t s_weight[3 * 88];
+    __shared__ int8_t s_err[4096];
+
+    const int tid = threadIdx.x;
+    int b = blockIdx.x;
+    int plane, sby, sub, ux;
+    if (b < n_luma_units) {
+        plane = 0;
+        ux = b % nux_l;
+        b /= nux_l;
+    } else {
+        b -= n_luma_units;
+        int per = f.sbh * 2 * nux_c;
+        plane = 1 + b / per;
+        b %= per;
+        ux = b % nux_c;
+        b /= nux_c;
+    }
+    sub = b & 1;
+    sby = b >> 1;
+    UnitGeom g;
+    unit_geom(f, plane, sby, sub, ux, g);
+    if (g.sh <= 0) return;
+    const int chroma = plane != 0;
+    const int64_t stride = f.stride[chroma];
+    const P *Cp = plane_ptr<const P>(f.C[plane]);
+    const P *Dp = plane_ptr<const P>(f.R[plane]);
+    P *Lp = plane_ptr<P>(f.L[plane]);
+    const R2gFrameParams &fp = f.fp;
+    const int bitdepth = f.bitdepth, bdmax = f.bdmax;
+
+    // ---- kernel selection (looprestoration.rs:1880-1920) ----
+    int wkind = W_NONE;
+    bool plane_on = (f.restore_planes >> plane) & 1;
+    if (plane_on && g.valid) {
+        int wt = (f.inloop & R2G_INLOOP_WIENER) ? g.unit->restoration_type : 0;
+        const R2gRestorationPlane &pd = fp.restoration[plane];
+        if (wt == R2G_RESTORE_NS_WIENER)
+            wkind = (pd.frame_filters_on && pd.num_classes != 1) ? W_NS_MULTI : W_NS_SINGLE;
+        else if (wt == R2G_RESTORE_PC_WIENER)
+            wkind = W_PC;
+    }
+    const int inc = ((g.edges & LR_HAVE_TOP) && g.y0 + 8 < ((f.bh4 * 4) >> chroma)) ? 8 : 0;
+    const int sb256_idx = f.sb256w * (((g.y0 << chroma) + inc) >> 8) + g.sb256x;
+    const int nsb = f.sb256w * f.sb256h;
+    const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && sb256_idx < nsb &&
+                        f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
+
+    if (wkind == W_NONE && !gdf_on) {
+        for (int i = tid; i < g.sh * g.uw; i += 256) {
+            int r = i / g.uw, c = i % g.uw;
+            Lp[(int64_t)(g.y0 + r) * stride + g.x0 + c] = Cp[(int64_t)(g.y0 + r) * stride + g.x0 + c];
+        }
+        return;
+    }
+
+    // ---- lossless rows of the stripe (looprestoration.rs:2037-2075) ----
+    const int ll_rows = imax_(g.sh >> 2, 1) + 1;
+    if (tid < 17) {
+        uint16_t v = 0;
+        if (tid < ll_rows && sb256_idx < nsb) {
+            const R2gAv2Filter &m = f.masks[sb256_idx];
+            int y4 = ((g.y0 << chroma) & 255) >> 2;
+            if (plane == 0) {
+                int yy = y4 + tid;
+                if (yy < 64) v = m.lossless_mask_y[yy][g.sb64x_idx];
+            } else {
+                int init_y = g.y0 >> 2, end_y = (g.y0 + g.sh) >> 2;
+                int base = y4 >> 1;
+                if (init_y + tid < end_y) {
+                    int sy = base + tid;
+                    if (sy < 64) {
+                        uint16_t lo = m.lossless_mask_uv[sy][g.sb64x_idx];
+                        uint16_t hi = g.sb64x_idx + 1 < 4 ? m.lossless_mask_uv[sy][g.sb64x_idx + 1] : 0;
+                        v = (uint16_t)((lo & 0xff) | ((hi & 0xff) << 8));
+                    }
+                }
+            }
+        }
+        llm[tid] = v;
+    }
+    // ---- multi-class noskip rows (looprestoration.rs:1922-1944) ----
+    if ((wkind == W_NS_MULTI || wkind == W_PC) && tid < 18) {
+        uint16_t v = 0;
+        int by = (g.y0 >> 2) + tid;
+        if (by < ((g.y0 + g.sh) >> 2)) {
+            int sidx = f.sb256w * (by >> 6) + g.sb256x;
+            if (sidx < nsb) {
+                v = f.masks[sidx].lr_noskip_mask[by & 63][g.sb64x_idx];
+                if (!(g.edges & LR_HAVE_RIGHT) && (g.uw & 63) != 0) {
+                    int sh = ((g.uw >> 2) & 15) - 1;
+                    uint16_t eb = (uint16_t)(v >> sh);
+                    v = (uint16_t)(v | (uint16_t)(eb << (sh + 1)));
+                }
+            }
+        }
+        noskip[tid] = v;
+    }
+
+    if (!chroma) {
+        // ---- luma window: rows -6 .. sh+5, columns -6 .. uw+5 ----
+        const int wh = g.sh + 12, ww = g.uw + 12;
+        for (int i = tid; i < wh * ww; i += 256) {
+            int r = i / ww - 6, c = i % ww - 6;
+            int row;
+            bool from_d;
+            row_src(g, r, row, from_d);
+            const P *src = from_d ? Dp : Cp;
+            win[(r + 6) * LW + (c + 6)] = (int16_t)src[(int64_t)row * stride + col_src(g, c)];
+        }
+        if (gdf_on) {
+            const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
+            const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
+            const int weight_base = ref_dst_idx * 1584 + qp_idx * 264;
+            const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
+                                                    : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
+            const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
+            for (int i = tid; i < 88; i += 256) s_alpha[i] = f.tab.GDF_ALPHA[alpha_base + i];
+            for (int i = tid; i < 264; i += 256) s_weight[i] = f.tab.GDF_WEIGHT[weight_base + i];
+            for (int i = tid; i < nerr; i += 256) s_err[i] = errtab[i];
+        }
+    } else {
+        // ---- chroma window: rows -2 .. sh+1, columns -2 .. uw+1 ----
+        const int wh = g.sh + 4, ww = g.uw + 4;
+        for (int i = tid; i < wh * ww; i += 256) {
+            int r = i / ww - 2, c = i % ww - 2;
+            int row;
+            bool from_d;
+            row_src(g, r, row, from_d);
+            const P *src = from_d ? Dp : Cp;
+            win[(r + 2) * CWW + (c + 2)] = (int16_t)src[(int64_t)row * stride + col_src(g, c)];
+        }
+        if (wkind == W_NS_SINGLE) {
+            // downsampled luma for chroma rows -2 .. sh+1 at chroma columns
+            // -2 .. uw+1 (backup_row_luma with the ns_wiener_single_uv row
+            // selection, looprestoration.rs:1207-1350)
+            const P *Cy = plane_ptr<const P>(f.C[0]);
+            const P *Dy = plane_ptr<const P>(f.R[0]);
+            const int64_t ls = f.stride[0];
+            const int ds = fp.cfl_ds_filter_index;
+            const int lw = g.uw << 1, lx0 = g.x0 << 1;
+            for (int i = tid; i < wh * ww; i += 256) {
+                int r = i / ww - 2, j = i % ww - 2;
+                // chroma row -> (luma source, rowA, rowB)
+                int rr = r;
+                if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
+                if (!(g.edges & LR_HAVE_BOTTOM) && rr >= g.sh) rr = g.sh - 1;
+                const P *src;
+                int ra, rb;
+                if (rr == -2) {
+                    src = Dy;
+                    ra = rb = 2 * g.y0 - 2;
+                } else if (rr == -1) {
+                    src = Dy;
+                    ra = 2 * g.y0 - 2;
+                    rb = 2 * g.y0 - 1;
+                } else if (rr == g.sh) {
+                    src = Dy;
+                    ra = 2 * (g.y0 + g.sh);
+                    rb = ra + 1;
+                } else if (rr == g.sh + 1) {
+                    src = Dy;
+                    ra = rb = 2 * (g.y0 + g.sh) + 1;
+                } else {
+                    src = Cy;
+                    ra = 2 * (g.y0 + rr);
+                    rb = ra + 1;
+                }
+                // luma position 2j, with the left / right fills
+                int pos = 2 * j;
+                if (pos < 0 && !(g.edges & LR_HAVE_LEFT)) pos = 0;
+                if (pos >= lw && !(g.edges & LR_HAVE_RIGHT)) pos = lw - 2;
+                const P *a = src + (int64_t)ra * ls + lx0 + pos;
+                const P *bb = src + (int64_t)rb * ls + lx0 + pos;
+                int v;
+                if (ds == 0)
+                    v = ((int)a[0] + bb[0] + a[1] + bb[1]) >> 2;
+                else if (ds == 1)
+                    v = ((int)a[0] + bb[0]) >> 1;
+                else
+                    v = a[0];
+                lwin[(r + 2) * CWW + (j + 2)] = (int16_t)v;
+            }
+        }
+    }
+    __syncthreads();
+
+    if (!chroma) {
+        const int b8 = bitdepth - 8;
+        // ---- GDF prep (looprestoration.rs:1432-1640) ----
+        if (gdf_on) {
+            const uint32_t down = bitdepth == 12 ? 2 : 0, up = bitdepth == 8 ? 2 : 0;
+            const int ref_dst_idx = f.gdf_ref_dst_idx;
+            const int bias_idx = ref_dst_idx * 6 + fp.gdf_qp_idx;
+            const int scale = ref_dst_idx == 0 ? 8 : 5;
+            const int npairs = g.sh * (g.uw >> 1);
+            for (int i = tid; i < npairs; i += 256) {
+                int y = i / (g.uw >> 1), x1 = (i % (g.uw >> 1)) * 2;
+                int y1 = y & ~1;
+                int gs[4] = {0, 0, 0, 0};
+                const int dys[4] = {1, 0, 1, -1}, dxs[4] = {0, 1, 1, 1};
+                for (int rr = y1 - 1; rr <= y1 + 2; rr++)
+                    for (int cc = x1 - 1; cc <= x1 + 2; cc++) {
+                        int bv = win[(rr + 6) * LW + cc + 6] >> down;
+#pragma unroll
+                        for (int d = 0; d < 4; d++) {
+                            int av = win[(rr - dys[d] + 6) * LW + cc - dxs[d] + 6] >> down;
+                            int cv = win[(rr + dys[d] + 6) * LW + cc + dxs[d] + 6] >> down;
+                            int t = bv * 2 - av - cv;
+                            gs[d] += t < 0 ? -t : t;
+                        }
+                    }
+                int cls = (gs[0] <= gs[1]) | ((gs[2] <= gs[3]) << 1);
+                int shared[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) shared[k] = f.tab.GDF_BIAS[bias_idx * 3 + k];
+#pragma unroll
+                for (int d = 0; d < 4; d++) {
+                    int k = d + 18;
+                    int alpha = s_alpha[k * 4 + cls];
+                    int v = imin_(gs[d] >> (4 - up), alpha);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) shared[q] += v * s_weight[q * 88 + k * 4 + cls];
+                }
+                for (int x2 = 0; x2 < 2; x2++) {
+                    int x = x1 + x2;
+                    int iv[3] = {shared[0], shared[1], shared[2]};
+                    int m = win[(y + 6) * LW + x + 6] >> down;
+#pragma unroll
+                    for (int k = 0; k < 18; k++) {
+                        int alpha = s_alpha[k * 4 + cls];
+                        int dy = c_gdf_coords[k][0], dx = c_gdf_coords[k][1];
+                        int a = win[(y - dy + 6) * LW + x - dx + 6] >> down;
+                        int bvv = win[(y + dy + 6) * LW + x + dx + 6] >> down;
+                        int above = iclip_((a - m) << up, -alpha, alpha);
+                        int below = iclip_((bvv - m) << up, -alpha, alpha);
+                        int v = iclip_(above + below, -512, 511);
+#pragma unroll
+                        for (int q = 0; q < 3; q++) iv[q] += v * s_weight[q * 88 + k * 4 + cls];
+                    }
+                    int full = 0;
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        int sv = iv[q] * scale;
+                        int asv = sv < 0 ? -sv : sv;
+                        int v = apply_sign_((asv + (1 << 14)) >> 15, sv);
+                        int sub = iclip_(v, -scale, scale - 1) + scale;
+                        full = full * (scale * 2) + sub;
+                    }
+                    gerr[y * 64 + x] = s_err[full];
+                }
+            }
+        }
+        // ---- classification for PC-Wiener / NS-multi (:195-271, :870-896) ----
+        const int bh4 = g.sh >> 2, bw4 = g.uw >> 2;
+        if (wkind == W_NS_MULTI || wkind == W_PC) {
+            const uint8_t *sub_lut = wkind == W_PC
+                                         ? f.tab.PC_WIENER_SUB_CLASSIFY + f.wiener_idx * 256
+                                         : f.tab.PC_WIENER_SUB_CLASSIFY_NS + (f.wiener_idx * 7 + (f.ns_ci >= 0 ? imin_(f.ns_ci, 6) : 0)) * 256;
+            for (int i = tid; i < bh4 * bw4; i += 256) {
+                int by = i / bw4, bx = i % bw4;
+                int fs[3] = {0, 0, 0};
+                for (int dy = -1; dy <= 4; dy++)
+                    for (int dx = -1; dx <= 4; dx++) {
+                        int y = by * 4 + dy + 6, x = bx * 4 + dx + 6;
+                        int m = win[y * LW + x];
+                        int vert = win[(y - 1) * LW + x] - 2 * m + win[(y + 1) * LW + x];
+                        int anti = win[(y - 1) * LW + x + 1] - 2 * m + win[(y + 1) * LW + x - 1];
+                        int diag = win[(y - 1) * LW + x - 1] - 2 * m + win[(y + 1) * LW + x + 1];
+                        fs[0] += vert < 0 ? -vert : vert;
+                        fs[1] += anti < 0 ? -anti : anti;
+                        fs[2] += diag < 0 ? -diag : diag;
+                    }
+                int s = 0;
+                const int np[3] = {16, 4, 1};
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        int e = (dy != 0) + (dx != 0);
+                        int fx = iclip_((bx & 15) + dx, 0, 15);
+                        int fy = iclip_(by + dy, 0, bh4 - 1);
+                        s += np[e] * (((noskip[fy] >> fx) & 1) == 0);
+                    }
+                int rnd = (1 << b8) >> 1;
+#pragma unroll
+                for (int k = 0; k < 3; k++) fs[k] = (int)((uint32_t)fs[k] * (uint32_t)c_pcw_norm[k] + (uint32_t)rnd) >> b8;
+                s *= c_pcw_norm[3];
+                int qv = (imax_(0, get_qval(f.base_q, s, 0, b8)) + (1 << 13)) >> 14;
+                qv = imin_(qv, 255) >> 5;
+                int lut_idx = qv << 9;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    qv = (imax_(0, fs[k] + get_qval(f.base_q, s, k + 1, b8)) + (1 << 13)) >> 14;
+                    qv = imin_(qv, 255) >> 5;
+                    lut_idx |= qv << (3 * (2 - k));
+                }
+                classes[by][bx] = sub_lut[f.tab.PC_WIENER_LUT_TO_CLASS[lut_idx]];
+            }
+        }
+        __syncthreads();
+        // ---- Wiener FIR + GDF add, one output sample per iteration ----
+        int8_t single[16];
+        if (wkind == W_NS_SINGLE) {
+            const int8_t *src = fp.restoration[0].frame_filters_on ? fp.restoration[0].filter[0] : g.unit->ns_filter[0];
+#pragma unroll
+            for (int k = 0; k < 16; k++) single[k] = src[k];
+        }
+        const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
+        for (int i = tid; i < g.sh * g.uw; i += 256) {
+            int y = i / g.uw, x = i % g.uw;
+            int m = win[(y + 6) * LW + x + 6];
+            int v = m;
+            bool ll = (llm[y >> 2] >> (x >> 2)) & 1;
+            if (!ll && wkind != W_NONE) {
+                int s;
+                if (wkind == W_PC) {
+                    const int16_t *flt = f.tab.PC_WIENER_FILTERS + (f.wiener_idx * 64 + classes[y >> 2][x >> 2]) * 13;
+                    s = m * flt[12];
+#pragma unroll
+                    for (int k = 0; k < 12; k++) {
+                        int dy = c_cfg_pc[k][0], dx = c_cfg_pc[k][1];
+                        s += (win[(y + dy + 6) * LW + x + dx + 6] + win[(y - dy + 6) * LW + x - dx + 6]) * flt[k];
+                    }
+                } else {
+                    const int8_t *flt = wkind == W_NS_SINGLE ? single : fp.restoration[0].filter[classes[y >> 2][x >> 2]];
+                    s = m << 7;
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        int dy = c_cfg_y[k][0], dx = c_cfg_y[k][1];
+                        s += (win[(y + dy + 6) * LW + x + dx + 6] + win[(y - dy + 6) * LW + x - dx + 6] - 2 * m) * flt[k];
+                    }
+                }
+                v = iclip_((s + 64) >> 7, 0, bdmax);
+            }
+            if (gdf_on && !ll) {
+                int diff = gerr[y * 64 + x] * gscale;
+                int ad = diff < 0 ? -diff : diff;
+                v = iclip_(v + apply_sign_((ad + grnd) >> gshift, diff), 0, bdmax);
+            }
+            Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
+        }
+    } else {
+        // ---- chroma NS-Wiener with cross-component luma taps (:1145-1430) ----
+        int8_t flt[18];
+        if (wkind == W_NS_SINGLE) {
+            const int8_t *src = fp.restoration[plane].frame_filters_on ? fp.restoration[plane].filter[0]
+                                                                       : g.unit->ns_filter[0];
+#pragma unroll
+            for (int k = 0; k < 18; k++) flt[k] = src[k];
+        }
+        for (int i = tid; i < g.sh * g.uw; i += 256) {
+            int y = i / g.uw, x = i % g.uw;
+            int m = win[(y + 2) * CWW + x + 2];
+            int v = m;
+            bool ll = (llm[y >> 2] >> (x >> 2)) & 1;
+            if (!ll && wkind == W_NS_SINGLE) {
+                int s = m << 7;
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    int dy = c_cfg_uv[k][0], dx = c_cfg_uv[k][1];
+                    s += (win[(y + dy + 2) * CWW + x + dx + 2] + win[(y - dy + 2) * CWW + x - dx + 2] - 2 * m) * flt[k];
+                }
+                int l = lwin[(y + 2) * CWW + x + 2];
+#pragma unroll
+                for (int k = 0; k < 12; k++) {
+                    int dy = c_cfg_uv_from_y[k][0], dx = c_cfg_uv_from_y[k][1];
+                    s += (lwin[(y + dy + 2) * CWW + x + dx + 2] - l) * flt[6 + k];
+                }
+                v = iclip_((s + 64) >> 7, 0, bdmax);
+            }
+            Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
+        }
+    }
+}
+
+}  // namespace
+
+void r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
+    if (!f.lr_on) return;
+    int nux_l = (f.w + 63) / 64, nux_c = (f.cw + 63) / 64;
+    int n_luma = f.sbh * 2 * nux_l;
+    int n = n_luma + 2 * f.sbh * 2 * nux_c;
+    if (f.bitdepth > 8)
+        lr_kernel<uint16_t><<<n, 256, 0, s>>>(f, n_luma, nux_l, nux_c);
+    else
+        lr_kernel<uint8_t><<<n, 256, 0, s>>>(f, n_luma, nux_l, nux_c);
+}

@@ -1,0 +1,74 @@
+// Shared device-side definitions of the B200 in-loop filter library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rav2d_gpu.h"
+
+#define R2G_HD __host__ __device__ __forceinline__
+#define R2G_D __device__ __forceinline__
+
+// Device addresses of the AV2 constant tables (defined once in tables.cu).
+struct DevTables {
+    const int8_t *CDEF_DIRECTIONS;          // [12][2]
+    const uint16_t *CCSO_QUANT_SZ;          // [4][4]
+    const int8_t *CCSO_OFFSET;              // [4][8]
+    const int16_t *DEBLOCK_SIDE_THRESHOLDS; // [296]
+    const int16_t *PC_WIENER_FILTERS;       // [4][64][13]
+    const uint8_t *PC_WIENER_SUB_CLASSIFY;  // [4][256]
+    const uint8_t *PC_WIENER_SUB_CLASSIFY_NS;  // [4][7][256]
+    const int16_t *GAUSSIAN_SEQUENCE;       // [2048]
+    const uint8_t *PC_WIENER_LUT_TO_CLASS;  // [4096]
+    const uint16_t *GDF_ALPHA;              // [3168]
+    const int16_t *GDF_WEIGHT;              // [9504]
+    const int16_t *GDF_BIAS;                // [36][3]
+    const int8_t *GDF_INTRA_ERROR;          // [24576]
+    const int8_t *GDF_INTER_ERROR;          // [30000]
+};
+// Fills `t` with this device's table addresses (the current device).
+cudaError_t r2g_get_tables(DevTables *t);
+
+// Frame descriptor handed to every stage kernel (by value, or from a device
+// array in batched launches).  All derived per-frame scalars of the
+// reference's LoopFilterState are computed once on the host.
+struct DevFrame {
+    int w, h;          // luma size in samples
+    int cw, ch;        // chroma size in samples (4:2:0)
+    int bw4, bh4;      // luma size in 4x4 units (bw, bh of the reference)
+    int sb256w, sb256h, sbh;
+    int bitdepth, hbd, bdmax;
+    int64_t stride[2];  // in samples: luma, chroma
+    void *R[3];         // recon; deblocked in place (the reference's D)
+    void *C[3];         // CDEF+CCSO output
+    void *L[3];         // loop-restoration output (the filtered frame)
+    void *G[3];         // film-grain display copy
+    const R2gAv2Filter *masks;
+    const R2gAv2Restoration *lr;
+    const uint8_t *segmap;
+    const uint8_t *segmap_uv;
+    int segmap_stride, segmap_uv_stride;
+    uint32_t inloop;
+    int deblock_on, cdef_stage_on, ccso_on, cdef_on, lr_on, any_lossless;
+    int restore_planes, base_q, wiener_idx, ns_ci, gdf_ref_dst_idx;
+    DevTables tab;
+    R2gFrameParams fp;
+};
+
+R2G_HD int imin_(int a, int b) { return a < b ? a : b; }
+R2G_HD int imax_(int a, int b) { return a > b ? a : b; }
+R2G_HD int iclip_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+R2G_HD int apply_sign_(int v, int s) { return s < 0 ? -v : v; }
+R2G_D int ulog2_(uint32_t v) { return 31 - __clz((int)v); }
+
+template <typename P>
+R2G_D P *plane_ptr(void *base) {
+    return reinterpret_cast<P *>(base);
+}
+
+// Launch helpers implemented per stage (deblock.cu, cdef.cu, lr.cu, grain.cu).
+void r2g_launch_deblock(const DevFrame &f, cudaStream_t s);
+void r2g_launch_cdef(const DevFrame &f, cudaStream_t s);
+void r2g_launch_lr(const DevFrame &f, cudaStream_t s);
+
+struct GrainDev;  // grain.cu

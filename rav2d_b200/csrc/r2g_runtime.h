@@ -1,0 +1,53 @@
+// Host-side definitions of the opaque ABI handles, shared by the runtime,
+// the batch scheduler and the film-grain stage.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "r2g_common.cuh"
+
+struct Ticket {
+    uint64_t id;
+    cudaEvent_t ev;
+};
+
+struct GrainCtx;  // grain.cu
+
+struct R2gCtx {
+    int device = 0;
+    int64_t budget = 0, used = 0;
+    cudaStream_t stream = nullptr;       // filter stages
+    cudaStream_t side_stream = nullptr;  // grain templates (frame-independent)
+    DevTables tab{};
+    std::string err;
+    std::vector<Ticket> tickets;
+    uint64_t next_ticket = 0;
+    GrainCtx *grain = nullptr;
+};
+
+struct R2gFrame {
+    int w = 0, h = 0, bd = 8;
+    int64_t stride[2] = {0, 0};  // bytes
+    int64_t rows[2] = {0, 0};
+    size_t plane_bytes[2] = {0, 0};
+    size_t buf_bytes = 0;
+    void *buf[4] = {nullptr, nullptr, nullptr, nullptr};  // recon/D, C, L, G
+    int n_sb256 = 0;
+    size_t side_bytes = 0;
+    void *side_dev = nullptr;
+    void *side_host = nullptr;  // pinned staging
+    void *seg_dev = nullptr;
+    void *seg_host = nullptr;
+    size_t seg_bytes = 0;
+    int out_buf = -1, grain_buf = -1;
+    DevFrame desc{};
+};
+
+int r2g_dev_alloc(R2gCtx *ctx, void **p, size_t bytes);
+void r2g_dev_free(R2gCtx *ctx, void *p, size_t bytes);
+int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t inloop,
+                DevFrame &d);
+void r2g_launch_pipeline(const DevFrame &d, cudaStream_t s);
+int r2g_ticket_record(R2gCtx *ctx, uint64_t *ticket);
+void r2g_grain_ctx_free(R2gCtx *ctx);

@@ -1,0 +1,500 @@
+// Host runtime of the C ABI declared in include/rav2d_gpu.h: contexts,
+// device-resident frames, side-info staging, stage gating and launch order.
+//
+// The per-frame pipeline replaces the reference's Phase-B loop of
+// filter_sbrow (decode.rs:3597-3625, :3718-4058) with whole-frame stages:
+//   deblock (in place on the recon: vertical edges, then horizontal edges)
+//   -> CDEF+CCSO (deblocked -> C) -> loop restoration (C, deblocked -> L)
+//   -> film grain (L -> display copy G).
+// A disabled stage aliases its output to its input, as the reference simply
+// skips it.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "r2g_common.cuh"
+#include "r2g_runtime.h"
+
+#define R2G_VERSION 1
+
+static void set_err(R2gCtx *ctx, const char *fmt, const char *a = "") {
+    if (!ctx) return;
+    char buf[512];
+    snprintf(buf, sizeof(buf), fmt, a);
+    ctx->err = buf;
+}
+
+#define CK(call)                                                                    \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            set_err(ctx, "CUDA error: %s", cudaGetErrorString(e_));                 \
+            return R2G_E_DEVICE;                                                    \
+        }                                                                           \
+    } while (0)
+
+extern "C" int r2g_version(void) { return R2G_VERSION; }
+
+extern "C" int r2g_plane_geometry(int width, int height, int bitdepth, int64_t *y_stride, int64_t *uv_stride,
+                                  int64_t *y_rows, int64_t *uv_rows) {
+    if (width <= 0 || height <= 0 || (bitdepth != 8 && bitdepth != 10)) return R2G_E_INVALID;
+    int hbd = bitdepth > 8;
+    int64_t aw = (width + 127) & ~127, ah = (height + 127) & ~127;
+    int64_t ys = aw << hbd, uvs = ys >> 1;
+    if ((ys & 1023) == 0) ys += 64;
+    if ((uvs & 1023) == 0) uvs += 64;
+    if (y_stride) *y_stride = ys;
+    if (uv_stride) *uv_stride = uvs;
+    if (y_rows) *y_rows = ah;
+    if (uv_rows) *uv_rows = ah >> 1;
+    return R2G_OK;
+}
+
+extern "C" int r2g_struct_sizes(int32_t *sizes, int n) {
+    const int32_t v[] = {(int32_t)sizeof(R2gAv2Filter), (int32_t)sizeof(R2gAv2RestorationUnit),
+                         (int32_t)sizeof(R2gAv2Restoration), (int32_t)sizeof(R2gFrameParams),
+                         (int32_t)sizeof(R2gFilmGrainData), (int32_t)sizeof(R2gSideInfo),
+                         (int32_t)sizeof(R2gBatchItem)};
+    int m = (int)(sizeof(v) / sizeof(v[0]));
+    for (int i = 0; i < n && i < m; i++) sizes[i] = v[i];
+    return m;
+}
+
+// ---------------------------------------------------------------- context
+extern "C" int r2g_ctx_create(int device, int64_t mem_budget, R2gCtx **out) {
+    if (!out) return R2G_E_INVALID;
+    *out = nullptr;
+    R2gCtx *ctx = new R2gCtx();
+    ctx->device = device;
+    ctx->budget = mem_budget;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        delete ctx;
+        return R2G_E_DEVICE;
+    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        r2g_get_tables(&ctx->tab) != cudaSuccess) {
+        delete ctx;
+        return R2G_E_DEVICE;
+    }
+    *out = ctx;
+    return R2G_OK;
+}
+
+extern "C" int r2g_ctx_destroy(R2gCtx *ctx) {
+    if (!ctx) return R2G_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->side_stream);
+    for (auto &t : ctx->tickets) cudaEventDestroy(t.ev);
+    ctx->tickets.clear();
+    r2g_grain_ctx_free(ctx);
+    cudaStreamDestroy(ctx->stream);
+    cudaStreamDestroy(ctx->side_stream);
+    delete ctx;
+    return R2G_OK;
+}
+
+extern "C" const char *r2g_last_error(R2gCtx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int r2g_dev_alloc(R2gCtx *ctx, void **p, size_t bytes) {
+    if (ctx->budget > 0 && ctx->used + (int64_t)bytes > ctx->budget) {
+        set_err(ctx, "device-memory budget exhausted");
+        return R2G_E_OOM;
+    }
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(ctx, "cudaMalloc failed");
+        return R2G_E_OOM;
+    }
+    ctx->used += (int64_t)bytes;
+    return R2G_OK;
+}
+
+void r2g_dev_free(R2gCtx *ctx, void *p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    ctx->used -= (int64_t)bytes;
+}
+
+// ---------------------------------------------------------------- frames
+extern "C" int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth, R2gFrame **out) {
+    if (!ctx || !out) return R2G_E_INVALID;
+    *out = nullptr;
+    if ((width & 7) || (height & 7) || width <= 0 || height <= 0 || (bitdepth != 8 && bitdepth != 10)) {
+        set_err(ctx, "unsupported frame geometry");
+        return R2G_E_INVALID;
+    }
+    CK(cudaSetDevice(ctx->device));
+    R2gFrame *f = new R2gFrame();
+    f->w = width;
+    f->h = height;
+    f->bd = bitdepth;
+    r2g_plane_geometry(width, height, bitdepth, &f->stride[0], &f->stride[1], &f->rows[0], &f->rows[1]);
+    f->plane_bytes[0] = (size_t)(f->stride[0] * f->rows[0]);
+    f->plane_bytes[1] = (size_t)(f->stride[1] * f->rows[1]);
+    f->buf_bytes = f->plane_bytes[0] + 2 * f->plane_bytes[1];
+    int bw4 = ((width + 7) >> 3) << 1, bh4 = ((height + 7) >> 3) << 1;
+    f->n_sb256 = ((bw4 + 63) >> 6) * ((bh4 + 63) >> 6);
+    f->side_bytes = (size_t)f->n_sb256 * (sizeof(R2gAv2Filter) + sizeof(R2gAv2Restoration));
+    int rc;
+    for (int i = 0; i < 4; i++)
+        if ((rc = r2g_dev_alloc(ctx, &f->buf[i], f->buf_bytes)) != R2G_OK) {
+            r2g_frame_free(ctx, f);
+            return rc;
+        }
+    if ((rc = r2g_dev_alloc(ctx, &f->side_dev, f->side_bytes)) != R2G_OK) {
+        r2g_frame_free(ctx, f);
+        return rc;
+    }
+    if (cudaMallocHost(&f->side_host, f->side_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        r2g_frame_free(ctx, f);
+        set_err(ctx, "pinned allocation failed");
+        return R2G_E_OOM;
+    }
+    // the display copy starts as a copy of whatever is filtered; zero it so
+    // downloads of an ungrained frame are deterministic
+    for (int i = 0; i < 4; i++) CK(cudaMemsetAsync(f->buf[i], 0, f->buf_bytes, ctx->stream));
+    *out = f;
+    return R2G_OK;
+}
+
+extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
+    if (!ctx || !f) return R2G_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < 4; i++) r2g_dev_free(ctx, f->buf[i], f->buf_bytes);
+    r2g_dev_free(ctx, f->side_dev, f->side_bytes);
+    r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
+    if (f->side_host) cudaFreeHost(f->side_host);
+    if (f->seg_host) cudaFreeHost(f->seg_host);
+    delete f;
+    return R2G_OK;
+}
+
+static void plane_ptrs(const R2gFrame *f, int buf, void *p[3]) {
+    char *b = (char *)f->buf[buf];
+    p[0] = b;
+    p[1] = b + f->plane_bytes[0];
+    p[2] = b + f->plane_bytes[0] + f->plane_bytes[1];
+}
+
+static int copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, int64_t ys, const void *u,
+                       const void *v, int64_t uvs, bool upload) {
+    void *p[3];
+    plane_ptrs(f, buf, p);
+    int bps = f->bd > 8 ? 2 : 1;
+    const void *hs[3] = {y, u, v};
+    for (int i = 0; i < 3; i++) {
+        int64_t hstride = i ? uvs : ys;
+        int64_t dstride = f->stride[i ? 1 : 0];
+        int64_t wbytes = (int64_t)(i ? f->w / 2 : f->w) * bps;
+        int64_t rows = i ? f->h / 2 : f->h;
+        if (!hs[i]) continue;
+        if (hstride < wbytes) {
+            set_err(ctx, "host stride smaller than the plane width");
+            return R2G_E_INVALID;
+        }
+        if (upload)
+            CK(cudaMemcpy2DAsync(p[i], dstride, hs[i], hstride, wbytes, rows, cudaMemcpyHostToDevice, ctx->stream));
+        else
+            CK(cudaMemcpy2DAsync((void *)hs[i], hstride, p[i], dstride, wbytes, rows, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    }
+    return R2G_OK;
+}
+
+extern "C" int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, int64_t y_stride, const void *u,
+                                      const void *v, int64_t uv_stride) {
+    if (!ctx || !f || !y || !u || !v) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    return copy_planes(ctx, f, 0, y, y_stride, u, v, uv_stride, true);
+}
+
+extern "C" int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_t y_stride, void *u, void *v,
+                            int64_t uv_stride) {
+    if (!ctx || !f || (which != 0 && which != 1)) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    int buf = which == 0 ? f->out_buf : f->grain_buf;
+    if (buf < 0) {
+        set_err(ctx, which ? "frame has no grained copy" : "frame not filtered");
+        return R2G_E_INVALID;
+    }
+    return copy_planes(ctx, f, buf, y, y_stride, u, v, uv_stride, false);
+}
+
+extern "C" int r2g_sync(R2gCtx *ctx) {
+    if (!ctx) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->side_stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return R2G_OK;
+}
+
+// ---------------------------------------------------------------- filtering
+// decode.rs:27-57 init_wiener, :59-65 compute_restore_planes, :67-80
+// compute_gdf_ref_dst_idx, dq_lookup (quantizer.rs:31)
+static int host_dq_lookup(int qidx) {
+    static const uint8_t T[24] = {40, 41, 43, 44, 45, 47, 48, 49, 51, 52, 54, 55,
+                                  57, 59, 60, 62, 64, 66, 68, 70, 72, 74, 76, 78};
+    qidx = qidx < 0 ? 0 : (qidx > 255 ? 255 : qidx);
+    if (qidx == 0) return 64;
+    qidx -= 1;
+    return (int)T[qidx % 24] << (qidx / 24);
+}
+
+int r2g_validate(R2gCtx *ctx, const R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side) {
+    if (!fp || !side || !side->masks || !side->lr) {
+        set_err(ctx, "missing frame parameters or side-info");
+        return R2G_E_INVALID;
+    }
+    if (fp->width != f->w || fp->height != f->h || fp->bitdepth != f->bd) {
+        set_err(ctx, "frame parameters do not match the frame buffer");
+        return R2G_E_INVALID;
+    }
+    if (fp->layout != 1 || fp->sb128 != 0) {
+        set_err(ctx, "only 4:2:0 with 64x64 superblocks is supported");
+        return R2G_E_INVALID;
+    }
+    if (side->n_sb256 != f->n_sb256) {
+        set_err(ctx, "side-info count does not match the frame size");
+        return R2G_E_INVALID;
+    }
+    for (int pl = 1; pl < 3; pl++)
+        if (fp->restoration[pl].frame_filters_on && fp->restoration[pl].num_classes != 1) {
+            set_err(ctx, "multi-class chroma restoration is not supported");
+            return R2G_E_INVALID;
+        }
+    for (int i = 0; i < side->n_sb256; i++)
+        for (int pl = 1; pl < 3; pl++)
+            for (int u = 0; u < 16; u++)
+                if (side->lr[i].lr[pl][u].restoration_type == R2G_RESTORE_PC_WIENER) {
+                    set_err(ctx, "PC-Wiener on a chroma unit is not supported");
+                    return R2G_E_INVALID;
+                }
+    if (fp->restoration_unit_size[0] < 5 || fp->restoration_unit_size[0] > 9 ||
+        fp->restoration_unit_size[1] < 5 || fp->restoration_unit_size[1] > 9) {
+        set_err(ctx, "restoration unit size out of range");
+        return R2G_E_INVALID;
+    }
+    if (fp->seg_enabled && (!side->segmap)) {
+        // segmentation with no map: every block is segment 0
+    }
+    return R2G_OK;
+}
+
+// deblock.rs:1572-1606 deblock_crop_bottom_edge, applied to the staged masks
+// for every superblock row (it only touches the last 64-row band).
+static void crop_bottom_edge(R2gAv2Filter *mask, int n, int sb256w, int bw, int bh) {
+    int sbh = (bh + 15) >> 4;
+    for (int y64 = 0; y64 < sbh; y64++) {
+        if ((y64 + 1) * 16 + 4 <= bh) continue;
+        int starty4 = (y64 * 16) & 0x30;
+        int h4 = bh - y64 * 16 < 16 ? bh - y64 * 16 : 16;
+        int crop_y4 = starty4 + h4 - 2;
+        if (crop_y4 < 0) continue;
+        int mask_row = (y64 >> 2) * sb256w;
+        for (int x256 = 0; x256 < sb256w; x256++) {
+            if (mask_row + x256 >= n) break;
+            int w = 64 < bw - x256 * 64 ? 64 : bw - x256 * 64;
+            uint16_t(*yv)[4] = mask[mask_row + x256].filter_y[1][crop_y4];
+            for (int i = 0; i < ((w + 15) >> 4); i++) {
+                uint16_t m = yv[3][i];
+                yv[3][i] = 0;
+                yv[2][i] |= m;
+            }
+        }
+    }
+}
+
+int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t inloop,
+                DevFrame &d) {
+    int rc = r2g_validate(ctx, f, fp, side);
+    if (rc != R2G_OK) return rc;
+    memset(&d, 0, sizeof(d));
+    d.w = f->w;
+    d.h = f->h;
+    d.cw = f->w >> 1;
+    d.ch = f->h >> 1;
+    d.bw4 = ((f->w + 7) >> 3) << 1;
+    d.bh4 = ((f->h + 7) >> 3) << 1;
+    d.sb256w = (d.bw4 + 63) >> 6;
+    d.sb256h = (d.bh4 + 63) >> 6;
+    d.sbh = (d.bh4 + 15) / 16;
+    d.bitdepth = f->bd;
+    d.hbd = (f->bd - 8) >> 1;
+    d.bdmax = (1 << f->bd) - 1;
+    int bps = f->bd > 8 ? 2 : 1;
+    d.stride[0] = f->stride[0] / bps;
+    d.stride[1] = f->stride[1] / bps;
+    d.fp = *fp;
+    d.tab = ctx->tab;
+    d.inloop = inloop;
+    d.deblock_on = (inloop & R2G_INLOOP_DEBLOCK) && (fp->deblock_level_y[0] || fp->deblock_level_y[1]);
+    d.cdef_stage_on = fp->seq_cdef && (inloop & (R2G_INLOOP_CDEF | R2G_INLOOP_CCSO));
+    d.ccso_on = (inloop & R2G_INLOOP_CCSO) && (fp->ccso[0].enabled || fp->ccso[1].enabled || fp->ccso[2].enabled);
+    d.cdef_on = (inloop & R2G_INLOOP_CDEF) != 0;
+    d.any_lossless = 0;
+    if (fp->seg_enabled)
+        for (int i = 0; i < 8; i++) d.any_lossless |= fp->seg_lossless[i] != 0;
+    d.restore_planes = (fp->restoration[0].restoration_type != R2G_RESTORE_NONE || fp->gdf_enabled != 0) |
+                       ((fp->restoration[1].restoration_type != R2G_RESTORE_NONE) << 1) |
+                       ((fp->restoration[2].restoration_type != R2G_RESTORE_NONE) << 2);
+    d.lr_on = d.restore_planes != 0 && (inloop & (R2G_INLOOP_WIENER | R2G_INLOOP_GDF));
+    d.base_q = 0;
+    d.wiener_idx = 0;
+    d.ns_ci = -1;
+    int rtype = fp->restoration[0].restoration_type;
+    if (rtype != R2G_RESTORE_NONE) {
+        int q = fp->quant_yac;
+        d.base_q = host_dq_lookup(q);
+        d.wiener_idx = q < 130 ? 0 : q < 190 ? 1 : q < 220 ? 2 : 3;
+        if (rtype == R2G_RESTORE_NS_WIENER || rtype == R2G_RESTORE_SWITCHABLE) {
+            int nci = fp->restoration[0].num_classes_idx;
+            d.ns_ci = nci > 0 ? nci - 1 : -1;
+        }
+    }
+    d.gdf_ref_dst_idx = 0;
+    if (fp->gdf_enabled && (fp->frame_type & 1)) {
+        static const int TBL[12] = {5, 1, 2, 3, 3, 3, 4, 4, 4, 4, 4, 5};
+        int md = 0;
+        int nr = fp->n_ref_frames < 2 ? fp->n_ref_frames : 2;
+        for (int i = 0; i < nr; i++) md = md > fp->absrefdist[i] ? md : fp->absrefdist[i];
+        d.gdf_ref_dst_idx = TBL[md < 11 ? md : 11];
+    }
+
+    // stage side-info: masks (cropped) + restoration records, then segmaps
+    size_t mbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Filter);
+    size_t lbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Restoration);
+    memcpy(f->side_host, side->masks, mbytes);
+    memcpy((char *)f->side_host + mbytes, side->lr, lbytes);
+    if (d.deblock_on) crop_bottom_edge((R2gAv2Filter *)f->side_host, f->n_sb256, d.sb256w, d.bw4, d.bh4);
+    CK(cudaMemcpyAsync(f->side_dev, f->side_host, mbytes + lbytes, cudaMemcpyHostToDevice, ctx->stream));
+    d.masks = (const R2gAv2Filter *)f->side_dev;
+    d.lr = (const R2gAv2Restoration *)((char *)f->side_dev + mbytes);
+    size_t seg_y = side->segmap ? (size_t)side->segmap_stride * d.bh4 : 0;
+    size_t seg_uv = side->segmap_uv ? (size_t)side->segmap_uv_stride * (d.bh4 >> 1) : 0;
+    if (seg_y + seg_uv) {
+        if (f->seg_bytes < seg_y + seg_uv) {
+            r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
+            if (f->seg_host) cudaFreeHost(f->seg_host);
+            f->seg_dev = nullptr;
+            f->seg_host = nullptr;
+            f->seg_bytes = 0;
+            int rc2 = r2g_dev_alloc(ctx, &f->seg_dev, seg_y + seg_uv);
+            if (rc2 != R2G_OK) return rc2;
+            CK(cudaMallocHost(&f->seg_host, seg_y + seg_uv));
+            f->seg_bytes = seg_y + seg_uv;
+        }
+        if (seg_y) memcpy(f->seg_host, side->segmap, seg_y);
+        if (seg_uv) memcpy((char *)f->seg_host + seg_y, side->segmap_uv, seg_uv);
+        CK(cudaMemcpyAsync(f->seg_dev, f->seg_host, seg_y + seg_uv, cudaMemcpyHostToDevice, ctx->stream));
+        d.segmap = seg_y ? (const uint8_t *)f->seg_dev : nullptr;
+        d.segmap_uv = seg_uv ? (const uint8_t *)f->seg_dev + seg_y : nullptr;
+        d.segmap_stride = side->segmap_stride;
+        d.segmap_uv_stride = side->segmap_uv_stride;
+    }
+
+    // buffers: 0 = recon / deblocked, 1 = CDEF out, 2 = LR out, 3 = grain
+    void *p[4][3];
+    for (int i = 0; i < 4; i++) plane_ptrs(f, i, p[i]);
+    for (int i = 0; i < 3; i++) {
+        d.R[i] = p[0][i];
+        d.C[i] = d.cdef_stage_on ? p[1][i] : p[0][i];
+        d.L[i] = d.lr_on ? p[2][i] : d.C[i];
+        d.G[i] = p[3][i];
+    }
+    f->out_buf = d.lr_on ? 2 : (d.cdef_stage_on ? 1 : 0);
+    f->grain_buf = -1;
+    return R2G_OK;
+}
+
+void r2g_launch_pipeline(const DevFrame &d, cudaStream_t s) {
+    r2g_launch_deblock(d, s);
+    r2g_launch_cdef(d, s);
+    r2g_launch_lr(d, s);
+}
+
+extern "C" int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
+                                uint32_t inloop_mask) {
+    if (!ctx || !f) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    int rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc);
+    if (rc != R2G_OK) return rc;
+    r2g_launch_pipeline(f->desc, ctx->stream);
+    CK(cudaGetLastError());
+    return R2G_OK;
+}
+
+extern "C" int r2g_filter_frame_host(R2gCtx *ctx, const R2gFrameParams *fp, const R2gSideInfo *side,
+                                     uint32_t inloop_mask, const R2gFilmGrainData *fgd, uint32_t grain_seed,
+                                     const void *src_y, const void *src_u, const void *src_v, int64_t y_stride,
+                                     int64_t uv_stride, void *dst_y, void *dst_u, void *dst_v, void *grain_y,
+                                     void *grain_u, void *grain_v) {
+    if (!ctx || !fp) return R2G_E_INVALID;
+    R2gFrame *f = nullptr;
+    int rc = r2g_frame_alloc(ctx, fp->width, fp->height, fp->bitdepth, &f);
+    if (rc != R2G_OK) return rc;
+    if ((rc = r2g_frame_upload_recon(ctx, f, src_y, y_stride, src_u, src_v, uv_stride)) == R2G_OK &&
+        (rc = r2g_frame_filter(ctx, f, fp, side, inloop_mask)) == R2G_OK &&
+        (rc = r2g_download(ctx, f, 0, dst_y, y_stride, dst_u, dst_v, uv_stride)) == R2G_OK) {
+        if (fgd && grain_y) {
+            if ((rc = r2g_frame_grain(ctx, f, fgd, grain_seed)) == R2G_OK)
+                rc = r2g_download(ctx, f, 1, grain_y, y_stride, grain_u, grain_v, uv_stride);
+        }
+        if (rc == R2G_OK) rc = r2g_sync(ctx);
+    }
+    r2g_frame_free(ctx, f);
+    return rc;
+}
+
+// ---------------------------------------------------------------- tickets
+int r2g_ticket_record(R2gCtx *ctx, uint64_t *ticket) {
+    Ticket t;
+    CK(cudaEventCreateWithFlags(&t.ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(t.ev, ctx->stream));
+    t.id = ++ctx->next_ticket;
+    ctx->tickets.push_back(t);
+    *ticket = t.id;
+    return R2G_OK;
+}
+
+extern "C" int r2g_wait(R2gCtx *ctx, uint64_t ticket, int timeout_ms) {
+    if (!ctx) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    size_t i = 0;
+    for (; i < ctx->tickets.size(); i++)
+        if (ctx->tickets[i].id == ticket) break;
+    if (i == ctx->tickets.size()) {
+        set_err(ctx, "unknown or already completed ticket");
+        return R2G_E_INVALID;
+    }
+    cudaEvent_t ev = ctx->tickets[i].ev;
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t q = cudaEventQuery(ev);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) {
+            set_err(ctx, "CUDA error: %s", cudaGetErrorString(q));
+            return R2G_E_DEVICE;
+        }
+        if (timeout_ms == 0) return R2G_E_NOTREADY;
+        if (timeout_ms > 0) {
+            auto el = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0);
+            if (el.count() >= timeout_ms) {
+                set_err(ctx, "wait timed out");
+                return R2G_E_TIMEOUT;
+            }
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    cudaEventDestroy(ev);
+    ctx->tickets.erase(ctx->tickets.begin() + i);
+    return R2G_OK;
+}

@@ -1,0 +1,169 @@
+"""Python binding of librav2d_gpu.so, the B200 in-loop filter library.
+
+Mirrors the reference's per-frame filter entry points: `filter_frame`
+stands for looping `filter_sbrow` (decode.rs:3718) over a frame and `grain`
+for `apply_grain_to_picture_mt` (decode.rs:4672).  The CUDA library is the
+only implementation: if it is missing this module raises at import-time use.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "librav2d_gpu.so")
+_lib = None
+
+SYMBOLS = [
+    "r2g_version", "r2g_plane_geometry", "r2g_struct_sizes", "r2g_ctx_create", "r2g_ctx_destroy",
+    "r2g_last_error", "r2g_frame_alloc", "r2g_frame_free", "r2g_frame_upload_recon", "r2g_frame_filter",
+    "r2g_frame_grain", "r2g_download", "r2g_sync", "r2g_filter_frame_host", "r2g_batch_submit", "r2g_wait",
+]
+
+
+class R2gError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rav2d_gpu error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        L.r2g_last_error.restype = C.c_char_p
+        L.r2g_last_error.argtypes = [C.c_void_p]
+        L.r2g_ctx_create.argtypes = [C.c_int, C.c_int64, C.POINTER(C.c_void_p)]
+        L.r2g_ctx_destroy.argtypes = [C.c_void_p]
+        L.r2g_frame_alloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.r2g_frame_free.argtypes = [C.c_void_p, C.c_void_p]
+        L.r2g_frame_upload_recon.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                             C.c_int64]
+        L.r2g_frame_filter.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.FrameParams),
+                                       C.POINTER(abi.SideInfo), C.c_uint32]
+        L.r2g_frame_grain.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.FilmGrainData), C.c_uint32]
+        L.r2g_download.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                   C.c_int64]
+        L.r2g_sync.argtypes = [C.c_void_p]
+        L.r2g_batch_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_uint64)]
+        L.r2g_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int]
+        L.r2g_plane_geometry.argtypes = [C.c_int, C.c_int, C.c_int] + [C.POINTER(C.c_int64)] * 4
+        L.r2g_struct_sizes.argtypes = [C.POINTER(C.c_int32), C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One device context (streams, tables, memory budget)."""
+
+    def __init__(self, device=0, mem_budget=0):
+        h = C.c_void_p()
+        rc = lib().r2g_ctx_create(device, mem_budget, C.byref(h))
+        if rc != 0:
+            raise R2gError(rc, "context creation failed")
+        self.h = h
+
+    def check(self, rc):
+        if rc != 0:
+            raise R2gError(rc, lib().r2g_last_error(self.h).decode())
+        return rc
+
+    def sync(self):
+        self.check(lib().r2g_sync(self.h))
+
+    def close(self):
+        if self.h:
+            lib().r2g_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def frame(self, width, height, bitdepth):
+        return Frame(self, width, height, bitdepth)
+
+    def batch_submit(self, items):
+        """items: list of (Frame, SynthFrame-like with fp/side()/inloop/fgd/grain_seed)."""
+        arr = (abi.BatchItem * len(items))()
+        keep = []
+        for i, (fr, sf) in enumerate(items):
+            side = sf.side()
+            keep.append(side)
+            arr[i].frame = fr.h
+            arr[i].fp = C.pointer(sf.fp)
+            arr[i].side = C.pointer(side)
+            arr[i].inloop_mask = sf.inloop
+            arr[i].fgd = C.pointer(sf.fgd) if sf.fgd is not None else None
+            arr[i].grain_seed = sf.grain_seed
+        t = C.c_uint64()
+        self.check(lib().r2g_batch_submit(self.h, C.cast(arr, C.c_void_p), len(items), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        return lib().r2g_wait(self.h, C.c_uint64(ticket), timeout_ms)
+
+
+class Frame:
+    """A device-resident frame: recon, filtered and display buffers."""
+
+    def __init__(self, ctx, width, height, bitdepth):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(lib().r2g_frame_alloc(ctx.h, width, height, bitdepth, C.byref(h)))
+        self.h = h
+        self.width, self.height, self.bitdepth = width, height, bitdepth
+        self.dtype = np.uint16 if bitdepth > 8 else np.uint8
+
+    def free(self):
+        if self.h:
+            lib().r2g_frame_free(self.ctx.h, self.h)
+            self.h = None
+
+    def upload(self, planes):
+        y, u, v = planes
+        self.ctx.check(lib().r2g_frame_upload_recon(self.ctx.h, self.h, _ptr(y), y.strides[0], _ptr(u), _ptr(v),
+                                                    u.strides[0]))
+
+    def filter(self, sf, inloop=None):
+        side = sf.side()
+        self._side = side
+        self.ctx.check(lib().r2g_frame_filter(self.ctx.h, self.h, C.byref(sf.fp), C.byref(side),
+                                              sf.inloop if inloop is None else inloop))
+
+    def grain(self, fgd, seed):
+        self.ctx.check(lib().r2g_frame_grain(self.ctx.h, self.h, C.byref(fgd), seed))
+
+    def download(self, like, which=0):
+        out = [np.zeros_like(p) for p in like]
+        self.ctx.check(lib().r2g_download(self.ctx.h, self.h, which, _ptr(out[0]), out[0].strides[0],
+                                          _ptr(out[1]), _ptr(out[2]), out[1].strides[0]))
+        self.ctx.sync()
+        return out
+
+
+def filter_frame(ctx, sf, grain=False):
+    """Upload, filter (and optionally grain) one SynthFrame; returns the
+    filtered planes (and the display planes when grain=True)."""
+    fr = Frame(ctx, sf.width, sf.height, sf.bitdepth)
+    try:
+        fr.upload(sf.planes)
+        fr.filter(sf)
+        out = fr.download(sf.planes, 0)
+        if grain:
+            fr.grain(sf.fgd, sf.grain_seed)
+            g = fr.download(sf.planes, 1)
+            return out, g
+        return out
+    finally:
+        fr.free()
