@@ -1,0 +1,342 @@
+"""Benchmark of the B200 in-loop filter + film-grain path.
+
+Metric: filtered Mpix/s (luma pixels of frames through the full configured
+chain).  The headline workload is one 1920x1080 10-bit 4:2:0 frame per step
+through deblock + CDEF + CCSO + loop restoration (NS/PC-Wiener, GDF), seeded
+synthetic recon and side-info (no dataset is named; see rav2d_b200/synth.py).
+
+  value       device-resident: recon and side-info staged in HBM before the
+              timed region; each step filters a different resident frame
+              (a ring larger than L2), timed with CUDA events.
+  e2e         through the C ABI with pinned host buffers: every step uploads
+              the recon and the side-info, filters and downloads the result.
+  roofline    the dominant kernel's algorithmic bytes per launch over its
+              event-timed average launch duration, against the measured HBM
+              copy bandwidth.
+  cpu_baseline  the CPU oracle (a restatement of the reference's scalar Rust
+              filter path; the Rust reference cannot be built on this image)
+              on a bounded sample of the same workload.
+
+`--impl reference` times that CPU path alone with all host threads.
+Multi-GPU: frames are independent, so N ranks run N replicas (no collective
+on the data path); value = frames of all ranks / max rank time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W_, H_, BD_ = 1920, 1080, 10
+SEED = 0x5EED0001
+MPIX = W_ * H_ / 1e6
+# algorithmic HBM bytes per luma pixel at 10-bit (read each input sample once,
+# write each output sample once; 4:2:0 = 1.5 samples / px, 2 B / sample)
+BYTES_PER_PX = {"deblock_vert": 6.0, "deblock_horz": 6.0, "cdef_ccso": 6.0,
+                "loop_restoration": 8.0, "film_grain": 8.0}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(n_distinct=4):
+    from rav2d_b200 import synth
+
+    return [synth.make_frame(W_, H_, BD_, SEED + 16 * i, chain="full") for i in range(n_distinct)]
+
+
+def pinned_like(planes):
+    import torch
+
+    out = []
+    for p in planes:
+        t = torch.empty(p.shape, dtype=torch.int16 if p.dtype == np.uint16 else torch.uint8, pin_memory=True)
+        a = t.numpy().view(p.dtype)
+        a[:] = p
+        out.append((t, a))
+    return out
+
+
+def run_ours(args, rank, world, device):
+    import torch
+
+    from rav2d_b200 import gpu
+
+    torch.cuda.set_device(device)
+    # a dedicated (non-default) stream: the library enqueues every kernel and
+    # copy on it and the CUDA events below are recorded on it
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+    ctx = gpu.Context(device)
+    assert stream.cuda_stream != 0
+    ctx.set_stream(stream.cuda_stream)
+    sfs = make_inputs()
+    n = args.warmup + args.steps
+    frames = []
+    for i in range(n):
+        fr = ctx.frame(W_, H_, BD_)
+        sf = sfs[i % len(sfs)]
+        fr.upload(sf.planes)
+        fr.stage(sf)
+        frames.append(fr)
+    ctx.sync()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---- device-resident timed region ----
+    for i in range(args.warmup):
+        frames[i].run()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        ev0.record(stream)
+        for i in range(args.steps):
+            frames[args.warmup + i].run()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count() - l0
+    ms = ev0.elapsed_time(ev1)
+    barrier()
+    t = torch.tensor([ms], device=f"cuda:{device}")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+
+    # ---- profiled pass: per-stage kernel durations from CUDA events ----
+    for i, fr in enumerate(frames):
+        sf = sfs[i % len(sfs)]
+        fr.upload(sf.planes)
+        fr.stage(sf)
+    ctx.sync()
+    for i in range(args.warmup):
+        frames[i].run()
+    ctx.profile(True)
+    for i in range(args.steps):
+        frames[args.warmup + i].run()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+
+    # ---- end to end through the ABI with pinned host buffers ----
+    pins = [pinned_like(sf.planes) for sf in sfs]
+    outs = pinned_like(sfs[0].planes)
+    out_planes = [a for _, a in outs]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def e2e_step(i):
+        k = i % len(sfs)
+        fr = frames[i]
+        fr.upload([a for _, a in pins[k]])
+        fr.stage(sfs[k])
+        fr.run()
+        fr.download_into(out_planes, 0)
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    for i in range(args.steps):
+        e2e_step(args.warmup + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], device=f"cuda:{device}")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms_max = float(t.item())
+    recon_bytes = int(W_ * H_ * 1.5 * 2)
+    side_bytes = int(sfs[0].masks.nbytes + sfs[0].lr.nbytes)
+
+    for fr in frames:
+        fr.free()
+    ctx.close()
+    return {
+        "ms": ms_max, "launches": launches, "prof": prof, "e2e_ms": e2e_ms_max, "clocks": clk.summary(),
+        "h2d": recon_bytes + side_bytes, "d2h": recon_bytes,
+    }
+
+
+def cpu_baseline(seconds=12.0, threads=1):
+    """The oracle on `threads` host threads, one frame per thread, for about
+    `seconds`; returns (Mpix/s, frames, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    sfs = make_inputs(2)
+    pyoracle.lib()
+    done = [0]
+    lock = threading.Lock()
+    t0 = time.time()
+
+    def worker(k):
+        while time.time() - t0 < seconds:
+            pyoracle.filter_frame(sfs[k % len(sfs)])
+            with lock:
+                done[0] += 1
+
+    ths = [threading.Thread(target=worker, args=(k,)) for k in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    dt = time.time() - t0
+    return done[0] * MPIX / dt, done[0], dt
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": "per-frame 1920x1080 10-bit 4:2:0, deblock+CDEF+CCSO+LR(NS/PC-Wiener+GDF), no grain",
+              "frames_per_step": 1, "width": W_, "height": H_, "bitdepth": BD_, "inloop_mask": 31,
+              "l2": "inputs larger than L2: every step filters a different resident frame",
+              "parallelism": f"replicas{args.gpus}"}
+    metric = "filtered Mpix/s (luma), 10-bit per-frame pipeline on 1 B200"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        nthreads = os.cpu_count() or 1
+        per = []
+        for i in range(args.warmup + args.steps):
+            v, n, dt = cpu_baseline(seconds=0.5, threads=nthreads)
+            if i >= args.warmup:
+                per.append((v, dt))
+        tot_t = sum(dt for _, dt in per)
+        val = sum(v * dt for v, dt in per) / tot_t
+        line = {"impl": "reference", "metric": metric, "value": round(val, 3), "unit": "Mpix/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1000 * tot_t / len(per), 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u16", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": round(val, 3), "unit": "Mpix/s", "cores": nthreads, "kind": "port",
+                                 "sample": "each step: one 0.5 s window of whole 1080p frames through the oracle "
+                                           "(C++ restatement of the reference scalar Rust path), one frame per "
+                                           "thread"},
+                "e2e": {"value": round(val, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    if world > 1:
+        torch.distributed.init_process_group("nccl", init_method="env://",
+                                             timeout=__import__("datetime").timedelta(seconds=120))
+    res = run_ours(args, rank, world, local)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    n = args.gpus
+    ms_step = res["ms"] / args.steps
+    value = n * MPIX * args.steps / (res["ms"] / 1e3)
+    e2e = n * MPIX * args.steps / (res["e2e_ms"] / 1e3)
+    prof = res["prof"]
+    dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    avg_launch_s = dom_ms / dom_n / 1e3
+    achieved = BYTES_PER_PX[dom] * W_ * H_ / avg_launch_s / 1e9
+    peak, peak_kind = peaks()
+    cpu_v, cpu_n, cpu_dt = cpu_baseline(seconds=args.cpu_seconds, threads=1)
+    line = {
+        "metric": metric, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": n, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded recon + side-info, rav2d_b200/synth.py)",
+        "config": config,
+        "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": res["h2d"],
+                "d2h_bytes_per_step": res["d2h"]},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": int(BYTES_PER_PX[dom] * W_ * H_),
+                     "avg_launch_us": round(avg_launch_s * 1e6, 2)},
+        "stages_us_per_frame": {k: round(v[0] / max(1, args.steps) * 1e3, 2) for k, v in prof.items() if v[1]},
+        "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpix/s", "cores": 1, "kind": "port",
+                         "sample": f"{cpu_n} whole 1080p 10-bit frames through the oracle (C++ restatement of the "
+                                   f"reference scalar Rust filter path) on 1 host core in {cpu_dt:.1f} s"},
+        "clocks": res["clocks"], "gpu_launches": res["launches"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -210,6 +210,18 @@ int r2g_struct_sizes(int32_t *sizes, int n);
 int r2g_ctx_create(int device, int64_t mem_budget, R2gCtx **out);
 int r2g_ctx_destroy(R2gCtx *ctx);
 const char *r2g_last_error(R2gCtx *ctx);
+/* Enqueue the context's filter work on a caller-owned CUDA stream
+ * (a cudaStream_t passed as void*; NULL restores the context's own stream). */
+int r2g_ctx_set_stream(R2gCtx *ctx, void *stream);
+/* Instrumentation (no counterpart in the reference): when enabled, every
+ * r2g_frame_run / r2g_frame_grain records CUDA events between its kernels;
+ * r2g_ctx_profile_read synchronises and returns per-stage milliseconds and
+ * launch counts summed since enabling, for stages 0 deblock-vertical,
+ * 1 deblock-horizontal, 2 CDEF+CCSO, 3 loop restoration, 4 film grain. */
+int r2g_ctx_profile(R2gCtx *ctx, int enable);
+int r2g_ctx_profile_read(R2gCtx *ctx, double *stage_ms, int64_t *stage_launches, int n);
+/* Number of kernels this context has launched since creation. */
+int64_t r2g_ctx_launch_count(R2gCtx *ctx);
 
 /* ---- device-resident frames (frame buffers live in the context) ---- */
 int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth, R2gFrame **out);
@@ -217,7 +229,16 @@ int r2g_frame_free(R2gCtx *ctx, R2gFrame *f);
 /* Upload the reconstructed planes (host pointers, byte strides). */
 int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, int64_t y_stride,
                            const void *u, const void *v, int64_t uv_stride);
-/* Run every enabled stage for the whole frame.  Equivalent to calling the
+/* Stage the frame's side-info on the device (validate, apply the bottom-edge
+ * crop, upload masks / restoration records / segment maps) without running
+ * any stage; r2g_frame_run then runs the stages on the staged side-info. */
+int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
+                    uint32_t inloop_mask);
+/* Run the filter stages of a staged frame on its uploaded recon. The recon
+ * buffer is consumed: deblocking runs in place on it. */
+int r2g_frame_run(R2gCtx *ctx, R2gFrame *f);
+/* Run every enabled stage for the whole frame (r2g_frame_stage followed by
+ * r2g_frame_run).  Equivalent to calling the
  * reference's `filter_sbrow` (decode.rs:3718-4058) for every sby of the frame
  * in order; replaces the Phase-B loop at decode.rs:3597-3625. */
 int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp,

@@ -11,7 +11,8 @@ extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, u
         if (!f) return R2G_E_INVALID;
         int rc = r2g_prepare(ctx, f, items[i].fp, items[i].side, items[i].inloop_mask, f->desc);
         if (rc != R2G_OK) return rc;
-        r2g_launch_pipeline(f->desc, ctx->stream);
+        f->staged = true;
+        r2g_launch_pipeline(ctx, f->desc);
         if (items[i].fgd) {
             if (items[i].grain_seed > 0xffff) return R2G_E_INVALID;
             rc = r2g_grain_enqueue(ctx, f, items[i].fgd, items[i].grain_seed);

@@ -413,11 +413,12 @@ __global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
 
 }  // namespace
 
-void r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
-    if (!f.cdef_stage_on) return;
+int r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
+    if (!f.cdef_stage_on) return 0;
     dim3 grid((f.w + 63) / 64, f.h / 8);
     if (f.bitdepth > 8)
         cdef_ccso_kernel<uint16_t><<<grid, 256, 0, s>>>(f);
     else
         cdef_ccso_kernel<uint8_t><<<grid, 256, 0, s>>>(f);
+    return 1;
 }

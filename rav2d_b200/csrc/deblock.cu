@@ -349,15 +349,20 @@ __global__ void __launch_bounds__(256) deblock_kernel(const DevFrame f) {
 
 }  // namespace
 
-void r2g_launch_deblock(const DevFrame &f, cudaStream_t s) {
-    if (!f.deblock_on) return;
+int r2g_launch_deblock_dir(const DevFrame &f, int dir, cudaStream_t s) {
+    if (!f.deblock_on) return 0;
     int items = f.bw4 * f.bh4 + (f.bw4 >> 1) * (f.bh4 >> 1);
     int blocks = (items + 255) / 256;
     if (f.bitdepth > 8) {
-        deblock_kernel<uint16_t, 0><<<blocks, 256, 0, s>>>(f);
-        deblock_kernel<uint16_t, 1><<<blocks, 256, 0, s>>>(f);
+        if (dir == 0)
+            deblock_kernel<uint16_t, 0><<<blocks, 256, 0, s>>>(f);
+        else
+            deblock_kernel<uint16_t, 1><<<blocks, 256, 0, s>>>(f);
     } else {
-        deblock_kernel<uint8_t, 0><<<blocks, 256, 0, s>>>(f);
-        deblock_kernel<uint8_t, 1><<<blocks, 256, 0, s>>>(f);
+        if (dir == 0)
+            deblock_kernel<uint8_t, 0><<<blocks, 256, 0, s>>>(f);
+        else
+            deblock_kernel<uint8_t, 1><<<blocks, 256, 0, s>>>(f);
     }
+    return 1;
 }

@@ -416,10 +416,12 @@ int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uin
     }
     int bs = 16 << fgd->block_size;
     dim3 grid((f->w + bs - 1) / bs, (f->h + bs - 1) / bs);
+    r2g_prof_stage(ctx, 4, true, 0);
     if (f->bd > 8)
         grain_apply_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
     else
         grain_apply_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
+    r2g_prof_stage(ctx, 4, false, 1 + (any ? 1 : 0));
     if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
     if (cudaEventRecord(ctx->grain->freed, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
     ctx->grain->used = true;

@@ -523,8 +523,8 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
 
 }  // namespace
 
-void r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
-    if (!f.lr_on) return;
+int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
+    if (!f.lr_on) return 0;
     int nux_l = (f.w + 63) / 64, nux_c = (f.cw + 63) / 64;
     int n_luma = f.sbh * 2 * nux_l;
     int n = n_luma + 2 * f.sbh * 2 * nux_c;
@@ -532,4 +532,5 @@ void r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
         lr_kernel<uint16_t><<<n, 256, 0, s>>>(f, n_luma, nux_l, nux_c);
     else
         lr_kernel<uint8_t><<<n, 256, 0, s>>>(f, n_luma, nux_l, nux_c);
+    return 1;
 }

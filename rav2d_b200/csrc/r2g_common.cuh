@@ -67,8 +67,9 @@ R2G_D P *plane_ptr(void *base) {
 }
 
 // Launch helpers implemented per stage (deblock.cu, cdef.cu, lr.cu, grain.cu).
-void r2g_launch_deblock(const DevFrame &f, cudaStream_t s);
-void r2g_launch_cdef(const DevFrame &f, cudaStream_t s);
-void r2g_launch_lr(const DevFrame &f, cudaStream_t s);
+// Each returns the number of kernels it launched.
+int r2g_launch_deblock_dir(const DevFrame &f, int dir, cudaStream_t s);
+int r2g_launch_cdef(const DevFrame &f, cudaStream_t s);
+int r2g_launch_lr(const DevFrame &f, cudaStream_t s);
 
 struct GrainDev;  // grain.cu

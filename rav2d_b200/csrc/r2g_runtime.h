@@ -14,6 +14,14 @@ struct Ticket {
 
 struct GrainCtx;  // grain.cu
 
+enum { R2G_N_STAGES = 5 };
+
+// Per-run profiling events: ev[i] .. ev[i+1] brackets stage i.
+struct ProfRun {
+    cudaEvent_t ev[R2G_N_STAGES + 1];
+    int have[R2G_N_STAGES];
+};
+
 struct R2gCtx {
     int device = 0;
     int64_t budget = 0, used = 0;
@@ -24,6 +32,12 @@ struct R2gCtx {
     std::vector<Ticket> tickets;
     uint64_t next_ticket = 0;
     GrainCtx *grain = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int64_t launches = 0;
+    bool profiling = false;
+    std::vector<ProfRun> prof;
+    double prof_ms[R2G_N_STAGES] = {0};
+    int64_t prof_launches[R2G_N_STAGES] = {0};
 };
 
 struct R2gFrame {
@@ -37,10 +51,12 @@ struct R2gFrame {
     size_t side_bytes = 0;
     void *side_dev = nullptr;
     void *side_host = nullptr;  // pinned staging
+    cudaEvent_t side_done = nullptr;  // last upload out of side_host finished
     void *seg_dev = nullptr;
     void *seg_host = nullptr;
     size_t seg_bytes = 0;
     int out_buf = -1, grain_buf = -1;
+    bool staged = false;
     DevFrame desc{};
 };
 
@@ -48,6 +64,8 @@ int r2g_dev_alloc(R2gCtx *ctx, void **p, size_t bytes);
 void r2g_dev_free(R2gCtx *ctx, void *p, size_t bytes);
 int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t inloop,
                 DevFrame &d);
-void r2g_launch_pipeline(const DevFrame &d, cudaStream_t s);
+void r2g_launch_pipeline(R2gCtx *ctx, const DevFrame &d);
+// Profiling hooks around one stage (no-ops unless profiling is enabled).
+void r2g_prof_stage(R2gCtx *ctx, int stage, bool begin, int launches);
 int r2g_ticket_record(R2gCtx *ctx, uint64_t *ticket);
 void r2g_grain_ctx_free(R2gCtx *ctx);

@@ -94,7 +94,8 @@ extern "C" int r2g_ctx_destroy(R2gCtx *ctx) {
     for (auto &t : ctx->tickets) cudaEventDestroy(t.ev);
     ctx->tickets.clear();
     r2g_grain_ctx_free(ctx);
-    cudaStreamDestroy(ctx->stream);
+    r2g_ctx_profile(ctx, 0);
+    cudaStreamDestroy(ctx->own_stream ? ctx->own_stream : ctx->stream);
     cudaStreamDestroy(ctx->side_stream);
     delete ctx;
     return R2G_OK;
@@ -174,6 +175,7 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
     if (f->side_host) cudaFreeHost(f->side_host);
     if (f->seg_host) cudaFreeHost(f->seg_host);
+    if (f->side_done) cudaEventDestroy(f->side_done);
     delete f;
     return R2G_OK;
 }
@@ -369,7 +371,10 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
         d.gdf_ref_dst_idx = TBL[md < 11 ? md : 11];
     }
 
-    // stage side-info: masks (cropped) + restoration records, then segmaps
+    // stage side-info: masks (cropped) + restoration records, then segmaps;
+    // the pinned staging buffer is reused, so wait for its previous upload
+    if (!f->side_done) CK(cudaEventCreateWithFlags(&f->side_done, cudaEventDisableTiming));
+    CK(cudaEventSynchronize(f->side_done));
     size_t mbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Filter);
     size_t lbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Restoration);
     memcpy(f->side_host, side->masks, mbytes);
@@ -400,6 +405,7 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
         d.segmap_stride = side->segmap_stride;
         d.segmap_uv_stride = side->segmap_uv_stride;
     }
+    CK(cudaEventRecord(f->side_done, ctx->stream));
 
     // buffers: 0 = recon / deblocked, 1 = CDEF out, 2 = LR out, 3 = grain
     void *p[4][3];
@@ -415,21 +421,122 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
     return R2G_OK;
 }
 
-void r2g_launch_pipeline(const DevFrame &d, cudaStream_t s) {
-    r2g_launch_deblock(d, s);
-    r2g_launch_cdef(d, s);
-    r2g_launch_lr(d, s);
+// ---------------------------------------------------------------- profiling
+void r2g_prof_stage(R2gCtx *ctx, int stage, bool begin, int launches) {
+    ctx->launches += launches;
+    if (!ctx->profiling) return;
+    if (begin) {
+        if (stage == 0 || ctx->prof.empty()) {
+            ProfRun r;
+            for (int i = 0; i <= R2G_N_STAGES; i++) r.ev[i] = nullptr;
+            for (int i = 0; i < R2G_N_STAGES; i++) r.have[i] = 0;
+            ctx->prof.push_back(r);
+        }
+        ProfRun &r = ctx->prof.back();
+        if (!r.ev[stage]) {
+            cudaEventCreate(&r.ev[stage]);
+            cudaEventRecord(r.ev[stage], ctx->stream);
+        }
+    } else {
+        ProfRun &r = ctx->prof.back();
+        if (!r.ev[stage + 1]) cudaEventCreate(&r.ev[stage + 1]);
+        cudaEventRecord(r.ev[stage + 1], ctx->stream);
+        r.have[stage] = launches;
+    }
 }
 
-extern "C" int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
-                                uint32_t inloop_mask) {
+extern "C" int r2g_ctx_profile(R2gCtx *ctx, int enable) {
+    if (!ctx) return R2G_E_INVALID;
+    ctx->profiling = enable != 0;
+    for (auto &r : ctx->prof)
+        for (int i = 0; i <= R2G_N_STAGES; i++)
+            if (r.ev[i]) cudaEventDestroy(r.ev[i]);
+    ctx->prof.clear();
+    for (int i = 0; i < R2G_N_STAGES; i++) {
+        ctx->prof_ms[i] = 0;
+        ctx->prof_launches[i] = 0;
+    }
+    return R2G_OK;
+}
+
+extern "C" int r2g_ctx_profile_read(R2gCtx *ctx, double *stage_ms, int64_t *stage_launches, int n) {
+    if (!ctx) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto &r : ctx->prof) {
+        for (int i = 0; i < R2G_N_STAGES; i++) {
+            if (!r.have[i] || !r.ev[i] || !r.ev[i + 1]) continue;
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, r.ev[i], r.ev[i + 1]) == cudaSuccess) {
+                ctx->prof_ms[i] += ms;
+                ctx->prof_launches[i] += r.have[i];
+            }
+        }
+        for (int i = 0; i <= R2G_N_STAGES; i++)
+            if (r.ev[i]) cudaEventDestroy(r.ev[i]);
+    }
+    ctx->prof.clear();
+    for (int i = 0; i < n && i < R2G_N_STAGES; i++) {
+        if (stage_ms) stage_ms[i] = ctx->prof_ms[i];
+        if (stage_launches) stage_launches[i] = ctx->prof_launches[i];
+    }
+    return R2G_OK;
+}
+
+extern "C" int64_t r2g_ctx_launch_count(R2gCtx *ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int r2g_ctx_set_stream(R2gCtx *ctx, void *stream) {
+    if (!ctx) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->own_stream) ctx->own_stream = ctx->stream;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return R2G_OK;
+}
+
+void r2g_launch_pipeline(R2gCtx *ctx, const DevFrame &d) {
+    cudaStream_t s = ctx->stream;
+    r2g_prof_stage(ctx, 0, true, 0);
+    int n = r2g_launch_deblock_dir(d, 0, s);
+    r2g_prof_stage(ctx, 0, false, n);
+    r2g_prof_stage(ctx, 1, true, 0);
+    n = r2g_launch_deblock_dir(d, 1, s);
+    r2g_prof_stage(ctx, 1, false, n);
+    r2g_prof_stage(ctx, 2, true, 0);
+    n = r2g_launch_cdef(d, s);
+    r2g_prof_stage(ctx, 2, false, n);
+    r2g_prof_stage(ctx, 3, true, 0);
+    n = r2g_launch_lr(d, s);
+    r2g_prof_stage(ctx, 3, false, n);
+}
+
+extern "C" int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
+                               uint32_t inloop_mask) {
     if (!ctx || !f) return R2G_E_INVALID;
     CK(cudaSetDevice(ctx->device));
     int rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc);
     if (rc != R2G_OK) return rc;
-    r2g_launch_pipeline(f->desc, ctx->stream);
+    f->staged = true;
+    return R2G_OK;
+}
+
+extern "C" int r2g_frame_run(R2gCtx *ctx, R2gFrame *f) {
+    if (!ctx || !f) return R2G_E_INVALID;
+    if (!f->staged) {
+        set_err(ctx, "frame has no staged side-info");
+        return R2G_E_INVALID;
+    }
+    CK(cudaSetDevice(ctx->device));
+    r2g_launch_pipeline(ctx, f->desc);
     CK(cudaGetLastError());
     return R2G_OK;
+}
+
+extern "C" int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
+                                uint32_t inloop_mask) {
+    int rc = r2g_frame_stage(ctx, f, fp, side, inloop_mask);
+    if (rc != R2G_OK) return rc;
+    return r2g_frame_run(ctx, f);
 }
 
 extern "C" int r2g_filter_frame_host(R2gCtx *ctx, const R2gFrameParams *fp, const R2gSideInfo *side,

@@ -20,6 +20,8 @@ SYMBOLS = [
     "r2g_version", "r2g_plane_geometry", "r2g_struct_sizes", "r2g_ctx_create", "r2g_ctx_destroy",
     "r2g_last_error", "r2g_frame_alloc", "r2g_frame_free", "r2g_frame_upload_recon", "r2g_frame_filter",
     "r2g_frame_grain", "r2g_download", "r2g_sync", "r2g_filter_frame_host", "r2g_batch_submit", "r2g_wait",
+    "r2g_frame_stage", "r2g_frame_run", "r2g_ctx_set_stream", "r2g_ctx_profile", "r2g_ctx_profile_read",
+    "r2g_ctx_launch_count",
 ]
 
 
@@ -53,6 +55,14 @@ def lib():
         L.r2g_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int]
         L.r2g_plane_geometry.argtypes = [C.c_int, C.c_int, C.c_int] + [C.POINTER(C.c_int64)] * 4
         L.r2g_struct_sizes.argtypes = [C.POINTER(C.c_int32), C.c_int]
+        L.r2g_frame_stage.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.FrameParams), C.POINTER(abi.SideInfo),
+                                      C.c_uint32]
+        L.r2g_frame_run.argtypes = [C.c_void_p, C.c_void_p]
+        L.r2g_ctx_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        L.r2g_ctx_profile.argtypes = [C.c_void_p, C.c_int]
+        L.r2g_ctx_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
+        L.r2g_ctx_launch_count.argtypes = [C.c_void_p]
+        L.r2g_ctx_launch_count.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -89,6 +99,24 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_stream(self, stream_handle):
+        """Enqueue on a caller-owned cudaStream_t (an int handle; 0 = own)."""
+        self.check(lib().r2g_ctx_set_stream(self.h, C.c_void_p(stream_handle or None)))
+
+    def profile(self, enable=True):
+        self.check(lib().r2g_ctx_profile(self.h, int(enable)))
+
+    STAGES = ("deblock_vert", "deblock_horz", "cdef_ccso", "loop_restoration", "film_grain")
+
+    def profile_read(self):
+        ms = (C.c_double * 5)()
+        n = (C.c_int64 * 5)()
+        self.check(lib().r2g_ctx_profile_read(self.h, ms, n, 5))
+        return {s: (ms[i], n[i]) for i, s in enumerate(self.STAGES)}
+
+    def launch_count(self):
+        return lib().r2g_ctx_launch_count(self.h)
 
     def frame(self, width, height, bitdepth):
         return Frame(self, width, height, bitdepth)
@@ -134,6 +162,20 @@ class Frame:
         y, u, v = planes
         self.ctx.check(lib().r2g_frame_upload_recon(self.ctx.h, self.h, _ptr(y), y.strides[0], _ptr(u), _ptr(v),
                                                     u.strides[0]))
+
+    def stage(self, sf, inloop=None):
+        side = sf.side()
+        self._side = side
+        self.ctx.check(lib().r2g_frame_stage(self.ctx.h, self.h, C.byref(sf.fp), C.byref(side),
+                                             sf.inloop if inloop is None else inloop))
+
+    def run(self):
+        self.ctx.check(lib().r2g_frame_run(self.ctx.h, self.h))
+
+    def download_into(self, out, which=0):
+        """Enqueue a download into preallocated (ideally pinned) planes."""
+        self.ctx.check(lib().r2g_download(self.ctx.h, self.h, which, _ptr(out[0]), out[0].strides[0],
+                                          _ptr(out[1]), _ptr(out[2]), out[1].strides[0]))
 
     def filter(self, sf, inloop=None):
         side = sf.side()
