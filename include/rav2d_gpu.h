@@ -40,6 +40,7 @@ extern "C" {
 #define R2G_E_TIMEOUT (-3)  /* r2g_wait deadline passed; work still queued */
 #define R2G_E_DEVICE (-4)   /* CUDA error or device-side watchdog tripped */
 #define R2G_E_NOTREADY (-5) /* ticket not complete (non-blocking poll) */
+#define R2G_E_TOO_LARGE (-6) /* request exceeds a fixed-size buffer's limit */
 
 /* ---- inloop filter bitmask (looprestoration.rs:1697-1706) ---- */
 #define R2G_INLOOP_DEBLOCK (1u << 0)
@@ -274,6 +275,26 @@ int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ti
 /* Wait for a ticket; R2G_E_TIMEOUT after timeout_ms (<0 = forever),
  * timeout_ms == 0 polls (R2G_E_NOTREADY when pending). */
 int r2g_wait(R2gCtx *ctx, uint64_t ticket, int timeout_ms);
+
+/* ---- film grain without any device allocation ----
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * a decoder embedded in a framework whose device memory is owned by that
+ * framework's allocator or a fixed pool, or a latency-critical output thread
+ * that must not block in the driver's allocator.  Applies the same film grain
+ * as r2g_frame_grain from the caller's device planes src_* (filtered frame,
+ * 4:2:0) to the caller's device planes dst_* (display copy), byte strides,
+ * enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream).
+ * Allocates nothing: its only scratch (grain templates and scaling LUTs, 40 KB)
+ * is a fixed device array that every GPU loading the library holds until the
+ * process exits.  The first call on a device (with that device current) looks
+ * up the array's address and should come before any stream capture.  All
+ * calls share the array, so calls whose GPU work overlaps race; serialise
+ * them (one stream).  Bit depths above 10 exceed the array's LUT capacity and
+ * return R2G_E_TOO_LARGE; other bad arguments return R2G_E_INVALID. */
+int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u, const void *src_v, void *dst_y,
+                                 void *dst_u, void *dst_v, int64_t y_stride, int64_t uv_stride, int width,
+                                 int height, int bitdepth, const R2gFilmGrainData *fgd, uint32_t seed,
+                                 void *stream);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,7 @@ R2G_E_OOM = -2
 R2G_E_TIMEOUT = -3
 R2G_E_DEVICE = -4
 R2G_E_NOTREADY = -5
+R2G_E_TOO_LARGE = -6
 
 INLOOP_DEBLOCK = 1 << 0
 INLOOP_CDEF = 1 << 1

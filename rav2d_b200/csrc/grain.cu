@@ -443,3 +443,108 @@ extern "C" int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData 
     if (cudaSetDevice(ctx->device) != cudaSuccess) return R2G_E_DEVICE;
     return r2g_grain_enqueue(ctx, f, fgd, seed);
 }
+
+// ---------------------------------------------------------------------------
+// Film grain without any device allocation.
+//
+// Some callers cannot call cudaMalloc: a decoder embedded in a host framework
+// whose device memory is owned by that framework's own allocator or by a
+// fixed-size pool, or a latency-critical output thread that must not block in
+// the driver's allocator.  This entry point takes the caller's input and
+// output planes and keeps its only scratch (the three grain templates and the
+// three scaling LUTs) in a file-scope device array of fixed size, resident on
+// every GPU that loads this library until the process exits.
+//
+// * The first call on a device (made with that device current) looks up the
+//   array's device address and the constant tables; make that first call
+//   before any stream capture.  Later calls do no set-up.
+// * Every call on a device shares the one array, and each call rewrites every
+//   scratch byte it later reads, so nothing has to start at zero.  Calls whose
+//   GPU work overlaps (for example on two streams) race on the array; callers
+//   must serialise them, e.g. by issuing them on one stream.
+// * The array holds scaling LUTs of at most 1024 entries, i.e. bit depths up
+//   to 10; larger bit depths are rejected with R2G_E_TOO_LARGE.
+
+#include <mutex>
+
+#define R2G_NOALLOC_LUT_BYTES (3 * GH * GW * 2)
+#define R2G_NOALLOC_SCALING_BYTES (3 * 1024)
+#define R2G_NOALLOC_SCRATCH_BYTES (40 * 1024)
+static_assert(R2G_NOALLOC_LUT_BYTES + R2G_NOALLOC_SCALING_BYTES <= R2G_NOALLOC_SCRATCH_BYTES, "scratch too small");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[R2G_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
+    DevTables tab{};
+};
+NoallocDevice g_noalloc[64];
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u, const void *src_v, void *dst_y,
+                                            void *dst_u, void *dst_v, int64_t y_stride, int64_t uv_stride, int width,
+                                            int height, int bitdepth, const R2gFilmGrainData *fgd, uint32_t seed,
+                                            void *stream) {
+    if (!src_y || !src_u || !src_v || !dst_y || !dst_u || !dst_v || !fgd) return R2G_E_INVALID;
+    if (bitdepth > 10) return R2G_E_TOO_LARGE;  // scaling LUTs would not fit the scratch
+    if (bitdepth != 8 && bitdepth != 10) return R2G_E_INVALID;
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || seed > 0xffff) return R2G_E_INVALID;
+    if (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
+        fgd->scaling_shift < 8 || fgd->scaling_shift > 11)
+        return R2G_E_INVALID;
+    const int bps = bitdepth > 8 ? 2 : 1;
+    if (y_stride < (int64_t)width * bps || uv_stride < (int64_t)((width + 1) >> 1) * bps || (y_stride % bps) ||
+        (uv_stride % bps))
+        return R2G_E_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return R2G_E_DEVICE;
+    NoallocDevice &nd = g_noalloc[dev];
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!nd.ready) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return R2G_E_DEVICE;
+            if (r2g_get_tables(&nd.tab) != cudaSuccess) return R2G_E_DEVICE;
+            if (init_lfsr_pow(dev) != cudaSuccess) return R2G_E_DEVICE;
+            nd.scratch = (unsigned char *)p;
+            nd.ready = true;
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    int16_t *lut = (int16_t *)nd.scratch;
+    uint8_t *scaling = nd.scratch + R2G_NOALLOC_LUT_BYTES;
+
+    GrainParams gp;
+    gp.d = *fgd;
+    gp.seed = seed;
+    gp.bitdepth = bitdepth;
+    bool any;
+    grain_planes(*fgd, gp.has_y, gp.has_u, gp.has_v, any);
+    DevFrame d;
+    memset(&d, 0, sizeof(d));
+    d.w = width;
+    d.h = height;
+    d.cw = (width + 1) >> 1;
+    d.ch = (height + 1) >> 1;
+    d.bitdepth = bitdepth;
+    d.bdmax = (1 << bitdepth) - 1;
+    d.stride[0] = y_stride / bps;
+    d.stride[1] = uv_stride / bps;
+    d.L[0] = (void *)src_y;
+    d.L[1] = (void *)src_u;
+    d.L[2] = (void *)src_v;
+    d.G[0] = dst_y;
+    d.G[1] = dst_u;
+    d.G[2] = dst_v;
+    if (any) grain_template_kernel<<<1, 256, 0, s>>>(gp, nd.tab, lut, scaling);
+    int bs = 16 << fgd->block_size;
+    dim3 grid((width + bs - 1) / bs, (height + bs - 1) / bs);
+    if (bitdepth > 8)
+        grain_apply_kernel<uint16_t><<<grid, 256, 0, s>>>(d, gp, lut, scaling);
+    else
+        grain_apply_kernel<uint8_t><<<grid, 256, 0, s>>>(d, gp, lut, scaling);
+    return cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
+}
