@@ -217,8 +217,8 @@ int r2g_ctx_set_stream(R2gCtx *ctx, void *stream);
 /* Instrumentation (no counterpart in the reference): when enabled, every
  * r2g_frame_run / r2g_frame_grain records CUDA events between its kernels;
  * r2g_ctx_profile_read synchronises and returns per-stage milliseconds and
- * launch counts summed since enabling, for stages 0 deblock-vertical,
- * 1 deblock-horizontal, 2 CDEF+CCSO, 3 loop restoration, 4 film grain. */
+ * launch counts summed since enabling, for stages 0 deblock, 1 CDEF+CCSO,
+ * 2 loop restoration, 3 film grain. */
 int r2g_ctx_profile(R2gCtx *ctx, int enable);
 int r2g_ctx_profile_read(R2gCtx *ctx, double *stage_ms, int64_t *stage_launches, int n);
 /* Number of kernels this context has launched since creation. */
@@ -235,8 +235,8 @@ int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, int64_t y_st
  * any stage; r2g_frame_run then runs the stages on the staged side-info. */
 int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
                     uint32_t inloop_mask);
-/* Run the filter stages of a staged frame on its uploaded recon. The recon
- * buffer is consumed: deblocking runs in place on it. */
+/* Run the filter stages of a staged frame on its uploaded recon (the recon
+ * buffer is left unchanged, so a staged frame can be run again). */
 int r2g_frame_run(R2gCtx *ctx, R2gFrame *f);
 /* Run every enabled stage for the whole frame (r2g_frame_stage followed by
  * r2g_frame_run).  Equivalent to calling the

@@ -34,6 +34,7 @@ struct BlockParams {
     int active;   // any CDEF filtering of this 8x8 (luma or chroma)
     int y_pri, y_sec, y_dir, y_on;
     int uv_pri, uv_sec, uv_dir, uv_on;
+    int yoff[6], uvoff[6];  // tap offsets in the luma / chroma padded tiles
 };
 
 R2G_D int constrain(int diff, int threshold, int shift) {
@@ -60,11 +61,12 @@ R2G_D int load_px(const P *p) {
     return (int)*p;
 }
 
-// cdef_filter_block (cdef.rs:320-458) for one sample.  `tap(dy, dx)`
-// returns the padded neighbour value.
-template <typename TapF>
-R2G_D int cdef_px(int px, int pri, int sec, int dir, int damping, int bd8, const DevTables &tab, TapF tap) {
-    const int8_t *D = tab.CDEF_DIRECTIONS;
+// cdef_filter_block (cdef.rs:320-458) for one sample.  `t` points at the
+// sample in a padded tile (INT16_MIN outside the frame, as cdef_padding
+// writes); off[0..1] are the primary taps (dir + 2, k = 0, 1), off[2..3] the
+// secondary taps of dir + 4 and off[4..5] those of dir, as linear offsets.
+R2G_D int cdef_px(const int16_t *t, int pri, int sec, const int *off, int damping, int bd8) {
+    const int px = t[0];
     if (pri != 0) {
         int pri_tap = 4 - ((pri >> bd8) & 1);
         int pri_shift = imax_(0, damping - ulog2_((uint32_t)pri));
@@ -73,41 +75,24 @@ R2G_D int cdef_px(int px, int pri, int sec, int dir, int damping, int bd8, const
             int sec_shift = damping - ulog2_((uint32_t)sec);
 #pragma unroll
             for (int k = 0; k < 2; k++) {
-                int dy, dx;
-                dir_off(D[(dir + 2) * 2 + k], dy, dx);
-                int p0 = tap(dy, dx), p1 = tap(-dy, -dx);
+                int p0 = t[off[k]], p1 = t[-off[k]];
                 sum += tk * constrain(p0 - px, pri, pri_shift);
                 sum += tk * constrain(p1 - px, pri, pri_shift);
                 tk = (tk & 3) | 2;
-                mn = imin_(p0, mn);
-                mx = imax_(p0, mx);
-                mn = imin_(p1, mn);
-                mx = imax_(p1, mx);
-                int ay, ax, by, bx;
-                dir_off(D[(dir + 4) * 2 + k], ay, ax);
-                dir_off(D[dir * 2 + k], by, bx);
-                int s0 = tap(ay, ax), s1 = tap(-ay, -ax), s2 = tap(by, bx), s3 = tap(-by, -bx);
+                mn = imin_(imin_(p0, p1), mn);
+                mx = imax_(imax_(p0, p1), mx);
+                int s0 = t[off[2 + k]], s1 = t[-off[2 + k]], s2 = t[off[4 + k]], s3 = t[-off[4 + k]];
                 int st = 2 - k;
-                sum += st * constrain(s0 - px, sec, sec_shift);
-                sum += st * constrain(s1 - px, sec, sec_shift);
-                sum += st * constrain(s2 - px, sec, sec_shift);
-                sum += st * constrain(s3 - px, sec, sec_shift);
-                mn = imin_(s0, mn);
-                mx = imax_(s0, mx);
-                mn = imin_(s1, mn);
-                mx = imax_(s1, mx);
-                mn = imin_(s2, mn);
-                mx = imax_(s2, mx);
-                mn = imin_(s3, mn);
-                mx = imax_(s3, mx);
+                sum += st * (constrain(s0 - px, sec, sec_shift) + constrain(s1 - px, sec, sec_shift) +
+                             constrain(s2 - px, sec, sec_shift) + constrain(s3 - px, sec, sec_shift));
+                mn = imin_(imin_(imin_(s0, s1), imin_(s2, s3)), mn);
+                mx = imax_(imax_(imax_(s0, s1), imax_(s2, s3)), mx);
             }
             return iclip_(px + ((sum - (sum < 0) + 8) >> 4), mn, mx);
         }
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-            int dy, dx;
-            dir_off(D[(dir + 2) * 2 + k], dy, dx);
-            int p0 = tap(dy, dx), p1 = tap(-dy, -dx);
+            int p0 = t[off[k]], p1 = t[-off[k]];
             sum += tk * constrain(p0 - px, pri, pri_shift);
             sum += tk * constrain(p1 - px, pri, pri_shift);
             tk = (tk & 3) | 2;
@@ -118,17 +103,25 @@ R2G_D int cdef_px(int px, int pri, int sec, int dir, int damping, int bd8, const
     int sum = 0;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-        int ay, ax, by, bx;
-        dir_off(D[(dir + 4) * 2 + k], ay, ax);
-        dir_off(D[dir * 2 + k], by, bx);
-        int s0 = tap(ay, ax), s1 = tap(-ay, -ax), s2 = tap(by, bx), s3 = tap(-by, -bx);
+        int s0 = t[off[2 + k]], s1 = t[-off[2 + k]], s2 = t[off[4 + k]], s3 = t[-off[4 + k]];
         int st = 2 - k;
-        sum += st * constrain(s0 - px, sec, sec_shift);
-        sum += st * constrain(s1 - px, sec, sec_shift);
-        sum += st * constrain(s2 - px, sec, sec_shift);
-        sum += st * constrain(s3 - px, sec, sec_shift);
+        sum += st * (constrain(s0 - px, sec, sec_shift) + constrain(s1 - px, sec, sec_shift) +
+                     constrain(s2 - px, sec, sec_shift) + constrain(s3 - px, sec, sec_shift));
     }
     return px + ((sum - (sum < 0) + 8) >> 4);
+}
+
+// Linear tap offsets of direction `dir` in a tile of row pitch `pitch`.
+R2G_D void tap_offsets(const int8_t *dirs, int dir, int pitch, int *off) {
+    const int which[3] = {dir + 2, dir + 4, dir};
+#pragma unroll
+    for (int w = 0; w < 3; w++)
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            int dy, dx;
+            dir_off(dirs[which[w] * 2 + k], dy, dx);
+            off[w * 2 + k] = dy * pitch + dx;
+        }
 }
 
 // ccso_score (ccso.rs:16-24)
@@ -140,8 +133,10 @@ R2G_D uint32_t ccso_score(int diff, int q, uint32_t clf) {
 
 template <typename P>
 __global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
-    __shared__ int16_t ty[TH][TW];
+    __shared__ int16_t ty[TH][TW];      // clamped to the frame (CCSO padding)
     __shared__ int16_t tc[2][CH][CW];
+    __shared__ int16_t pty[TH][TW];     // INT16_MIN outside the frame (CDEF padding)
+    __shared__ int16_t ptc[2][CH][CW];
     __shared__ int bins[8][96];
     __shared__ BlockParams bp[8];
     __shared__ int s_ccso[3];
@@ -152,22 +147,32 @@ __global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
     const int cx0 = gx0 >> 1, cy0 = gy0 >> 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int bd8 = f.bitdepth - 8;
-    const P *Dy = plane_ptr<const P>(f.R[0]);
-    const P *Du = plane_ptr<const P>(f.R[1]);
-    const P *Dv = plane_ptr<const P>(f.R[2]);
+    const P *Dy = plane_ptr<const P>(f.D[0]);
+    const P *Du = plane_ptr<const P>(f.D[1]);
+    const P *Dv = plane_ptr<const P>(f.D[2]);
     const int64_t ys = f.stride[0], uvs = f.stride[1];
 
     // ---- stage the band (clamped coordinates) ----
-    for (int i = tid; i < TH * TW; i += 256) {
-        int r = i / TW, c = i % TW;
-        int gy = iclip_(gy0 - 2 + r, 0, f.h - 1), gx = iclip_(gx0 - 2 + c, 0, f.w - 1);
-        ty[r][c] = (int16_t)Dy[gy * ys + gx];
+    for (int r = warp; r < TH; r += 8) {
+        const int ry = gy0 - 2 + r, gy = iclip_(ry, 0, f.h - 1);
+        const P *row = Dy + gy * ys;
+        for (int c = lane; c < TW; c += 32) {
+            int rx = gx0 - 2 + c;
+            int16_t v = (int16_t)row[iclip_(rx, 0, f.w - 1)];
+            ty[r][c] = v;
+            pty[r][c] = (ry < 0 || ry >= f.h || rx < 0 || rx >= f.w) ? (int16_t)INT16_MIN : v;
+        }
     }
-    for (int i = tid; i < 2 * CH * CW; i += 256) {
-        int pl = i / (CH * CW), j = i % (CH * CW);
-        int r = j / CW, c = j % CW;
-        int gy = iclip_(cy0 - 2 + r, 0, f.ch - 1), gx = iclip_(cx0 - 2 + c, 0, f.cw - 1);
-        tc[pl][r][c] = (int16_t)(pl ? Dv : Du)[gy * uvs + gx];
+    for (int rr = warp; rr < 2 * CH; rr += 8) {
+        const int pl = rr / CH, r = rr % CH;
+        const int ry = cy0 - 2 + r, gy = iclip_(ry, 0, f.ch - 1);
+        const P *row = (pl ? Dv : Du) + gy * uvs;
+        for (int c = lane; c < CW; c += 32) {
+            int rx = cx0 - 2 + c;
+            int16_t v = (int16_t)row[iclip_(rx, 0, f.cw - 1)];
+            tc[pl][r][c] = v;
+            ptc[pl][r][c] = (ry < 0 || ry >= f.ch || rx < 0 || rx >= f.cw) ? (int16_t)INT16_MIN : v;
+        }
     }
     for (int i = tid; i < 8 * 96; i += 256) (&bins[0][0])[i] = 0;
 
@@ -303,111 +308,92 @@ __global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
                 p.y_pri = yp;
                 p.y_dir = yd;
                 p.uv_dir = p.uv_pri != 0 ? c_uv_dirs[dir] : 0;
+                tap_offsets(f.tab.CDEF_DIRECTIONS, p.y_dir, TW, p.yoff);
+                tap_offsets(f.tab.CDEF_DIRECTIONS, p.uv_dir, CW, p.uvoff);
             }
             bp[warp] = p;
         }
     }
     __syncthreads();
 
-    // ---- phase 2: filter + CCSO, row-contiguous ----
+    // ---- phase 2: filter + CCSO; warp w produces 8x8 block w (uniform
+    // parameters per warp), lane -> 2 luma samples and 1 chroma sample ----
     const int bitdepth = f.bitdepth, bdmax = f.bdmax;
-    // luma: thread -> row tid/32, samples 2*(tid%32) and +1
-    {
-        int r = tid >> 5, c0 = (tid & 31) * 2;
+    const BlockParams &p = bp[warp];
+    const int bx0 = warp * 8;
+    if (gx0 + bx0 < f.w) {
+        // luma
+        const int r = lane >> 2, c0 = bx0 + (lane & 3) * 2;
         P *Cy = plane_ptr<P>(f.C[0]);
-        int gy = gy0 + r;
+        const int gy = gy0 + r;
         int out[2];
+        const R2gCcsoPlane &cp = fp.ccso[0];
+        const int cq = f.tab.CCSO_QUANT_SZ[cp.scale_idx * 4 + cp.quant_idx];
+        const int coff = c_ccso_pos[cp.ext_filter_support][0] * TW + c_ccso_pos[cp.ext_filter_support][1];
+        const bool lossy_row = !(f.any_lossless &&
+                                 ((m.lossless_mask_y[2 * by_idx + (r >> 2)][sb64x_idx] >> (c0 >> 2)) & 1));
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-            int c = c0 + k, gx = gx0 + c;
-            int px = ty[2 + r][2 + c];
-            const BlockParams &p = bp[c >> 3];
+            const int c = c0 + k;
+            const int16_t *t = &ty[2 + r][2 + c];
+            const int px = t[0];
             int v = px;
             if (p.active && p.y_on) {
-                auto tap = [&](int dy, int dx) -> int {
-                    int yy = gy + dy, xx = gx + dx;
-                    if (yy < 0 || yy >= f.h || xx < 0 || xx >= f.w) return INT16_MIN;
-                    return ty[2 + r + dy][2 + c + dx];
-                };
-                v = cdef_px(px, p.y_pri, p.y_sec, p.y_dir, damping, bd8, f.tab, tap);
+                v = cdef_px(&pty[2 + r][2 + c], p.y_pri, p.y_sec, p.yoff, damping, bd8);
                 v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
             }
-            if (s_ccso[0]) {
-                const R2gCcsoPlane &cp = fp.ccso[0];
-                int cl = px;
-                int band_ = (int)((uint32_t)cl >> (bitdepth - cp.max_band_log2));
+            if (s_ccso[0] && lossy_row) {
+                // ccso_prep (ccso.rs:115-185): the clamped tile is the padding
+                int band_ = (int)((uint32_t)px >> (bitdepth - cp.max_band_log2));
                 int idx;
-                if (cp.bo_only) {
-                    idx = band_;
-                } else {
-                    int dy = c_ccso_pos[cp.ext_filter_support][0], dx = c_ccso_pos[cp.ext_filter_support][1];
-                    int q = f.tab.CCSO_QUANT_SZ[cp.scale_idx * 4 + cp.quant_idx];
-                    int a = ty[iclip_(gy + dy, 0, f.h - 1) - gy0 + 2][iclip_(gx + dx, 0, f.w - 1) - gx0 + 2];
-                    int b = ty[iclip_(gy - dy, 0, f.h - 1) - gy0 + 2][iclip_(gx - dx, 0, f.w - 1) - gx0 + 2];
-                    idx = (int)((ccso_score(a - cl, q, cp.edge_clf) << 5) | (ccso_score(b - cl, q, cp.edge_clf) << 3)) | band_;
-                    idx &= 0xff;
-                }
-                bool ll = false;
-                if (f.any_lossless) ll = (m.lossless_mask_y[2 * by_idx + (r >> 2)][sb64x_idx] >> (c >> 2)) & 1;
-                if (!ll) {
-                    int bi = idx >> 1;
-                    int packed = bi < 64 ? cp.filter_off[bi] : 0;
-                    int oi = 7 & (packed >> (4 * (idx & 1)));
-                    v = iclip_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + oi], 0, bdmax);
-                }
+                if (cp.bo_only)
+                    idx = band_ & 0xff;
+                else
+                    idx = ((int)((ccso_score(t[coff] - px, cq, cp.edge_clf) << 5) |
+                                 (ccso_score(t[-coff] - px, cq, cp.edge_clf) << 3)) |
+                           band_) & 0xff;
+                int bi = idx >> 1;
+                int packed = bi < 64 ? cp.filter_off[bi] : 0;
+                v = iclip_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], 0, bdmax);
             }
             out[k] = v;
         }
-        if (gx0 + c0 < f.w) {
-            Cy[gy * ys + gx0 + c0] = (P)out[0];
-            Cy[gy * ys + gx0 + c0 + 1] = (P)out[1];
+        Cy[gy * ys + gx0 + c0] = (P)out[0];
+        Cy[gy * ys + gx0 + c0 + 1] = (P)out[1];
+        // chroma: lane -> plane lane/16, row (lane%16)/4, column lane%4
+        const int pl = lane >> 4, cr = (lane & 15) >> 2, cc = (bx0 >> 1) + (lane & 3);
+        const int cgy = cy0 + cr, cgx = cx0 + cc;
+        P *Cp = plane_ptr<P>(f.C[1 + pl]);
+        int px = tc[pl][2 + cr][2 + cc];
+        int v = px;
+        if (p.active && p.uv_on) {
+            v = cdef_px(&ptc[pl][2 + cr][2 + cc], p.uv_pri, p.uv_sec, p.uvoff, damping - 1, bd8);
+            v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
         }
-    }
-    // chroma: thread -> plane tid/128, row (tid%128)/32, column tid%32
-    {
-        int pl = tid >> 7, r = (tid & 127) >> 5, c = tid & 31;
-        int gy = cy0 + r, gx = cx0 + c;
-        if (gx < f.cw) {
-            P *Cp = plane_ptr<P>(f.C[1 + pl]);
-            int px = tc[pl][2 + r][2 + c];
-            const BlockParams &p = bp[c >> 2];
-            int v = px;
-            if (p.active && p.uv_on) {
-                auto tap = [&](int dy, int dx) -> int {
-                    int yy = gy + dy, xx = gx + dx;
-                    if (yy < 0 || yy >= f.ch || xx < 0 || xx >= f.cw) return INT16_MIN;
-                    return tc[pl][2 + r + dy][2 + c + dx];
-                };
-                v = cdef_px(px, p.uv_pri, p.uv_sec, p.uv_dir, damping - 1, bd8, f.tab, tap);
-                v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
-            }
-            if (s_ccso[1 + pl]) {
-                const R2gCcsoPlane &cp = fp.ccso[1 + pl];
-                int lx = gx << 1, ly = gy << 1;  // co-located luma
-                int cl = ty[ly - gy0 + 2][lx - gx0 + 2];
-                int band_ = (int)((uint32_t)cl >> (bitdepth - cp.max_band_log2));
+        if (s_ccso[1 + pl]) {
+            const R2gCcsoPlane &cpc = fp.ccso[1 + pl];
+            bool ll = f.any_lossless && ((m.lossless_mask_uv[by_idx][sb64x_idx] >> (cc >> 2)) & 1);
+            if (!ll) {
+                // co-located luma of the chroma sample (ccso_prep, 4:2:0)
+                const int16_t *t = &ty[2 + 2 * cr][2 + 2 * cc];
+                int cl = t[0];
+                int band_ = (int)((uint32_t)cl >> (bitdepth - cpc.max_band_log2));
                 int idx;
-                if (cp.bo_only) {
-                    idx = band_;
+                if (cpc.bo_only) {
+                    idx = band_ & 0xff;
                 } else {
-                    int dy = c_ccso_pos[cp.ext_filter_support][0], dx = c_ccso_pos[cp.ext_filter_support][1];
-                    int q = f.tab.CCSO_QUANT_SZ[cp.scale_idx * 4 + cp.quant_idx];
-                    int a = ty[iclip_(ly + dy, 0, f.h - 1) - gy0 + 2][iclip_(lx + dx, 0, f.w - 1) - gx0 + 2];
-                    int b = ty[iclip_(ly - dy, 0, f.h - 1) - gy0 + 2][iclip_(lx - dx, 0, f.w - 1) - gx0 + 2];
-                    idx = (int)((ccso_score(a - cl, q, cp.edge_clf) << 5) | (ccso_score(b - cl, q, cp.edge_clf) << 3)) | band_;
-                    idx &= 0xff;
+                    const int q = f.tab.CCSO_QUANT_SZ[cpc.scale_idx * 4 + cpc.quant_idx];
+                    const int o = c_ccso_pos[cpc.ext_filter_support][0] * TW + c_ccso_pos[cpc.ext_filter_support][1];
+                    idx = ((int)((ccso_score(t[o] - cl, q, cpc.edge_clf) << 5) |
+                                 (ccso_score(t[-o] - cl, q, cpc.edge_clf) << 3)) |
+                           band_) & 0xff;
                 }
-                bool ll = false;
-                if (f.any_lossless) ll = (m.lossless_mask_uv[by_idx][sb64x_idx] >> (c >> 2)) & 1;
-                if (!ll) {
-                    int bi = idx >> 1;
-                    int packed = bi < 64 ? cp.filter_off[bi] : 0;
-                    int oi = 7 & (packed >> (4 * (idx & 1)));
-                    v = iclip_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + oi], 0, bdmax);
-                }
+                int bi = idx >> 1;
+                int packed = bi < 64 ? cpc.filter_off[bi] : 0;
+                v = iclip_(v + f.tab.CCSO_OFFSET[cpc.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], 0, bdmax);
             }
-            Cp[gy * uvs + gx] = (P)v;
         }
+        Cp[cgy * uvs + cgx] = (P)v;
     }
 }
 

@@ -1,19 +1,23 @@
-// AV2 deblocking on the GPU: one launch for all vertical edges of a frame
-// (luma + both chroma planes), then one for all horizontal edges.
+// AV2 deblocking on the GPU, fused and out of place: recon R -> deblocked D.
 //
 // Reference: crates/rav2d/src/deblock.rs (deblock_bd :217, filter_choice_bd
 // :81, deblock64_cols :1623, deblock64_rows :1866, setup_thr_* :1477/:1520)
 // and lf_mask.rs:332-358.  The reference walks the frame per 64-row band,
-// edge by edge; here every 4-line edge segment is one thread.  Transform
-// sizes bound each edge's filter length (MAX_WIDTH_* by edge class), so the
-// pixels one edge reads never overlap the pixels another edge of the same
-// direction writes, and the segments can run in any order in place.
+// all vertical edges of a band, then its horizontal edges.  Transform sizes
+// bound each edge's filter length (MAX_WIDTH_* by edge class), so the samples
+// one edge reads never overlap the samples another edge of the same direction
+// writes: the edges of one direction can run in any order, and the result is
+// "all vertical edges of the frame, then all horizontal edges".
 //
-// Each thread keeps a 4 x 16 window of the edge neighbourhood in registers:
-// line l (0..3) along the edge, position j (0..15) across it, j = 8 is the
-// first sample on the positive side.  Vertical edges load each line as four
-// 4-sample vectors; horizontal edges load each position row as one 4-sample
-// vector covering all four lines.
+// One CTA produces one 64x64 luma tile and its 32x32 chroma tiles.  A luma
+// edge moves samples at most 8 away and reads at most 8 away, so the tile
+// stages R over [-12, 76) in both directions (chroma: width <= 4, reads <= 5,
+// staged over [-8, 40)), applies every vertical edge whose effect can reach a
+// sample the horizontal pass reads, synchronises, applies every horizontal
+// edge that can reach the tile, and writes the tile.  Each edge segment (4
+// lines) is one thread working on a 4 x 16 register window read from shared
+// memory: line l along the edge, position j across it, j = 8 the first sample
+// on the positive side.
 #include "r2g_common.cuh"
 
 namespace {
@@ -73,11 +77,11 @@ R2G_D int edge_thr(int cur, int prev) { return (cur != 0 && prev != 0) ? (cur + 
 
 R2G_D uint32_t uabs_(int v) { return (uint32_t)(v < 0 ? -v : v); }
 
-// filter_choice_bd (deblock.rs:81-210) on window lines ls and lt; position
-// p(k) = win[line][8 + k].
-R2G_D int filter_choice(const int (*win)[16], int ls, int lt, int mwn, int mwp, uint32_t q_thr, uint32_t side_thr) {
-#define S(k) win[ls][8 + (k)]
-#define T(k) win[lt][8 + (k)]
+// filter_choice_bd (deblock.rs:81-210) on window lines 0 and 3; position
+// p(k) = win[line][8 + k].  Every index is a compile-time constant.
+R2G_D int filter_choice(const int *ws, const int *wt, int mwn, int mwp, uint32_t q_thr, uint32_t side_thr) {
+#define S(k) ws[8 + (k)]
+#define T(k) wt[8 + (k)]
     uint32_t sd[4];
 #pragma unroll
     for (int d = -2; d < 2; d++) {
@@ -107,11 +111,14 @@ R2G_D int filter_choice(const int (*win)[16], int ls, int lt, int mwn, int mwp, 
     if (mwp == 3) return 3;
     transition <<= 4;
     int prev = 3;
-    for (int dist = 4; dist <= mwp; dist += 2) {
-        uint32_t q4 = q_thr * (uint32_t)c_q_first[(dist - 4) >> 1];
+#pragma unroll
+    for (int di = 0; di < 3; di++) {
+        const int dist = 4 + 2 * di;
+        if (dist > mwp) break;
+        const int d2 = dist < 7 ? dist : 7;
+        uint32_t q4 = q_thr * (uint32_t)c_q_first[di];
         uint32_t e4 = (side_thr * (uint32_t)dist) >> 4;
         if (transition > q4) return prev;
-        int d2 = imin_(7, dist);
         if (mwn >= d2) {
             uint32_t ds = uabs_(S(-1) - S(-d2 - 1) - d2 * (S(-1) - S(-2)));
             uint32_t dt = uabs_(T(-1) - T(-d2 - 1) - d2 * (T(-1) - T(-2)));
@@ -127,37 +134,85 @@ R2G_D int filter_choice(const int (*win)[16], int ls, int lt, int mwn, int mwp, 
 #undef T
 }
 
-// deblock_bd (deblock.rs:217-281) on the register window.  Returns the
-// number of modified samples on each side through wn / wp.
-R2G_D void deblock_window(int (*win)[16], uint32_t q_thr, uint32_t side_thr, int mwp, int mwn, bool pos_ll,
-                          bool neg_ll, int bdmax, int &wn_out, int &wp_out) {
-    wn_out = wp_out = 0;
-    int width = filter_choice(win, 0, 3, mwn, mwp, q_thr, side_thr);
+// deblock_bd (deblock.rs:217-281) on a shared-memory edge: `e` points at the
+// first positive-side sample of line 0; `along` steps between the 4 lines,
+// `across` steps across the edge.
+R2G_D void filter_edge(int16_t *e, int along, int across, uint32_t q_thr, uint32_t side_thr, int mwp, int mwn,
+                       bool pos_ll, bool neg_ll, int bdmax) {
+    int width;
+    {
+        int w0[16], w3[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            w0[j] = e[(j - 8) * across];
+            w3[j] = e[3 * along + (j - 8) * across];
+        }
+        width = filter_choice(w0, w3, mwn, mwp, q_thr, side_thr);
+    }
     if (width < 1) return;
     int wn = imin_(width, mwn), wp = width;
     int clampv = (int)q_thr * c_q_thresh_mults[width - 1];
     int mneg = c_w_mult[wn - 1], mpos = c_w_mult[wp - 1];
-#pragma unroll
+    // lines are independent once the width is chosen: one at a time keeps
+    // only 16 samples live
+#pragma unroll 1
     for (int l = 0; l < 4; l++) {
-        int *L = win[l];
+        int16_t *ln = e + l * along;
+        int L[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) L[j] = ln[(j - 8) * across];
         int delta = iclip_(4 * (3 * (L[8] - L[7]) - (L[9] - L[6])), -clampv, clampv);
-        if (!neg_ll) {
-            int dn = delta * mneg;
-            for (int j = 0; j < wn; j++) {
+        int dn = delta * mneg, dp = delta * mpos;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (!neg_ll && j < wn) {
                 int diff = (dn * (wn - j) + (1 << 10)) >> 11;
-                L[7 - j] = iclip_(L[7 - j] + diff, 0, bdmax);
+                ln[(-j - 1) * across] = (int16_t)iclip_(L[7 - j] + diff, 0, bdmax);
             }
-        }
-        if (!pos_ll) {
-            int dp = delta * mpos;
-            for (int j = 0; j < wp; j++) {
+            if (!pos_ll && j < wp) {
                 int diff = (dp * (wp - j) + (1 << 10)) >> 11;
-                L[8 + j] = iclip_(L[8 + j] - diff, 0, bdmax);
+                ln[j * across] = (int16_t)iclip_(L[8 + j] - diff, 0, bdmax);
             }
         }
     }
-    wn_out = neg_ll ? 0 : wn;
-    wp_out = pos_ll ? 0 : wp;
+}
+
+R2G_D bool ll_y(const R2gAv2Filter &m, int x4, int y4) {
+    return (m.lossless_mask_y[y4 & 63][(x4 >> 4) & 3] >> (x4 & 15)) & 1;
+}
+R2G_D bool ll_uv(const R2gAv2Filter &m, int cx4, int cy4) {
+    return (m.lossless_mask_uv[cy4 & 31][(cx4 >> 3) & 3] >> (cx4 & 7)) & 1;
+}
+R2G_D int seg_y(const DevFrame &f, int x4, int y4) {
+    return f.segmap ? f.segmap[(int64_t)y4 * f.segmap_stride + x4] : 0;
+}
+R2G_D int seg_uv(const DevFrame &f, int cx4, int cy4) {
+    return f.segmap_uv ? f.segmap_uv[(int64_t)cy4 * f.segmap_uv_stride + cx4] : 0;
+}
+
+// Edge-threshold pair for a 4x4 and its neighbour (setup_thr_* :1477/:1520):
+// the neighbour is the 4x4 to the left (vertical edge) or above.
+R2G_D void luma_thr(const DevFrame &f, int dir, int x4, int y4, int nx4, int ny4, bool subpu, uint32_t &q,
+                    uint32_t &s) {
+    const R2gAv2Filter &mc = f.masks[(y4 >> 6) * f.sb256w + (x4 >> 6)];
+    const R2gAv2Filter &mn = f.masks[(ny4 >> 6) * f.sb256w + (nx4 >> 6)];
+    int cq, cs, pq, ps;
+    thr_of(f, dir, mc.qidx[((x4 >> 4) & 3) + (((y4 >> 4) & 3) << 2)], seg_y(f, x4, y4), cq, cs);
+    thr_of(f, dir, mn.qidx[((nx4 >> 4) & 3) + (((ny4 >> 4) & 3) << 2)], seg_y(f, nx4, ny4), pq, ps);
+    int sh = subpu ? 3 : 0;
+    q = (uint32_t)(uint16_t)(edge_thr(cq, pq) >> sh);
+    s = (uint32_t)(uint16_t)(edge_thr(cs, ps) >> sh);
+}
+R2G_D void chroma_thr(const DevFrame &f, int pl, int cx4, int cy4, int nx4, int ny4, bool subpu, uint32_t &q,
+                      uint32_t &s) {
+    const R2gAv2Filter &mc = f.masks[(cy4 >> 5) * f.sb256w + (cx4 >> 5)];
+    const R2gAv2Filter &mn = f.masks[(ny4 >> 5) * f.sb256w + (nx4 >> 5)];
+    int cq, cs, pq, ps;
+    thr_of(f, 2 + pl, mc.qidx[((cx4 >> 3) & 3) + (((cy4 >> 3) & 3) << 2)], seg_uv(f, cx4, cy4), cq, cs);
+    thr_of(f, 2 + pl, mn.qidx[((nx4 >> 3) & 3) + (((ny4 >> 3) & 3) << 2)], seg_uv(f, nx4, ny4), pq, ps);
+    int sh = subpu ? 3 : 0;
+    q = (uint32_t)(uint16_t)(edge_thr(cq, pq) >> sh);
+    s = (uint32_t)(uint16_t)(edge_thr(cs, ps) >> sh);
 }
 
 template <typename P>
@@ -189,180 +244,189 @@ struct Vec4<uint16_t> {
     }
 };
 
-R2G_D bool ll_y(const R2gAv2Filter &m, int x4, int y4) {
-    return (m.lossless_mask_y[y4 & 63][(x4 >> 4) & 3] >> (x4 & 15)) & 1;
-}
-R2G_D bool ll_uv(const R2gAv2Filter &m, int cx4, int cy4) {
-    return (m.lossless_mask_uv[cy4 & 31][(cx4 >> 3) & 3] >> (cx4 & 7)) & 1;
-}
+// Shared-memory tile geometry.
+constexpr int LT = 88;   // luma staged span: tile origin - 12 .. + 76
+constexpr int LO = 12;   // luma halo
+constexpr int LP = 90;   // luma row pitch (int16)
+constexpr int CT = 48;   // chroma staged span: origin - 8 .. + 40
+constexpr int CO = 8;    // chroma halo
+constexpr int CP = 50;   // chroma row pitch
 
-R2G_D int seg_y(const DevFrame &f, int x4, int y4) {
-    return f.segmap ? f.segmap[(int64_t)y4 * f.segmap_stride + x4] : 0;
-}
-R2G_D int seg_uv(const DevFrame &f, int cx4, int cy4) {
-    return f.segmap_uv ? f.segmap_uv[(int64_t)cy4 * f.segmap_uv_stride + cx4] : 0;
-}
+struct DeblockSmem {
+    int16_t y[LT * LP];
+    int16_t uv[2][CT * CP];
+};
 
-// Edge-threshold pair for a luma 4x4 and its neighbour (setup_thr_* :1477).
-R2G_D void luma_thr(const DevFrame &f, int dir, int x4, int y4, int nx4, int ny4, bool subpu, uint32_t &q,
-                    uint32_t &s) {
-    const R2gAv2Filter &mc = f.masks[(y4 >> 6) * f.sb256w + (x4 >> 6)];
+// One luma edge segment.  dir 0: vertical edge at column x, rows y..y+3;
+// dir 1: horizontal edge at row y, columns x..x+3.  (x, y) are frame
+// coordinates; `sy`/`sx` the tile origin of the staged span.
+R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, int sx, int sy) {
+    const int x4 = x >> 2, y4 = y >> 2;
+    if (x4 >= f.bw4 || y4 >= f.bh4 || x < 0 || y < 0) return;
+    if ((dir == 0 ? x4 : y4) == 0) return;
+    const R2gAv2Filter &m = f.masks[(y4 >> 6) * f.sb256w + (x4 >> 6)];
+    const int pos = dir == 0 ? (x4 & 63) : (y4 & 63);
+    const int idx = dir == 0 ? ((y4 >> 4) & 3) : ((x4 >> 4) & 3);
+    const int bit = dir == 0 ? (y4 & 15) : (x4 & 15);
+    const uint16_t(*km)[4] = m.filter_y[dir][pos];
+    int k3 = (km[3][idx] >> bit) & 1, k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1,
+        k0 = (km[0][idx] >> bit) & 1;
+    if (!(k0 | k1 | k2 | k3)) return;
+    int cls = k3 ? 3 : k2 ? 2 : k1;
+    int mwp = c_max_width_y[cls];
+    int mwn = (dir == 1 && (y4 & 15) == 0) ? imin_(6, mwp) : mwp;
+    bool subpu = (km[4][idx] >> bit) & 1;
+    int nx4 = dir == 0 ? x4 - 1 : x4, ny4 = dir == 0 ? y4 : y4 - 1;
+    uint32_t q, s;
+    luma_thr(f, dir, x4, y4, nx4, ny4, subpu, q, s);
     const R2gAv2Filter &mn = f.masks[(ny4 >> 6) * f.sb256w + (nx4 >> 6)];
-    int cq, cs, pq, ps;
-    thr_of(f, dir, mc.qidx[((x4 >> 4) & 3) + (((y4 >> 4) & 3) << 2)], seg_y(f, x4, y4), cq, cs);
-    thr_of(f, dir, mn.qidx[((nx4 >> 4) & 3) + (((ny4 >> 4) & 3) << 2)], seg_y(f, nx4, ny4), pq, ps);
-    int sh = subpu ? 3 : 0;
-    q = (uint32_t)(uint16_t)(edge_thr(cq, pq) >> sh);
-    s = (uint32_t)(uint16_t)(edge_thr(cs, ps) >> sh);
-}
-R2G_D void chroma_thr(const DevFrame &f, int pl, int cx4, int cy4, int nx4, int ny4, bool subpu, uint32_t &q,
-                      uint32_t &s) {
-    const R2gAv2Filter &mc = f.masks[(cy4 >> 5) * f.sb256w + (cx4 >> 5)];
-    const R2gAv2Filter &mn = f.masks[(ny4 >> 5) * f.sb256w + (nx4 >> 5)];
-    int cq, cs, pq, ps;
-    thr_of(f, 2 + pl, mc.qidx[((cx4 >> 3) & 3) + (((cy4 >> 3) & 3) << 2)], seg_uv(f, cx4, cy4), cq, cs);
-    thr_of(f, 2 + pl, mn.qidx[((nx4 >> 3) & 3) + (((ny4 >> 3) & 3) << 2)], seg_uv(f, nx4, ny4), pq, ps);
-    int sh = subpu ? 3 : 0;
-    q = (uint32_t)(uint16_t)(edge_thr(cq, pq) >> sh);
-    s = (uint32_t)(uint16_t)(edge_thr(cs, ps) >> sh);
+    bool pos_ll = ll_y(m, x4, y4), neg_ll = ll_y(mn, nx4, ny4);
+    int16_t *e = &sm.y[(y - sy) * LP + (x - sx)];
+    if (dir == 0)
+        filter_edge(e, LP, 1, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+    else
+        filter_edge(e, 1, LP, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
 }
 
-// Vertical edge at sample column x (x % 4 == 0), rows y..y+3.
-// Window samples outside the plane (pw x ph) read as 0; the edge classes of
-// a valid stream never let the filter use them.
-template <typename P>
-R2G_D void vert_edge(P *plane, int64_t stride, int pw, int x, int y, uint32_t q, uint32_t s, int mwp, int mwn,
-                     bool pos_ll, bool neg_ll, int bdmax) {
-    typedef Vec4<P> V;
-    int win[4][16];
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-        const P *row = plane + (int64_t)(y + l) * stride;
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            int x0 = x - 8 + 4 * c;
-            if (x0 >= 0 && x0 + 3 < pw)
-                V::unpack(*reinterpret_cast<const typename V::T *>(row + x0), &win[l][4 * c]);
-            else
-                win[l][4 * c] = win[l][4 * c + 1] = win[l][4 * c + 2] = win[l][4 * c + 3] = 0;
-        }
-    }
-    int wn, wp;
-    deblock_window(win, q, s, mwp, mwn, pos_ll, neg_ll, bdmax, wn, wp);
-    if (wn == 0 && wp == 0) return;
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-        P *row = plane + (int64_t)(y + l) * stride;
-        for (int j = 8 - wn; j < 8 + wp; j++) row[x - 8 + j] = (P)win[l][j];
-    }
-}
-
-// Horizontal edge at sample row y (y % 4 == 0), columns x..x+3.
-template <typename P>
-R2G_D void horz_edge(P *plane, int64_t stride, int ph, int x, int y, uint32_t q, uint32_t s, int mwp, int mwn,
-                     bool pos_ll, bool neg_ll, int bdmax) {
-    typedef Vec4<P> V;
-    int win[4][16];
-#pragma unroll
-    for (int j = 0; j < 16; j++) {
-        int yy = y - 8 + j;
-        int v[4] = {0, 0, 0, 0};
-        if (yy >= 0 && yy < ph) V::unpack(*reinterpret_cast<const typename V::T *>(plane + (int64_t)yy * stride + x), v);
-#pragma unroll
-        for (int l = 0; l < 4; l++) win[l][j] = v[l];
-    }
-    int wn, wp;
-    deblock_window(win, q, s, mwp, mwn, pos_ll, neg_ll, bdmax, wn, wp);
-    for (int j = 8 - wn; j < 8 + wp; j++) {
-        int v[4] = {win[0][j], win[1][j], win[2][j], win[3][j]};
-        *reinterpret_cast<typename V::T *>(plane + (int64_t)(y - 8 + j) * stride + x) = V::pack(v);
-    }
-}
-
-// One launch per direction; items [0, nl) are luma 4x4s, [nl, nl + nc)
-// chroma 4x4s (U and V share mask decode and run in the same thread).
-template <typename P, int DIR>
-__global__ void __launch_bounds__(256) deblock_kernel(const DevFrame f) {
-    const int nl = f.bw4 * f.bh4;
-    const int cbw4 = f.bw4 >> 1, cbh4 = f.bh4 >> 1;
-    const int nc = cbw4 * cbh4;
+// One chroma edge segment, both planes (U and V share masks and widths).
+R2G_D void chroma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int cx, int cy, int sx, int sy) {
     const R2gFrameParams &fp = f.fp;
-    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < nl + nc; it += gridDim.x * blockDim.x) {
-        if (it < nl) {
-            if (!fp.deblock_level_y[DIR]) continue;
-            int x4 = it % f.bw4, y4 = it / f.bw4;
-            if ((DIR == 0 ? x4 : y4) == 0) continue;
-            const R2gAv2Filter &m = f.masks[(y4 >> 6) * f.sb256w + (x4 >> 6)];
-            int pos = DIR == 0 ? (x4 & 63) : (y4 & 63);
-            int idx = DIR == 0 ? ((y4 >> 4) & 3) : ((x4 >> 4) & 3);
-            int bit = DIR == 0 ? (y4 & 15) : (x4 & 15);
-            const uint16_t(*km)[4] = m.filter_y[DIR][pos];
-            int k3 = (km[3][idx] >> bit) & 1, k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1,
-                k0 = (km[0][idx] >> bit) & 1;
-            if (!(k0 | k1 | k2 | k3)) continue;
-            int cls = k3 ? 3 : k2 ? 2 : k1;
-            int mwp = c_max_width_y[cls];
-            int mwn = (DIR == 1 && (y4 & 15) == 0) ? imin_(6, mwp) : mwp;
-            bool subpu = (km[4][idx] >> bit) & 1;
-            int nx4 = DIR == 0 ? x4 - 1 : x4, ny4 = DIR == 0 ? y4 : y4 - 1;
-            uint32_t q, s;
-            luma_thr(f, DIR, x4, y4, nx4, ny4, subpu, q, s);
-            const R2gAv2Filter &mn = f.masks[(ny4 >> 6) * f.sb256w + (nx4 >> 6)];
-            bool pos_ll = ll_y(m, x4, y4), neg_ll = ll_y(mn, nx4, ny4);
-            P *pl = plane_ptr<P>(f.R[0]);
-            if (DIR == 0)
-                vert_edge<P>(pl, f.stride[0], f.w, x4 * 4, y4 * 4, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+    const int cx4 = cx >> 2, cy4 = cy >> 2;
+    const int cbw4 = f.bw4 >> 1, cbh4 = f.bh4 >> 1;
+    if (cx4 >= cbw4 || cy4 >= cbh4 || cx < 0 || cy < 0) return;
+    if ((dir == 0 ? cx4 : cy4) == 0) return;
+    const R2gAv2Filter &m = f.masks[(cy4 >> 5) * f.sb256w + (cx4 >> 5)];
+    const int pos = dir == 0 ? (cx4 & 31) : (cy4 & 31);
+    const int idx = dir == 0 ? ((cy4 & 31) >> 4) : ((cx4 & 31) >> 4);
+    const int bit = dir == 0 ? (cy4 & 15) : (cx4 & 15);
+    const uint16_t(*km)[4] = m.filter_uv[dir][pos];
+    int k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1, k0 = (km[0][idx] >> bit) & 1;
+    if (!(k0 | k1 | k2)) return;
+    int cls = k2 ? 2 : k1;
+    int mwp = c_max_width_uv[cls];
+    int mwn = (dir == 1 && (cy4 & 7) == 0) ? imin_(2, mwp) : mwp;
+    bool subpu = (km[4][idx] >> bit) & 1;
+    int nx4 = dir == 0 ? cx4 - 1 : cx4, ny4 = dir == 0 ? cy4 : cy4 - 1;
+    const R2gAv2Filter &mn = f.masks[(ny4 >> 5) * f.sb256w + (nx4 >> 5)];
+    bool pos_ll = ll_uv(m, cx4, cy4), neg_ll = ll_uv(mn, nx4, ny4);
+    for (int pl = 0; pl < 2; pl++) {
+        if (!(pl ? fp.deblock_level_v : fp.deblock_level_u)) continue;
+        uint32_t q, s;
+        chroma_thr(f, pl, cx4, cy4, nx4, ny4, subpu, q, s);
+        int16_t *e = &sm.uv[pl][(cy - sy) * CP + (cx - sx)];
+        if (dir == 0)
+            filter_edge(e, CP, 1, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+        else
+            filter_edge(e, 1, CP, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+    }
+}
+
+// The deblock work of one tile (tx, ty); callable from the per-frame kernel
+// and from the batched persistent kernel.
+template <typename P>
+R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
+    const R2gFrameParams &fp = f.fp;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int x0 = tx * 64, y0 = ty * 64, cx0 = x0 >> 1, cy0 = y0 >> 1;
+    const int lsx = x0 - LO, lsy = y0 - LO, csx = cx0 - CO, csy = cy0 - CO;
+    const P *Ry = plane_ptr<const P>(f.R[0]);
+    const int64_t ys = f.stride[0], uvs = f.stride[1];
+    // ---- stage R (samples outside the frame read 0; no valid edge uses them)
+    for (int i = tid; i < LT * (LT / 4); i += nt) {
+        int r = i / (LT / 4), c4 = (i % (LT / 4)) * 4;
+        int gy = lsy + r, gx = lsx + c4;
+        int v[4] = {0, 0, 0, 0};
+        if (gy >= 0 && gy < f.h) {
+            if (gx >= 0 && gx + 3 < f.w)
+                Vec4<P>::unpack(*reinterpret_cast<const typename Vec4<P>::T *>(Ry + gy * ys + gx), v);
             else
-                horz_edge<P>(pl, f.stride[0], f.h, x4 * 4, y4 * 4, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
-        } else {
-            if (!fp.deblock_level_u && !fp.deblock_level_v) continue;
-            int c = it - nl;
-            int cx4 = c % cbw4, cy4 = c / cbw4;
-            if ((DIR == 0 ? cx4 : cy4) == 0) continue;
-            const R2gAv2Filter &m = f.masks[(cy4 >> 5) * f.sb256w + (cx4 >> 5)];
-            int pos = DIR == 0 ? (cx4 & 31) : (cy4 & 31);
-            int idx = DIR == 0 ? ((cy4 & 31) >> 4) : ((cx4 & 31) >> 4);
-            int bit = DIR == 0 ? (cy4 & 15) : (cx4 & 15);
-            const uint16_t(*km)[4] = m.filter_uv[DIR][pos];
-            int k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1, k0 = (km[0][idx] >> bit) & 1;
-            if (!(k0 | k1 | k2)) continue;
-            int cls = k2 ? 2 : k1;
-            int mwp = c_max_width_uv[cls];
-            int mwn = (DIR == 1 && (cy4 & 7) == 0) ? imin_(2, mwp) : mwp;
-            bool subpu = (km[4][idx] >> bit) & 1;
-            int nx4 = DIR == 0 ? cx4 - 1 : cx4, ny4 = DIR == 0 ? cy4 : cy4 - 1;
-            const R2gAv2Filter &mn = f.masks[(ny4 >> 5) * f.sb256w + (nx4 >> 5)];
-            bool pos_ll = ll_uv(m, cx4, cy4), neg_ll = ll_uv(mn, nx4, ny4);
-            for (int pl = 0; pl < 2; pl++) {
-                if (!(pl ? fp.deblock_level_v : fp.deblock_level_u)) continue;
-                uint32_t q, s;
-                chroma_thr(f, pl, cx4, cy4, nx4, ny4, subpu, q, s);
-                P *plane = plane_ptr<P>(f.R[1 + pl]);
-                if (DIR == 0)
-                    vert_edge<P>(plane, f.stride[1], f.cw, cx4 * 4, cy4 * 4, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
-                else
-                    horz_edge<P>(plane, f.stride[1], f.ch, cx4 * 4, cy4 * 4, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+                for (int k = 0; k < 4; k++)
+                    if (gx + k >= 0 && gx + k < f.w) v[k] = Ry[gy * ys + gx + k];
+        }
+        for (int k = 0; k < 4; k++) sm.y[r * LP + c4 + k] = (int16_t)v[k];
+    }
+    for (int i = tid; i < 2 * CT * (CT / 4); i += nt) {
+        int pl = i / (CT * (CT / 4)), j = i % (CT * (CT / 4));
+        int r = j / (CT / 4), c4 = (j % (CT / 4)) * 4;
+        int gy = csy + r, gx = csx + c4;
+        const P *Rc = plane_ptr<const P>(f.R[1 + pl]);
+        int v[4] = {0, 0, 0, 0};
+        if (gy >= 0 && gy < f.ch) {
+            if (gx >= 0 && gx + 3 < f.cw)
+                Vec4<P>::unpack(*reinterpret_cast<const typename Vec4<P>::T *>(Rc + gy * uvs + gx), v);
+            else
+                for (int k = 0; k < 4; k++)
+                    if (gx + k >= 0 && gx + k < f.cw) v[k] = Rc[gy * uvs + gx + k];
+        }
+        for (int k = 0; k < 4; k++) sm.uv[pl][r * CP + c4 + k] = (int16_t)v[k];
+    }
+    __syncthreads();
+    const bool do_y_v = fp.deblock_level_y[0] != 0, do_y_h = fp.deblock_level_y[1] != 0;
+    const bool do_uv = fp.deblock_level_u || fp.deblock_level_v;
+    // ---- vertical edges: luma columns x0-4 .. x0+68 on rows y0-12 .. y0+75,
+    // chroma columns cx0 .. cx0+32 on rows cy0-8 .. cy0+39
+    {
+        const int nlv = do_y_v ? 19 * 22 : 0, ncv = do_uv ? 9 * 12 : 0;
+        for (int i = tid; i < nlv + ncv; i += nt) {
+            if (i < nlv)
+                luma_edge(f, sm, 0, x0 - 4 + 4 * (i % 19), lsy + 4 * (i / 19), lsx, lsy);
+            else {
+                int j = i - nlv;
+                chroma_edge(f, sm, 0, cx0 + 4 * (j % 9), csy + 4 * (j / 9), csx, csy);
             }
         }
     }
+    __syncthreads();
+    // ---- horizontal edges: luma rows y0-4 .. y0+68 on columns x0 .. x0+63,
+    // chroma rows cy0 .. cy0+32 on columns cx0 .. cx0+31
+    {
+        const int nlh = do_y_h ? 19 * 16 : 0, nch = do_uv ? 9 * 8 : 0;
+        for (int i = tid; i < nlh + nch; i += nt) {
+            if (i < nlh)
+                luma_edge(f, sm, 1, x0 + 4 * (i % 16), y0 - 4 + 4 * (i / 16), lsx, lsy);
+            else {
+                int j = i - nlh;
+                chroma_edge(f, sm, 1, cx0 + 4 * (j % 8), cy0 + 4 * (j / 8), csx, csy);
+            }
+        }
+    }
+    __syncthreads();
+    // ---- write the tile
+    P *Dy = plane_ptr<P>(f.D[0]);
+    for (int i = tid; i < 64 * 16; i += nt) {
+        int r = i >> 4, c4 = (i & 15) * 4;
+        int gy = y0 + r, gx = x0 + c4;
+        if (gy >= f.h || gx >= f.w) continue;
+        const int16_t *src = &sm.y[(r + LO) * LP + c4 + LO];
+        int v[4] = {src[0], src[1], src[2], src[3]};
+        *reinterpret_cast<typename Vec4<P>::T *>(Dy + gy * ys + gx) = Vec4<P>::pack(v);
+    }
+    for (int i = tid; i < 2 * 32 * 8; i += nt) {
+        int pl = i >> 8, j = i & 255;
+        int r = j >> 3, c4 = (j & 7) * 4;
+        int gy = cy0 + r, gx = cx0 + c4;
+        if (gy >= f.ch || gx >= f.cw) continue;
+        P *Dc = plane_ptr<P>(f.D[1 + pl]);
+        const int16_t *src = &sm.uv[pl][(r + CO) * CP + c4 + CO];
+        int v[4] = {src[0], src[1], src[2], src[3]};
+        *reinterpret_cast<typename Vec4<P>::T *>(Dc + gy * uvs + gx) = Vec4<P>::pack(v);
+    }
+}
+
+template <typename P>
+__global__ void __launch_bounds__(256, 4) deblock_tile_kernel(const DevFrame f) {
+    __shared__ DeblockSmem sm;
+    deblock_tile<P>(f, sm, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace
 
-int r2g_launch_deblock_dir(const DevFrame &f, int dir, cudaStream_t s) {
+int r2g_launch_deblock(const DevFrame &f, cudaStream_t s) {
     if (!f.deblock_on) return 0;
-    int items = f.bw4 * f.bh4 + (f.bw4 >> 1) * (f.bh4 >> 1);
-    int blocks = (items + 255) / 256;
-    if (f.bitdepth > 8) {
-        if (dir == 0)
-            deblock_kernel<uint16_t, 0><<<blocks, 256, 0, s>>>(f);
-        else
-            deblock_kernel<uint16_t, 1><<<blocks, 256, 0, s>>>(f);
-    } else {
-        if (dir == 0)
-            deblock_kernel<uint8_t, 0><<<blocks, 256, 0, s>>>(f);
-        else
-            deblock_kernel<uint8_t, 1><<<blocks, 256, 0, s>>>(f);
-    }
+    dim3 grid((f.w + 63) / 64, (f.h + 63) / 64);
+    if (f.bitdepth > 8)
+        deblock_tile_kernel<uint16_t><<<grid, 256, 0, s>>>(f);
+    else
+        deblock_tile_kernel<uint8_t><<<grid, 256, 0, s>>>(f);
     return 1;
 }

@@ -399,7 +399,7 @@ int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uin
     grain_planes(*fgd, gp.has_y, gp.has_u, gp.has_v, any);
     DevFrame d = f->desc;
     void *p[3];
-    char *base = (char *)f->buf[3];
+    char *base = (char *)f->buf[4];
     p[0] = base;
     p[1] = base + f->plane_bytes[0];
     p[2] = base + f->plane_bytes[0] + f->plane_bytes[1];
@@ -416,16 +416,16 @@ int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uin
     }
     int bs = 16 << fgd->block_size;
     dim3 grid((f->w + bs - 1) / bs, (f->h + bs - 1) / bs);
-    r2g_prof_stage(ctx, 4, true, 0);
+    r2g_prof_stage(ctx, 3, true, 0);
     if (f->bd > 8)
         grain_apply_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
     else
         grain_apply_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
-    r2g_prof_stage(ctx, 4, false, 1 + (any ? 1 : 0));
+    r2g_prof_stage(ctx, 3, false, 1 + (any ? 1 : 0));
     if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
     if (cudaEventRecord(ctx->grain->freed, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
     ctx->grain->used = true;
-    f->grain_buf = 3;
+    f->grain_buf = 4;
     return R2G_OK;
 }
 

@@ -30,15 +30,6 @@ constexpr int CWH = 36;  // chroma window height: -2 .. 33 (stripe <= 32 rows)
 __constant__ uint16_t c_pcw_norm[4] = {3739, 3273, 3074, 7};
 __constant__ int16_t c_mode_weights[4][3] = {{-527, 15325, 321}, {26436, -17705, 17905}, {366, -147, -194}, {202, -267, -179}};
 __constant__ int16_t c_mode_offsets[4] = {-547, -21565, -573, -680};
-__constant__ int8_t c_gdf_coords[18][2] = {{6, 0}, {5, 0}, {4, 0}, {3, 0}, {2, 1}, {2, 0}, {2, -1}, {1, 2}, {1, 1},
-                                           {1, 0}, {1, -1}, {1, -2}, {0, 6}, {0, 5}, {0, 4}, {0, 3}, {0, 2}, {0, 1}};
-__constant__ int8_t c_cfg_uv[6][2] = {{1, 0}, {0, 1}, {1, 1}, {-1, 1}, {2, 0}, {0, 2}};
-__constant__ int8_t c_cfg_uv_from_y[12][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1},
-                                              {-1, 1}, {1, -1}, {2, 0}, {-2, 0}, {0, 2}, {0, -2}};
-__constant__ int8_t c_cfg_pc[12][2] = {{1, 0}, {0, 1}, {2, 0}, {0, 2}, {1, 1}, {-1, 1},
-                                       {2, 1}, {2, -1}, {1, 2}, {1, -2}, {3, 0}, {0, 3}};
-__constant__ int8_t c_cfg_y[16][2] = {{1, 0}, {0, 1}, {2, 0}, {0, 2}, {1, 1}, {-1, 1}, {2, 1}, {2, -1},
-                                      {1, 2}, {1, -2}, {3, 0}, {0, 3}, {4, 0}, {0, 4}, {3, 3}, {3, -3}};
 
 enum { W_NONE = 0, W_NS_SINGLE = 1, W_NS_MULTI = 2, W_PC = 3 };
 
@@ -138,19 +129,37 @@ R2G_D int col_src(const UnitGeom &g, int c) {
     return g.x0 + c;
 }
 
+// Compile-time tap tables (the reference's WIENER_NS_CONFIG_Y :389,
+// PC_WIENER_CONFIG :374, GDF_COORDS :334, WIENER_NS_CONFIG_UV[_FROM_Y]
+// :357/:359): with the loops unrolled every window offset is an immediate.
+namespace TapsY {
+__device__ constexpr int8_t ns[16][2] = {{1, 0}, {0, 1}, {2, 0}, {0, 2}, {1, 1}, {-1, 1}, {2, 1}, {2, -1},
+                                         {1, 2}, {1, -2}, {3, 0}, {0, 3}, {4, 0}, {0, 4}, {3, 3}, {3, -3}};
+__device__ constexpr int8_t pc[12][2] = {{1, 0}, {0, 1}, {2, 0}, {0, 2}, {1, 1}, {-1, 1},
+                                         {2, 1}, {2, -1}, {1, 2}, {1, -2}, {3, 0}, {0, 3}};
+__device__ constexpr int8_t gdf[18][2] = {{6, 0}, {5, 0}, {4, 0}, {3, 0}, {2, 1}, {2, 0}, {2, -1}, {1, 2}, {1, 1},
+                                          {1, 0}, {1, -1}, {1, -2}, {0, 6}, {0, 5}, {0, 4}, {0, 3}, {0, 2}, {0, 1}};
+__device__ constexpr int8_t uv[6][2] = {{1, 0}, {0, 1}, {1, 1}, {-1, 1}, {2, 0}, {0, 2}};
+__device__ constexpr int8_t uvy[12][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1},
+                                          {-1, 1}, {1, -1}, {2, 0}, {-2, 0}, {0, 2}, {0, -2}};
+}  // namespace TapsY
+
+struct LrSmem {
+    int16_t win[LH * LW];      // luma window, or chroma window (pitch CWW)
+    int16_t lwin[CWH * CWW];   // chroma: downsampled luma window
+    uint16_t gcell[33 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
+    int8_t gerr[64 * 64];
+    int8_t s_err[4096];
+    short4 s_par[4][22];       // per class: alpha, 3 weights of each GDF feature
+    uint8_t classes[16][16];
+    uint16_t noskip[18];
+    uint16_t llm[17];
+};
+
 template <typename P>
 __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_units, int nux_l, int nux_c) {
-    __shared__ int16_t win[LH * LW];  // luma window, or chroma window
-    __shared__ int16_t lwin[CWH * CWW];  // chroma: downsampled luma window
-    __shared__ int8_t gerr[64 * 64];
-    __shared__ uint8_t classes[16][16];
-    __shared__ uint16_t noskip[18];
-    __shared__ uint16_t llm[17];
-    __shared__ uint16_t s_alpha[88];
-    __shared__ int16_t s_weight[3 * 88];
-    __shared__ int8_t s_err[4096];
-
-    const int tid = threadIdx.x;
+    __shared__ LrSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int b = blockIdx.x;
     int plane, sby, sub, ux;
     if (b < n_luma_units) {
@@ -173,7 +182,7 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
     const int chroma = plane != 0;
     const int64_t stride = f.stride[chroma];
     const P *Cp = plane_ptr<const P>(f.C[plane]);
-    const P *Dp = plane_ptr<const P>(f.R[plane]);
+    const P *Dp = plane_ptr<const P>(f.D[plane]);
     P *Lp = plane_ptr<P>(f.L[plane]);
     const R2gFrameParams &fp = f.fp;
     const int bitdepth = f.bitdepth, bdmax = f.bdmax;
@@ -196,10 +205,9 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
                         f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
 
     if (wkind == W_NONE && !gdf_on) {
-        for (int i = tid; i < g.sh * g.uw; i += 256) {
-            int r = i / g.uw, c = i % g.uw;
-            Lp[(int64_t)(g.y0 + r) * stride + g.x0 + c] = Cp[(int64_t)(g.y0 + r) * stride + g.x0 + c];
-        }
+        for (int r = warp; r < g.sh; r += 8)
+            for (int c = lane; c < g.uw; c += 32)
+                Lp[(int64_t)(g.y0 + r) * stride + g.x0 + c] = Cp[(int64_t)(g.y0 + r) * stride + g.x0 + c];
         return;
     }
 
@@ -226,7 +234,7 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
                 }
             }
         }
-        llm[tid] = v;
+        sm.llm[tid] = v;
     }
     // ---- multi-class noskip rows (looprestoration.rs:1922-1944) ----
     if ((wkind == W_NS_MULTI || wkind == W_PC) && tid < 18) {
@@ -243,55 +251,30 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
                 }
             }
         }
-        noskip[tid] = v;
+        sm.noskip[tid] = v;
     }
 
-    if (!chroma) {
-        // ---- luma window: rows -6 .. sh+5, columns -6 .. uw+5 ----
-        const int wh = g.sh + 12, ww = g.uw + 12;
-        for (int i = tid; i < wh * ww; i += 256) {
-            int r = i / ww - 6, c = i % ww - 6;
-            int row;
-            bool from_d;
-            row_src(g, r, row, from_d);
-            const P *src = from_d ? Dp : Cp;
-            win[(r + 6) * LW + (c + 6)] = (int16_t)src[(int64_t)row * stride + col_src(g, c)];
-        }
-        if (gdf_on) {
-            const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
-            const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
-            const int weight_base = ref_dst_idx * 1584 + qp_idx * 264;
-            const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
-                                                    : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
-            const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
-            for (int i = tid; i < 88; i += 256) s_alpha[i] = f.tab.GDF_ALPHA[alpha_base + i];
-            for (int i = tid; i < 264; i += 256) s_weight[i] = f.tab.GDF_WEIGHT[weight_base + i];
-            for (int i = tid; i < nerr; i += 256) s_err[i] = errtab[i];
-        }
-    } else {
+    if (chroma) {
         // ---- chroma window: rows -2 .. sh+1, columns -2 .. uw+1 ----
         const int wh = g.sh + 4, ww = g.uw + 4;
-        for (int i = tid; i < wh * ww; i += 256) {
-            int r = i / ww - 2, c = i % ww - 2;
+        for (int r = warp; r < wh; r += 8) {
             int row;
             bool from_d;
-            row_src(g, r, row, from_d);
-            const P *src = from_d ? Dp : Cp;
-            win[(r + 2) * CWW + (c + 2)] = (int16_t)src[(int64_t)row * stride + col_src(g, c)];
+            row_src(g, r - 2, row, from_d);
+            const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
+            for (int c = lane; c < ww; c += 32) sm.win[r * CWW + c] = (int16_t)src[col_src(g, c - 2)];
         }
         if (wkind == W_NS_SINGLE) {
             // downsampled luma for chroma rows -2 .. sh+1 at chroma columns
             // -2 .. uw+1 (backup_row_luma with the ns_wiener_single_uv row
             // selection, looprestoration.rs:1207-1350)
             const P *Cy = plane_ptr<const P>(f.C[0]);
-            const P *Dy = plane_ptr<const P>(f.R[0]);
+            const P *Dy = plane_ptr<const P>(f.D[0]);
             const int64_t ls = f.stride[0];
             const int ds = fp.cfl_ds_filter_index;
             const int lw = g.uw << 1, lx0 = g.x0 << 1;
-            for (int i = tid; i < wh * ww; i += 256) {
-                int r = i / ww - 2, j = i % ww - 2;
-                // chroma row -> (luma source, rowA, rowB)
-                int rr = r;
+            for (int r = warp; r < wh; r += 8) {
+                int rr = r - 2;
                 if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
                 if (!(g.edges & LR_HAVE_BOTTOM) && rr >= g.sh) rr = g.sh - 1;
                 const P *src;
@@ -315,179 +298,24 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
                     ra = 2 * (g.y0 + rr);
                     rb = ra + 1;
                 }
-                // luma position 2j, with the left / right fills
-                int pos = 2 * j;
-                if (pos < 0 && !(g.edges & LR_HAVE_LEFT)) pos = 0;
-                if (pos >= lw && !(g.edges & LR_HAVE_RIGHT)) pos = lw - 2;
-                const P *a = src + (int64_t)ra * ls + lx0 + pos;
-                const P *bb = src + (int64_t)rb * ls + lx0 + pos;
-                int v;
-                if (ds == 0)
-                    v = ((int)a[0] + bb[0] + a[1] + bb[1]) >> 2;
-                else if (ds == 1)
-                    v = ((int)a[0] + bb[0]) >> 1;
-                else
-                    v = a[0];
-                lwin[(r + 2) * CWW + (j + 2)] = (int16_t)v;
-            }
-        }
-    }
-    __syncthreads();
-
-    if (!chroma) {
-        const int b8 = bitdepth - 8;
-        // ---- GDF prep (looprestoration.rs:1432-1640) ----
-        if (gdf_on) {
-            const uint32_t down = bitdepth == 12 ? 2 : 0, up = bitdepth == 8 ? 2 : 0;
-            const int ref_dst_idx = f.gdf_ref_dst_idx;
-            const int bias_idx = ref_dst_idx * 6 + fp.gdf_qp_idx;
-            const int scale = ref_dst_idx == 0 ? 8 : 5;
-            const int npairs = g.sh * (g.uw >> 1);
-            for (int i = tid; i < npairs; i += 256) {
-                int y = i / (g.uw >> 1), x1 = (i % (g.uw >> 1)) * 2;
-                int y1 = y & ~1;
-                int gs[4] = {0, 0, 0, 0};
-                const int dys[4] = {1, 0, 1, -1}, dxs[4] = {0, 1, 1, 1};
-                for (int rr = y1 - 1; rr <= y1 + 2; rr++)
-                    for (int cc = x1 - 1; cc <= x1 + 2; cc++) {
-                        int bv = win[(rr + 6) * LW + cc + 6] >> down;
-#pragma unroll
-                        for (int d = 0; d < 4; d++) {
-                            int av = win[(rr - dys[d] + 6) * LW + cc - dxs[d] + 6] >> down;
-                            int cv = win[(rr + dys[d] + 6) * LW + cc + dxs[d] + 6] >> down;
-                            int t = bv * 2 - av - cv;
-                            gs[d] += t < 0 ? -t : t;
-                        }
-                    }
-                int cls = (gs[0] <= gs[1]) | ((gs[2] <= gs[3]) << 1);
-                int shared[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) shared[k] = f.tab.GDF_BIAS[bias_idx * 3 + k];
-#pragma unroll
-                for (int d = 0; d < 4; d++) {
-                    int k = d + 18;
-                    int alpha = s_alpha[k * 4 + cls];
-                    int v = imin_(gs[d] >> (4 - up), alpha);
-#pragma unroll
-                    for (int q = 0; q < 3; q++) shared[q] += v * s_weight[q * 88 + k * 4 + cls];
+                const P *rowa = src + (int64_t)ra * ls + lx0;
+                const P *rowb = src + (int64_t)rb * ls + lx0;
+                for (int j = lane; j < ww; j += 32) {
+                    int pos = 2 * (j - 2);
+                    if (pos < 0 && !(g.edges & LR_HAVE_LEFT)) pos = 0;
+                    if (pos >= lw && !(g.edges & LR_HAVE_RIGHT)) pos = lw - 2;
+                    int v;
+                    if (ds == 0)
+                        v = ((int)rowa[pos] + rowb[pos] + rowa[pos + 1] + rowb[pos + 1]) >> 2;
+                    else if (ds == 1)
+                        v = ((int)rowa[pos] + rowb[pos]) >> 1;
+                    else
+                        v = rowa[pos];
+                    sm.lwin[r * CWW + j] = (int16_t)v;
                 }
-                for (int x2 = 0; x2 < 2; x2++) {
-                    int x = x1 + x2;
-                    int iv[3] = {shared[0], shared[1], shared[2]};
-                    int m = win[(y + 6) * LW + x + 6] >> down;
-#pragma unroll
-                    for (int k = 0; k < 18; k++) {
-                        int alpha = s_alpha[k * 4 + cls];
-                        int dy = c_gdf_coords[k][0], dx = c_gdf_coords[k][1];
-                        int a = win[(y - dy + 6) * LW + x - dx + 6] >> down;
-                        int bvv = win[(y + dy + 6) * LW + x + dx + 6] >> down;
-                        int above = iclip_((a - m) << up, -alpha, alpha);
-                        int below = iclip_((bvv - m) << up, -alpha, alpha);
-                        int v = iclip_(above + below, -512, 511);
-#pragma unroll
-                        for (int q = 0; q < 3; q++) iv[q] += v * s_weight[q * 88 + k * 4 + cls];
-                    }
-                    int full = 0;
-#pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        int sv = iv[q] * scale;
-                        int asv = sv < 0 ? -sv : sv;
-                        int v = apply_sign_((asv + (1 << 14)) >> 15, sv);
-                        int sub = iclip_(v, -scale, scale - 1) + scale;
-                        full = full * (scale * 2) + sub;
-                    }
-                    gerr[y * 64 + x] = s_err[full];
-                }
-            }
-        }
-        // ---- classification for PC-Wiener / NS-multi (:195-271, :870-896) ----
-        const int bh4 = g.sh >> 2, bw4 = g.uw >> 2;
-        if (wkind == W_NS_MULTI || wkind == W_PC) {
-            const uint8_t *sub_lut = wkind == W_PC
-                                         ? f.tab.PC_WIENER_SUB_CLASSIFY + f.wiener_idx * 256
-                                         : f.tab.PC_WIENER_SUB_CLASSIFY_NS + (f.wiener_idx * 7 + (f.ns_ci >= 0 ? imin_(f.ns_ci, 6) : 0)) * 256;
-            for (int i = tid; i < bh4 * bw4; i += 256) {
-                int by = i / bw4, bx = i % bw4;
-                int fs[3] = {0, 0, 0};
-                for (int dy = -1; dy <= 4; dy++)
-                    for (int dx = -1; dx <= 4; dx++) {
-                        int y = by * 4 + dy + 6, x = bx * 4 + dx + 6;
-                        int m = win[y * LW + x];
-                        int vert = win[(y - 1) * LW + x] - 2 * m + win[(y + 1) * LW + x];
-                        int anti = win[(y - 1) * LW + x + 1] - 2 * m + win[(y + 1) * LW + x - 1];
-                        int diag = win[(y - 1) * LW + x - 1] - 2 * m + win[(y + 1) * LW + x + 1];
-                        fs[0] += vert < 0 ? -vert : vert;
-                        fs[1] += anti < 0 ? -anti : anti;
-                        fs[2] += diag < 0 ? -diag : diag;
-                    }
-                int s = 0;
-                const int np[3] = {16, 4, 1};
-                for (int dy = -1; dy <= 1; dy++)
-                    for (int dx = -1; dx <= 1; dx++) {
-                        int e = (dy != 0) + (dx != 0);
-                        int fx = iclip_((bx & 15) + dx, 0, 15);
-                        int fy = iclip_(by + dy, 0, bh4 - 1);
-                        s += np[e] * (((noskip[fy] >> fx) & 1) == 0);
-                    }
-                int rnd = (1 << b8) >> 1;
-#pragma unroll
-                for (int k = 0; k < 3; k++) fs[k] = (int)((uint32_t)fs[k] * (uint32_t)c_pcw_norm[k] + (uint32_t)rnd) >> b8;
-                s *= c_pcw_norm[3];
-                int qv = (imax_(0, get_qval(f.base_q, s, 0, b8)) + (1 << 13)) >> 14;
-                qv = imin_(qv, 255) >> 5;
-                int lut_idx = qv << 9;
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    qv = (imax_(0, fs[k] + get_qval(f.base_q, s, k + 1, b8)) + (1 << 13)) >> 14;
-                    qv = imin_(qv, 255) >> 5;
-                    lut_idx |= qv << (3 * (2 - k));
-                }
-                classes[by][bx] = sub_lut[f.tab.PC_WIENER_LUT_TO_CLASS[lut_idx]];
             }
         }
         __syncthreads();
-        // ---- Wiener FIR + GDF add, one output sample per iteration ----
-        int8_t single[16];
-        if (wkind == W_NS_SINGLE) {
-            const int8_t *src = fp.restoration[0].frame_filters_on ? fp.restoration[0].filter[0] : g.unit->ns_filter[0];
-#pragma unroll
-            for (int k = 0; k < 16; k++) single[k] = src[k];
-        }
-        const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
-        for (int i = tid; i < g.sh * g.uw; i += 256) {
-            int y = i / g.uw, x = i % g.uw;
-            int m = win[(y + 6) * LW + x + 6];
-            int v = m;
-            bool ll = (llm[y >> 2] >> (x >> 2)) & 1;
-            if (!ll && wkind != W_NONE) {
-                int s;
-                if (wkind == W_PC) {
-                    const int16_t *flt = f.tab.PC_WIENER_FILTERS + (f.wiener_idx * 64 + classes[y >> 2][x >> 2]) * 13;
-                    s = m * flt[12];
-#pragma unroll
-                    for (int k = 0; k < 12; k++) {
-                        int dy = c_cfg_pc[k][0], dx = c_cfg_pc[k][1];
-                        s += (win[(y + dy + 6) * LW + x + dx + 6] + win[(y - dy + 6) * LW + x - dx + 6]) * flt[k];
-                    }
-                } else {
-                    const int8_t *flt = wkind == W_NS_SINGLE ? single : fp.restoration[0].filter[classes[y >> 2][x >> 2]];
-                    s = m << 7;
-#pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        int dy = c_cfg_y[k][0], dx = c_cfg_y[k][1];
-                        s += (win[(y + dy + 6) * LW + x + dx + 6] + win[(y - dy + 6) * LW + x - dx + 6] - 2 * m) * flt[k];
-                    }
-                }
-                v = iclip_((s + 64) >> 7, 0, bdmax);
-            }
-            if (gdf_on && !ll) {
-                int diff = gerr[y * 64 + x] * gscale;
-                int ad = diff < 0 ? -diff : diff;
-                v = iclip_(v + apply_sign_((ad + grnd) >> gshift, diff), 0, bdmax);
-            }
-            Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
-        }
-    } else {
         // ---- chroma NS-Wiener with cross-component luma taps (:1145-1430) ----
         int8_t flt[18];
         if (wkind == W_NS_SINGLE) {
@@ -496,29 +324,249 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
 #pragma unroll
             for (int k = 0; k < 18; k++) flt[k] = src[k];
         }
-        for (int i = tid; i < g.sh * g.uw; i += 256) {
-            int y = i / g.uw, x = i % g.uw;
-            int m = win[(y + 2) * CWW + x + 2];
-            int v = m;
-            bool ll = (llm[y >> 2] >> (x >> 2)) & 1;
-            if (!ll && wkind == W_NS_SINGLE) {
-                int s = m << 7;
+        for (int y = warp; y < g.sh; y += 8)
+            for (int x = lane; x < g.uw; x += 32) {
+                const int16_t *w = &sm.win[(y + 2) * CWW + x + 2];
+                const int16_t *lw_ = &sm.lwin[(y + 2) * CWW + x + 2];
+                int m = w[0];
+                int v = m;
+                bool ll = (sm.llm[y >> 2] >> (x >> 2)) & 1;
+                if (!ll && wkind == W_NS_SINGLE) {
+                    int s = m << 7;
 #pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    int dy = c_cfg_uv[k][0], dx = c_cfg_uv[k][1];
-                    s += (win[(y + dy + 2) * CWW + x + dx + 2] + win[(y - dy + 2) * CWW + x - dx + 2] - 2 * m) * flt[k];
+                    for (int k = 0; k < 6; k++) {
+                        const int o = TapsY::uv[k][0] * CWW + TapsY::uv[k][1];
+                        s += (w[o] + w[-o] - 2 * m) * flt[k];
+                    }
+                    int l = lw_[0];
+#pragma unroll
+                    for (int k = 0; k < 12; k++) {
+                        const int o = TapsY::uvy[k][0] * CWW + TapsY::uvy[k][1];
+                        s += (lw_[o] - l) * flt[6 + k];
+                    }
+                    v = iclip_((s + 64) >> 7, 0, bdmax);
                 }
-                int l = lwin[(y + 2) * CWW + x + 2];
+                Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
+            }
+        return;
+    }
+
+    // ---- luma window: rows -6 .. sh+5, columns -6 .. uw+5 ----
+    const int wh = g.sh + 12, ww = g.uw + 12;
+    for (int r = warp; r < wh; r += 8) {
+        int row;
+        bool from_d;
+        row_src(g, r - 6, row, from_d);
+        const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
+        for (int c = lane; c < ww; c += 32) sm.win[r * LW + c] = (int16_t)src[col_src(g, c - 6)];
+    }
+    if (gdf_on) {
+        const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
+        const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
+        const int weight_base = ref_dst_idx * 1584 + qp_idx * 264;
+        const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
+                                                : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
+        const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
+        for (int i = tid; i < 88; i += 256) {
+            int k = i >> 2, c = i & 3;
+            short4 p;
+            p.x = (short)f.tab.GDF_ALPHA[alpha_base + i];
+            p.y = f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i];
+            p.z = f.tab.GDF_WEIGHT[weight_base + 1 * 88 + i];
+            p.w = f.tab.GDF_WEIGHT[weight_base + 2 * 88 + i];
+            sm.s_par[c][k] = p;
+        }
+        for (int i = tid; i < nerr; i += 256) sm.s_err[i] = errtab[i];
+    }
+    __syncthreads();
+
+    const int b8 = bitdepth - 8;
+    const int bh4 = g.sh >> 2, bw4 = g.uw >> 2;
+    // ---- GDF prep (looprestoration.rs:1432-1640) ----
+    if (gdf_on) {
+        // GDF works in a 10-bit domain (looprestoration.rs:1450-1453): 8-bit
+        // samples shift up by 2; 12-bit (not accepted at the boundary) would
+        // shift down by 2.
+        constexpr int down = 0, up = sizeof(P) == 1 ? 2 : 0;
+        // gradient cell (j, i): rows 2j-1, 2j; columns 2i-1, 2i
+        // (compute_gradient_row :114-193); pair (y1, x1) sums cells
+        // (y1/2 .. y1/2+1, x1/2 .. x1/2+1)
+        const int cj = (g.sh >> 1) + 1, ci = (g.uw >> 1) + 1;
+        for (int i = tid; i < cj * ci; i += 256) {
+            int j = i / ci, c = i % ci;
+            int gs[4] = {0, 0, 0, 0};
 #pragma unroll
-                for (int k = 0; k < 12; k++) {
-                    int dy = c_cfg_uv_from_y[k][0], dx = c_cfg_uv_from_y[k][1];
-                    s += (lwin[(y + dy + 2) * CWW + x + dx + 2] - l) * flt[6 + k];
+            for (int yy = 0; yy < 2; yy++)
+#pragma unroll
+                for (int xx = 0; xx < 2; xx++) {
+                    const int16_t *w = &sm.win[(2 * j - 1 + yy + 6) * LW + 2 * c - 1 + xx + 6];
+                    int bv = w[0] >> down;
+                    int t;
+                    t = 2 * bv - (w[-LW] >> down) - (w[LW] >> down);
+                    gs[0] += t < 0 ? -t : t;
+                    t = 2 * bv - (w[-1] >> down) - (w[1] >> down);
+                    gs[1] += t < 0 ? -t : t;
+                    t = 2 * bv - (w[-LW - 1] >> down) - (w[LW + 1] >> down);
+                    gs[2] += t < 0 ? -t : t;
+                    t = 2 * bv - (w[LW - 1] >> down) - (w[-LW + 1] >> down);
+                    gs[3] += t < 0 ? -t : t;
+                }
+#pragma unroll
+            for (int d = 0; d < 4; d++) sm.gcell[i * 4 + d] = (uint16_t)gs[d];
+        }
+        __syncthreads();
+        const int ref_dst_idx = f.gdf_ref_dst_idx;
+        const int bias_idx = ref_dst_idx * 6 + fp.gdf_qp_idx;
+        const int scale = ref_dst_idx == 0 ? 8 : 5;
+        const int b0 = f.tab.GDF_BIAS[bias_idx * 3], b1 = f.tab.GDF_BIAS[bias_idx * 3 + 1],
+                  b2 = f.tab.GDF_BIAS[bias_idx * 3 + 2];
+        const int npairs = g.sh * (g.uw >> 1);
+        for (int i = tid; i < npairs; i += 256) {
+            int y = i / (g.uw >> 1), x1 = (i % (g.uw >> 1)) * 2;
+            int j = y >> 1, c = x1 >> 1;
+            int gsum[4];
+#pragma unroll
+            for (int d = 0; d < 4; d++)
+                gsum[d] = sm.gcell[(j * ci + c) * 4 + d] + sm.gcell[(j * ci + c + 1) * 4 + d] +
+                          sm.gcell[((j + 1) * ci + c) * 4 + d] + sm.gcell[((j + 1) * ci + c + 1) * 4 + d];
+            int cls = (gsum[0] <= gsum[1]) | ((gsum[2] <= gsum[3]) << 1);
+            const short4 *par = sm.s_par[cls];
+            int sh0 = b0, sh1 = b1, sh2 = b2;
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                short4 p = par[18 + d];
+                int v = imin_(gsum[d] >> (4 - up), p.x);
+                sh0 += v * p.y;
+                sh1 += v * p.z;
+                sh2 += v * p.w;
+            }
+#pragma unroll
+            for (int x2 = 0; x2 < 2; x2++) {
+                const int x = x1 + x2;
+                const int16_t *w = &sm.win[(y + 6) * LW + x + 6];
+                int m = w[0] >> down;
+                int i0 = sh0, i1 = sh1, i2 = sh2;
+#pragma unroll
+                for (int k = 0; k < 18; k++) {
+                    const int o = TapsY::gdf[k][0] * LW + TapsY::gdf[k][1];
+                    short4 p = par[k];
+                    int alpha = p.x;
+                    int above = iclip_(((w[-o] >> down) - m) << up, -alpha, alpha);
+                    int below = iclip_(((w[o] >> down) - m) << up, -alpha, alpha);
+                    int v = iclip_(above + below, -512, 511);
+                    i0 += v * p.y;
+                    i1 += v * p.z;
+                    i2 += v * p.w;
+                }
+                int full = 0;
+                const int iv[3] = {i0, i1, i2};
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    int sv = iv[q] * scale;
+                    int asv = sv < 0 ? -sv : sv;
+                    int v = apply_sign_((asv + (1 << 14)) >> 15, sv);
+                    int subi = iclip_(v, -scale, scale - 1) + scale;
+                    full = full * (scale * 2) + subi;
+                }
+                sm.gerr[y * 64 + x] = sm.s_err[full];
+            }
+        }
+    }
+    // ---- classification for PC-Wiener / NS-multi (:195-271, :870-896) ----
+    if (wkind == W_NS_MULTI || wkind == W_PC) {
+        const uint8_t *sub_lut = wkind == W_PC
+                                     ? f.tab.PC_WIENER_SUB_CLASSIFY + f.wiener_idx * 256
+                                     : f.tab.PC_WIENER_SUB_CLASSIFY_NS +
+                                           (f.wiener_idx * 7 + (f.ns_ci >= 0 ? imin_(f.ns_ci, 6) : 0)) * 256;
+        for (int i = tid; i < bh4 * bw4; i += 256) {
+            int by = i / bw4, bx = i % bw4;
+            int fs0 = 0, fs1 = 0, fs2 = 0;
+#pragma unroll
+            for (int dy = -1; dy <= 4; dy++)
+#pragma unroll
+                for (int dx = -1; dx <= 4; dx++) {
+                    const int16_t *w = &sm.win[(by * 4 + dy + 6) * LW + bx * 4 + dx + 6];
+                    int m2 = 2 * w[0];
+                    int vert = w[-LW] - m2 + w[LW];
+                    int anti = w[-LW + 1] - m2 + w[LW - 1];
+                    int diag = w[-LW - 1] - m2 + w[LW + 1];
+                    fs0 += vert < 0 ? -vert : vert;
+                    fs1 += anti < 0 ? -anti : anti;
+                    fs2 += diag < 0 ? -diag : diag;
+                }
+            int s = 0;
+            const int np[3] = {16, 4, 1};
+#pragma unroll
+            for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                for (int dx = -1; dx <= 1; dx++) {
+                    int e = (dy != 0) + (dx != 0);
+                    int fx = iclip_((bx & 15) + dx, 0, 15);
+                    int fy = iclip_(by + dy, 0, bh4 - 1);
+                    s += np[e] * (((sm.noskip[fy] >> fx) & 1) == 0);
+                }
+            int rnd = (1 << b8) >> 1;
+            int fs[3] = {fs0, fs1, fs2};
+#pragma unroll
+            for (int k = 0; k < 3; k++) fs[k] = (int)((uint32_t)fs[k] * (uint32_t)c_pcw_norm[k] + (uint32_t)rnd) >> b8;
+            s *= c_pcw_norm[3];
+            int qv = (imax_(0, get_qval(f.base_q, s, 0, b8)) + (1 << 13)) >> 14;
+            qv = imin_(qv, 255) >> 5;
+            int lut_idx = qv << 9;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                qv = (imax_(0, fs[k] + get_qval(f.base_q, s, k + 1, b8)) + (1 << 13)) >> 14;
+                qv = imin_(qv, 255) >> 5;
+                lut_idx |= qv << (3 * (2 - k));
+            }
+            sm.classes[by][bx] = sub_lut[f.tab.PC_WIENER_LUT_TO_CLASS[lut_idx]];
+        }
+    }
+    __syncthreads();
+    // ---- Wiener FIR + GDF add, one output sample per iteration ----
+    int8_t single[16];
+    if (wkind == W_NS_SINGLE) {
+        const int8_t *src = fp.restoration[0].frame_filters_on ? fp.restoration[0].filter[0] : g.unit->ns_filter[0];
+#pragma unroll
+        for (int k = 0; k < 16; k++) single[k] = src[k];
+    }
+    const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
+    for (int y = warp; y < g.sh; y += 8)
+        for (int x = lane; x < g.uw; x += 32) {
+            const int16_t *w = &sm.win[(y + 6) * LW + x + 6];
+            int m = w[0];
+            int v = m;
+            bool ll = (sm.llm[y >> 2] >> (x >> 2)) & 1;
+            if (!ll && wkind != W_NONE) {
+                int s;
+                if (wkind == W_PC) {
+                    const int16_t *flt =
+                        f.tab.PC_WIENER_FILTERS + (f.wiener_idx * 64 + sm.classes[y >> 2][x >> 2]) * 13;
+                    s = m * __ldg(flt + 12);
+#pragma unroll
+                    for (int k = 0; k < 12; k++) {
+                        const int o = TapsY::pc[k][0] * LW + TapsY::pc[k][1];
+                        s += (w[o] + w[-o]) * __ldg(flt + k);
+                    }
+                } else {
+                    const int8_t *flt =
+                        wkind == W_NS_SINGLE ? single : fp.restoration[0].filter[sm.classes[y >> 2][x >> 2]];
+                    s = m << 7;
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const int o = TapsY::ns[k][0] * LW + TapsY::ns[k][1];
+                        s += (w[o] + w[-o] - 2 * m) * flt[k];
+                    }
                 }
                 v = iclip_((s + 64) >> 7, 0, bdmax);
             }
+            if (gdf_on && !ll) {
+                int diff = sm.gerr[y * 64 + x] * gscale;
+                int ad = diff < 0 ? -diff : diff;
+                v = iclip_(v + apply_sign_((ad + grnd) >> gshift, diff), 0, bdmax);
+            }
             Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
         }
-    }
 }
 
 }  // namespace

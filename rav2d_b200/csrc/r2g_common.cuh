@@ -39,7 +39,8 @@ struct DevFrame {
     int sb256w, sb256h, sbh;
     int bitdepth, hbd, bdmax;
     int64_t stride[2];  // in samples: luma, chroma
-    void *R[3];         // recon; deblocked in place (the reference's D)
+    void *R[3];         // recon (input, preserved)
+    void *D[3];         // deblocked frame
     void *C[3];         // CDEF+CCSO output
     void *L[3];         // loop-restoration output (the filtered frame)
     void *G[3];         // film-grain display copy
@@ -68,7 +69,7 @@ R2G_D P *plane_ptr(void *base) {
 
 // Launch helpers implemented per stage (deblock.cu, cdef.cu, lr.cu, grain.cu).
 // Each returns the number of kernels it launched.
-int r2g_launch_deblock_dir(const DevFrame &f, int dir, cudaStream_t s);
+int r2g_launch_deblock(const DevFrame &f, cudaStream_t s);
 int r2g_launch_cdef(const DevFrame &f, cudaStream_t s);
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s);
 

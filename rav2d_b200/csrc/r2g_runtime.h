@@ -14,7 +14,7 @@ struct Ticket {
 
 struct GrainCtx;  // grain.cu
 
-enum { R2G_N_STAGES = 5 };
+enum { R2G_N_STAGES = 4 };
 
 // Per-run profiling events: ev[i] .. ev[i+1] brackets stage i.
 struct ProfRun {
@@ -46,7 +46,7 @@ struct R2gFrame {
     int64_t rows[2] = {0, 0};
     size_t plane_bytes[2] = {0, 0};
     size_t buf_bytes = 0;
-    void *buf[4] = {nullptr, nullptr, nullptr, nullptr};  // recon/D, C, L, G
+    void *buf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // R, D, C, L, G
     int n_sb256 = 0;
     size_t side_bytes = 0;
     void *side_dev = nullptr;

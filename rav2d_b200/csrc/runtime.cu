@@ -144,7 +144,7 @@ extern "C" int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth,
     f->n_sb256 = ((bw4 + 63) >> 6) * ((bh4 + 63) >> 6);
     f->side_bytes = (size_t)f->n_sb256 * (sizeof(R2gAv2Filter) + sizeof(R2gAv2Restoration));
     int rc;
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 5; i++)
         if ((rc = r2g_dev_alloc(ctx, &f->buf[i], f->buf_bytes)) != R2G_OK) {
             r2g_frame_free(ctx, f);
             return rc;
@@ -161,7 +161,7 @@ extern "C" int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth,
     }
     // the display copy starts as a copy of whatever is filtered; zero it so
     // downloads of an ungrained frame are deterministic
-    for (int i = 0; i < 4; i++) CK(cudaMemsetAsync(f->buf[i], 0, f->buf_bytes, ctx->stream));
+    for (int i = 0; i < 5; i++) CK(cudaMemsetAsync(f->buf[i], 0, f->buf_bytes, ctx->stream));
     *out = f;
     return R2G_OK;
 }
@@ -170,7 +170,7 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     if (!ctx || !f) return R2G_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (int i = 0; i < 4; i++) r2g_dev_free(ctx, f->buf[i], f->buf_bytes);
+    for (int i = 0; i < 5; i++) r2g_dev_free(ctx, f->buf[i], f->buf_bytes);
     r2g_dev_free(ctx, f->side_dev, f->side_bytes);
     r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
     if (f->side_host) cudaFreeHost(f->side_host);
@@ -407,16 +407,18 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
     }
     CK(cudaEventRecord(f->side_done, ctx->stream));
 
-    // buffers: 0 = recon / deblocked, 1 = CDEF out, 2 = LR out, 3 = grain
-    void *p[4][3];
-    for (int i = 0; i < 4; i++) plane_ptrs(f, i, p[i]);
+    // buffers: 0 = recon (preserved), 1 = deblocked, 2 = CDEF out,
+    // 3 = LR out, 4 = grain display copy
+    void *p[5][3];
+    for (int i = 0; i < 5; i++) plane_ptrs(f, i, p[i]);
     for (int i = 0; i < 3; i++) {
         d.R[i] = p[0][i];
-        d.C[i] = d.cdef_stage_on ? p[1][i] : p[0][i];
-        d.L[i] = d.lr_on ? p[2][i] : d.C[i];
-        d.G[i] = p[3][i];
+        d.D[i] = d.deblock_on ? p[1][i] : p[0][i];
+        d.C[i] = d.cdef_stage_on ? p[2][i] : d.D[i];
+        d.L[i] = d.lr_on ? p[3][i] : d.C[i];
+        d.G[i] = p[4][i];
     }
-    f->out_buf = d.lr_on ? 2 : (d.cdef_stage_on ? 1 : 0);
+    f->out_buf = d.lr_on ? 3 : (d.cdef_stage_on ? 2 : (d.deblock_on ? 1 : 0));
     f->grain_buf = -1;
     return R2G_OK;
 }
@@ -497,17 +499,14 @@ extern "C" int r2g_ctx_set_stream(R2gCtx *ctx, void *stream) {
 void r2g_launch_pipeline(R2gCtx *ctx, const DevFrame &d) {
     cudaStream_t s = ctx->stream;
     r2g_prof_stage(ctx, 0, true, 0);
-    int n = r2g_launch_deblock_dir(d, 0, s);
+    int n = r2g_launch_deblock(d, s);
     r2g_prof_stage(ctx, 0, false, n);
     r2g_prof_stage(ctx, 1, true, 0);
-    n = r2g_launch_deblock_dir(d, 1, s);
+    n = r2g_launch_cdef(d, s);
     r2g_prof_stage(ctx, 1, false, n);
     r2g_prof_stage(ctx, 2, true, 0);
-    n = r2g_launch_cdef(d, s);
-    r2g_prof_stage(ctx, 2, false, n);
-    r2g_prof_stage(ctx, 3, true, 0);
     n = r2g_launch_lr(d, s);
-    r2g_prof_stage(ctx, 3, false, n);
+    r2g_prof_stage(ctx, 2, false, n);
 }
 
 extern "C" int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,

@@ -107,12 +107,12 @@ class Context:
     def profile(self, enable=True):
         self.check(lib().r2g_ctx_profile(self.h, int(enable)))
 
-    STAGES = ("deblock_vert", "deblock_horz", "cdef_ccso", "loop_restoration", "film_grain")
+    STAGES = ("deblock", "cdef_ccso", "loop_restoration", "film_grain")
 
     def profile_read(self):
-        ms = (C.c_double * 5)()
-        n = (C.c_int64 * 5)()
-        self.check(lib().r2g_ctx_profile_read(self.h, ms, n, 5))
+        ms = (C.c_double * 4)()
+        n = (C.c_int64 * 4)()
+        self.check(lib().r2g_ctx_profile_read(self.h, ms, n, 4))
         return {s: (ms[i], n[i]) for i, s in enumerate(self.STAGES)}
 
     def launch_count(self):
