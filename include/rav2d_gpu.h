@@ -270,11 +270,19 @@ typedef struct R2gBatchItem {
     const R2gFilmGrainData *fgd; /* NULL = no grain */
     uint32_t grain_seed;
 } R2gBatchItem;
-/* Enqueue the whole batch; returns a ticket for r2g_wait. */
+/* Enqueue the whole batch (at most 1023 distinct frames) as one persistent
+ * launch per stage; returns a ticket for r2g_wait.  An item whose fp and side
+ * are both NULL runs with the side-info of the frame's last r2g_frame_stage
+ * (as r2g_frame_run does); its inloop_mask is then ignored.  Film grain is
+ * applied per item when fgd is non-NULL (read it back with which = 1). */
 int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ticket);
 /* Wait for a ticket; R2G_E_TIMEOUT after timeout_ms (<0 = forever),
  * timeout_ms == 0 polls (R2G_E_NOTREADY when pending). */
 int r2g_wait(R2gCtx *ctx, uint64_t ticket, int timeout_ms);
+/* Instrumentation (no counterpart in the reference): the CTAs per SM the
+ * last batch used for stages 0 deblock, 1 CDEF+CCSO, 2 loop restoration,
+ * 3 film grain (autotuned); returns the SM count. */
+int r2g_batch_config(R2gCtx *ctx, int32_t *ctas_per_sm, int n);
 
 /* ---- film grain without any device allocation ----
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:

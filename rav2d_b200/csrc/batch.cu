@@ -1,24 +1,386 @@
-// Batched submission: many frames, one ticket.
+// Batched execution: many frames, one persistent launch per stage.
+//
+// Every frame of a batch is staged as in the per-frame path (side-info on
+// the device, DevFrame descriptor); then one staging blob carries the
+// descriptors, the film-grain parameters and a work list per stage (item =
+// frame << 22 | the frame's own item index) to the device, and a CUDA graph
+// runs the persistent stage kernels over those lists:
+//   deblock -> CDEF+CCSO -> loop restoration -> grain apply, with the grain
+//   templates on a forked branch (they depend only on the grain parameters)
+//   joined before the apply.
+// The graph's kernels read the item counts from device memory, so one
+// instantiated graph serves every batch that fits the slot's capacity.  Two
+// slots alternate, so the host can stage batch k+1 while batch k runs.
+//
+// The grid of each persistent kernel (CTAs per SM) is chosen by a small
+// autotuner: on the first batch of a given bit-depth mix it times every
+// occupancy-legal choice per stage and keeps the fastest; the choice is
+// cached per device in a text file ($R2G_TUNE_CACHE, default
+// $HOME/.cache/rav2d_b200/autotune-v1.txt).  R2G_AUTOTUNE=0 skips tuning and
+// uses the occupancy limit.
+#include <sys/stat.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "r2g_runtime.h"
 
-int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed);
+int r2g_grain_ready(int device);
+
+namespace {
+
+enum { N_BSTAGES = 4 };  // deblock, cdef, lr, grain apply
+
+struct Layout {
+    int max_frames = 0;
+    int max_items[N_BSTAGES] = {0, 0, 0, 0};
+    size_t off_frames = 0, off_grain = 0, off_work[N_BSTAGES] = {0, 0, 0, 0}, bytes = 0;
+};
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+static Layout make_layout(int frames, const int *items) {
+    Layout L;
+    L.max_frames = frames;
+    size_t o = 256;  // counts
+    L.off_frames = o;
+    o = align256(o + sizeof(DevFrame) * frames);
+    L.off_grain = o;
+    o = align256(o + sizeof(GrainBatch) * frames);
+    for (int k = 0; k < N_BSTAGES; k++) {
+        L.max_items[k] = items[k];
+        L.off_work[k] = o;
+        o = align256(o + sizeof(uint32_t) * items[k]);
+    }
+    L.bytes = o;
+    return L;
+}
+
+struct Slot {
+    Layout L;
+    char *host = nullptr;
+    char *dev = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int grids[N_BSTAGES + 1] = {0, 0, 0, 0, 0};
+    cudaEvent_t done = nullptr;
+    bool used = false;
+};
+
+}  // namespace
+
+struct BatchState {
+    Slot slot[2];
+    int next = 0;
+    int num_sms = 0;
+    int occ[N_BSTAGES] = {0, 0, 0, 0};
+    int tuned[3][N_BSTAGES] = {{0}};  // [8-bit, 10-bit, mixed][stage] CTAs per SM
+    int last[N_BSTAGES] = {0, 0, 0, 0};
+    bool cache_loaded = false;
+    std::string dev_name;
+    cudaEvent_t fork = nullptr, join = nullptr, t0 = nullptr, t1 = nullptr;
+};
+
+static std::string cache_path() {
+    const char *p = getenv("R2G_TUNE_CACHE");
+    if (p && *p) return p;
+    const char *h = getenv("HOME");
+    return std::string(h ? h : "/tmp") + "/.cache/rav2d_b200/autotune-v1.txt";
+}
+
+static void load_cache(BatchState &b) {
+    b.cache_loaded = true;
+    FILE *fp = fopen(cache_path().c_str(), "r");
+    if (!fp) return;
+    char line[512];
+    while (fgets(line, sizeof(line), fp)) {
+        char name[256];
+        int cls, k, v;
+        if (sscanf(line, "%255[^|]|%d|%d|%d", name, &cls, &k, &v) == 4 && b.dev_name == name && cls >= 0 &&
+            cls < 3 && k >= 0 && k < N_BSTAGES && v > 0 && v <= b.occ[k])
+            b.tuned[cls][k] = v;
+    }
+    fclose(fp);
+}
+
+static void save_cache(const BatchState &b, int cls) {
+    std::string path = cache_path();
+    std::string dir = path.substr(0, path.find_last_of('/'));
+    std::string mk = dir;
+    for (size_t i = 1; i <= mk.size(); i++)
+        if (i == mk.size() || mk[i] == '/') mkdir(mk.substr(0, i).c_str(), 0755);
+    FILE *fp = fopen(path.c_str(), "a");
+    if (!fp) return;
+    for (int k = 0; k < N_BSTAGES; k++)
+        if (b.tuned[cls][k] > 0) fprintf(fp, "%s|%d|%d|%d\n", b.dev_name.c_str(), cls, k, b.tuned[cls][k]);
+    fclose(fp);
+}
+
+static void launch_stage(int k, const BatchArgs &a, int grid, cudaStream_t s) {
+    switch (k) {
+        case 0: r2g_batch_launch_deblock(a, grid, s); break;
+        case 1: r2g_batch_launch_cdef(a, grid, s); break;
+        case 2: r2g_batch_launch_lr(a, grid, s); break;
+        default: r2g_batch_launch_grain_apply(a, grid, s); break;
+    }
+}
+
+static BatchArgs args_of(const Slot &s) {
+    BatchArgs a;
+    a.count = (const int *)s.dev;
+    a.frames = (const DevFrame *)(s.dev + s.L.off_frames);
+    a.grain = (const GrainBatch *)(s.dev + s.L.off_grain);
+    for (int k = 0; k < N_BSTAGES; k++) a.work[k] = (const uint32_t *)(s.dev + s.L.off_work[k]);
+    return a;
+}
+
+void r2g_batch_free(R2gCtx *ctx) {
+    BatchState *b = ctx->batch;
+    if (!b) return;
+    for (auto &s : b->slot) {
+        if (s.exec) cudaGraphExecDestroy(s.exec);
+        if (s.graph) cudaGraphDestroy(s.graph);
+        if (s.host) cudaFreeHost(s.host);
+        if (s.dev) r2g_dev_free(ctx, s.dev, s.L.bytes);
+        if (s.done) cudaEventDestroy(s.done);
+    }
+    for (cudaEvent_t e : {b->fork, b->join, b->t0, b->t1})
+        if (e) cudaEventDestroy(e);
+    delete b;
+    ctx->batch = nullptr;
+}
+
+static int ensure_state(R2gCtx *ctx) {
+    if (ctx->batch) return R2G_OK;
+    BatchState *b = new BatchState();
+    ctx->batch = b;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) return R2G_E_DEVICE;
+    b->num_sms = prop.multiProcessorCount;
+    b->dev_name = prop.name;
+    b->occ[0] = r2g_batch_occupancy_deblock();
+    b->occ[1] = r2g_batch_occupancy_cdef();
+    b->occ[2] = r2g_batch_occupancy_lr();
+    b->occ[3] = r2g_batch_occupancy_grain_apply();
+    for (int k = 0; k < N_BSTAGES; k++)
+        if (b->occ[k] < 1) b->occ[k] = 1;
+    for (cudaEvent_t *e : {&b->fork, &b->join})
+        if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) return R2G_E_DEVICE;
+    for (auto &s : b->slot)
+        if (cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) return R2G_E_DEVICE;
+    return R2G_OK;
+}
+
+// Times every legal grid of each stage on the staged batch (stage outputs
+// are pure functions of their inputs, so re-running a stage is harmless).
+static int autotune(R2gCtx *ctx, BatchState &b, const Slot &s, const int *counts, int cls) {
+    const char *env = getenv("R2G_AUTOTUNE");
+    bool enabled = !(env && env[0] == '0');
+    BatchArgs a = args_of(s);
+    for (int k = 0; k < N_BSTAGES; k++) {
+        if (b.tuned[cls][k] > 0) continue;
+        if (!enabled || counts[k] == 0) {
+            if (!enabled) b.tuned[cls][k] = b.occ[k];
+            if (k == 3 && counts[4] > 0)
+                r2g_batch_launch_grain_template(a, counts[4] < b.num_sms ? counts[4] : b.num_sms, ctx->stream);
+            continue;
+        }
+        if (k == 3 && counts[4] > 0)
+            r2g_batch_launch_grain_template(a, counts[4] < b.num_sms ? counts[4] : b.num_sms, ctx->stream);
+        float best = 1e30f;
+        int best_v = b.occ[k];
+        for (int v = 1; v <= b.occ[k]; v++) {
+            int grid = v * b.num_sms;
+            launch_stage(k, a, grid, ctx->stream);  // warm
+            cudaEventRecord(b.t0, ctx->stream);
+            launch_stage(k, a, grid, ctx->stream);
+            launch_stage(k, a, grid, ctx->stream);
+            cudaEventRecord(b.t1, ctx->stream);
+            if (cudaEventSynchronize(b.t1) != cudaSuccess) return R2G_E_DEVICE;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, b.t0, b.t1);
+            if (ms < best) {
+                best = ms;
+                best_v = v;
+            }
+        }
+        b.tuned[cls][k] = best_v;
+    }
+    if (enabled) save_cache(b, cls);
+    return cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
+}
+
+static int build_graph(R2gCtx *ctx, BatchState &b, Slot &s, const int *grids, int tpl_grid) {
+    if (s.exec) cudaGraphExecDestroy(s.exec);
+    if (s.graph) cudaGraphDestroy(s.graph);
+    s.exec = nullptr;
+    s.graph = nullptr;
+    BatchArgs a = args_of(s);
+    cudaStream_t st = ctx->stream;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return R2G_E_DEVICE;
+    cudaEventRecord(b.fork, st);
+    cudaStreamWaitEvent(ctx->side_stream, b.fork, 0);
+    r2g_batch_launch_grain_template(a, tpl_grid, ctx->side_stream);
+    cudaEventRecord(b.join, ctx->side_stream);
+    for (int k = 0; k < 3; k++) launch_stage(k, a, grids[k], st);
+    cudaStreamWaitEvent(st, b.join, 0);
+    launch_stage(3, a, grids[3], st);
+    if (cudaStreamEndCapture(st, &s.graph) != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaGraphInstantiate(&s.exec, s.graph, 0) != cudaSuccess) return R2G_E_DEVICE;
+    for (int k = 0; k < N_BSTAGES; k++) s.grids[k] = grids[k];
+    s.grids[N_BSTAGES] = tpl_grid;
+    return R2G_OK;
+}
+
+int r2g_grain_validate(const R2gFilmGrainData *fgd, uint32_t seed) {
+    return (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
+            fgd->scaling_shift < 8 || fgd->scaling_shift > 11 || seed > 0xffff)
+               ? R2G_E_INVALID
+               : R2G_OK;
+}
 
 extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ticket) {
-    if (!ctx || (!items && n > 0) || n < 0 || !ticket) return R2G_E_INVALID;
+    if (!ctx || (!items && n > 0) || n < 0 || n > 1023 || !ticket) return R2G_E_INVALID;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return R2G_E_DEVICE;
+    int rc = ensure_state(ctx);
+    if (rc != R2G_OK) return rc;
+    BatchState &b = *ctx->batch;
+    if (!b.cache_loaded) load_cache(b);
+    if (r2g_grain_ready(ctx->device) != R2G_OK) return R2G_E_DEVICE;
+
+    // stage every frame; collect descriptors and grain parameters
+    std::vector<DevFrame> frames(n);
+    std::vector<GrainBatch> grains;
+    int counts[8] = {0};
+    bool any8 = false, any10 = false;
     for (int i = 0; i < n; i++) {
         R2gFrame *f = items[i].frame;
         if (!f) return R2G_E_INVALID;
-        int rc = r2g_prepare(ctx, f, items[i].fp, items[i].side, items[i].inloop_mask, f->desc);
-        if (rc != R2G_OK) return rc;
-        f->staged = true;
-        r2g_launch_pipeline(ctx, f->desc);
-        if (items[i].fgd) {
-            if (items[i].grain_seed > 0xffff) return R2G_E_INVALID;
-            rc = r2g_grain_enqueue(ctx, f, items[i].fgd, items[i].grain_seed);
+        if (items[i].fp || items[i].side) {
+            rc = r2g_prepare(ctx, f, items[i].fp, items[i].side, items[i].inloop_mask, f->desc);
             if (rc != R2G_OK) return rc;
+            f->staged = true;
+        } else if (!f->staged) {
+            ctx->err = "batch item without side-info on a frame that was never staged";
+            return R2G_E_INVALID;
         }
+        frames[i] = f->desc;
+        (f->bd > 8 ? any10 : any8) = true;
+        counts[0] += r2g_deblock_items(f->desc);
+        counts[1] += r2g_cdef_items(f->desc);
+        counts[2] += r2g_lr_items(f->desc);
+        if (items[i].fgd) {
+            if (r2g_grain_validate(items[i].fgd, items[i].grain_seed) != R2G_OK) {
+                ctx->err = "film-grain parameters out of range";
+                return R2G_E_INVALID;
+            }
+            if (!f->grain_scratch) {
+                rc = r2g_dev_alloc(ctx, &f->grain_scratch, R2G_GRAIN_SCRATCH);
+                if (rc != R2G_OK) return rc;
+            }
+            GrainBatch g;
+            memset(&g, 0, sizeof(g));
+            r2g_grain_params(*items[i].fgd, items[i].grain_seed, f->bd, g);
+            g.frame = i;
+            g.lut = (int16_t *)f->grain_scratch;
+            g.scaling = (uint8_t *)f->grain_scratch + 3 * 73 * 82 * 2;
+            int bs = 16 << items[i].fgd->block_size;
+            counts[3] += ((f->w + bs - 1) / bs) * ((f->h + bs - 1) / bs);
+            grains.push_back(g);
+            f->grain_buf = 4;
+        }
+    }
+    counts[4] = (int)grains.size();
+    const int cls = any8 && any10 ? 2 : (any10 ? 1 : 0);
+
+    // slot and capacity
+    Slot &s = b.slot[b.next];
+    b.next ^= 1;
+    if (s.used && cudaEventSynchronize(s.done) != cudaSuccess) return R2G_E_DEVICE;
+    bool fits = n <= s.L.max_frames;
+    for (int k = 0; k < N_BSTAGES; k++) fits = fits && counts[k] <= s.L.max_items[k];
+    if (!fits) {
+        int want_items[N_BSTAGES];
+        for (int k = 0; k < N_BSTAGES; k++)
+            want_items[k] = counts[k] > s.L.max_items[k] ? counts[k] + counts[k] / 2 + 64 : s.L.max_items[k];
+        Layout L = make_layout(n > s.L.max_frames ? n + n / 2 + 4 : s.L.max_frames, want_items);
+        if (s.host) cudaFreeHost(s.host);
+        if (s.dev) r2g_dev_free(ctx, s.dev, s.L.bytes);
+        s.host = nullptr;
+        s.dev = nullptr;
+        if (s.exec) cudaGraphExecDestroy(s.exec);
+        if (s.graph) cudaGraphDestroy(s.graph);
+        s.exec = nullptr;
+        s.graph = nullptr;
+        s.L = Layout();
+        if (cudaMallocHost((void **)&s.host, L.bytes) != cudaSuccess) return R2G_E_OOM;
+        rc = r2g_dev_alloc(ctx, (void **)&s.dev, L.bytes);
+        if (rc != R2G_OK) return rc;
+        s.L = L;
+    }
+    // fill the staging blob
+    memset(s.host, 0, 256);
+    memcpy(s.host, counts, sizeof(counts));
+    memcpy(s.host + s.L.off_frames, frames.data(), sizeof(DevFrame) * n);
+    if (!grains.empty()) memcpy(s.host + s.L.off_grain, grains.data(), sizeof(GrainBatch) * grains.size());
+    {
+        uint32_t *w0 = (uint32_t *)(s.host + s.L.off_work[0]);
+        uint32_t *w1 = (uint32_t *)(s.host + s.L.off_work[1]);
+        uint32_t *w2 = (uint32_t *)(s.host + s.L.off_work[2]);
+        int c0 = 0, c1 = 0, c2 = 0;
+        for (int i = 0; i < n; i++) {
+            uint32_t hi = (uint32_t)i << 22;
+            for (int j = 0, e = r2g_deblock_items(frames[i]); j < e; j++) w0[c0++] = hi | j;
+            for (int j = 0, e = r2g_cdef_items(frames[i]); j < e; j++) w1[c1++] = hi | j;
+            for (int j = 0, e = r2g_lr_items(frames[i]); j < e; j++) w2[c2++] = hi | j;
+        }
+        uint32_t *w3 = (uint32_t *)(s.host + s.L.off_work[3]);
+        int c3 = 0;
+        for (size_t gi = 0; gi < grains.size(); gi++) {
+            const DevFrame &f = frames[grains[gi].frame];
+            int bs = 16 << grains[gi].gp.d.block_size;
+            int e = ((f.w + bs - 1) / bs) * ((f.h + bs - 1) / bs);
+            for (int j = 0; j < e; j++) w3[c3++] = ((uint32_t)gi << 22) | j;
+        }
+    }
+    size_t used = s.L.off_work[N_BSTAGES - 1] + sizeof(uint32_t) * counts[3];
+    if (cudaMemcpyAsync(s.dev, s.host, used, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
+
+    // grid choice (autotuned per bit-depth mix), graph (re)build, launch
+    rc = autotune(ctx, b, s, counts, cls);
+    if (rc != R2G_OK) return rc;
+    int grids[N_BSTAGES];
+    for (int k = 0; k < N_BSTAGES; k++) {
+        int v = b.tuned[cls][k] > 0 ? b.tuned[cls][k] : b.occ[k];
+        b.last[k] = v;
+        grids[k] = v * b.num_sms;
+    }
+    const int tpl_grid = b.num_sms;
+    bool same = s.exec != nullptr && s.grids[N_BSTAGES] == tpl_grid;
+    for (int k = 0; k < N_BSTAGES; k++) same = same && s.grids[k] == grids[k];
+    if (!same) {
+        rc = build_graph(ctx, b, s, grids, tpl_grid);
+        if (rc != R2G_OK) return rc;
+    }
+    if (cudaGraphLaunch(s.exec, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
+    ctx->launches += 5;
+    if (cudaEventRecord(s.done, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
+    s.used = true;
+    for (int i = 0; i < n; i++) {
+        R2gFrame *f = items[i].frame;
+        f->out_buf = f->desc.lr_on ? 3 : (f->desc.cdef_stage_on ? 2 : (f->desc.deblock_on ? 1 : 0));
     }
     if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
     return r2g_ticket_record(ctx, ticket);
+}
+
+extern "C" int r2g_batch_config(R2gCtx *ctx, int32_t *ctas_per_sm, int n) {
+    if (!ctx || !ctas_per_sm) return R2G_E_INVALID;
+    if (!ctx->batch) return 0;
+    for (int k = 0; k < n && k < N_BSTAGES; k++) ctas_per_sm[k] = ctx->batch->last[k];
+    return ctx->batch->num_sms;
 }

@@ -131,18 +131,27 @@ R2G_D uint32_t ccso_score(int diff, int q, uint32_t clf) {
     return 1;
 }
 
-template <typename P>
-__global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
-    __shared__ int16_t ty[TH][TW];      // clamped to the frame (CCSO padding)
-    __shared__ int16_t tc[2][CH][CW];
-    __shared__ int16_t pty[TH][TW];     // INT16_MIN outside the frame (CDEF padding)
-    __shared__ int16_t ptc[2][CH][CW];
-    __shared__ int bins[8][96];
-    __shared__ BlockParams bp[8];
-    __shared__ int s_ccso[3];
+struct CdefSmem {
+    int16_t ty[TH][TW];   // clamped to the frame (CCSO padding)
+    int16_t tc[2][CH][CW];
+    int16_t pty[TH][TW];  // INT16_MIN outside the frame (CDEF padding)
+    int16_t ptc[2][CH][CW];
+    int bins[8][96];
+    BlockParams bp[8];
+    int s_ccso[3];
+};
 
-    const int sbx = blockIdx.x;
-    const int band = blockIdx.y;  // 8-row luma band
+// One 64x8 band of superblock column sbx (the work of one CTA); shared by
+// the per-frame kernel and the batched persistent kernel.
+template <typename P>
+R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
+    auto &ty = sm.ty;
+    auto &tc = sm.tc;
+    auto &pty = sm.pty;
+    auto &ptc = sm.ptc;
+    auto &bins = sm.bins;
+    auto &bp = sm.bp;
+    auto &s_ccso = sm.s_ccso;
     const int gx0 = sbx * 64, gy0 = band * 8;
     const int cx0 = gx0 >> 1, cy0 = gy0 >> 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -397,7 +406,38 @@ __global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
     }
 }
 
+template <typename P>
+__global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
+    __shared__ CdefSmem sm;
+    cdef_band<P>(f, sm, blockIdx.x, blockIdx.y);
+}
+
+// Persistent kernel over a cross-frame work list: item = frame << 22 | band
+// * sb64w + sbx.
+__global__ void __launch_bounds__(256) cdef_batch_kernel(BatchArgs a) {
+    __shared__ CdefSmem sm;
+    const int n = a.count[1];
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const uint32_t it = a.work[1][w];
+        const DevFrame &f = a.frames[it >> 22];
+        const int b = it & 0x3fffff, sb64w = (f.w + 63) >> 6;
+        if (f.bitdepth > 8)
+            cdef_band<uint16_t>(f, sm, b % sb64w, b / sb64w);
+        else
+            cdef_band<uint8_t>(f, sm, b % sb64w, b / sb64w);
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void r2g_batch_launch_cdef(const BatchArgs &a, int grid, cudaStream_t s) { cdef_batch_kernel<<<grid, 256, 0, s>>>(a); }
+int r2g_batch_occupancy_cdef() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cdef_batch_kernel, 256, 0);
+    return nb;
+}
+int r2g_cdef_items(const DevFrame &f) { return f.cdef_stage_on ? ((f.w + 63) >> 6) * (f.h >> 3) : 0; }
 
 int r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
     if (!f.cdef_stage_on) return 0;

@@ -419,7 +419,34 @@ __global__ void __launch_bounds__(256, 4) deblock_tile_kernel(const DevFrame f) 
     deblock_tile<P>(f, sm, blockIdx.x, blockIdx.y);
 }
 
+// Persistent kernel over a cross-frame work list: item = frame << 22 | ty *
+// tiles_w + tx.
+__global__ void __launch_bounds__(256, 4) deblock_batch_kernel(BatchArgs a) {
+    __shared__ DeblockSmem sm;
+    const int n = a.count[0];
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const uint32_t it = a.work[0][w];
+        const DevFrame &f = a.frames[it >> 22];
+        const int b = it & 0x3fffff, tw = (f.w + 63) >> 6;
+        if (f.bitdepth > 8)
+            deblock_tile<uint16_t>(f, sm, b % tw, b / tw);
+        else
+            deblock_tile<uint8_t>(f, sm, b % tw, b / tw);
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void r2g_batch_launch_deblock(const BatchArgs &a, int grid, cudaStream_t s) {
+    deblock_batch_kernel<<<grid, 256, 0, s>>>(a);
+}
+int r2g_batch_occupancy_deblock() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, deblock_batch_kernel, 256, 0);
+    return nb;
+}
+int r2g_deblock_items(const DevFrame &f) { return f.deblock_on ? ((f.w + 63) >> 6) * ((f.h + 63) >> 6) : 0; }
 
 int r2g_launch_deblock(const DevFrame &f, cudaStream_t s) {
     if (!f.deblock_on) return 0;

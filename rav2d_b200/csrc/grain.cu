@@ -50,19 +50,17 @@ R2G_D uint32_t lfsr_jump(uint32_t s, uint32_t k) {
 
 R2G_D int round2(int x, int shift) { return (x + ((1 << shift) >> 1)) >> shift; }
 
-struct GrainParams {
-    R2gFilmGrainData d;
-    uint32_t seed;
-    int bitdepth;
-    int has_y, has_u, has_v;  // which planes are grained
-};
-
 // Templates: luma 73x82, chroma 38x44 (stored in 73x82 arrays as the
 // reference's GrainLut does); scaling LUTs per plane (1 << bitdepth).
-__global__ void __launch_bounds__(256) grain_template_kernel(const GrainParams gp, const DevTables tab,
-                                                             int16_t *lut, uint8_t *scaling) {
-    __shared__ int16_t ly[GH][GW];
-    __shared__ int16_t lc[2][SGH][SGW];
+struct GrainTplSmem {
+    int16_t ly[GH][GW];
+    int16_t lc[2][SGH][SGW];
+};
+
+R2G_D void grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling,
+                          GrainTplSmem &sm) {
+    auto &ly = sm.ly;
+    auto &lc = sm.lc;
     const int tid = threadIdx.x;
     const R2gFilmGrainData &d = gp.d;
     const int b8 = gp.bitdepth - 8;
@@ -182,6 +180,12 @@ __global__ void __launch_bounds__(256) grain_template_kernel(const GrainParams g
     }
 }
 
+__global__ void __launch_bounds__(256) grain_template_kernel(const GrainParams gp, const DevTables tab,
+                                                             int16_t *lut, uint8_t *scaling) {
+    __shared__ GrainTplSmem sm;
+    grain_template(gp, tab, lut, scaling, sm);
+}
+
 // Offsets of block b for row band `row` and seed index i (filmgrain.rs:
 // 274-305): draws 8b + 4n + 1 of the band's seed.
 R2G_D int block_offset(uint32_t in_seed, int row, int i, int b, int n, int block_size) {
@@ -195,13 +199,11 @@ R2G_D int block_offset(uint32_t in_seed, int row, int i, int b, int n, int block
 // One CTA per (row band, 32-px block): luma 32x32 (or the frame remainder)
 // and both chroma 16x16 blocks.
 template <typename P>
-__global__ void __launch_bounds__(256) grain_apply_kernel(const DevFrame f, const GrainParams gp, const int16_t *lut,
-                                                          const uint8_t *scaling) {
-    __shared__ int off[2][2][2];  // [cur/prev block][seed i][n]
+R2G_D void grain_block(const DevFrame &f, const GrainParams &gp, const int16_t *lut, const uint8_t *scaling, int row,
+                       int b, int (&off)[2][2][2]) {
     const int tid = threadIdx.x;
     const R2gFilmGrainData &d = gp.d;
     const int bs = 16 << d.block_size;
-    const int row = blockIdx.y, b = blockIdx.x;
     const int rows = 1 + (d.overlap_flag && row > 0);
     if (tid < 8) {
         int which = tid >> 2, i = (tid >> 1) & 1, n = tid & 1;
@@ -329,9 +331,56 @@ __global__ void __launch_bounds__(256) grain_apply_kernel(const DevFrame f, cons
     }
 }
 
+template <typename P>
+__global__ void __launch_bounds__(256) grain_apply_kernel(const DevFrame f, const GrainParams gp, const int16_t *lut,
+                                                          const uint8_t *scaling) {
+    __shared__ int off[2][2][2];  // [cur/prev block][seed i][n]
+    grain_block<P>(f, gp, lut, scaling, blockIdx.y, blockIdx.x, off);
+}
+
+// Persistent kernels of the batched path: one template set per grained
+// frame, then the apply over (grained frame << 22 | row * blocks_w + block).
+__global__ void __launch_bounds__(256) grain_template_batch_kernel(BatchArgs a) {
+    __shared__ GrainTplSmem sm;
+    const int n = a.count[4];
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const GrainBatch &g = a.grain[i];
+        if (g.any) grain_template(g.gp, a.frames[g.frame].tab, g.lut, g.scaling, sm);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) grain_apply_batch_kernel(BatchArgs a) {
+    __shared__ int off[2][2][2];
+    const int n = a.count[3];
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const uint32_t it = a.work[3][w];
+        const GrainBatch &g = a.grain[it >> 22];
+        const DevFrame &f = a.frames[g.frame];
+        const int b = it & 0x3fffff, bs = 16 << g.gp.d.block_size, bw = (f.w + bs - 1) / bs;
+        if (f.bitdepth > 8)
+            grain_block<uint16_t>(f, g.gp, g.lut, g.scaling, b / bw, b % bw, off);
+        else
+            grain_block<uint8_t>(f, g.gp, g.lut, g.scaling, b / bw, b % bw, off);
+        __syncthreads();
+    }
+}
+
 bool g_pow_ready[64] = {false};
 
 }  // namespace
+
+void r2g_batch_launch_grain_template(const BatchArgs &a, int grid, cudaStream_t s) {
+    grain_template_batch_kernel<<<grid, 256, 0, s>>>(a);
+}
+void r2g_batch_launch_grain_apply(const BatchArgs &a, int grid, cudaStream_t s) {
+    grain_apply_batch_kernel<<<grid, 256, 0, s>>>(a);
+}
+int r2g_batch_occupancy_grain_apply() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, grain_apply_batch_kernel, 256, 0);
+    return nb;
+}
 
 // Per-context grain scratch: templates (3 x 73 x 82 int16) + scaling LUTs.
 struct GrainCtx {
@@ -379,6 +428,17 @@ static void grain_planes(const R2gFilmGrainData &d, int &has_y, int &has_u, int 
     has_u = any && (d.num_points[1] > 0 || d.chroma_scaling_from_luma) && (!d.chroma_scaling_from_luma || luma_lut);
     has_v = any && (d.num_points[2] > 0 || d.chroma_scaling_from_luma) && (!d.chroma_scaling_from_luma || luma_lut);
 }
+
+void r2g_grain_params(const R2gFilmGrainData &fgd, uint32_t seed, int bitdepth, GrainBatch &g) {
+    g.gp.d = fgd;
+    g.gp.seed = seed;
+    g.gp.bitdepth = bitdepth;
+    bool any;
+    grain_planes(fgd, g.gp.has_y, g.gp.has_u, g.gp.has_v, any);
+    g.any = any;
+}
+
+int r2g_grain_ready(int device) { return init_lfsr_pow(device) == cudaSuccess ? R2G_OK : R2G_E_DEVICE; }
 
 int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed) {
     if (init_lfsr_pow(ctx->device) != cudaSuccess) return R2G_E_DEVICE;

@@ -156,11 +156,13 @@ struct LrSmem {
     uint16_t llm[17];
 };
 
+// One (plane, stripe, 64-wide unit) work item; b is the per-frame item index:
+// luma items first (sby, sub-stripe, unit), then U, then V.
 template <typename P>
-__global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_units, int nux_l, int nux_c) {
-    __shared__ LrSmem sm;
+R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int b = blockIdx.x;
+    const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
+    const int n_luma_units = f.sbh * 2 * nux_l;
     int plane, sby, sub, ux;
     if (b < n_luma_units) {
         plane = 0;
@@ -569,16 +571,47 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f, int n_luma_un
         }
 }
 
+template <typename P>
+__global__ void __launch_bounds__(256) lr_kernel(const DevFrame f) {
+    __shared__ LrSmem sm;
+    lr_unit<P>(f, sm, blockIdx.x);
+}
+
+// Persistent kernel over a cross-frame work list: item = frame << 22 |
+// per-frame item index.
+__global__ void __launch_bounds__(256, 3) lr_batch_kernel(BatchArgs a) {
+    __shared__ LrSmem sm;
+    const int n = a.count[2];
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const uint32_t it = a.work[2][w];
+        const DevFrame &f = a.frames[it >> 22];
+        if (f.bitdepth > 8)
+            lr_unit<uint16_t>(f, sm, it & 0x3fffff);
+        else
+            lr_unit<uint8_t>(f, sm, it & 0x3fffff);
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s) { lr_batch_kernel<<<grid, 256, 0, s>>>(a); }
+int r2g_batch_occupancy_lr() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lr_batch_kernel, 256, 0);
+    return nb;
+}
+int r2g_lr_items(const DevFrame &f) {
+    if (!f.lr_on) return 0;
+    return f.sbh * 2 * ((f.w + 63) >> 6) + 2 * f.sbh * 2 * ((f.cw + 63) >> 6);
+}
 
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     if (!f.lr_on) return 0;
-    int nux_l = (f.w + 63) / 64, nux_c = (f.cw + 63) / 64;
-    int n_luma = f.sbh * 2 * nux_l;
-    int n = n_luma + 2 * f.sbh * 2 * nux_c;
+    int n = r2g_lr_items(f);
     if (f.bitdepth > 8)
-        lr_kernel<uint16_t><<<n, 256, 0, s>>>(f, n_luma, nux_l, nux_c);
+        lr_kernel<uint16_t><<<n, 256, 0, s>>>(f);
     else
-        lr_kernel<uint8_t><<<n, 256, 0, s>>>(f, n_luma, nux_l, nux_c);
+        lr_kernel<uint8_t><<<n, 256, 0, s>>>(f);
     return 1;
 }

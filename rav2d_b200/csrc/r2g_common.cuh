@@ -68,6 +68,50 @@ R2G_D P *plane_ptr(void *base) {
 }
 
 // Launch helpers implemented per stage (deblock.cu, cdef.cu, lr.cu, grain.cu).
+// Arguments of the batched persistent kernels: a device array of frame
+// descriptors, per-stage work lists (item = frame index << 22 | per-frame
+// item index) and the per-stage item counts in device memory, so one CUDA
+// graph serves every batch.  Stages: 0 deblock, 1 CDEF+CCSO, 2 loop
+// restoration, 3 film-grain apply.
+// Film-grain parameters of one frame (R2gFilmGrainData + seed + the planes
+// the reference grains, decode.rs:4641 / filmgrain.rs:688-830).
+struct GrainParams {
+    R2gFilmGrainData d;
+    uint32_t seed;
+    int bitdepth;
+    int has_y, has_u, has_v;
+};
+// One grained frame of a batch: its parameters, its frame index in the
+// batch and its template / scaling-LUT scratch.
+struct GrainBatch {
+    GrainParams gp;
+    int frame;
+    int any;  // some plane is grained: the templates must be generated
+    int16_t *lut;
+    uint8_t *scaling;
+};
+struct BatchArgs {
+    const DevFrame *frames;
+    const uint32_t *work[4];
+    const int *count;  // [0..3] items per stage, [4] grained frames
+    const GrainBatch *grain;
+};
+void r2g_batch_launch_grain_template(const BatchArgs &a, int grid, cudaStream_t s);
+void r2g_batch_launch_grain_apply(const BatchArgs &a, int grid, cudaStream_t s);
+int r2g_batch_occupancy_grain_apply();
+// Sets the grain fields of a GrainBatch from the frame's parameters.
+void r2g_grain_params(const R2gFilmGrainData &fgd, uint32_t seed, int bitdepth, GrainBatch &g);
+void r2g_batch_launch_deblock(const BatchArgs &a, int grid, cudaStream_t s);
+void r2g_batch_launch_cdef(const BatchArgs &a, int grid, cudaStream_t s);
+void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s);
+int r2g_batch_occupancy_deblock();
+int r2g_batch_occupancy_cdef();
+int r2g_batch_occupancy_lr();
+// Work-item counts of one frame per stage (0 when the stage is off).
+int r2g_deblock_items(const DevFrame &f);
+int r2g_cdef_items(const DevFrame &f);
+int r2g_lr_items(const DevFrame &f);
+
 // Each returns the number of kernels it launched.
 int r2g_launch_deblock(const DevFrame &f, cudaStream_t s);
 int r2g_launch_cdef(const DevFrame &f, cudaStream_t s);

@@ -12,7 +12,12 @@ struct Ticket {
     cudaEvent_t ev;
 };
 
-struct GrainCtx;  // grain.cu
+struct GrainCtx;    // grain.cu
+struct BatchState;  // batch.cu
+
+// Per-frame film-grain scratch of the batched path: three 82x73 templates and
+// three 1024-entry scaling LUTs.
+#define R2G_GRAIN_SCRATCH (3 * 73 * 82 * 2 + 3 * 1024)
 
 enum { R2G_N_STAGES = 4 };
 
@@ -32,6 +37,7 @@ struct R2gCtx {
     std::vector<Ticket> tickets;
     uint64_t next_ticket = 0;
     GrainCtx *grain = nullptr;
+    BatchState *batch = nullptr;
     cudaStream_t own_stream = nullptr;
     int64_t launches = 0;
     bool profiling = false;
@@ -57,6 +63,7 @@ struct R2gFrame {
     size_t seg_bytes = 0;
     int out_buf = -1, grain_buf = -1;
     bool staged = false;
+    void *grain_scratch = nullptr;  // batched film grain (R2G_GRAIN_SCRATCH)
     DevFrame desc{};
 };
 
@@ -69,3 +76,4 @@ void r2g_launch_pipeline(R2gCtx *ctx, const DevFrame &d);
 void r2g_prof_stage(R2gCtx *ctx, int stage, bool begin, int launches);
 int r2g_ticket_record(R2gCtx *ctx, uint64_t *ticket);
 void r2g_grain_ctx_free(R2gCtx *ctx);
+void r2g_batch_free(R2gCtx *ctx);

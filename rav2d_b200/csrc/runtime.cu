@@ -94,6 +94,7 @@ extern "C" int r2g_ctx_destroy(R2gCtx *ctx) {
     for (auto &t : ctx->tickets) cudaEventDestroy(t.ev);
     ctx->tickets.clear();
     r2g_grain_ctx_free(ctx);
+    r2g_batch_free(ctx);
     r2g_ctx_profile(ctx, 0);
     cudaStreamDestroy(ctx->own_stream ? ctx->own_stream : ctx->stream);
     cudaStreamDestroy(ctx->side_stream);
@@ -173,6 +174,7 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     for (int i = 0; i < 5; i++) r2g_dev_free(ctx, f->buf[i], f->buf_bytes);
     r2g_dev_free(ctx, f->side_dev, f->side_bytes);
     r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
+    r2g_dev_free(ctx, f->grain_scratch, R2G_GRAIN_SCRATCH);
     if (f->side_host) cudaFreeHost(f->side_host);
     if (f->seg_host) cudaFreeHost(f->seg_host);
     if (f->side_done) cudaEventDestroy(f->side_done);

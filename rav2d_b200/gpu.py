@@ -21,7 +21,7 @@ SYMBOLS = [
     "r2g_last_error", "r2g_frame_alloc", "r2g_frame_free", "r2g_frame_upload_recon", "r2g_frame_filter",
     "r2g_frame_grain", "r2g_download", "r2g_sync", "r2g_filter_frame_host", "r2g_batch_submit", "r2g_wait",
     "r2g_frame_stage", "r2g_frame_run", "r2g_ctx_set_stream", "r2g_ctx_profile", "r2g_ctx_profile_read",
-    "r2g_ctx_launch_count",
+    "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config",
 ]
 
 
@@ -63,6 +63,7 @@ def lib():
         L.r2g_ctx_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
         L.r2g_ctx_launch_count.argtypes = [C.c_void_p]
         L.r2g_ctx_launch_count.restype = C.c_int64
+        L.r2g_batch_config.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int]
         _lib = L
     return _lib
 
@@ -121,17 +122,19 @@ class Context:
     def frame(self, width, height, bitdepth):
         return Frame(self, width, height, bitdepth)
 
-    def batch_submit(self, items):
-        """items: list of (Frame, SynthFrame-like with fp/side()/inloop/fgd/grain_seed)."""
+    def batch_submit(self, items, staged=False):
+        """items: list of (Frame, SynthFrame-like with fp/side()/inloop/fgd/grain_seed).
+        staged=True runs every frame with its last Frame.stage() side-info."""
         arr = (abi.BatchItem * len(items))()
         keep = []
         for i, (fr, sf) in enumerate(items):
-            side = sf.side()
-            keep.append(side)
             arr[i].frame = fr.h
-            arr[i].fp = C.pointer(sf.fp)
-            arr[i].side = C.pointer(side)
-            arr[i].inloop_mask = sf.inloop
+            if not staged:
+                side = sf.side()
+                keep.append(side)
+                arr[i].fp = C.pointer(sf.fp)
+                arr[i].side = C.pointer(side)
+                arr[i].inloop_mask = sf.inloop
             arr[i].fgd = C.pointer(sf.fgd) if sf.fgd is not None else None
             arr[i].grain_seed = sf.grain_seed
         t = C.c_uint64()
@@ -140,6 +143,12 @@ class Context:
 
     def wait(self, ticket, timeout_ms=-1):
         return lib().r2g_wait(self.h, C.c_uint64(ticket), timeout_ms)
+
+    def batch_config(self):
+        """(SM count, CTAs per SM of the last batch per stage)."""
+        v = (C.c_int32 * 4)()
+        sms = lib().r2g_batch_config(self.h, v, 4)
+        return sms, dict(zip(("deblock", "cdef_ccso", "loop_restoration", "film_grain"), list(v)))
 
 
 class Frame:
