@@ -37,9 +37,16 @@ sys.path.insert(0, ROOT)
 W_, H_, BD_ = 1920, 1080, 10
 SEED = 0x5EED0001
 MPIX = W_ * H_ / 1e6
-# algorithmic HBM bytes per luma pixel at 10-bit (read each input sample once,
-# write each output sample once; 4:2:0 = 1.5 samples / px, 2 B / sample)
-BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film_grain": 8.0}
+# algorithmic HBM bytes per luma pixel at 10-bit: each stage reads its input
+# frame once and writes its output frame once (4:2:0 = 1.5 samples / px,
+# 2 B / sample: 3 B read + 3 B written); loop restoration's deblocked stripe
+# boundary rows (2 of every 64 rows) and film grain's templates are <2 % and
+# not counted
+BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 6.0, "film_grain": 6.0}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload,
+# from `ncu --set full` (profiles/stages_full_1080p10.md); the outputs were
+# still in L2 when the capture ended, so the write term was 0
+NCU_TRAFFIC = {"deblock": 6605568, "cdef_ccso": 6272768, "loop_restoration": 6915584}
 
 
 def log(*a):
@@ -219,11 +226,96 @@ def run_ours(args, rank, world, device):
 
     for fr in frames:
         fr.free()
+    batch = run_batched(args, ctx, stream, device) if args.batch_steps > 0 else None
     ctx.close()
     return {
+        "batched": batch,
         "ms": ms_max, "launches": launches, "prof": prof, "nprof": nprof, "e2e_ms": e2e_ms_max, "n_e2e": n_e2e,
         "clocks": clk.summary(),
         "h2d": recon_bytes + side_bytes, "d2h": recon_bytes,
+    }
+
+
+MIX_RES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+
+
+def make_mix(n=64, seed=0x5EED0003):
+    """The batching workload: n frames, resolution drawn from MIX_RES, bit
+    depth from {8, 10}, film grain on for a random half; full filter chain.
+    Frames of the same (resolution, bit depth, grain) class share one seeded
+    synthetic recon + side-info (the GPU does the same work either way)."""
+    from rav2d_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    specs = [(MIX_RES[rng.integers(len(MIX_RES))], int(rng.choice([8, 10])), bool(rng.integers(2))) for _ in range(n)]
+    cache = {}
+    out = []
+    for wh, bd, g in specs:
+        k = (wh, bd, g)
+        if k not in cache:
+            cache[k] = synth.make_frame(wh[0], wh[1], bd, seed + 0x100 + len(cache), chain="full", grain=g)
+        out.append(cache[k])
+    return out
+
+
+def run_batched(args, ctx, stream, device):
+    """64-frame mixed workload: one batch (one persistent launch per stage,
+    CUDA graph) per step vs the per-frame pipeline over the same frames."""
+    import torch
+
+    sfs = make_mix()
+    frames = []
+    for sf in sfs:
+        fr = ctx.frame(sf.width, sf.height, sf.bitdepth)
+        fr.upload(sf.planes)
+        fr.stage(sf)
+        frames.append(fr)
+    ctx.sync()
+    mpix = sum(sf.width * sf.height for sf in sfs) / 1e6
+    items = list(zip(frames, sfs))
+
+    def per_frame():
+        for fr, sf in items:
+            fr.run()
+            if sf.fgd is not None:
+                fr.grain(sf.fgd, sf.grain_seed)
+
+    def batched():
+        ctx.batch_submit(items, staged=True)
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        l0 = ctx.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, (ctx.launch_count() - l0) / reps
+
+    reps = max(3, min(args.batch_steps, args.steps))
+    pf_ms, pf_l = timed(per_frame, reps)
+    b_ms, b_l = timed(batched, reps)
+    sms, cfg = ctx.batch_config()
+    for fr in frames:
+        fr.free()
+    mix = {}
+    for sf in sfs:
+        k = f"{sf.width}x{sf.height}/{sf.bitdepth}bit{'+grain' if sf.fgd is not None else ''}"
+        mix[k] = mix.get(k, 0) + 1
+    return {
+        "workload": "64 frames/batch, resolutions {640x360,1280x720,1920x1080,3840x2160} x {8,10}-bit, "
+                    "full chain, film grain on a random half", "mix": mix,
+        "mpix_per_batch": round(mpix, 3), "steps": reps,
+        "value": round(mpix / b_ms * 1e3, 2), "unit": "Mpix/s", "ms_per_batch": round(b_ms, 4),
+        "launches_per_batch": b_l,
+        "per_frame_value": round(mpix / pf_ms * 1e3, 2), "per_frame_ms": round(pf_ms, 4),
+        "per_frame_launches": pf_l,
+        "speedup_vs_per_frame": round(pf_ms / b_ms, 3), "ctas_per_sm": cfg, "sms": sms,
+        "l2": f"inputs larger than L2: {round(mpix * 1.5 * 1.5, 0)} MB of recon per batch",
     }
 
 
@@ -262,6 +354,7 @@ def main():
     ap.add_argument("--ring", type=int, default=48)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--batch-steps", type=int, default=30, help="timed batches of the 64-frame mix (0 = skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -326,7 +419,8 @@ def main():
                 "d2h_bytes_per_step": res["d2h"], "steps": res["n_e2e"],
                 "path": "r2g_frame_upload_recon + r2g_frame_stage + r2g_frame_run + r2g_download, pinned host"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": NCU_TRAFFIC.get(dom),
+                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum, one launch",
                      "bytes_per_launch": int(BYTES_PER_PX[dom] * W_ * H_),
                      "avg_launch_us": round(avg_launch_s * 1e6, 2)},
         "stages_us_per_frame": {k: round(v[0] / max(1, res["nprof"]) * 1e3, 2) for k, v in prof.items() if v[1]},
@@ -334,6 +428,7 @@ def main():
                          "sample": f"{cpu_n} whole 1080p 10-bit frames through the oracle (C++ restatement of the "
                                    f"reference scalar Rust filter path) on 1 host core in {cpu_dt:.1f} s"},
         "clocks": res["clocks"], "gpu_launches": res["launches"],
+        "batched": res["batched"],
     }
     print(json.dumps(line), flush=True)
 
