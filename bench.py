@@ -319,6 +319,85 @@ def run_batched(args, ctx, stream, device):
     }
 
 
+def run_serving(args, device):
+    """32 streams, resolutions 360p..4K, 8/10-bit, film grain on half the
+    streams; each stream's frames arrive as a Poisson process at 30 fps and
+    go through the continuous-batching server (40 GB device budget, pinned
+    host buffers).  A warm-up second fills the streams' resident frames and
+    the autotuner cache, then the statistics are reset and the measured
+    window runs for --serve-seconds."""
+    import heapq
+
+    import torch
+
+    from rav2d_b200 import gpu, synth
+
+    rng = np.random.default_rng(0x5EED0004)
+    n_streams, fps = 32, 30.0
+    specs = [(MIX_RES[k % len(MIX_RES)], 8 + 2 * ((k // len(MIX_RES)) % 2), k % 2 == 0) for k in range(n_streams)]
+    cache = {}
+    for wh, bd, g in specs:
+        if (wh, bd, g) not in cache:
+            sf = synth.make_frame(wh[0], wh[1], bd, 0x5EED2000 + len(cache), chain="full", grain=g)
+            cache[(wh, bd, g)] = (sf, [a for _, a in pinned_like(sf.planes)])
+    outs = [[[a for _, a in pinned_like(cache[sp][0].planes)] for _ in range(4)] for sp in specs]
+    ctx = gpu.Context(device)
+    srv = gpu.Server(ctx, mem_budget=40 << 30, max_batch=64)
+    results = []
+    lock = threading.Lock()
+
+    def drive(seconds):
+        heap = [(rng.exponential(1.0 / fps), k) for k in range(n_streams)]
+        heapq.heapify(heap)
+        t0 = time.perf_counter()
+        ids = []
+        cnt = [0] * n_streams
+        while True:
+            t, k = heapq.heappop(heap)
+            if t > seconds:
+                break
+            dt = t0 + t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            sf, src = cache[specs[k]]
+            ids.append(srv.submit(k, sf, src, outs[k][cnt[k] % 4]))
+            cnt[k] += 1
+            heapq.heappush(heap, (t + rng.exponential(1.0 / fps), k))
+        return ids
+
+    def collect(ids):
+        for rid in ids:
+            rc, res = srv.wait(rid, 60000)
+            with lock:
+                results.append((rc, res.status, res.latency_us, res.batch_frames))
+
+    collect(drive(1.0))
+    srv.stats(reset=True)
+    results.clear()
+    with ClockSampler(device) as clk:
+        ids = drive(args.serve_seconds)
+        collect(ids)
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    torch.cuda.synchronize()
+    offered = sum(w * h for (w, h), _, _ in specs) * fps / 1e6
+    ok = [r for r in results if r[0] == 0 and r[1] == 0]
+    return {
+        "workload": "32 streams x 30 fps Poisson arrivals, 360p/720p/1080p/4K x 8/10-bit, full chain, film grain "
+                    "on half the streams, 40 GB device budget, continuous batching (<=64 frames/batch)",
+        "seconds": args.serve_seconds, "frames": len(results), "ok": len(ok),
+        "offered_mpix_s": round(offered, 1),
+        "value": round(st["mpix"] / st["span_s"], 1) if st["span_s"] else None, "unit": "Mpix/s",
+        "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3),
+        "mean_ms": round(st["mean_us"] / 1e3, 3), "max_ms": round(st["max_us"] / 1e3, 3),
+        "batches": st["batches"], "mean_batch": round(st["mean_batch"], 2),
+        "resident_gb": round(st["resident_bytes"] / 2 ** 30, 2), "evictions": st["evictions"],
+        "latency": "submit -> display frame in pinned host memory (upload, filter, grain, download)",
+        "clocks": clk.summary(),
+    }
+
+
 def cpu_baseline(seconds=12.0, threads=1):
     """The oracle on `threads` host threads, one frame per thread, for about
     `seconds`; returns (Mpix/s, frames, seconds)."""
@@ -355,6 +434,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-steps", type=int, default=30, help="timed batches of the 64-frame mix (0 = skip)")
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="measured serving window (0 = skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -395,6 +475,7 @@ def main():
         torch.distributed.init_process_group("nccl", init_method="env://",
                                              timeout=__import__("datetime").timedelta(seconds=120))
     res = run_ours(args, rank, world, local)
+    res["serving"] = run_serving(args, local) if args.serve_seconds > 0 and rank == 0 else None
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank != 0:
@@ -428,7 +509,7 @@ def main():
                          "sample": f"{cpu_n} whole 1080p 10-bit frames through the oracle (C++ restatement of the "
                                    f"reference scalar Rust filter path) on 1 host core in {cpu_dt:.1f} s"},
         "clocks": res["clocks"], "gpu_launches": res["launches"],
-        "batched": res["batched"],
+        "batched": res["batched"], "serving": res["serving"],
     }
     print(json.dumps(line), flush=True)
 

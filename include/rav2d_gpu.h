@@ -279,6 +279,64 @@ int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ti
 /* Wait for a ticket; R2G_E_TIMEOUT after timeout_ms (<0 = forever),
  * timeout_ms == 0 polls (R2G_E_NOTREADY when pending). */
 int r2g_wait(R2gCtx *ctx, uint64_t ticket, int timeout_ms);
+/* ---- serving: continuous batching over many concurrent streams ----
+ * No counterpart in the reference (its decoder filters one frame at a time
+ * inside Decoder::decode_frame, decode.rs:3597-3625).  A server owns one
+ * worker thread that admits queued frames under a device-memory budget,
+ * keeps each stream's frame buffers and side-info resident on the device,
+ * and issues every admitted frame in the next batch while earlier batches
+ * run (uploads, kernels and downloads of consecutive batches overlap).
+ * While a server is attached, drive its context only through the server. */
+typedef struct R2gServer R2gServer;
+typedef struct R2gServeConfig {
+    int64_t mem_budget;        /* bytes for resident frames; 0 = the context budget (or none) */
+    int32_t max_batch;         /* frames per batch, 1..1023 (0 = 64) */
+    int32_t frames_per_stream; /* resident device frames per stream (0 = 2) */
+} R2gServeConfig;
+typedef struct R2gServeRequest {
+    int32_t stream_id;
+    const R2gFrameParams *fp; /* copied at submit */
+    const R2gSideInfo *side;  /* the records it points to stay valid until r2g_server_wait */
+    uint32_t inloop_mask;
+    const R2gFilmGrainData *fgd; /* NULL = no grain; copied at submit */
+    uint32_t grain_seed;
+    /* recon planes (host; pinned memory lets the upload overlap compute) */
+    const void *src_y, *src_u, *src_v;
+    int64_t src_y_stride, src_uv_stride; /* bytes */
+    /* display output (grained when fgd, else filtered) */
+    void *dst_y, *dst_u, *dst_v;
+    int64_t dst_y_stride, dst_uv_stride; /* bytes; also used for ref_* */
+    /* optional: the filtered (reference) frame as well; NULL = skip */
+    void *ref_y, *ref_u, *ref_v;
+} R2gServeRequest;
+typedef struct R2gServeResult {
+    int32_t status;       /* R2G_OK, or the error that failed this frame */
+    int32_t batch_frames; /* frames in the batch it ran in */
+    double queue_us;      /* submit -> issued */
+    double latency_us;    /* submit -> output in host memory */
+} R2gServeResult;
+typedef struct R2gServeStats {
+    int64_t completed, failed, batches;
+    double mean_batch, mpix;
+    double p50_us, p99_us, mean_us, max_us;
+    double span_s;  /* first submit -> last completion */
+    double issue_s; /* worker time spent enqueuing */
+    int64_t evictions, resident_bytes, pending;
+} R2gServeStats;
+int r2g_server_create(R2gCtx *ctx, const R2gServeConfig *cfg, R2gServer **out);
+/* Queue one frame; any thread.  Returns its id for r2g_server_wait. */
+int r2g_server_submit(R2gServer *s, const R2gServeRequest *req, uint64_t *id);
+/* Wait for a frame (timeout_ms < 0: forever; 0: poll -> R2G_E_NOTREADY;
+ * R2G_E_TIMEOUT when it runs out).  On R2G_OK `res` holds the frame's own
+ * status and the id is released. */
+int r2g_server_wait(R2gServer *s, uint64_t id, int timeout_ms, R2gServeResult *res);
+/* Free a stream's resident frames once its queued frames have completed. */
+int r2g_server_close_stream(R2gServer *s, int32_t stream_id);
+/* Latency / throughput statistics since creation or the last reset. */
+int r2g_server_stats(R2gServer *s, R2gServeStats *st, int reset);
+/* Completes every queued frame, then stops the worker and frees all. */
+int r2g_server_destroy(R2gServer *s);
+
 /* Instrumentation (no counterpart in the reference): the CTAs per SM the
  * last batch used for stages 0 deblock, 1 CDEF+CCSO, 2 loop restoration,
  * 3 film grain (autotuned); returns the SM count. */

@@ -158,6 +158,41 @@ class BatchItem(C.Structure):
     ]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [("mem_budget", C.c_int64), ("max_batch", C.c_int32), ("frames_per_stream", C.c_int32)]
+
+
+class ServeRequest(C.Structure):
+    _fields_ = [
+        ("stream_id", C.c_int32),
+        ("fp", C.POINTER(FrameParams)),
+        ("side", C.POINTER(SideInfo)),
+        ("inloop_mask", C.c_uint32),
+        ("fgd", C.POINTER(FilmGrainData)),
+        ("grain_seed", C.c_uint32),
+        ("src_y", C.c_void_p), ("src_u", C.c_void_p), ("src_v", C.c_void_p),
+        ("src_y_stride", C.c_int64), ("src_uv_stride", C.c_int64),
+        ("dst_y", C.c_void_p), ("dst_u", C.c_void_p), ("dst_v", C.c_void_p),
+        ("dst_y_stride", C.c_int64), ("dst_uv_stride", C.c_int64),
+        ("ref_y", C.c_void_p), ("ref_u", C.c_void_p), ("ref_v", C.c_void_p),
+    ]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batch_frames", C.c_int32), ("queue_us", C.c_double),
+                ("latency_us", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_int64), ("failed", C.c_int64), ("batches", C.c_int64),
+        ("mean_batch", C.c_double), ("mpix", C.c_double),
+        ("p50_us", C.c_double), ("p99_us", C.c_double), ("mean_us", C.c_double), ("max_us", C.c_double),
+        ("span_s", C.c_double), ("issue_s", C.c_double),
+        ("evictions", C.c_int64), ("resident_bytes", C.c_int64), ("pending", C.c_int64),
+    ]
+
+
 # order of r2g_struct_sizes()
 STRUCT_SIZES = [
     ("R2gAv2Filter", AV2_FILTER_DTYPE.itemsize),
@@ -167,6 +202,10 @@ STRUCT_SIZES = [
     ("R2gFilmGrainData", C.sizeof(FilmGrainData)),
     ("R2gSideInfo", C.sizeof(SideInfo)),
     ("R2gBatchItem", C.sizeof(BatchItem)),
+    ("R2gServeConfig", C.sizeof(ServeConfig)),
+    ("R2gServeRequest", C.sizeof(ServeRequest)),
+    ("R2gServeResult", C.sizeof(ServeResult)),
+    ("R2gServeStats", C.sizeof(ServeStats)),
 ]
 
 

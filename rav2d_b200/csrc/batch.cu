@@ -81,7 +81,7 @@ struct BatchState {
     int last[N_BSTAGES] = {0, 0, 0, 0};
     bool cache_loaded = false;
     std::string dev_name;
-    cudaEvent_t fork = nullptr, join = nullptr, t0 = nullptr, t1 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, copied = nullptr, t0 = nullptr, t1 = nullptr;
 };
 
 static std::string cache_path() {
@@ -147,7 +147,7 @@ void r2g_batch_free(R2gCtx *ctx) {
         if (s.dev) r2g_dev_free(ctx, s.dev, s.L.bytes);
         if (s.done) cudaEventDestroy(s.done);
     }
-    for (cudaEvent_t e : {b->fork, b->join, b->t0, b->t1})
+    for (cudaEvent_t e : {b->fork, b->join, b->copied, b->t0, b->t1})
         if (e) cudaEventDestroy(e);
     delete b;
     ctx->batch = nullptr;
@@ -167,7 +167,7 @@ static int ensure_state(R2gCtx *ctx) {
     b->occ[3] = r2g_batch_occupancy_grain_apply();
     for (int k = 0; k < N_BSTAGES; k++)
         if (b->occ[k] < 1) b->occ[k] = 1;
-    for (cudaEvent_t *e : {&b->fork, &b->join})
+    for (cudaEvent_t *e : {&b->fork, &b->join, &b->copied})
         if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return R2G_E_DEVICE;
     if (cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) return R2G_E_DEVICE;
     for (auto &s : b->slot)
@@ -243,8 +243,8 @@ int r2g_grain_validate(const R2gFilmGrainData *fgd, uint32_t seed) {
                : R2G_OK;
 }
 
-extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ticket) {
-    if (!ctx || (!items && n > 0) || n < 0 || n > 1023 || !ticket) return R2G_E_INVALID;
+int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_t copy_stream) {
+    if (!ctx || (!items && n > 0) || n < 0 || n > 1023) return R2G_E_INVALID;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return R2G_E_DEVICE;
     int rc = ensure_state(ctx);
     if (rc != R2G_OK) return rc;
@@ -261,7 +261,7 @@ extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, u
         R2gFrame *f = items[i].frame;
         if (!f) return R2G_E_INVALID;
         if (items[i].fp || items[i].side) {
-            rc = r2g_prepare(ctx, f, items[i].fp, items[i].side, items[i].inloop_mask, f->desc);
+            rc = r2g_prepare(ctx, f, items[i].fp, items[i].side, items[i].inloop_mask, f->desc, copy_stream);
             if (rc != R2G_OK) return rc;
             f->staged = true;
         } else if (!f->staged) {
@@ -347,6 +347,13 @@ extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, u
             for (int j = 0; j < e; j++) w3[c3++] = ((uint32_t)gi << 22) | j;
         }
     }
+    if (copy_stream && copy_stream != ctx->stream) {
+        // the kernels wait for this batch's side-info (and any recon uploads
+        // the caller enqueued before) on the copy stream
+        if (cudaEventRecord(b.copied, copy_stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ctx->stream, b.copied, 0) != cudaSuccess)
+            return R2G_E_DEVICE;
+    }
     size_t used = s.L.off_work[N_BSTAGES - 1] + sizeof(uint32_t) * counts[3];
     if (cudaMemcpyAsync(s.dev, s.host, used, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
 
@@ -375,6 +382,13 @@ extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, u
         f->out_buf = f->desc.lr_on ? 3 : (f->desc.cdef_stage_on ? 2 : (f->desc.deblock_on ? 1 : 0));
     }
     if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
+    return R2G_OK;
+}
+
+extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, uint64_t *ticket) {
+    if (!ticket) return R2G_E_INVALID;
+    int rc = r2g_batch_enqueue(ctx, items, n, nullptr);
+    if (rc != R2G_OK) return rc;
     return r2g_ticket_record(ctx, ticket);
 }
 

@@ -69,8 +69,20 @@ struct R2gFrame {
 
 int r2g_dev_alloc(R2gCtx *ctx, void **p, size_t bytes);
 void r2g_dev_free(R2gCtx *ctx, void *p, size_t bytes);
+// Validate and stage one frame's side-info (copies on `cs`, or the context
+// stream when null) and fill its stage descriptor.
 int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t inloop,
-                DevFrame &d);
+                DevFrame &d, cudaStream_t cs);
+// 2-D plane copies between host planes and plane set `buf` of a frame.
+int r2g_copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, int64_t ys, const void *u,
+                    const void *v, int64_t uvs, bool upload, cudaStream_t st);
+size_t r2g_frame_device_bytes(int width, int height, int bitdepth);
+// Parameter checks of r2g_prepare / r2g_frame_grain (no device work).
+int r2g_validate(R2gCtx *ctx, const R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side);
+int r2g_grain_validate(const R2gFilmGrainData *fgd, uint32_t seed);
+// Stage and launch a batch: side-info copies on `copy_stream` (null = the
+// context stream), kernels on the context stream after them.
+int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_t copy_stream);
 void r2g_launch_pipeline(R2gCtx *ctx, const DevFrame &d);
 // Profiling hooks around one stage (no-ops unless profiling is enabled).
 void r2g_prof_stage(R2gCtx *ctx, int stage, bool begin, int launches);

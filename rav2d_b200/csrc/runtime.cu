@@ -58,7 +58,9 @@ extern "C" int r2g_struct_sizes(int32_t *sizes, int n) {
     const int32_t v[] = {(int32_t)sizeof(R2gAv2Filter), (int32_t)sizeof(R2gAv2RestorationUnit),
                          (int32_t)sizeof(R2gAv2Restoration), (int32_t)sizeof(R2gFrameParams),
                          (int32_t)sizeof(R2gFilmGrainData), (int32_t)sizeof(R2gSideInfo),
-                         (int32_t)sizeof(R2gBatchItem)};
+                         (int32_t)sizeof(R2gBatchItem), (int32_t)sizeof(R2gServeConfig),
+                         (int32_t)sizeof(R2gServeRequest), (int32_t)sizeof(R2gServeResult),
+                         (int32_t)sizeof(R2gServeStats)};
     int m = (int)(sizeof(v) / sizeof(v[0]));
     for (int i = 0; i < n && i < m; i++) sizes[i] = v[i];
     return m;
@@ -125,6 +127,17 @@ void r2g_dev_free(R2gCtx *ctx, void *p, size_t bytes) {
 }
 
 // ---------------------------------------------------------------- frames
+// Device bytes r2g_frame_alloc takes for one frame (five plane sets and the
+// side-info records), plus the batched film-grain scratch.
+size_t r2g_frame_device_bytes(int width, int height, int bitdepth) {
+    int64_t ys, uvs, yr, uvr;
+    if (r2g_plane_geometry(width, height, bitdepth, &ys, &uvs, &yr, &uvr) != R2G_OK) return 0;
+    size_t buf = (size_t)(ys * yr + 2 * uvs * uvr);
+    int bw4 = ((width + 7) >> 3) << 1, bh4 = ((height + 7) >> 3) << 1;
+    size_t nsb = (size_t)((bw4 + 63) >> 6) * ((bh4 + 63) >> 6);
+    return 5 * buf + nsb * (sizeof(R2gAv2Filter) + sizeof(R2gAv2Restoration)) + R2G_GRAIN_SCRATCH;
+}
+
 extern "C" int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth, R2gFrame **out) {
     if (!ctx || !out) return R2G_E_INVALID;
     *out = nullptr;
@@ -189,8 +202,8 @@ static void plane_ptrs(const R2gFrame *f, int buf, void *p[3]) {
     p[2] = b + f->plane_bytes[0] + f->plane_bytes[1];
 }
 
-static int copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, int64_t ys, const void *u,
-                       const void *v, int64_t uvs, bool upload) {
+int r2g_copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, int64_t ys, const void *u,
+                    const void *v, int64_t uvs, bool upload, cudaStream_t st) {
     void *p[3];
     plane_ptrs(f, buf, p);
     int bps = f->bd > 8 ? 2 : 1;
@@ -206,10 +219,9 @@ static int copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, i
             return R2G_E_INVALID;
         }
         if (upload)
-            CK(cudaMemcpy2DAsync(p[i], dstride, hs[i], hstride, wbytes, rows, cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpy2DAsync(p[i], dstride, hs[i], hstride, wbytes, rows, cudaMemcpyHostToDevice, st));
         else
-            CK(cudaMemcpy2DAsync((void *)hs[i], hstride, p[i], dstride, wbytes, rows, cudaMemcpyDeviceToHost,
-                                 ctx->stream));
+            CK(cudaMemcpy2DAsync((void *)hs[i], hstride, p[i], dstride, wbytes, rows, cudaMemcpyDeviceToHost, st));
     }
     return R2G_OK;
 }
@@ -218,7 +230,7 @@ extern "C" int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, i
                                       const void *v, int64_t uv_stride) {
     if (!ctx || !f || !y || !u || !v) return R2G_E_INVALID;
     CK(cudaSetDevice(ctx->device));
-    return copy_planes(ctx, f, 0, y, y_stride, u, v, uv_stride, true);
+    return r2g_copy_planes(ctx, f, 0, y, y_stride, u, v, uv_stride, true, ctx->stream);
 }
 
 extern "C" int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_t y_stride, void *u, void *v,
@@ -230,7 +242,7 @@ extern "C" int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_
         set_err(ctx, which ? "frame has no grained copy" : "frame not filtered");
         return R2G_E_INVALID;
     }
-    return copy_planes(ctx, f, buf, y, y_stride, u, v, uv_stride, false);
+    return r2g_copy_planes(ctx, f, buf, y, y_stride, u, v, uv_stride, false, ctx->stream);
 }
 
 extern "C" int r2g_sync(R2gCtx *ctx) {
@@ -318,7 +330,8 @@ static void crop_bottom_edge(R2gAv2Filter *mask, int n, int sb256w, int bw, int 
 }
 
 int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t inloop,
-                DevFrame &d) {
+                DevFrame &d, cudaStream_t cs) {
+    if (!cs) cs = ctx->stream;
     int rc = r2g_validate(ctx, f, fp, side);
     if (rc != R2G_OK) return rc;
     memset(&d, 0, sizeof(d));
@@ -382,7 +395,7 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
     memcpy(f->side_host, side->masks, mbytes);
     memcpy((char *)f->side_host + mbytes, side->lr, lbytes);
     if (d.deblock_on) crop_bottom_edge((R2gAv2Filter *)f->side_host, f->n_sb256, d.sb256w, d.bw4, d.bh4);
-    CK(cudaMemcpyAsync(f->side_dev, f->side_host, mbytes + lbytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(f->side_dev, f->side_host, mbytes + lbytes, cudaMemcpyHostToDevice, cs));
     d.masks = (const R2gAv2Filter *)f->side_dev;
     d.lr = (const R2gAv2Restoration *)((char *)f->side_dev + mbytes);
     size_t seg_y = side->segmap ? (size_t)side->segmap_stride * d.bh4 : 0;
@@ -401,13 +414,13 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
         }
         if (seg_y) memcpy(f->seg_host, side->segmap, seg_y);
         if (seg_uv) memcpy((char *)f->seg_host + seg_y, side->segmap_uv, seg_uv);
-        CK(cudaMemcpyAsync(f->seg_dev, f->seg_host, seg_y + seg_uv, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(f->seg_dev, f->seg_host, seg_y + seg_uv, cudaMemcpyHostToDevice, cs));
         d.segmap = seg_y ? (const uint8_t *)f->seg_dev : nullptr;
         d.segmap_uv = seg_uv ? (const uint8_t *)f->seg_dev + seg_y : nullptr;
         d.segmap_stride = side->segmap_stride;
         d.segmap_uv_stride = side->segmap_uv_stride;
     }
-    CK(cudaEventRecord(f->side_done, ctx->stream));
+    CK(cudaEventRecord(f->side_done, cs));
 
     // buffers: 0 = recon (preserved), 1 = deblocked, 2 = CDEF out,
     // 3 = LR out, 4 = grain display copy
@@ -515,7 +528,7 @@ extern "C" int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *f
                                uint32_t inloop_mask) {
     if (!ctx || !f) return R2G_E_INVALID;
     CK(cudaSetDevice(ctx->device));
-    int rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc);
+    int rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, nullptr);
     if (rc != R2G_OK) return rc;
     f->staged = true;
     return R2G_OK;

@@ -21,7 +21,8 @@ SYMBOLS = [
     "r2g_last_error", "r2g_frame_alloc", "r2g_frame_free", "r2g_frame_upload_recon", "r2g_frame_filter",
     "r2g_frame_grain", "r2g_download", "r2g_sync", "r2g_filter_frame_host", "r2g_batch_submit", "r2g_wait",
     "r2g_frame_stage", "r2g_frame_run", "r2g_ctx_set_stream", "r2g_ctx_profile", "r2g_ctx_profile_read",
-    "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config",
+    "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config", "r2g_server_create",
+    "r2g_server_submit", "r2g_server_wait", "r2g_server_close_stream", "r2g_server_stats", "r2g_server_destroy",
 ]
 
 
@@ -64,6 +65,12 @@ def lib():
         L.r2g_ctx_launch_count.argtypes = [C.c_void_p]
         L.r2g_ctx_launch_count.restype = C.c_int64
         L.r2g_batch_config.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int]
+        L.r2g_server_create.argtypes = [C.c_void_p, C.POINTER(abi.ServeConfig), C.POINTER(C.c_void_p)]
+        L.r2g_server_submit.argtypes = [C.c_void_p, C.POINTER(abi.ServeRequest), C.POINTER(C.c_uint64)]
+        L.r2g_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(abi.ServeResult)]
+        L.r2g_server_close_stream.argtypes = [C.c_void_p, C.c_int32]
+        L.r2g_server_stats.argtypes = [C.c_void_p, C.POINTER(abi.ServeStats), C.c_int]
+        L.r2g_server_destroy.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -218,3 +225,65 @@ def filter_frame(ctx, sf, grain=False):
         return out
     finally:
         fr.free()
+
+
+class Server:
+    """Continuous-batching server over one context (r2g_server_*)."""
+
+    def __init__(self, ctx, mem_budget=0, max_batch=64, frames_per_stream=2):
+        self.ctx = ctx
+        cfg = abi.ServeConfig(mem_budget, max_batch, frames_per_stream)
+        h = C.c_void_p()
+        ctx.check(lib().r2g_server_create(ctx.h, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, stream_id, sf, src, dst, ref=None, grain=True):
+        """src/dst/ref: [y, u, v] host arrays (the allocator geometry); the
+        arrays and sf's side-info must stay alive until wait()."""
+        side = sf.side()
+        r = abi.ServeRequest()
+        r.stream_id = stream_id
+        r.fp = C.pointer(sf.fp)
+        r.side = C.pointer(side)
+        r.inloop_mask = sf.inloop
+        r.fgd = C.pointer(sf.fgd) if (grain and sf.fgd is not None) else None
+        r.grain_seed = sf.grain_seed
+        r.src_y, r.src_u, r.src_v = (p.ctypes.data for p in src)
+        r.src_y_stride, r.src_uv_stride = src[0].strides[0], src[1].strides[0]
+        r.dst_y, r.dst_u, r.dst_v = (p.ctypes.data for p in dst)
+        r.dst_y_stride, r.dst_uv_stride = dst[0].strides[0], dst[1].strides[0]
+        if ref is not None:
+            r.ref_y, r.ref_u, r.ref_v = (p.ctypes.data for p in ref)
+        i = C.c_uint64()
+        self.ctx.check(lib().r2g_server_submit(self.h, C.byref(r), C.byref(i)))
+        self._keep[i.value] = (side, r, src, dst, ref)
+        return i.value
+
+    def wait(self, rid, timeout_ms=-1):
+        """Returns (rc, ServeResult); rc is the wait's own status."""
+        res = abi.ServeResult()
+        rc = lib().r2g_server_wait(self.h, C.c_uint64(rid), timeout_ms, C.byref(res))
+        if rc == 0:
+            self._keep.pop(rid, None)
+        return rc, res
+
+    def close_stream(self, stream_id):
+        return lib().r2g_server_close_stream(self.h, stream_id)
+
+    def stats(self, reset=False):
+        st = abi.ServeStats()
+        self.ctx.check(lib().r2g_server_stats(self.h, C.byref(st), int(reset)))
+        return {k: getattr(st, k) for k, _ in abi.ServeStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().r2g_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
