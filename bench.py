@@ -37,12 +37,13 @@ sys.path.insert(0, ROOT)
 W_, H_, BD_ = 1920, 1080, 10
 SEED = 0x5EED0001
 MPIX = W_ * H_ / 1e6
-# algorithmic HBM bytes per luma pixel at 10-bit: each stage reads its input
-# frame once and writes its output frame once (4:2:0 = 1.5 samples / px,
-# 2 B / sample: 3 B read + 3 B written); loop restoration's deblocked stripe
-# boundary rows (2 of every 64 rows) and film grain's templates are <2 % and
-# not counted
-BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 6.0, "film_grain": 6.0}
+# algorithmic HBM bytes per luma pixel at 10-bit (4:2:0 = 1.5 samples / px,
+# 2 B / sample): each stage reads its input frame once and writes its output
+# once (3 + 3 B); loop restoration with chroma NS-Wiener and film grain also
+# read the luma plane once more for the chroma planes' cross-component taps /
+# scaling index (+2 B).  The deblock kernel runs both edge directions in one
+# pass over the frame, so its minimum is one read and one write.
+BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film_grain": 8.0}
 # dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload,
 # from `ncu --set full` (profiles/stages_full_1080p10.md); the outputs were
 # still in L2 when the capture ended, so the write term was 0
@@ -157,9 +158,9 @@ def run_ours(args, rank, world, device):
     ctx.sync()
     torch.cuda.synchronize()
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+    from rav2d_b200 import replicas
+
+    barrier = replicas.barrier
 
     # ---- device-resident timed region ----
     for i in range(args.warmup):
@@ -179,10 +180,7 @@ def run_ours(args, rank, world, device):
     launches = ctx.launch_count() - l0
     ms = ev0.elapsed_time(ev1)
     barrier()
-    t = torch.tensor([ms], device=f"cuda:{device}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = replicas.max_over_ranks(ms, f"cuda:{device}")
 
     # ---- profiled pass: per-stage kernel durations from CUDA events ----
     ctx.profile(True)
@@ -217,10 +215,7 @@ def run_ours(args, rank, world, device):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    t = torch.tensor([e2e_ms], device=f"cuda:{device}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms_max = float(t.item())
+    e2e_ms_max = replicas.max_over_ranks(e2e_ms, f"cuda:{device}")
     recon_bytes = int(W_ * H_ * 1.5 * 2)
     side_bytes = int(sfs[0].masks.nbytes + sfs[0].lr.nbytes)
 
@@ -425,6 +420,48 @@ def cpu_baseline(seconds=12.0, threads=1):
     return done[0] * MPIX / dt, done[0], dt
 
 
+def reference_arm(args, config, metric):
+    """The reference's CPU filter path (the oracle: the Rust reference cannot
+    be built here) on all host threads, on the same workload.  Each step
+    filters one sample frame per thread: 1920 x `rows` 10-bit with the full
+    chain, `rows` chosen so the whole --steps/--warmup run takes about
+    --ref-seconds (whole 1080p frames when the step count allows)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from concurrent.futures import ThreadPoolExecutor
+
+    from rav2d_b200 import synth
+
+    pyoracle.lib()
+    nthreads = os.cpu_count() or 1
+    full = make_inputs(1)[0]
+    t = time.perf_counter()
+    pyoracle.filter_frame(full)
+    rate = MPIX / (time.perf_counter() - t)  # Mpix/s on one thread
+    per_step = args.ref_seconds * rate / (args.steps + args.warmup)
+    rows = int(min(H_, max(64, per_step * 1e6 / W_))) // 8 * 8
+    samples = [synth.make_frame(W_, rows, BD_, SEED + 16 * k, chain="full") for k in range(min(nthreads, 4))]
+    mpix_step = nthreads * W_ * rows / 1e6
+    times = []
+    with ThreadPoolExecutor(nthreads) as pool:
+        for i in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            list(pool.map(lambda k: pyoracle.filter_frame(samples[k % len(samples)]), range(nthreads)))
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t)
+    tot = sum(times)
+    val = mpix_step * len(times) / tot
+    sample = (f"each step: one 1920x{rows} 10-bit frame (full chain) per host thread through the oracle (C++ "
+              f"restatement of the reference scalar Rust filter path), {nthreads} threads")
+    return {"impl": "reference", "metric": metric, "value": round(val, 3), "unit": "Mpix/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1000 * tot / len(times), 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16", "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": round(val, 3), "unit": "Mpix/s", "cores": nthreads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(val, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -435,11 +472,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-steps", type=int, default=30, help="timed batches of the 64-frame mix (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="measured serving window (0 = skip)")
+    ap.add_argument("--ref-seconds", type=float, default=120.0, help="target duration of --impl reference")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from rav2d_b200 import replicas
+
+    rank, world, local = replicas.env()
     config = {"workload": "per-frame 1920x1080 10-bit 4:2:0, deblock+CDEF+CCSO+LR(NS/PC-Wiener+GDF), no grain",
               "frames_per_step": 1, "width": W_, "height": H_, "bitdepth": BD_, "inloop_mask": 31,
               "l2": "inputs larger than L2: a ring of 48 resident frames (~330 MB), step i filters frame i % 48",
@@ -447,43 +485,22 @@ def main():
     metric = "filtered Mpix/s (luma), 10-bit per-frame pipeline on 1 B200"
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        nthreads = os.cpu_count() or 1
-        per = []
-        for i in range(args.warmup + args.steps):
-            v, n, dt = cpu_baseline(seconds=0.5, threads=nthreads)
-            if i >= args.warmup:
-                per.append((v, dt))
-        tot_t = sum(dt for _, dt in per)
-        val = sum(v * dt for v, dt in per) / tot_t
-        line = {"impl": "reference", "metric": metric, "value": round(val, 3), "unit": "Mpix/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": round(1000 * tot_t / len(per), 3), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "u16", "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": round(val, 3), "unit": "Mpix/s", "cores": nthreads, "kind": "port",
-                                 "sample": "each step: one 0.5 s window of whole 1080p frames through the oracle "
-                                           "(C++ restatement of the reference scalar Rust path), one frame per "
-                                           "thread"},
-                "e2e": {"value": round(val, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        if rank == 0:
+            print(json.dumps(reference_arm(args, config, metric)), flush=True)
         return
 
     import torch
 
-    if world > 1:
-        torch.distributed.init_process_group("nccl", init_method="env://",
-                                             timeout=__import__("datetime").timedelta(seconds=120))
+    replicas.init("nccl")
     res = run_ours(args, rank, world, local)
     res["serving"] = run_serving(args, local) if args.serve_seconds > 0 and rank == 0 else None
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish()
     if rank != 0:
         return
     n = args.gpus
     ms_step = res["ms"] / args.steps
-    value = n * MPIX * args.steps / (res["ms"] / 1e3)
-    e2e = n * MPIX * res["n_e2e"] / (res["e2e_ms"] / 1e3)
+    value = replicas.aggregate_rate(MPIX * args.steps, res["ms"], n)
+    e2e = replicas.aggregate_rate(MPIX * res["n_e2e"], res["e2e_ms"], n)
     prof = res["prof"]
     dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
     dom_ms, dom_n = prof[dom]
@@ -491,6 +508,8 @@ def main():
     achieved = BYTES_PER_PX[dom] * W_ * H_ / avg_launch_s / 1e9
     peak, peak_kind = peaks()
     cpu_v, cpu_n, cpu_dt = cpu_baseline(seconds=args.cpu_seconds, threads=1)
+    ncores = os.cpu_count() or 1
+    cpu_all = cpu_baseline(seconds=min(args.cpu_seconds, 6.0), threads=ncores) if args.cpu_seconds >= 1 else None
     line = {
         "metric": metric, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": n, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak",
@@ -508,6 +527,9 @@ def main():
         "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpix/s", "cores": 1, "kind": "port",
                          "sample": f"{cpu_n} whole 1080p 10-bit frames through the oracle (C++ restatement of the "
                                    f"reference scalar Rust filter path) on 1 host core in {cpu_dt:.1f} s"},
+        "cpu_all_cores": ({"value": round(cpu_all[0], 3), "unit": "Mpix/s", "cores": ncores, "kind": "port",
+                           "sample": f"{cpu_all[1]} whole 1080p frames, one per thread, in {cpu_all[2]:.1f} s"}
+                          if cpu_all else None),
         "clocks": res["clocks"], "gpu_launches": res["launches"],
         "batched": res["batched"], "serving": res["serving"],
     }
