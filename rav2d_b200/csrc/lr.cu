@@ -145,16 +145,31 @@ __device__ constexpr int8_t uvy[12][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 
 }  // namespace TapsY
 
 struct LrSmem {
-    int16_t win[LH * LW];      // luma window, or chroma window (pitch CWW)
-    int16_t lwin[CWH * CWW];   // chroma: downsampled luma window
+    union {
+        // luma: every window position holds the sample and its right
+        // neighbour as a signed 16x2 pair, so GDF can work on two adjacent
+        // pixels (which share a GDF class) with one 32-bit load per tap;
+        // a scalar sample is the low half (16-bit loads at a 4-byte stride)
+        uint32_t wp[LH * LW];
+        struct {
+            int16_t win[CWH * CWW];   // chroma window
+            int16_t lwin[CWH * CWW];  // downsampled luma window
+        } ch;
+    } u;
     uint16_t gcell[33 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
     int8_t gerr[64 * 64];
     int8_t s_err[4096];
-    short4 s_par[4][22];       // per class: alpha, 3 weights of each GDF feature
+    uint2 s_aa[4][18];   // per class and tap: (alpha, alpha), (-alpha, -alpha) as s16x2
+    int4 s_w[4][22];     // per class and tap / feature: weights 0..2, alpha
+    int16_t s_pcf[64 * 13];  // PC-Wiener filters of this frame's wiener_idx
     uint8_t classes[16][16];
     uint16_t noskip[18];
     uint16_t llm[17];
 };
+
+// Sign-extended low / high halves of a 16x2 pair.
+R2G_D int lo16(uint32_t v) { return (int)(int16_t)(v & 0xffff); }
+R2G_D int hi16(uint32_t v) { return (int)v >> 16; }
 
 // One (plane, stripe, 64-wide unit) work item; b is the per-frame item index:
 // luma items first (sby, sub-stripe, unit), then U, then V.
@@ -264,7 +279,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
             bool from_d;
             row_src(g, r - 2, row, from_d);
             const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
-            for (int c = lane; c < ww; c += 32) sm.win[r * CWW + c] = (int16_t)src[col_src(g, c - 2)];
+            for (int c = lane; c < ww; c += 32) sm.u.ch.win[r * CWW + c] = (int16_t)src[col_src(g, c - 2)];
         }
         if (wkind == W_NS_SINGLE) {
             // downsampled luma for chroma rows -2 .. sh+1 at chroma columns
@@ -313,7 +328,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                         v = ((int)rowa[pos] + rowb[pos]) >> 1;
                     else
                         v = rowa[pos];
-                    sm.lwin[r * CWW + j] = (int16_t)v;
+                    sm.u.ch.lwin[r * CWW + j] = (int16_t)v;
                 }
             }
         }
@@ -328,8 +343,8 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         }
         for (int y = warp; y < g.sh; y += 8)
             for (int x = lane; x < g.uw; x += 32) {
-                const int16_t *w = &sm.win[(y + 2) * CWW + x + 2];
-                const int16_t *lw_ = &sm.lwin[(y + 2) * CWW + x + 2];
+                const int16_t *w = &sm.u.ch.win[(y + 2) * CWW + x + 2];
+                const int16_t *lw_ = &sm.u.ch.lwin[(y + 2) * CWW + x + 2];
                 int m = w[0];
                 int v = m;
                 bool ll = (sm.llm[y >> 2] >> (x >> 2)) & 1;
@@ -355,13 +370,28 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
 
     // ---- luma window: rows -6 .. sh+5, columns -6 .. uw+5 ----
     const int wh = g.sh + 12, ww = g.uw + 12;
-    for (int r = warp; r < wh; r += 8) {
-        int row;
-        bool from_d;
-        row_src(g, r - 6, row, from_d);
-        const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
-        for (int c = lane; c < ww; c += 32) sm.win[r * LW + c] = (int16_t)src[col_src(g, c - 6)];
+    {
+        // source columns of this lane's window columns (the same on every row)
+        int cs0[3], cs1[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int c = lane + 32 * j;
+            cs0[j] = col_src(g, c - 6);
+            cs1[j] = c + 1 < ww ? col_src(g, c - 5) : cs0[j];
+        }
+        for (int r = warp; r < wh; r += 8) {
+            int row;
+            bool from_d;
+            row_src(g, r - 6, row, from_d);
+            const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int c = lane + 32 * j;
+                if (c < ww) sm.u.wp[r * LW + c] = (uint32_t)src[cs0[j]] | ((uint32_t)src[cs1[j]] << 16);
+            }
+        }
     }
+    const int16_t *W16 = reinterpret_cast<const int16_t *>(sm.u.wp);  // scalar sample i at W16[2 * i]
     if (gdf_on) {
         const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
         const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
@@ -371,15 +401,19 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
         for (int i = tid; i < 88; i += 256) {
             int k = i >> 2, c = i & 3;
-            short4 p;
-            p.x = (short)f.tab.GDF_ALPHA[alpha_base + i];
-            p.y = f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i];
-            p.z = f.tab.GDF_WEIGHT[weight_base + 1 * 88 + i];
-            p.w = f.tab.GDF_WEIGHT[weight_base + 2 * 88 + i];
-            sm.s_par[c][k] = p;
+            const int a = f.tab.GDF_ALPHA[alpha_base + i];
+            sm.s_w[c][k] = make_int4(f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i],
+                                     f.tab.GDF_WEIGHT[weight_base + 1 * 88 + i],
+                                     f.tab.GDF_WEIGHT[weight_base + 2 * 88 + i], a);
+            if (k < 18) {
+                const uint32_t pa = (uint32_t)a & 0xffff, na = (uint32_t)(-a) & 0xffff;
+                sm.s_aa[c][k] = make_uint2(pa | (pa << 16), na | (na << 16));
+            }
         }
         for (int i = tid; i < nerr; i += 256) sm.s_err[i] = errtab[i];
     }
+    if (wkind == W_PC)
+        for (int i = tid; i < 64 * 13; i += 256) sm.s_pcf[i] = f.tab.PC_WIENER_FILTERS[f.wiener_idx * 64 * 13 + i];
     __syncthreads();
 
     const int b8 = bitdepth - 8;
@@ -401,16 +435,17 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
             for (int yy = 0; yy < 2; yy++)
 #pragma unroll
                 for (int xx = 0; xx < 2; xx++) {
-                    const int16_t *w = &sm.win[(2 * j - 1 + yy + 6) * LW + 2 * c - 1 + xx + 6];
+                    const int16_t *w = &W16[2 * ((2 * j - 1 + yy + 6) * LW + 2 * c - 1 + xx + 6)];
+                    constexpr int R = 2 * LW, C1 = 2;
                     int bv = w[0] >> down;
                     int t;
-                    t = 2 * bv - (w[-LW] >> down) - (w[LW] >> down);
+                    t = 2 * bv - (w[-R] >> down) - (w[R] >> down);
                     gs[0] += t < 0 ? -t : t;
-                    t = 2 * bv - (w[-1] >> down) - (w[1] >> down);
+                    t = 2 * bv - (w[-C1] >> down) - (w[C1] >> down);
                     gs[1] += t < 0 ? -t : t;
-                    t = 2 * bv - (w[-LW - 1] >> down) - (w[LW + 1] >> down);
+                    t = 2 * bv - (w[-R - C1] >> down) - (w[R + C1] >> down);
                     gs[2] += t < 0 ? -t : t;
-                    t = 2 * bv - (w[LW - 1] >> down) - (w[-LW + 1] >> down);
+                    t = 2 * bv - (w[R - C1] >> down) - (w[-R + C1] >> down);
                     gs[3] += t < 0 ? -t : t;
                 }
 #pragma unroll
@@ -432,36 +467,43 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 gsum[d] = sm.gcell[(j * ci + c) * 4 + d] + sm.gcell[(j * ci + c + 1) * 4 + d] +
                           sm.gcell[((j + 1) * ci + c) * 4 + d] + sm.gcell[((j + 1) * ci + c + 1) * 4 + d];
             int cls = (gsum[0] <= gsum[1]) | ((gsum[2] <= gsum[3]) << 1);
-            const short4 *par = sm.s_par[cls];
+            const int4 *wt = sm.s_w[cls];
+            const uint2 *aa = sm.s_aa[cls];
             int sh0 = b0, sh1 = b1, sh2 = b2;
 #pragma unroll
             for (int d = 0; d < 4; d++) {
-                short4 p = par[18 + d];
-                int v = imin_(gsum[d] >> (4 - up), p.x);
-                sh0 += v * p.y;
-                sh1 += v * p.z;
-                sh2 += v * p.w;
+                int4 p = wt[18 + d];
+                int v = imin_(gsum[d] >> (4 - up), p.w);
+                sh0 += v * p.x;
+                sh1 += v * p.y;
+                sh2 += v * p.z;
+            }
+            // the 18 clipped symmetric differences of both pixels at once,
+            // as signed 16x2 pairs: (pixel x, pixel x + 1)
+            const uint32_t *wc = &sm.u.wp[(y + 6) * LW + x1 + 6];
+            const uint32_t mm = wc[0] << up;  // samples < 2^10: no carry between halves
+            const uint32_t nm = __vneg2(mm);
+            int i0 = sh0, i1 = sh1, i2 = sh2, j0 = sh0, j1 = sh1, j2 = sh2;
+#pragma unroll
+            for (int k = 0; k < 18; k++) {
+                const int o = TapsY::gdf[k][0] * LW + TapsY::gdf[k][1];
+                const uint2 al = aa[k];
+                const int4 p = wt[k];
+                const uint32_t above = __vmins2(__viaddmax_s16x2(wc[-o] << up, nm, al.y), al.x);
+                const uint32_t below = __vmins2(__viaddmax_s16x2(wc[o] << up, nm, al.y), al.x);
+                const uint32_t v = __vmins2(__viaddmax_s16x2(above, below, 0xfe00fe00u), 0x01ff01ffu);
+                const int v0 = lo16(v), v1 = hi16(v);
+                i0 += v0 * p.x;
+                i1 += v0 * p.y;
+                i2 += v0 * p.z;
+                j0 += v1 * p.x;
+                j1 += v1 * p.y;
+                j2 += v1 * p.z;
             }
 #pragma unroll
             for (int x2 = 0; x2 < 2; x2++) {
-                const int x = x1 + x2;
-                const int16_t *w = &sm.win[(y + 6) * LW + x + 6];
-                int m = w[0] >> down;
-                int i0 = sh0, i1 = sh1, i2 = sh2;
-#pragma unroll
-                for (int k = 0; k < 18; k++) {
-                    const int o = TapsY::gdf[k][0] * LW + TapsY::gdf[k][1];
-                    short4 p = par[k];
-                    int alpha = p.x;
-                    int above = iclip_(((w[-o] >> down) - m) << up, -alpha, alpha);
-                    int below = iclip_(((w[o] >> down) - m) << up, -alpha, alpha);
-                    int v = iclip_(above + below, -512, 511);
-                    i0 += v * p.y;
-                    i1 += v * p.z;
-                    i2 += v * p.w;
-                }
+                const int iv[3] = {x2 ? j0 : i0, x2 ? j1 : i1, x2 ? j2 : i2};
                 int full = 0;
-                const int iv[3] = {i0, i1, i2};
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     int sv = iv[q] * scale;
@@ -470,7 +512,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                     int subi = iclip_(v, -scale, scale - 1) + scale;
                     full = full * (scale * 2) + subi;
                 }
-                sm.gerr[y * 64 + x] = sm.s_err[full];
+                sm.gerr[y * 64 + x1 + x2] = sm.s_err[full];
             }
         }
     }
@@ -487,11 +529,12 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
             for (int dy = -1; dy <= 4; dy++)
 #pragma unroll
                 for (int dx = -1; dx <= 4; dx++) {
-                    const int16_t *w = &sm.win[(by * 4 + dy + 6) * LW + bx * 4 + dx + 6];
+                    const int16_t *w = &W16[2 * ((by * 4 + dy + 6) * LW + bx * 4 + dx + 6)];
+                    constexpr int R = 2 * LW, C1 = 2;
                     int m2 = 2 * w[0];
-                    int vert = w[-LW] - m2 + w[LW];
-                    int anti = w[-LW + 1] - m2 + w[LW - 1];
-                    int diag = w[-LW - 1] - m2 + w[LW + 1];
+                    int vert = w[-R] - m2 + w[R];
+                    int anti = w[-R + C1] - m2 + w[R - C1];
+                    int diag = w[-R - C1] - m2 + w[R + C1];
                     fs0 += vert < 0 ? -vert : vert;
                     fs1 += anti < 0 ? -anti : anti;
                     fs2 += diag < 0 ? -diag : diag;
@@ -535,20 +578,19 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
     for (int y = warp; y < g.sh; y += 8)
         for (int x = lane; x < g.uw; x += 32) {
-            const int16_t *w = &sm.win[(y + 6) * LW + x + 6];
+            const int16_t *w = &W16[2 * ((y + 6) * LW + x + 6)];
             int m = w[0];
             int v = m;
             bool ll = (sm.llm[y >> 2] >> (x >> 2)) & 1;
             if (!ll && wkind != W_NONE) {
                 int s;
                 if (wkind == W_PC) {
-                    const int16_t *flt =
-                        f.tab.PC_WIENER_FILTERS + (f.wiener_idx * 64 + sm.classes[y >> 2][x >> 2]) * 13;
-                    s = m * __ldg(flt + 12);
+                    const int16_t *flt = sm.s_pcf + sm.classes[y >> 2][x >> 2] * 13;
+                    s = m * flt[12];
 #pragma unroll
                     for (int k = 0; k < 12; k++) {
-                        const int o = TapsY::pc[k][0] * LW + TapsY::pc[k][1];
-                        s += (w[o] + w[-o]) * __ldg(flt + k);
+                        const int o = 2 * (TapsY::pc[k][0] * LW + TapsY::pc[k][1]);
+                        s += (w[o] + w[-o]) * flt[k];
                     }
                 } else {
                     const int8_t *flt =
@@ -556,7 +598,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                     s = m << 7;
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
-                        const int o = TapsY::ns[k][0] * LW + TapsY::ns[k][1];
+                        const int o = 2 * (TapsY::ns[k][0] * LW + TapsY::ns[k][1]);
                         s += (w[o] + w[-o] - 2 * m) * flt[k];
                     }
                 }
@@ -579,6 +621,11 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f) {
 
 // Persistent kernel over a cross-frame work list: item = frame << 22 |
 // per-frame item index.
+// (one call per sample type, kept out of line so the two instantiations do
+// not share one register allocation)
+__device__ __noinline__ void lr_unit_hbd(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint16_t>(f, sm, b); }
+__device__ __noinline__ void lr_unit_8(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint8_t>(f, sm, b); }
+
 __global__ void __launch_bounds__(256, 3) lr_batch_kernel(BatchArgs a) {
     __shared__ LrSmem sm;
     const int n = a.count[2];
@@ -586,9 +633,9 @@ __global__ void __launch_bounds__(256, 3) lr_batch_kernel(BatchArgs a) {
         const uint32_t it = a.work[2][w];
         const DevFrame &f = a.frames[it >> 22];
         if (f.bitdepth > 8)
-            lr_unit<uint16_t>(f, sm, it & 0x3fffff);
+            lr_unit_hbd(f, sm, it & 0x3fffff);
         else
-            lr_unit<uint8_t>(f, sm, it & 0x3fffff);
+            lr_unit_8(f, sm, it & 0x3fffff);
         __syncthreads();
     }
 }
