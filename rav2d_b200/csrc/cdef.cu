@@ -8,23 +8,31 @@
 // seam pass), so every tap it takes is a deblocked, pre-CDEF sample.  Here
 // that is expressed directly: the kernel reads D and writes C.
 //
-// One CTA covers one 64x8 luma band of a 64-wide superblock column plus the
-// co-located 32x4 chroma bands.  The band and a 2-sample halo are staged in
-// shared memory (coordinates clamped to the frame, which is CCSO's padding;
-// CDEF substitutes INT16_MIN for taps outside the frame, its padding).
-//   phase 1: warp w runs the direction search of 8x8 block w: per-direction
-//            partial sums in shared memory, the 8 costs on lanes 0..7 and a
-//            shuffle argmax (first maximum wins, as in the reference);
-//   phase 2: every thread filters two luma samples of one row and one chroma
-//            sample, adds the CCSO offset and stores row-contiguous.
+// One CTA covers a 64x32 luma region of a 64-wide superblock column (32
+// 8x8 blocks) plus the co-located 32x16 chroma region.  The region and a
+// 2-sample halo are staged in shared memory (coordinates clamped to the
+// frame, which is CCSO's padding; CDEF substitutes INT16_MIN for taps outside
+// the frame, its padding), plus a block-major copy of the region's luma for
+// the direction search.
+//   phase 1: warp 0 decodes each block's strengths and skip / lossless state
+//            (lane = block);
+//   phase 2: warp d computes direction d's cost for every block (lane =
+//            block): partial sums in registers, no atomics;
+//   phase 3: warp 0 picks each block's direction (first maximum wins, as in
+//            the reference), its variance and adjusted strengths;
+//   phase 4: warp w filters blocks w, w+8, w+16, w+24: each lane two luma
+//            samples of one row and one chroma sample, plus the CCSO offset.
 #include "r2g_common.cuh"
 
 namespace {
 
-constexpr int TW = 68;  // luma tile width  (-2 .. 65)
-constexpr int TH = 12;  // luma tile height (-2 .. 9)
-constexpr int CW = 36;  // chroma tile width (-2 .. 33)
-constexpr int CH = 8;   // chroma tile height (-2 .. 5)
+constexpr int RH = 32;   // luma rows per CTA region
+constexpr int NB = 32;   // 8x8 blocks per region (8 wide, 4 high)
+constexpr int TW = 68;   // luma tile width  (-2 .. 65)
+constexpr int TH = RH + 4;   // luma tile height (-2 .. RH+1)
+constexpr int CW = 36;   // chroma tile width (-2 .. 33)
+constexpr int CH = RH / 2 + 4;  // chroma tile height
+constexpr int BKP = 66;  // block-major pitch (int16): conflict-free per-lane reads
 
 __constant__ int8_t c_ccso_pos[7][2] = {{-1, 0}, {0, -1}, {-1, -1}, {-1, 1}, {-1, -2}, {1, -2}, {0, 2}};
 __constant__ uint8_t c_uv_dirs[8] = {0, 1, 2, 3, 4, 5, 6, 7};
@@ -32,9 +40,10 @@ __constant__ uint32_t c_div_table[7] = {840, 420, 280, 210, 168, 140, 120};
 
 struct BlockParams {
     int active;   // any CDEF filtering of this 8x8 (luma or chroma)
+    int need_dir;
     int y_pri, y_sec, y_dir, y_on;
     int uv_pri, uv_sec, uv_dir, uv_on;
-    int yoff[6], uvoff[6];  // tap offsets in the luma / chroma padded tiles
+    int y_ll;     // luma lossless rows mask bits for CCSO: bit r>>2 of the block
 };
 
 R2G_D int constrain(int diff, int threshold, int shift) {
@@ -54,11 +63,6 @@ R2G_D void dir_off(int off, int &dy, int &dx) {
         dy -= 1;
         dx += 12;
     }
-}
-
-template <typename P>
-R2G_D int load_px(const P *p) {
-    return (int)*p;
 }
 
 // cdef_filter_block (cdef.rs:320-458) for one sample.  `t` points at the
@@ -111,19 +115,6 @@ R2G_D int cdef_px(const int16_t *t, int pri, int sec, const int *off, int dampin
     return px + ((sum - (sum < 0) + 8) >> 4);
 }
 
-// Linear tap offsets of direction `dir` in a tile of row pitch `pitch`.
-R2G_D void tap_offsets(const int8_t *dirs, int dir, int pitch, int *off) {
-    const int which[3] = {dir + 2, dir + 4, dir};
-#pragma unroll
-    for (int w = 0; w < 3; w++)
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            int dy, dx;
-            dir_off(dirs[which[w] * 2 + k], dy, dx);
-            off[w * 2 + k] = dy * pitch + dx;
-        }
-}
-
 // ccso_score (ccso.rs:16-24)
 R2G_D uint32_t ccso_score(int diff, int q, uint32_t clf) {
     if (diff > q && clf == 0) return 2;
@@ -131,28 +122,69 @@ R2G_D uint32_t ccso_score(int diff, int q, uint32_t clf) {
     return 1;
 }
 
+// Cost of direction D for one 8x8 block (cdef_find_dir_bd, cdef.rs:134-224):
+// `b` holds the block's 64 values (px >> bd8) - 128 in raster order.  The
+// per-direction lines are summed in registers (every index is a constant
+// after unrolling); squares and sums wrap in 32 bits as in the reference.
+template <int D>
+R2G_D uint32_t dir_cost(const int16_t *b) {
+    constexpr int NBIN = (D == 2 || D == 6) ? 8 : ((D == 0 || D == 4) ? 15 : 11);
+    int bin[NBIN];
+#pragma unroll
+    for (int n = 0; n < NBIN; n++) bin[n] = 0;
+#pragma unroll
+    for (int y = 0; y < 8; y++)
+#pragma unroll
+        for (int x = 0; x < 8; x++) {
+            const int v = b[y * 8 + x];
+            int k;
+            if (D == 0) k = y + x;
+            else if (D == 1) k = y + (x >> 1);
+            else if (D == 2) k = y;
+            else if (D == 3) k = 3 + y - (x >> 1);
+            else if (D == 4) k = 7 + y - x;
+            else if (D == 5) k = 3 - (y >> 1) + x;
+            else if (D == 6) k = x;
+            else k = (y >> 1) + x;
+            bin[k] += v;
+        }
+    auto sq = [](int v) -> uint32_t { return (uint32_t)v * (uint32_t)v; };
+    uint32_t cost = 0;
+    if (D == 2 || D == 6) {
+#pragma unroll
+        for (int n = 0; n < 8; n++) cost += sq(bin[n]);
+        cost *= 105u;
+    } else if (D == 0 || D == 4) {
+#pragma unroll
+        for (int n = 0; n < 7; n++) cost += (sq(bin[n]) + sq(bin[14 - n])) * c_div_table[n];
+        cost += sq(bin[7]) * 105u;
+    } else {
+#pragma unroll
+        for (int m = 0; m < 5; m++) cost += sq(bin[3 + m]);
+        cost *= 105u;
+#pragma unroll
+        for (int m = 0; m < 3; m++) cost += (sq(bin[m]) + sq(bin[10 - m])) * c_div_table[2 * m + 1];
+    }
+    return cost;
+}
+
 struct CdefSmem {
     int16_t ty[TH][TW];   // clamped to the frame (CCSO padding)
     int16_t tc[2][CH][CW];
     int16_t pty[TH][TW];  // INT16_MIN outside the frame (CDEF padding)
     int16_t ptc[2][CH][CW];
-    int bins[8][96];
-    BlockParams bp[8];
+    int16_t blk[NB][BKP]; // per block: (px >> bd8) - 128, raster order
+    uint32_t cost[8][NB];
+    BlockParams bp[NB];
+    int toff_y[8][6], toff_c[8][6];  // tap offsets per direction (tile pitches)
     int s_ccso[3];
 };
 
-// One 64x8 band of superblock column sbx (the work of one CTA); shared by
-// the per-frame kernel and the batched persistent kernel.
+// One 64x32 region (superblock column sbx, region row rr) of the frame; the
+// work of one CTA, shared by the per-frame and the batched kernels.
 template <typename P>
-R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
-    auto &ty = sm.ty;
-    auto &tc = sm.tc;
-    auto &pty = sm.pty;
-    auto &ptc = sm.ptc;
-    auto &bins = sm.bins;
-    auto &bp = sm.bp;
-    auto &s_ccso = sm.s_ccso;
-    const int gx0 = sbx * 64, gy0 = band * 8;
+R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
+    const int gx0 = sbx * 64, gy0 = rr * RH;
     const int cx0 = gx0 >> 1, cy0 = gy0 >> 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int bd8 = f.bitdepth - 8;
@@ -161,199 +193,208 @@ R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
     const P *Dv = plane_ptr<const P>(f.D[2]);
     const int64_t ys = f.stride[0], uvs = f.stride[1];
 
-    // ---- stage the band (clamped coordinates) ----
+    // ---- tap offsets of every direction in both tile pitches ----
+    if (tid < 96) {
+        const int chroma = tid >= 48, e = tid % 48, dir = e / 6, w = (e % 6) >> 1, k = e & 1;
+        const int which = w == 0 ? dir + 2 : (w == 1 ? dir + 4 : dir);
+        int dy, dx;
+        dir_off(f.tab.CDEF_DIRECTIONS[which * 2 + k], dy, dx);
+        if (chroma)
+            sm.toff_c[dir][w * 2 + k] = dy * CW + dx;
+        else
+            sm.toff_y[dir][w * 2 + k] = dy * TW + dx;
+    }
+    // ---- stage the region (clamped coordinates) ----
     for (int r = warp; r < TH; r += 8) {
         const int ry = gy0 - 2 + r, gy = iclip_(ry, 0, f.h - 1);
+        const bool row_out = ry < 0 || ry >= f.h;
         const P *row = Dy + gy * ys;
-        for (int c = lane; c < TW; c += 32) {
-            int rx = gx0 - 2 + c;
-            int16_t v = (int16_t)row[iclip_(rx, 0, f.w - 1)];
-            ty[r][c] = v;
-            pty[r][c] = (ry < 0 || ry >= f.h || rx < 0 || rx >= f.w) ? (int16_t)INT16_MIN : v;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int c = lane + 32 * j;
+            if (c < TW) {
+                const int rx = gx0 - 2 + c;
+                const int v = __ldg(row + iclip_(rx, 0, f.w - 1));
+                sm.ty[r][c] = (int16_t)v;
+                sm.pty[r][c] = (row_out || rx < 0 || rx >= f.w) ? (int16_t)INT16_MIN : (int16_t)v;
+                const int yy = r - 2, xx = c - 2;
+                if (yy >= 0 && yy < RH && xx >= 0 && xx < 64)
+                    sm.blk[(yy >> 3) * 8 + (xx >> 3)][(yy & 7) * 8 + (xx & 7)] = (int16_t)((v >> bd8) - 128);
+            }
         }
     }
-    for (int rr = warp; rr < 2 * CH; rr += 8) {
-        const int pl = rr / CH, r = rr % CH;
+    for (int r2 = warp; r2 < 2 * CH; r2 += 8) {
+        const int pl = r2 / CH, r = r2 % CH;
         const int ry = cy0 - 2 + r, gy = iclip_(ry, 0, f.ch - 1);
+        const bool row_out = ry < 0 || ry >= f.ch;
         const P *row = (pl ? Dv : Du) + gy * uvs;
-        for (int c = lane; c < CW; c += 32) {
-            int rx = cx0 - 2 + c;
-            int16_t v = (int16_t)row[iclip_(rx, 0, f.cw - 1)];
-            tc[pl][r][c] = v;
-            ptc[pl][r][c] = (ry < 0 || ry >= f.ch || rx < 0 || rx >= f.cw) ? (int16_t)INT16_MIN : v;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int c = lane + 32 * j;
+            if (c < CW) {
+                const int rx = cx0 - 2 + c;
+                const int v = __ldg(row + iclip_(rx, 0, f.cw - 1));
+                sm.tc[pl][r][c] = (int16_t)v;
+                sm.ptc[pl][r][c] = (row_out || rx < 0 || rx >= f.cw) ? (int16_t)INT16_MIN : (int16_t)v;
+            }
         }
     }
-    for (int i = tid; i < 8 * 96; i += 256) (&bins[0][0])[i] = 0;
 
-    // ---- superblock parameters (cdef.rs:787-907) ----
+    // ---- phase 1: superblock and per-block parameters (cdef.rs:787-907) ----
     const int sb256x = sbx >> 2, sb64x_idx = sbx & 3;
-    const int by = band * 2;  // 4x4 row of the band
-    const int by_idx = (by & 0x3e) >> 1;
-    const R2gAv2Filter &m = f.masks[(by >> 6) * f.sb256w + sb256x];
+    const int by0 = gy0 >> 2;  // 4x4 row of the region's top
+    const R2gAv2Filter &m = f.masks[(by0 >> 6) * f.sb256w + sb256x];
     const R2gFrameParams &fp = f.fp;
-    if (tid < 3) s_ccso[tid] = f.ccso_on ? m.ccso[tid] : 0;
-    const int cdef_idx = m.cdef_idx[((by & 0x30) >> 2) + (sbx & 3)];
+    if (tid < 3) sm.s_ccso[tid] = f.ccso_on ? m.ccso[tid] : 0;
+    const int cdef_idx = m.cdef_idx[((by0 & 0x30) >> 2) + (sbx & 3)];
     const int sidx = cdef_idx < 0 ? 0 : cdef_idx;
     const bool cdef_active = !(cdef_idx == -1 || !f.cdef_on ||
                                ((sidx < 8 ? fp.cdef_y_strength[sidx] : 0) == 0 &&
                                 (sidx < 8 ? fp.cdef_uv_strength[sidx] : 0) == 0));
     const int damping = fp.cdef_damping + bd8;
-    __syncthreads();
-
-    // ---- phase 1: per-8x8 decisions and direction search (warp = block) ----
-    {
-        const int bx = sbx * 16 + warp * 2;  // 4x4 column of this 8x8
+    if (warp == 0) {
+        const int b = lane, br = b >> 3, bc = b & 7;
+        const int bx = sbx * 16 + bc * 2;  // 4x4 column of this 8x8
+        const int by = by0 + br * 2;       // 4x4 row
+        const int by_idx = (by & 0x3e) >> 1;
         BlockParams p = {};
-        bool in_frame = bx < f.bw4;
-        bool need_dir = false;
+        const bool in_frame = bx < f.bw4 && gy0 + br * 8 < f.h;
+        if (f.any_lossless && in_frame) {
+            const int yr = imin_(2 * by_idx, 63);
+            const uint16_t l0 = m.lossless_mask_y[yr][sb64x_idx], l1 = m.lossless_mask_y[imin_(yr + 1, 63)][sb64x_idx];
+            // CCSO's luma lossless test is per 4x4: bits (row in block >> 2) * 2
+            // + (column in block >> 2)
+            p.y_ll = ((l0 >> (bc * 2)) & 3) | (((l1 >> (bc * 2)) & 3) << 2);
+        }
         if (cdef_active && in_frame) {
-            uint16_t noskip = fp.cdef_on_skiptx ? 0xffff : m.noskip_mask[by_idx][sb64x_idx];
+            const uint16_t noskip = fp.cdef_on_skiptx ? 0xffff : m.noskip_mask[by_idx][sb64x_idx];
             uint16_t y_ll0 = 0, y_ll1 = 0, uv_ll = 0;
             if (f.any_lossless) {
-                int yr = imin_(2 * by_idx, 63);
+                const int yr = imin_(2 * by_idx, 63);
                 y_ll0 = m.lossless_mask_y[yr][sb64x_idx];
                 y_ll1 = m.lossless_mask_y[imin_(yr + 1, 63)][sb64x_idx];
                 uv_ll = m.lossless_mask_uv[imin_(by_idx, 63)][sb64x_idx];
             }
-            uint16_t bx_mask = (uint16_t)(3u << (bx & 14));
-            bool y_lossless = ((y_ll0 | y_ll1) & bx_mask) != 0;
-            bool uv_lossless = (uv_ll & (uint16_t)(1u << ((bx & 14) >> 1))) != 0;
+            const uint16_t bx_mask = (uint16_t)(3u << (bx & 14));
+            const bool y_lossless = ((y_ll0 | y_ll1) & bx_mask) != 0;
+            const bool uv_lossless = (uv_ll & (uint16_t)(1u << ((bx & 14) >> 1))) != 0;
             if ((noskip & bx_mask) != 0 && !(y_lossless && uv_lossless)) {
-                int y_lvl = fp.cdef_y_strength[cdef_idx], uv_lvl = fp.cdef_uv_strength[cdef_idx];
-                int y_pri = (y_lvl >> 2) << bd8;
-                int y_sec = y_lvl & 3;
+                const int y_lvl = fp.cdef_y_strength[cdef_idx], uv_lvl = fp.cdef_uv_strength[cdef_idx];
+                int y_sec = y_lvl & 3, uv_sec = uv_lvl & 3;
                 y_sec += y_sec == 3;
-                y_sec <<= bd8;
-                int uv_pri = (uv_lvl >> 2) << bd8;
-                int uv_sec = uv_lvl & 3;
                 uv_sec += uv_sec == 3;
-                uv_sec <<= bd8;
                 p.active = 1;
-                p.y_pri = y_pri;
-                p.y_sec = y_sec;
-                p.uv_pri = uv_pri;
-                p.uv_sec = uv_sec;
+                p.y_pri = (y_lvl >> 2) << bd8;
+                p.y_sec = y_sec << bd8;
+                p.uv_pri = (uv_lvl >> 2) << bd8;
+                p.uv_sec = uv_sec << bd8;
                 p.y_on = !y_lossless;
                 p.uv_on = uv_lvl != 0 && !uv_lossless;
-                need_dir = y_pri != 0 || uv_pri != 0;
+                p.need_dir = p.y_pri != 0 || p.uv_pri != 0;
             }
         }
-        int dir = 0;
-        uint32_t var = 0;
-        if (need_dir) {
-            // cdef_find_dir_bd (cdef.rs:134-224): lane handles 2 samples
-            int *b = bins[warp];
-            int ly = lane >> 2, lx0 = (lane & 3) * 2;
-#pragma unroll
-            for (int k = 0; k < 2; k++) {
-                int x = lx0 + k, y = ly;
-                int px = ((int)ty[2 + y][2 + warp * 8 + x] >> bd8) - 128;
-                atomicAdd(&b[0 + (y + x)], px);            // diag0[15]
-                atomicAdd(&b[15 + (y + (x >> 1))], px);    // alt0[11]
-                atomicAdd(&b[26 + y], px);                 // hv0[8]
-                atomicAdd(&b[34 + (3 + y - (x >> 1))], px);  // alt1[11]
-                atomicAdd(&b[45 + (7 + y - x)], px);       // diag1[15]
-                atomicAdd(&b[60 + (3 - (y >> 1) + x)], px);  // alt2[11]
-                atomicAdd(&b[71 + x], px);                 // hv1[8]
-                atomicAdd(&b[79 + ((y >> 1) + x)], px);    // alt3[11]
+        sm.bp[b] = p;
+    }
+    __syncthreads();
+
+    // ---- phase 2: direction costs, warp = direction, lane = block ----
+    {
+        const int b = lane;
+        if (sm.bp[b].need_dir) {
+            const int16_t *bk = sm.blk[b];
+            uint32_t c;
+            switch (warp) {
+                case 0: c = dir_cost<0>(bk); break;
+                case 1: c = dir_cost<1>(bk); break;
+                case 2: c = dir_cost<2>(bk); break;
+                case 3: c = dir_cost<3>(bk); break;
+                case 4: c = dir_cost<4>(bk); break;
+                case 5: c = dir_cost<5>(bk); break;
+                case 6: c = dir_cost<6>(bk); break;
+                default: c = dir_cost<7>(bk); break;
             }
-            __syncwarp();
-            uint32_t cost = 0;
-            if (lane < 8) {
-                auto sq = [](int v) -> uint32_t { return (uint32_t)v * (uint32_t)v; };
-                if (lane == 2 || lane == 6) {
-                    const int *hv = b + (lane == 2 ? 26 : 71);
-                    for (int n = 0; n < 8; n++) cost += sq(hv[n]);
-                    cost *= 105u;
-                } else if (lane == 0 || lane == 4) {
-                    const int *dg = b + (lane == 0 ? 0 : 45);
-                    for (int n = 0; n < 7; n++) cost += (sq(dg[n]) + sq(dg[14 - n])) * c_div_table[n];
-                    cost += sq(dg[7]) * 105u;
-                } else {
-                    const int alt_base[4] = {15, 34, 60, 79};
-                    const int *al = b + alt_base[lane >> 1];
-                    for (int mm = 0; mm < 5; mm++) cost += sq(al[3 + mm]);
-                    cost *= 105u;
-                    for (int mm = 0; mm < 3; mm++) cost += (sq(al[mm]) + sq(al[10 - mm])) * c_div_table[2 * mm + 1];
-                }
-            }
-            // argmax over lanes 0..7, first maximum wins
-            uint32_t best = cost;
-            int bdir = lane;
-#pragma unroll
-            for (int st = 1; st < 8; st <<= 1) {
-                uint32_t oc = __shfl_xor_sync(0xffffffff, best, st);
-                int od = __shfl_xor_sync(0xffffffff, bdir, st);
-                if (oc > best || (oc == best && od < bdir)) {
-                    best = oc;
-                    bdir = od;
-                }
-            }
-            uint32_t opp = __shfl_sync(0xffffffff, cost, bdir ^ 4);
-            dir = bdir;
-            var = (best - opp) >> 10;
-        }
-        if (lane == 0) {
-            // luma strength adjust / path selection (cdef.rs:969-1012)
-            p.y_dir = dir;
-            if (p.active) {
-                int yp = 0, yd = 0;
-                bool yon = false;
-                if (p.y_pri != 0) {
-                    int adj = 0;
-                    if (var != 0) {
-                        int i = (var >> 6) != 0 ? imin_(31 - __clz((int)(var >> 6)), 12) : 0;
-                        adj = (p.y_pri * (4 + i) + 8) >> 4;
-                    }
-                    yon = (adj != 0 || p.y_sec != 0) && p.y_on;
-                    yp = adj;
-                    yd = dir;
-                } else if (p.y_sec != 0 && p.y_on) {
-                    yon = true;
-                    yp = 0;
-                    yd = 0;
-                }
-                p.y_on = yon;
-                p.y_pri = yp;
-                p.y_dir = yd;
-                p.uv_dir = p.uv_pri != 0 ? c_uv_dirs[dir] : 0;
-                tap_offsets(f.tab.CDEF_DIRECTIONS, p.y_dir, TW, p.yoff);
-                tap_offsets(f.tab.CDEF_DIRECTIONS, p.uv_dir, CW, p.uvoff);
-            }
-            bp[warp] = p;
+            sm.cost[warp][b] = c;
         }
     }
     __syncthreads();
 
-    // ---- phase 2: filter + CCSO; warp w produces 8x8 block w (uniform
-    // parameters per warp), lane -> 2 luma samples and 1 chroma sample ----
+    // ---- phase 3: direction, variance, strength adjust (cdef.rs:969-1012) ----
+    if (warp == 0) {
+        BlockParams &p = sm.bp[lane];
+        int dir = 0;
+        uint32_t var = 0;
+        if (p.need_dir) {
+            uint32_t best = sm.cost[0][lane];
+#pragma unroll
+            for (int d = 1; d < 8; d++) {
+                const uint32_t c = sm.cost[d][lane];
+                if (c > best) {
+                    best = c;
+                    dir = d;
+                }
+            }
+            var = (best - sm.cost[dir ^ 4][lane]) >> 10;
+        }
+        p.y_dir = dir;
+        if (p.active) {
+            int yp = 0, yd = 0;
+            bool yon = false;
+            if (p.y_pri != 0) {
+                int adj = 0;
+                if (var != 0) {
+                    const int i = (var >> 6) != 0 ? imin_(31 - __clz((int)(var >> 6)), 12) : 0;
+                    adj = (p.y_pri * (4 + i) + 8) >> 4;
+                }
+                yon = (adj != 0 || p.y_sec != 0) && p.y_on;
+                yp = adj;
+                yd = dir;
+            } else if (p.y_sec != 0 && p.y_on) {
+                yon = true;
+            }
+            p.y_on = yon;
+            p.y_pri = yp;
+            p.y_dir = yd;
+            p.uv_dir = p.uv_pri != 0 ? c_uv_dirs[dir] : 0;
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 4: filter + CCSO; warp w produces blocks w, w+8, w+16, w+24
+    // (uniform parameters per warp), lane -> 2 luma samples, 1 chroma sample
     const int bitdepth = f.bitdepth, bdmax = f.bdmax;
-    const BlockParams &p = bp[warp];
-    const int bx0 = warp * 8;
-    if (gx0 + bx0 < f.w) {
+    P *Cy = plane_ptr<P>(f.C[0]);
+    const R2gCcsoPlane &cp = fp.ccso[0];
+    const int cq = f.tab.CCSO_QUANT_SZ[cp.scale_idx * 4 + cp.quant_idx];
+    const int coff = c_ccso_pos[cp.ext_filter_support][0] * TW + c_ccso_pos[cp.ext_filter_support][1];
+#pragma unroll 1
+    for (int b = warp; b < NB; b += 8) {
+        const int br = b >> 3, bc = b & 7;
+        if (gx0 + bc * 8 >= f.w || gy0 + br * 8 >= f.h) continue;
+        const BlockParams &p = sm.bp[b];
+        int yoff[6], uvoff[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            yoff[k] = sm.toff_y[p.y_dir][k];
+            uvoff[k] = sm.toff_c[p.uv_dir][k];
+        }
         // luma
-        const int r = lane >> 2, c0 = bx0 + (lane & 3) * 2;
-        P *Cy = plane_ptr<P>(f.C[0]);
+        const int r = br * 8 + (lane >> 2), c0 = bc * 8 + (lane & 3) * 2;
         const int gy = gy0 + r;
         int out[2];
-        const R2gCcsoPlane &cp = fp.ccso[0];
-        const int cq = f.tab.CCSO_QUANT_SZ[cp.scale_idx * 4 + cp.quant_idx];
-        const int coff = c_ccso_pos[cp.ext_filter_support][0] * TW + c_ccso_pos[cp.ext_filter_support][1];
-        const bool lossy_row = !(f.any_lossless &&
-                                 ((m.lossless_mask_y[2 * by_idx + (r >> 2)][sb64x_idx] >> (c0 >> 2)) & 1));
+        const bool lossy_row = !(f.any_lossless && ((p.y_ll >> (((lane >> 2) >> 2) * 2 + ((lane & 3) >> 1))) & 1));
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const int c = c0 + k;
-            const int16_t *t = &ty[2 + r][2 + c];
+            const int16_t *t = &sm.ty[2 + r][2 + c];
             const int px = t[0];
             int v = px;
             if (p.active && p.y_on) {
-                v = cdef_px(&pty[2 + r][2 + c], p.y_pri, p.y_sec, p.yoff, damping, bd8);
+                v = cdef_px(&sm.pty[2 + r][2 + c], p.y_pri, p.y_sec, yoff, damping, bd8);
                 v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
             }
-            if (s_ccso[0] && lossy_row) {
+            if (sm.s_ccso[0] && lossy_row) {
                 // ccso_prep (ccso.rs:115-185): the clamped tile is the padding
-                int band_ = (int)((uint32_t)px >> (bitdepth - cp.max_band_log2));
+                const int band_ = (int)((uint32_t)px >> (bitdepth - cp.max_band_log2));
                 int idx;
                 if (cp.bo_only)
                     idx = band_ & 0xff;
@@ -361,8 +402,8 @@ R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
                     idx = ((int)((ccso_score(t[coff] - px, cq, cp.edge_clf) << 5) |
                                  (ccso_score(t[-coff] - px, cq, cp.edge_clf) << 3)) |
                            band_) & 0xff;
-                int bi = idx >> 1;
-                int packed = bi < 64 ? cp.filter_off[bi] : 0;
+                const int bi = idx >> 1;
+                const int packed = bi < 64 ? cp.filter_off[bi] : 0;
                 v = iclip_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], 0, bdmax);
             }
             out[k] = v;
@@ -370,23 +411,24 @@ R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
         Cy[gy * ys + gx0 + c0] = (P)out[0];
         Cy[gy * ys + gx0 + c0 + 1] = (P)out[1];
         // chroma: lane -> plane lane/16, row (lane%16)/4, column lane%4
-        const int pl = lane >> 4, cr = (lane & 15) >> 2, cc = (bx0 >> 1) + (lane & 3);
+        const int pl = lane >> 4, cr = br * 4 + ((lane & 15) >> 2), cc = bc * 4 + (lane & 3);
         const int cgy = cy0 + cr, cgx = cx0 + cc;
         P *Cp = plane_ptr<P>(f.C[1 + pl]);
-        int px = tc[pl][2 + cr][2 + cc];
+        const int px = sm.tc[pl][2 + cr][2 + cc];
         int v = px;
         if (p.active && p.uv_on) {
-            v = cdef_px(&ptc[pl][2 + cr][2 + cc], p.uv_pri, p.uv_sec, p.uvoff, damping - 1, bd8);
+            v = cdef_px(&sm.ptc[pl][2 + cr][2 + cc], p.uv_pri, p.uv_sec, uvoff, damping - 1, bd8);
             v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
         }
-        if (s_ccso[1 + pl]) {
+        if (sm.s_ccso[1 + pl]) {
             const R2gCcsoPlane &cpc = fp.ccso[1 + pl];
-            bool ll = f.any_lossless && ((m.lossless_mask_uv[by_idx][sb64x_idx] >> (cc >> 2)) & 1);
+            const int by_idx = ((by0 + br * 2) & 0x3e) >> 1;
+            const bool ll = f.any_lossless && ((m.lossless_mask_uv[by_idx][sb64x_idx] >> (cc >> 2)) & 1);
             if (!ll) {
                 // co-located luma of the chroma sample (ccso_prep, 4:2:0)
-                const int16_t *t = &ty[2 + 2 * cr][2 + 2 * cc];
-                int cl = t[0];
-                int band_ = (int)((uint32_t)cl >> (bitdepth - cpc.max_band_log2));
+                const int16_t *t = &sm.ty[2 + 2 * cr][2 + 2 * cc];
+                const int cl = t[0];
+                const int band_ = (int)((uint32_t)cl >> (bitdepth - cpc.max_band_log2));
                 int idx;
                 if (cpc.bo_only) {
                     idx = band_ & 0xff;
@@ -397,8 +439,8 @@ R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
                                  (ccso_score(t[-o] - cl, q, cpc.edge_clf) << 3)) |
                            band_) & 0xff;
                 }
-                int bi = idx >> 1;
-                int packed = bi < 64 ? cpc.filter_off[bi] : 0;
+                const int bi = idx >> 1;
+                const int packed = bi < 64 ? cpc.filter_off[bi] : 0;
                 v = iclip_(v + f.tab.CCSO_OFFSET[cpc.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], 0, bdmax);
             }
         }
@@ -409,12 +451,12 @@ R2G_D void cdef_band(const DevFrame &f, CdefSmem &sm, int sbx, int band) {
 template <typename P>
 __global__ void __launch_bounds__(256) cdef_ccso_kernel(const DevFrame f) {
     __shared__ CdefSmem sm;
-    cdef_band<P>(f, sm, blockIdx.x, blockIdx.y);
+    cdef_region<P>(f, sm, blockIdx.x, blockIdx.y);
 }
 
-// Persistent kernel over a cross-frame work list: item = frame << 22 | band
-// * sb64w + sbx.
-__global__ void __launch_bounds__(256) cdef_batch_kernel(BatchArgs a) {
+// Persistent kernel over a cross-frame work list: item = frame << 22 |
+// region row * sb64w + sbx.
+__global__ void __launch_bounds__(256, 6) cdef_batch_kernel(BatchArgs a) {
     __shared__ CdefSmem sm;
     const int n = a.count[1];
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
@@ -422,9 +464,9 @@ __global__ void __launch_bounds__(256) cdef_batch_kernel(BatchArgs a) {
         const DevFrame &f = a.frames[it >> 22];
         const int b = it & 0x3fffff, sb64w = (f.w + 63) >> 6;
         if (f.bitdepth > 8)
-            cdef_band<uint16_t>(f, sm, b % sb64w, b / sb64w);
+            cdef_region<uint16_t>(f, sm, b % sb64w, b / sb64w);
         else
-            cdef_band<uint8_t>(f, sm, b % sb64w, b / sb64w);
+            cdef_region<uint8_t>(f, sm, b % sb64w, b / sb64w);
         __syncthreads();
     }
 }
@@ -437,11 +479,11 @@ int r2g_batch_occupancy_cdef() {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cdef_batch_kernel, 256, 0);
     return nb;
 }
-int r2g_cdef_items(const DevFrame &f) { return f.cdef_stage_on ? ((f.w + 63) >> 6) * (f.h >> 3) : 0; }
+int r2g_cdef_items(const DevFrame &f) { return f.cdef_stage_on ? ((f.w + 63) >> 6) * ((f.h + RH - 1) / RH) : 0; }
 
 int r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
     if (!f.cdef_stage_on) return 0;
-    dim3 grid((f.w + 63) / 64, f.h / 8);
+    dim3 grid((f.w + 63) / 64, (f.h + RH - 1) / RH);
     if (f.bitdepth > 8)
         cdef_ccso_kernel<uint16_t><<<grid, 256, 0, s>>>(f);
     else
