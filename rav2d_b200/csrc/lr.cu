@@ -172,17 +172,21 @@ R2G_D int lo16(uint32_t v) { return (int)(int16_t)(v & 0xffff); }
 R2G_D int hi16(uint32_t v) { return (int)v >> 16; }
 
 // One (plane, stripe, 64-wide unit) work item; b is the per-frame item index:
-// luma items first (sby, sub-stripe, unit), then U, then V.
+// luma items first (sby, sub-stripe, 32-row half, unit), then U, then V
+// (sby, sub-stripe, unit).  A luma stripe is split into two 32-row halves
+// (separate CTAs) so that a frame gives twice as many, lighter work items.
 template <typename P>
 R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
-    const int n_luma_units = f.sbh * 2 * nux_l;
-    int plane, sby, sub, ux;
+    const int n_luma_units = f.sbh * 4 * nux_l;
+    int plane, sby, sub, ux, half = 0;
     if (b < n_luma_units) {
         plane = 0;
         ux = b % nux_l;
         b /= nux_l;
+        half = b & 1;
+        b >>= 1;
     } else {
         b -= n_luma_units;
         int per = f.sbh * 2 * nux_c;
@@ -197,6 +201,10 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     unit_geom(f, plane, sby, sub, ux, g);
     if (g.sh <= 0) return;
     const int chroma = plane != 0;
+    // rows [ro, ro + nr) of the stripe are this item's output rows (luma: one
+    // 32-row half; chroma: the whole stripe)
+    const int ro = half * 32, nr = chroma ? g.sh : imin_(32, g.sh - ro);
+    if (nr <= 0) return;
     const int64_t stride = f.stride[chroma];
     const P *Cp = plane_ptr<const P>(f.C[plane]);
     const P *Dp = plane_ptr<const P>(f.D[plane]);
@@ -222,7 +230,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                         f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
 
     if (wkind == W_NONE && !gdf_on) {
-        for (int r = warp; r < g.sh; r += 8)
+        for (int r = ro + warp; r < ro + nr; r += 8)
             for (int c = lane; c < g.uw; c += 32)
                 Lp[(int64_t)(g.y0 + r) * stride + g.x0 + c] = Cp[(int64_t)(g.y0 + r) * stride + g.x0 + c];
         return;
@@ -368,8 +376,8 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         return;
     }
 
-    // ---- luma window: rows -6 .. sh+5, columns -6 .. uw+5 ----
-    const int wh = g.sh + 12, ww = g.uw + 12;
+    // ---- luma window: rows ro-6 .. ro+nr+5 of the stripe, columns -6 .. uw+5 ----
+    const int wh = nr + 12, ww = g.uw + 12;
     {
         // source columns of this lane's window columns (the same on every row)
         int cs0[3], cs1[3];
@@ -382,7 +390,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         for (int r = warp; r < wh; r += 8) {
             int row;
             bool from_d;
-            row_src(g, r - 6, row, from_d);
+            row_src(g, ro + r - 6, row, from_d);
             const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
 #pragma unroll
             for (int j = 0; j < 3; j++) {
@@ -417,7 +425,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     __syncthreads();
 
     const int b8 = bitdepth - 8;
-    const int bh4 = g.sh >> 2, bw4 = g.uw >> 2;
+    const int bh4 = nr >> 2, bw4 = g.uw >> 2, sbh4 = g.sh >> 2;
     // ---- GDF prep (looprestoration.rs:1432-1640) ----
     if (gdf_on) {
         // GDF works in a 10-bit domain (looprestoration.rs:1450-1453): 8-bit
@@ -427,7 +435,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         // gradient cell (j, i): rows 2j-1, 2j; columns 2i-1, 2i
         // (compute_gradient_row :114-193); pair (y1, x1) sums cells
         // (y1/2 .. y1/2+1, x1/2 .. x1/2+1)
-        const int cj = (g.sh >> 1) + 1, ci = (g.uw >> 1) + 1;
+        const int cj = (nr >> 1) + 1, ci = (g.uw >> 1) + 1;
         for (int i = tid; i < cj * ci; i += 256) {
             int j = i / ci, c = i % ci;
             int gs[4] = {0, 0, 0, 0};
@@ -457,7 +465,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         const int scale = ref_dst_idx == 0 ? 8 : 5;
         const int b0 = f.tab.GDF_BIAS[bias_idx * 3], b1 = f.tab.GDF_BIAS[bias_idx * 3 + 1],
                   b2 = f.tab.GDF_BIAS[bias_idx * 3 + 2];
-        const int npairs = g.sh * (g.uw >> 1);
+        const int npairs = nr * (g.uw >> 1);
         for (int i = tid; i < npairs; i += 256) {
             int y = i / (g.uw >> 1), x1 = (i % (g.uw >> 1)) * 2;
             int j = y >> 1, c = x1 >> 1;
@@ -547,7 +555,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 for (int dx = -1; dx <= 1; dx++) {
                     int e = (dy != 0) + (dx != 0);
                     int fx = iclip_((bx & 15) + dx, 0, 15);
-                    int fy = iclip_(by + dy, 0, bh4 - 1);
+                    int fy = iclip_((ro >> 2) + by + dy, 0, sbh4 - 1);
                     s += np[e] * (((sm.noskip[fy] >> fx) & 1) == 0);
                 }
             int rnd = (1 << b8) >> 1;
@@ -576,12 +584,12 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         for (int k = 0; k < 16; k++) single[k] = src[k];
     }
     const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
-    for (int y = warp; y < g.sh; y += 8)
+    for (int y = warp; y < nr; y += 8)
         for (int x = lane; x < g.uw; x += 32) {
             const int16_t *w = &W16[2 * ((y + 6) * LW + x + 6)];
             int m = w[0];
             int v = m;
-            bool ll = (sm.llm[y >> 2] >> (x >> 2)) & 1;
+            bool ll = (sm.llm[(ro + y) >> 2] >> (x >> 2)) & 1;
             if (!ll && wkind != W_NONE) {
                 int s;
                 if (wkind == W_PC) {
@@ -609,7 +617,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 int ad = diff < 0 ? -diff : diff;
                 v = iclip_(v + apply_sign_((ad + grnd) >> gshift, diff), 0, bdmax);
             }
-            Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
+            Lp[(int64_t)(g.y0 + ro + y) * stride + g.x0 + x] = (P)v;
         }
 }
 
@@ -650,7 +658,7 @@ int r2g_batch_occupancy_lr() {
 }
 int r2g_lr_items(const DevFrame &f) {
     if (!f.lr_on) return 0;
-    return f.sbh * 2 * ((f.w + 63) >> 6) + 2 * f.sbh * 2 * ((f.cw + 63) >> 6);
+    return f.sbh * 4 * ((f.w + 63) >> 6) + 2 * f.sbh * 2 * ((f.cw + 63) >> 6);
 }
 
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
