@@ -214,6 +214,19 @@ const char *r2g_last_error(R2gCtx *ctx);
 /* Enqueue the context's filter work on a caller-owned CUDA stream
  * (a cudaStream_t passed as void*; NULL restores the context's own stream). */
 int r2g_ctx_set_stream(R2gCtx *ctx, void *stream);
+/* Copy overlap (no counterpart in the reference, whose filters work on host
+ * memory): when enabled, r2g_frame_upload_recon and r2g_frame_stage copy on
+ * an upload stream and r2g_download on a download stream of the context,
+ * each frame's copies and kernels ordered by events, so the transfers of one
+ * frame overlap the kernels of another.  r2g_sync waits for all three
+ * streams; r2g_ctx_fence makes the context stream wait for every copy issued
+ * so far (an event recorded on it afterwards marks the end of all of them).
+ * In this mode host buffers are read asynchronously: page-locked recon
+ * planes, and side-info records that are page-locked (they are then copied
+ * without staging), must stay unchanged until the frame's work completes.
+ * Off by default: then every call runs on the context stream in order. */
+int r2g_ctx_overlap_copies(R2gCtx *ctx, int enable);
+int r2g_ctx_fence(R2gCtx *ctx);
 /* Instrumentation (no counterpart in the reference): when enabled, every
  * r2g_frame_run / r2g_frame_grain records CUDA events between its kernels;
  * r2g_ctx_profile_read synchronises and returns per-stage milliseconds and
@@ -231,7 +244,8 @@ int r2g_frame_free(R2gCtx *ctx, R2gFrame *f);
 int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, int64_t y_stride,
                            const void *u, const void *v, int64_t uv_stride);
 /* Stage the frame's side-info on the device (validate, apply the bottom-edge
- * crop, upload masks / restoration records / segment maps) without running
+ * crop (applied by the deblock kernel), upload masks / restoration records /
+ * segment maps) without running
  * any stage; r2g_frame_run then runs the stages on the staged side-info. */
 int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,
                     uint32_t inloop_mask);

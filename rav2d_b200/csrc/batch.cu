@@ -373,7 +373,15 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
         rc = build_graph(ctx, b, s, grids, tpl_grid);
         if (rc != R2G_OK) return rc;
     }
+    for (int i = 0; i < n; i++) {
+        rc = r2g_frame_before_compute(ctx, items[i].frame);
+        if (rc != R2G_OK) return rc;
+    }
     if (cudaGraphLaunch(s.exec, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
+    for (int i = 0; i < n; i++) {
+        rc = r2g_frame_after_compute(ctx, items[i].frame);
+        if (rc != R2G_OK) return rc;
+    }
     ctx->launches += 5;
     if (cudaEventRecord(s.done, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
     s.used = true;

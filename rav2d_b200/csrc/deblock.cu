@@ -271,6 +271,17 @@ R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, 
     const uint16_t(*km)[4] = m.filter_y[dir][pos];
     int k3 = (km[3][idx] >> bit) & 1, k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1,
         k0 = (km[0][idx] >> bit) & 1;
+    if (dir == 1) {
+        // deblock_crop_bottom_edge (deblock.rs:1572-1606), applied as the
+        // masks are read: in a 64-row band that overhangs the frame bottom
+        // (by more than the last 4 rows of 4x4s), the horizontal edges of the
+        // band's second-to-last 4x4 row lose class 3 (32-long) to class 2
+        const int y64 = y4 >> 4;
+        if ((y64 + 1) * 16 + 4 > f.bh4 && (y4 & 15) == imin_(f.bh4 - y64 * 16, 16) - 2) {
+            k2 |= k3;
+            k3 = 0;
+        }
+    }
     if (!(k0 | k1 | k2 | k3)) return;
     int cls = k3 ? 3 : k2 ? 2 : k1;
     int mwp = c_max_width_y[cls];

@@ -501,7 +501,10 @@ extern "C" int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData 
         return R2G_E_INVALID;
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return R2G_E_DEVICE;
-    return r2g_grain_enqueue(ctx, f, fgd, seed);
+    int rc = r2g_frame_before_compute(ctx, f);
+    if (rc == R2G_OK) rc = r2g_grain_enqueue(ctx, f, fgd, seed);
+    if (rc == R2G_OK) rc = r2g_frame_after_compute(ctx, f);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

@@ -39,6 +39,11 @@ struct R2gCtx {
     GrainCtx *grain = nullptr;
     BatchState *batch = nullptr;
     cudaStream_t own_stream = nullptr;
+    // copy overlap (r2g_ctx_overlap_copies): per-frame uploads / staging on
+    // up_stream, downloads on down_stream, ordered by per-frame events
+    bool overlap = false;
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    cudaEvent_t fence_ev[2] = {nullptr, nullptr};
     int64_t launches = 0;
     bool profiling = false;
     std::vector<ProfRun> prof;
@@ -65,6 +70,10 @@ struct R2gFrame {
     bool staged = false;
     void *grain_scratch = nullptr;  // batched film grain (R2G_GRAIN_SCRATCH)
     DevFrame desc{};
+    // copy-overlap ordering: last upload / staging (up stream), last kernels
+    // (context stream), last download (down stream) of this frame
+    cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_down = nullptr;
+    bool pend_up = false, pend_comp = false, pend_down = false;
 };
 
 int r2g_dev_alloc(R2gCtx *ctx, void **p, size_t bytes);
@@ -84,6 +93,11 @@ int r2g_grain_validate(const R2gFilmGrainData *fgd, uint32_t seed);
 // context stream), kernels on the context stream after them.
 int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_t copy_stream);
 void r2g_launch_pipeline(R2gCtx *ctx, const DevFrame &d);
+// Copy-overlap ordering of one frame's kernels on the context stream: wait
+// for its pending upload and download before, record after (no-ops unless
+// the context overlaps copies).
+int r2g_frame_before_compute(R2gCtx *ctx, R2gFrame *f);
+int r2g_frame_after_compute(R2gCtx *ctx, R2gFrame *f);
 // Profiling hooks around one stage (no-ops unless profiling is enabled).
 void r2g_prof_stage(R2gCtx *ctx, int stage, bool begin, int launches);
 int r2g_ticket_record(R2gCtx *ctx, uint64_t *ticket);

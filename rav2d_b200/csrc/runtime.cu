@@ -98,6 +98,13 @@ extern "C" int r2g_ctx_destroy(R2gCtx *ctx) {
     r2g_grain_ctx_free(ctx);
     r2g_batch_free(ctx);
     r2g_ctx_profile(ctx, 0);
+    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    for (cudaEvent_t e : ctx->fence_ev)
+        if (e) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->own_stream ? ctx->own_stream : ctx->stream);
     cudaStreamDestroy(ctx->side_stream);
     delete ctx;
@@ -184,6 +191,10 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     if (!ctx || !f) return R2G_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
+        if (st) cudaStreamSynchronize(st);
+    for (cudaEvent_t e : {f->ev_up, f->ev_comp, f->ev_down})
+        if (e) cudaEventDestroy(e);
     for (int i = 0; i < 5; i++) r2g_dev_free(ctx, f->buf[i], f->buf_bytes);
     r2g_dev_free(ctx, f->side_dev, f->side_bytes);
     r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
@@ -226,11 +237,89 @@ int r2g_copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, int6
     return R2G_OK;
 }
 
+// ---- copy overlap: per-frame ordering across the three streams
+static int ensure_events(R2gCtx *ctx, R2gFrame *f) {
+    for (cudaEvent_t *e : {&f->ev_up, &f->ev_comp, &f->ev_down})
+        if (!*e) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return R2G_OK;
+}
+
+// The stream a frame's upload / staging goes on.  With overlap, the copy
+// must not overwrite the recon or side-info while earlier kernels of this
+// frame may still read them.
+static int upload_stream(R2gCtx *ctx, R2gFrame *f, cudaStream_t *st) {
+    *st = ctx->stream;
+    if (!ctx->overlap) return R2G_OK;
+    int rc = ensure_events(ctx, f);
+    if (rc != R2G_OK) return rc;
+    if (f->pend_comp) CK(cudaStreamWaitEvent(ctx->up_stream, f->ev_comp, 0));
+    *st = ctx->up_stream;
+    return R2G_OK;
+}
+
+static int upload_done(R2gCtx *ctx, R2gFrame *f) {
+    if (!ctx->overlap) return R2G_OK;
+    CK(cudaEventRecord(f->ev_up, ctx->up_stream));
+    f->pend_up = true;
+    return R2G_OK;
+}
+
+int r2g_frame_before_compute(R2gCtx *ctx, R2gFrame *f) {
+    if (!ctx->overlap || !f->ev_up) return R2G_OK;
+    // the kernels read this frame's uploads and overwrite planes a pending
+    // download may still read
+    if (f->pend_up) CK(cudaStreamWaitEvent(ctx->stream, f->ev_up, 0));
+    if (f->pend_down) CK(cudaStreamWaitEvent(ctx->stream, f->ev_down, 0));
+    return R2G_OK;
+}
+
+int r2g_frame_after_compute(R2gCtx *ctx, R2gFrame *f) {
+    if (!ctx->overlap) return R2G_OK;
+    int rc = ensure_events(ctx, f);
+    if (rc != R2G_OK) return rc;
+    CK(cudaEventRecord(f->ev_comp, ctx->stream));
+    f->pend_comp = true;
+    return R2G_OK;
+}
+
+extern "C" int r2g_ctx_overlap_copies(R2gCtx *ctx, int enable) {
+    if (!ctx) return R2G_E_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    if (enable && !ctx->up_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&ctx->down_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t &e : ctx->fence_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (!enable && ctx->up_stream) {
+        // later work goes on the context stream again: order it after every
+        // copy issued so far
+        int rc = r2g_ctx_fence(ctx);
+        if (rc != R2G_OK) return rc;
+    }
+    ctx->overlap = enable != 0;
+    return R2G_OK;
+}
+
+extern "C" int r2g_ctx_fence(R2gCtx *ctx) {
+    if (!ctx) return R2G_E_INVALID;
+    if (!ctx->up_stream) return R2G_OK;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventRecord(ctx->fence_ev[0], ctx->up_stream));
+    CK(cudaEventRecord(ctx->fence_ev[1], ctx->down_stream));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->fence_ev[0], 0));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->fence_ev[1], 0));
+    return R2G_OK;
+}
+
 extern "C" int r2g_frame_upload_recon(R2gCtx *ctx, R2gFrame *f, const void *y, int64_t y_stride, const void *u,
                                       const void *v, int64_t uv_stride) {
     if (!ctx || !f || !y || !u || !v) return R2G_E_INVALID;
     CK(cudaSetDevice(ctx->device));
-    return r2g_copy_planes(ctx, f, 0, y, y_stride, u, v, uv_stride, true, ctx->stream);
+    cudaStream_t st;
+    int rc = upload_stream(ctx, f, &st);
+    if (rc == R2G_OK) rc = r2g_copy_planes(ctx, f, 0, y, y_stride, u, v, uv_stride, true, st);
+    if (rc == R2G_OK) rc = upload_done(ctx, f);
+    return rc;
 }
 
 extern "C" int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_t y_stride, void *u, void *v,
@@ -242,7 +331,15 @@ extern "C" int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_
         set_err(ctx, which ? "frame has no grained copy" : "frame not filtered");
         return R2G_E_INVALID;
     }
-    return r2g_copy_planes(ctx, f, buf, y, y_stride, u, v, uv_stride, false, ctx->stream);
+    if (!ctx->overlap) return r2g_copy_planes(ctx, f, buf, y, y_stride, u, v, uv_stride, false, ctx->stream);
+    int rc = ensure_events(ctx, f);
+    if (rc != R2G_OK) return rc;
+    if (f->pend_comp) CK(cudaStreamWaitEvent(ctx->down_stream, f->ev_comp, 0));
+    rc = r2g_copy_planes(ctx, f, buf, y, y_stride, u, v, uv_stride, false, ctx->down_stream);
+    if (rc != R2G_OK) return rc;
+    CK(cudaEventRecord(f->ev_down, ctx->down_stream));
+    f->pend_down = true;
+    return R2G_OK;
 }
 
 extern "C" int r2g_sync(R2gCtx *ctx) {
@@ -250,6 +347,8 @@ extern "C" int r2g_sync(R2gCtx *ctx) {
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->side_stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
+        if (st) CK(cudaStreamSynchronize(st));
     return R2G_OK;
 }
 
@@ -303,30 +402,6 @@ int r2g_validate(R2gCtx *ctx, const R2gFrame *f, const R2gFrameParams *fp, const
         // segmentation with no map: every block is segment 0
     }
     return R2G_OK;
-}
-
-// deblock.rs:1572-1606 deblock_crop_bottom_edge, applied to the staged masks
-// for every superblock row (it only touches the last 64-row band).
-static void crop_bottom_edge(R2gAv2Filter *mask, int n, int sb256w, int bw, int bh) {
-    int sbh = (bh + 15) >> 4;
-    for (int y64 = 0; y64 < sbh; y64++) {
-        if ((y64 + 1) * 16 + 4 <= bh) continue;
-        int starty4 = (y64 * 16) & 0x30;
-        int h4 = bh - y64 * 16 < 16 ? bh - y64 * 16 : 16;
-        int crop_y4 = starty4 + h4 - 2;
-        if (crop_y4 < 0) continue;
-        int mask_row = (y64 >> 2) * sb256w;
-        for (int x256 = 0; x256 < sb256w; x256++) {
-            if (mask_row + x256 >= n) break;
-            int w = 64 < bw - x256 * 64 ? 64 : bw - x256 * 64;
-            uint16_t(*yv)[4] = mask[mask_row + x256].filter_y[1][crop_y4];
-            for (int i = 0; i < ((w + 15) >> 4); i++) {
-                uint16_t m = yv[3][i];
-                yv[3][i] = 0;
-                yv[2][i] |= m;
-            }
-        }
-    }
 }
 
 int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t inloop,
@@ -386,16 +461,32 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
         d.gdf_ref_dst_idx = TBL[md < 11 ? md : 11];
     }
 
-    // stage side-info: masks (cropped) + restoration records, then segmaps;
-    // the pinned staging buffer is reused, so wait for its previous upload
+    // stage side-info: masks + restoration records, then segmaps (the
+    // deblock kernel applies the reference's bottom-edge crop as it reads
+    // the masks).  Records in page-locked memory are copied straight to the
+    // device when the context overlaps copies (asynchronously: the caller
+    // keeps them unchanged until the frame's work completes); otherwise they
+    // go through the frame's pinned staging buffer, which is reused, so wait
+    // for its previous upload first.
     if (!f->side_done) CK(cudaEventCreateWithFlags(&f->side_done, cudaEventDisableTiming));
-    CK(cudaEventSynchronize(f->side_done));
     size_t mbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Filter);
     size_t lbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Restoration);
-    memcpy(f->side_host, side->masks, mbytes);
-    memcpy((char *)f->side_host + mbytes, side->lr, lbytes);
-    if (d.deblock_on) crop_bottom_edge((R2gAv2Filter *)f->side_host, f->n_sb256, d.sb256w, d.bw4, d.bh4);
-    CK(cudaMemcpyAsync(f->side_dev, f->side_host, mbytes + lbytes, cudaMemcpyHostToDevice, cs));
+    bool direct = false;
+    if (ctx->overlap) {
+        cudaPointerAttributes am, al;
+        direct = cudaPointerGetAttributes(&am, side->masks) == cudaSuccess && am.type == cudaMemoryTypeHost &&
+                 cudaPointerGetAttributes(&al, side->lr) == cudaSuccess && al.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+    }
+    if (direct) {
+        CK(cudaMemcpyAsync(f->side_dev, side->masks, mbytes, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpyAsync((char *)f->side_dev + mbytes, side->lr, lbytes, cudaMemcpyHostToDevice, cs));
+    } else {
+        CK(cudaEventSynchronize(f->side_done));
+        memcpy(f->side_host, side->masks, mbytes);
+        memcpy((char *)f->side_host + mbytes, side->lr, lbytes);
+        CK(cudaMemcpyAsync(f->side_dev, f->side_host, mbytes + lbytes, cudaMemcpyHostToDevice, cs));
+    }
     d.masks = (const R2gAv2Filter *)f->side_dev;
     d.lr = (const R2gAv2Restoration *)((char *)f->side_dev + mbytes);
     size_t seg_y = side->segmap ? (size_t)side->segmap_stride * d.bh4 : 0;
@@ -528,10 +619,12 @@ extern "C" int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *f
                                uint32_t inloop_mask) {
     if (!ctx || !f) return R2G_E_INVALID;
     CK(cudaSetDevice(ctx->device));
-    int rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, nullptr);
+    cudaStream_t st;
+    int rc = upload_stream(ctx, f, &st);
+    if (rc == R2G_OK) rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, st);
     if (rc != R2G_OK) return rc;
     f->staged = true;
-    return R2G_OK;
+    return upload_done(ctx, f);
 }
 
 extern "C" int r2g_frame_run(R2gCtx *ctx, R2gFrame *f) {
@@ -541,9 +634,11 @@ extern "C" int r2g_frame_run(R2gCtx *ctx, R2gFrame *f) {
         return R2G_E_INVALID;
     }
     CK(cudaSetDevice(ctx->device));
+    int rc = r2g_frame_before_compute(ctx, f);
+    if (rc != R2G_OK) return rc;
     r2g_launch_pipeline(ctx, f->desc);
     CK(cudaGetLastError());
-    return R2G_OK;
+    return r2g_frame_after_compute(ctx, f);
 }
 
 extern "C" int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,

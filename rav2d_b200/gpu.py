@@ -23,6 +23,7 @@ SYMBOLS = [
     "r2g_frame_stage", "r2g_frame_run", "r2g_ctx_set_stream", "r2g_ctx_profile", "r2g_ctx_profile_read",
     "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config", "r2g_server_create",
     "r2g_server_submit", "r2g_server_wait", "r2g_server_close_stream", "r2g_server_stats", "r2g_server_destroy",
+    "r2g_ctx_overlap_copies", "r2g_ctx_fence",
 ]
 
 
@@ -71,6 +72,8 @@ def lib():
         L.r2g_server_close_stream.argtypes = [C.c_void_p, C.c_int32]
         L.r2g_server_stats.argtypes = [C.c_void_p, C.POINTER(abi.ServeStats), C.c_int]
         L.r2g_server_destroy.argtypes = [C.c_void_p]
+        L.r2g_ctx_overlap_copies.argtypes = [C.c_void_p, C.c_int]
+        L.r2g_ctx_fence.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -111,6 +114,14 @@ class Context:
     def set_stream(self, stream_handle):
         """Enqueue on a caller-owned cudaStream_t (an int handle; 0 = own)."""
         self.check(lib().r2g_ctx_set_stream(self.h, C.c_void_p(stream_handle or None)))
+
+    def overlap_copies(self, enable=True):
+        """Uploads / downloads on their own streams, overlapping kernels."""
+        self.check(lib().r2g_ctx_overlap_copies(self.h, int(enable)))
+
+    def fence(self):
+        """Make the context stream wait for every copy issued so far."""
+        self.check(lib().r2g_ctx_fence(self.h))
 
     def profile(self, enable=True):
         self.check(lib().r2g_ctx_profile(self.h, int(enable)))
