@@ -23,7 +23,7 @@ namespace {
 enum { LR_HAVE_LEFT = 1, LR_HAVE_RIGHT = 2, LR_HAVE_TOP = 4, LR_HAVE_BOTTOM = 8 };
 
 constexpr int LW = 76;   // luma window width: -6 .. 69
-constexpr int LH = 76;   // luma window height: -6 .. 69 (stripe <= 64 rows)
+constexpr int LH = 44;   // luma window height: -6 .. 37 (a work item has <= 32 rows)
 constexpr int CWW = 68;  // chroma window width: -2 .. 65
 constexpr int CWH = 36;  // chroma window height: -2 .. 33 (stripe <= 32 rows)
 
@@ -156,13 +156,13 @@ struct LrSmem {
             int16_t lwin[CWH * CWW];  // downsampled luma window
         } ch;
     } u;
-    uint16_t gcell[33 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
-    int8_t gerr[64 * 64];
+    uint16_t gcell[17 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
+    int8_t gerr[32 * 64];
     int8_t s_err[4096];
     uint2 s_aa[4][18];   // per class and tap: (alpha, alpha), (-alpha, -alpha) as s16x2
     int4 s_w[4][22];     // per class and tap / feature: weights 0..2, alpha
     int16_t s_pcf[64 * 13];  // PC-Wiener filters of this frame's wiener_idx
-    uint8_t classes[16][16];
+    uint8_t classes[8][16];
     uint16_t noskip[18];
     uint16_t llm[17];
 };
@@ -622,7 +622,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
 }
 
 template <typename P>
-__global__ void __launch_bounds__(256) lr_kernel(const DevFrame f) {
+__global__ void __launch_bounds__(256, 4) lr_kernel(const DevFrame f) {
     __shared__ LrSmem sm;
     lr_unit<P>(f, sm, blockIdx.x);
 }
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(256) lr_kernel(const DevFrame f) {
 __device__ __noinline__ void lr_unit_hbd(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint16_t>(f, sm, b); }
 __device__ __noinline__ void lr_unit_8(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint8_t>(f, sm, b); }
 
-__global__ void __launch_bounds__(256, 3) lr_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(256, 4) lr_batch_kernel(BatchArgs a) {
     __shared__ LrSmem sm;
     const int n = a.count[2];
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
