@@ -252,14 +252,37 @@ constexpr int CT = 48;   // chroma staged span: origin - 8 .. + 40
 constexpr int CO = 8;    // chroma halo
 constexpr int CP = 50;   // chroma row pitch
 
+// One resolved edge segment: thresholds and geometry in the staged span.
+//   qs  = q_thr | side_thr << 16
+//   geo = x | y << 8 | mwp << 16 | mwn << 20 | pos_ll << 24 | neg_ll << 25
+struct EdgeDesc {
+    uint32_t qs, geo;
+};
+
+// Per-tile edge lists (upper bounds: every segment position of the span).
+constexpr int NVL = 19 * 22, NVC = 2 * 9 * 12, NHL = 19 * 16, NHC = 2 * 9 * 8;
+
 struct DeblockSmem {
     int16_t y[LT * LP];
     int16_t uv[2][CT * CP];
+    EdgeDesc vl[NVL], vc[NVC], hl[NHL], hc[NHC];  // vertical / horizontal, luma / chroma
+    int n[4];  // list lengths: vl, vc, hl, hc
 };
 
-// One luma edge segment.  dir 0: vertical edge at column x, rows y..y+3;
-// dir 1: horizontal edge at row y, columns x..x+3.  (x, y) are frame
-// coordinates; `sy`/`sx` the tile origin of the staged span.
+R2G_D void push_edge(DeblockSmem &sm, int list, EdgeDesc d) {
+    EdgeDesc *dst = list == 0 ? sm.vl : list == 1 ? sm.vc : list == 2 ? sm.hl : sm.hc;
+    dst[atomicAdd(&sm.n[list], 1)] = d;
+}
+
+R2G_D uint32_t pack_geo(int x, int y, int mwp, int mwn, bool pos_ll, bool neg_ll) {
+    return (uint32_t)x | ((uint32_t)y << 8) | ((uint32_t)mwp << 16) | ((uint32_t)mwn << 20) |
+           ((uint32_t)pos_ll << 24) | ((uint32_t)neg_ll << 25);
+}
+
+// Resolve one luma edge segment (masks, class, widths, thresholds, lossless
+// sides) into the tile's list.  dir 0: vertical edge at column x, rows
+// y..y+3; dir 1: horizontal edge at row y, columns x..x+3.  (x, y) are frame
+// coordinates; `sx`/`sy` the origin of the staged span.
 R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, int sx, int sy) {
     const int x4 = x >> 2, y4 = y >> 2;
     if (x4 >= f.bw4 || y4 >= f.bh4 || x < 0 || y < 0) return;
@@ -292,14 +315,12 @@ R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, 
     luma_thr(f, dir, x4, y4, nx4, ny4, subpu, q, s);
     const R2gAv2Filter &mn = f.masks[(ny4 >> 6) * f.sb256w + (nx4 >> 6)];
     bool pos_ll = ll_y(m, x4, y4), neg_ll = ll_y(mn, nx4, ny4);
-    int16_t *e = &sm.y[(y - sy) * LP + (x - sx)];
-    if (dir == 0)
-        filter_edge(e, LP, 1, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
-    else
-        filter_edge(e, 1, LP, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+    push_edge(sm, dir == 0 ? 0 : 2, EdgeDesc{q | (s << 16), pack_geo(x - sx, y - sy, mwp, mwn, pos_ll, neg_ll)});
 }
 
-// One chroma edge segment, both planes (U and V share masks and widths).
+// One chroma edge segment position: a descriptor per enabled plane (U and V
+// share masks and widths; thresholds differ); plane 1 (V) is flagged by
+// bit 26 of the geometry word.
 R2G_D void chroma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int cx, int cy, int sx, int sy) {
     const R2gFrameParams &fp = f.fp;
     const int cx4 = cx >> 2, cy4 = cy >> 2;
@@ -324,11 +345,27 @@ R2G_D void chroma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int cx, int 
         if (!(pl ? fp.deblock_level_v : fp.deblock_level_u)) continue;
         uint32_t q, s;
         chroma_thr(f, pl, cx4, cy4, nx4, ny4, subpu, q, s);
-        int16_t *e = &sm.uv[pl][(cy - sy) * CP + (cx - sx)];
-        if (dir == 0)
-            filter_edge(e, CP, 1, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
-        else
-            filter_edge(e, 1, CP, q, s, mwp, mwn, pos_ll, neg_ll, f.bdmax);
+        push_edge(sm, dir == 0 ? 1 : 3,
+                  EdgeDesc{q | (s << 16), pack_geo(cx - sx, cy - sy, mwp, mwn, pos_ll, neg_ll) | ((uint32_t)pl << 26)});
+    }
+}
+
+// Filter the listed luma edges, then the chroma edges, of one direction.
+template <int DIR>
+R2G_D void run_edges(DeblockSmem &sm, const EdgeDesc *lum, int nl, const EdgeDesc *chr, int nc, int bdmax) {
+    for (int i = threadIdx.x; i < nl + nc; i += blockDim.x) {
+        const bool luma = i < nl;
+        const EdgeDesc d = luma ? lum[i] : chr[i - nl];
+        const int x = d.geo & 0xff, y = (d.geo >> 8) & 0xff, mwp = (d.geo >> 16) & 15, mwn = (d.geo >> 20) & 15;
+        const bool pos_ll = (d.geo >> 24) & 1, neg_ll = (d.geo >> 25) & 1;
+        const uint32_t q = d.qs & 0xffff, s = d.qs >> 16;
+        if (luma) {
+            int16_t *e = &sm.y[y * LP + x];
+            filter_edge(e, DIR == 0 ? LP : 1, DIR == 0 ? 1 : LP, q, s, mwp, mwn, pos_ll, neg_ll, bdmax);
+        } else {
+            int16_t *e = &sm.uv[(d.geo >> 26) & 1][y * CP + x];
+            filter_edge(e, DIR == 0 ? CP : 1, DIR == 0 ? 1 : CP, q, s, mwp, mwn, pos_ll, neg_ll, bdmax);
+        }
     }
 }
 
@@ -342,6 +379,8 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
     const int lsx = x0 - LO, lsy = y0 - LO, csx = cx0 - CO, csy = cy0 - CO;
     const P *Ry = plane_ptr<const P>(f.R[0]);
     const int64_t ys = f.stride[0], uvs = f.stride[1];
+    if (tid < 4) sm.n[tid] = 0;
+    __syncthreads();  // list counters reset before any thread appends
     // ---- stage R (samples outside the frame read 0; no valid edge uses them)
     for (int i = tid; i < LT * (LT / 4); i += nt) {
         int r = i / (LT / 4), c4 = (i % (LT / 4)) * 4;
@@ -371,36 +410,42 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
         }
         for (int k = 0; k < 4; k++) sm.uv[pl][r * CP + c4 + k] = (int16_t)v[k];
     }
-    __syncthreads();
+    // (no barrier: resolving the edges reads only the masks, so it overlaps
+    // the staging loads; the barrier below covers both)
     const bool do_y_v = fp.deblock_level_y[0] != 0, do_y_h = fp.deblock_level_y[1] != 0;
     const bool do_uv = fp.deblock_level_u || fp.deblock_level_v;
-    // ---- vertical edges: luma columns x0-4 .. x0+68 on rows y0-12 .. y0+75,
-    // chroma columns cx0 .. cx0+32 on rows cy0-8 .. cy0+39
+    // ---- resolve every edge segment that can matter into the tile's lists:
+    // vertical luma columns x0-4 .. x0+68 on rows y0-12 .. y0+75, chroma
+    // columns cx0 .. cx0+32 on rows cy0-8 .. cy0+39; horizontal luma rows
+    // y0-4 .. y0+68 on columns x0 .. x0+63, chroma rows cy0 .. cy0+32 on
+    // columns cx0 .. cx0+31
     {
-        const int nlv = do_y_v ? 19 * 22 : 0, ncv = do_uv ? 9 * 12 : 0;
-        for (int i = tid; i < nlv + ncv; i += nt) {
-            if (i < nlv)
-                luma_edge(f, sm, 0, x0 - 4 + 4 * (i % 19), lsy + 4 * (i / 19), lsx, lsy);
-            else {
-                int j = i - nlv;
-                chroma_edge(f, sm, 0, cx0 + 4 * (j % 9), csy + 4 * (j / 9), csx, csy);
+        const int nlv = do_y_v ? NVL : 0, ncv = do_uv ? NVC / 2 : 0;
+        const int nlh = do_y_h ? NHL : 0, nch = do_uv ? NHC / 2 : 0;
+        for (int i = tid; i < nlv + ncv + nlh + nch; i += nt) {
+            int j = i;
+            if (j < nlv) {
+                luma_edge(f, sm, 0, x0 - 4 + 4 * (j % 19), lsy + 4 * (j / 19), lsx, lsy);
+                continue;
             }
+            j -= nlv;
+            if (j < ncv) {
+                chroma_edge(f, sm, 0, cx0 + 4 * (j % 9), csy + 4 * (j / 9), csx, csy);
+                continue;
+            }
+            j -= ncv;
+            if (j < nlh) {
+                luma_edge(f, sm, 1, x0 + 4 * (j % 16), y0 - 4 + 4 * (j / 16), lsx, lsy);
+                continue;
+            }
+            j -= nlh;
+            chroma_edge(f, sm, 1, cx0 + 4 * (j % 8), cy0 + 4 * (j / 8), csx, csy);
         }
     }
     __syncthreads();
-    // ---- horizontal edges: luma rows y0-4 .. y0+68 on columns x0 .. x0+63,
-    // chroma rows cy0 .. cy0+32 on columns cx0 .. cx0+31
-    {
-        const int nlh = do_y_h ? 19 * 16 : 0, nch = do_uv ? 9 * 8 : 0;
-        for (int i = tid; i < nlh + nch; i += nt) {
-            if (i < nlh)
-                luma_edge(f, sm, 1, x0 + 4 * (i % 16), y0 - 4 + 4 * (i / 16), lsx, lsy);
-            else {
-                int j = i - nlh;
-                chroma_edge(f, sm, 1, cx0 + 4 * (j % 8), cy0 + 4 * (j / 8), csx, csy);
-            }
-        }
-    }
+    run_edges<0>(sm, sm.vl, sm.n[0], sm.vc, sm.n[1], f.bdmax);
+    __syncthreads();
+    run_edges<1>(sm, sm.hl, sm.n[2], sm.hc, sm.n[3], f.bdmax);
     __syncthreads();
     // ---- write the tile
     P *Dy = plane_ptr<P>(f.D[0]);
