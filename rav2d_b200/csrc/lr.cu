@@ -16,6 +16,8 @@
 //   at the frame left / right: the row's first / last sample repeated.
 // Each CTA materialises exactly that window for one (plane, stripe, 64-wide
 // unit) in shared memory and evaluates every restoration tap from it.
+#include <type_traits>
+
 #include "r2g_common.cuh"
 
 namespace {
@@ -172,14 +174,16 @@ R2G_D int lo16(uint32_t v) { return (int)(int16_t)(v & 0xffff); }
 R2G_D int hi16(uint32_t v) { return (int)v >> 16; }
 
 // One (plane, stripe, 64-wide unit) work item; b is the per-frame item index:
-// luma items first (sby, sub-stripe, 32-row half, unit), then U, then V
-// (sby, sub-stripe, unit).  A luma stripe is split into two 32-row halves
-// (separate CTAs) so that a frame gives twice as many, lighter work items.
+// luma items first (stripe slot, 32-row half, unit), then U, then V (stripe
+// slot, unit).  Slots 0 .. sbh-1 are the superblock rows' first stripes;
+// slot sbh is the second stripe that only the last superblock row can have.
+// A luma stripe is split into two 32-row halves (separate CTAs) so that a
+// frame gives twice as many, lighter work items.
 template <typename P>
 R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
-    const int n_luma_units = f.sbh * 4 * nux_l;
+    const int n_luma_units = (f.sbh + 1) * 2 * nux_l;
     int plane, sby, sub, ux, half = 0;
     if (b < n_luma_units) {
         plane = 0;
@@ -189,14 +193,14 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         b >>= 1;
     } else {
         b -= n_luma_units;
-        int per = f.sbh * 2 * nux_c;
+        const int per = (f.sbh + 1) * nux_c;
         plane = 1 + b / per;
         b %= per;
         ux = b % nux_c;
         b /= nux_c;
     }
-    sub = b & 1;
-    sby = b >> 1;
+    sub = b >= f.sbh;
+    sby = sub ? f.sbh - 1 : b;
     UnitGeom g;
     unit_geom(f, plane, sby, sub, ux, g);
     if (g.sh <= 0) return;
@@ -230,9 +234,14 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                         f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
 
     if (wkind == W_NONE && !gdf_on) {
-        for (int r = ro + warp; r < ro + nr; r += 8)
-            for (int c = lane; c < g.uw; c += 32)
-                Lp[(int64_t)(g.y0 + r) * stride + g.x0 + c] = Cp[(int64_t)(g.y0 + r) * stride + g.x0 + c];
+        // unfiltered unit: copy C -> L in 4-byte words (unit widths are
+        // multiples of 4 samples; rows and unit origins are 64-byte aligned)
+        const int wpr = g.uw * (int)sizeof(P) / 4;
+        for (int i = tid; i < nr * wpr; i += 256) {
+            const int r = ro + i / wpr, q = i % wpr;
+            const int64_t o = (int64_t)(g.y0 + r) * stride + g.x0;
+            reinterpret_cast<uint32_t *>(Lp + o)[q] = __ldg(reinterpret_cast<const uint32_t *>(Cp + o) + q);
+        }
         return;
     }
 
@@ -378,7 +387,44 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
 
     // ---- luma window: rows ro-6 .. ro+nr+5 of the stripe, columns -6 .. uw+5 ----
     const int wh = nr + 12, ww = g.uw + 12;
-    {
+    if ((g.edges & LR_HAVE_LEFT) && (g.edges & LR_HAVE_RIGHT) && g.uw == 64) {
+        // interior unit: window columns are source columns x0-6 .. x0+69, all
+        // inside the frame.  Read them as 2-sample words U_j (samples
+        // x0-6+2j, x0-5+2j): pair 2j is U_j, pair 2j+1 joins U_j's second
+        // sample with U_{j+1}'s first.  Each thread issues four words' loads
+        // before storing any pair.
+        typedef typename std::conditional<sizeof(P) == 2, uint32_t, uint16_t>::type U;
+        constexpr int NJ = 38, SH = 8 * (int)sizeof(P);
+        constexpr uint32_t MK = (1u << SH) - 1;
+        const int total = wh * NJ;
+        for (int base = 0; base < total; base += 4 * 256) {
+            uint32_t a[4], nb[4];
+            int dst[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int i = base + q * 256 + tid;
+                dst[q] = -1;
+                a[q] = nb[q] = 0;
+                if (i < total) {
+                    const int r = i / NJ, j = i - r * NJ;
+                    int row;
+                    bool from_d;
+                    row_src(g, ro + r - 6, row, from_d);
+                    const U *src = reinterpret_cast<const U *>((from_d ? Dp : Cp) + (int64_t)row * stride + g.x0 - 6);
+                    a[q] = __ldg(src + j);
+                    nb[q] = __ldg(src + j + 1);
+                    dst[q] = r * LW + 2 * j;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (dst[q] >= 0) {
+                    const uint32_t s0 = a[q] & MK, s1 = a[q] >> SH, t0 = nb[q] & MK;
+                    sm.u.wp[dst[q]] = s0 | (s1 << 16);
+                    sm.u.wp[dst[q] + 1] = s1 | (t0 << 16);
+                }
+        }
+    } else {
         // source columns of this lane's window columns (the same on every row)
         int cs0[3], cs1[3];
 #pragma unroll
@@ -658,7 +704,7 @@ int r2g_batch_occupancy_lr() {
 }
 int r2g_lr_items(const DevFrame &f) {
     if (!f.lr_on) return 0;
-    return f.sbh * 4 * ((f.w + 63) >> 6) + 2 * f.sbh * 2 * ((f.cw + 63) >> 6);
+    return (f.sbh + 1) * 2 * ((f.w + 63) >> 6) + 2 * (f.sbh + 1) * ((f.cw + 63) >> 6);
 }
 
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
