@@ -38,7 +38,7 @@ enum { W_NONE = 0, W_NS_SINGLE = 1, W_NS_MULTI = 2, W_PC = 3 };
 struct UnitGeom {
     int plane, x0, uw, y0, sh, edges, valid;
     int sb256x, sb64x_idx;
-    const R2gAv2RestorationUnit *unit;
+    const LrUnitPacked *unit;
 };
 
 // looprestoration.rs:40-50
@@ -220,7 +220,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     int wkind = W_NONE;
     bool plane_on = (f.restore_planes >> plane) & 1;
     if (plane_on && g.valid) {
-        int wt = (f.inloop & R2G_INLOOP_WIENER) ? g.unit->restoration_type : 0;
+        int wt = (f.inloop & R2G_INLOOP_WIENER) ? g.unit->type : 0;
         const R2gRestorationPlane &pd = fp.restoration[plane];
         if (wt == R2G_RESTORE_NS_WIENER)
             wkind = (pd.frame_filters_on && pd.num_classes != 1) ? W_NS_MULTI : W_NS_SINGLE;
@@ -354,7 +354,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         int8_t flt[18];
         if (wkind == W_NS_SINGLE) {
             const int8_t *src = fp.restoration[plane].frame_filters_on ? fp.restoration[plane].filter[0]
-                                                                       : g.unit->ns_filter[0];
+                                                                       : g.unit->f;
 #pragma unroll
             for (int k = 0; k < 18; k++) flt[k] = src[k];
         }
@@ -625,7 +625,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     // ---- Wiener FIR + GDF add, one output sample per iteration ----
     int8_t single[16];
     if (wkind == W_NS_SINGLE) {
-        const int8_t *src = fp.restoration[0].frame_filters_on ? fp.restoration[0].filter[0] : g.unit->ns_filter[0];
+        const int8_t *src = fp.restoration[0].frame_filters_on ? fp.restoration[0].filter[0] : g.unit->f;
 #pragma unroll
         for (int k = 0; k < 16; k++) single[k] = src[k];
     }

@@ -32,6 +32,18 @@ cudaError_t r2g_get_tables(DevTables *t);
 // Frame descriptor handed to every stage kernel (by value, or from a device
 // array in batched launches).  All derived per-frame scalars of the
 // reference's LoopFilterState are computed once on the host.
+// Staged form of one R2gAv2RestorationUnit: its type and the (at most 18)
+// NS-Wiener taps the filters read; a SB256's 3 x 16 units take 960 bytes on
+// the device instead of 24624.
+struct LrUnitPacked {
+    uint8_t type;
+    int8_t f[18];
+    uint8_t pad;
+};
+struct LrPacked {
+    LrUnitPacked lr[3][16];
+};
+
 struct DevFrame {
     int w, h;          // luma size in samples
     int cw, ch;        // chroma size in samples (4:2:0)
@@ -45,7 +57,7 @@ struct DevFrame {
     void *L[3];         // loop-restoration output (the filtered frame)
     void *G[3];         // film-grain display copy
     const R2gAv2Filter *masks;
-    const R2gAv2Restoration *lr;
+    const LrPacked *lr;  // packed restoration records, one per SB256
     const uint8_t *segmap;
     const uint8_t *segmap_uv;
     int segmap_stride, segmap_uv_stride;

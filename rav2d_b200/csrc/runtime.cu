@@ -142,7 +142,7 @@ size_t r2g_frame_device_bytes(int width, int height, int bitdepth) {
     size_t buf = (size_t)(ys * yr + 2 * uvs * uvr);
     int bw4 = ((width + 7) >> 3) << 1, bh4 = ((height + 7) >> 3) << 1;
     size_t nsb = (size_t)((bw4 + 63) >> 6) * ((bh4 + 63) >> 6);
-    return 5 * buf + nsb * (sizeof(R2gAv2Filter) + sizeof(R2gAv2Restoration)) + R2G_GRAIN_SCRATCH;
+    return 5 * buf + nsb * (sizeof(R2gAv2Filter) + sizeof(LrPacked)) + R2G_GRAIN_SCRATCH;
 }
 
 extern "C" int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth, R2gFrame **out) {
@@ -163,7 +163,7 @@ extern "C" int r2g_frame_alloc(R2gCtx *ctx, int width, int height, int bitdepth,
     f->buf_bytes = f->plane_bytes[0] + 2 * f->plane_bytes[1];
     int bw4 = ((width + 7) >> 3) << 1, bh4 = ((height + 7) >> 3) << 1;
     f->n_sb256 = ((bw4 + 63) >> 6) * ((bh4 + 63) >> 6);
-    f->side_bytes = (size_t)f->n_sb256 * (sizeof(R2gAv2Filter) + sizeof(R2gAv2Restoration));
+    f->side_bytes = (size_t)f->n_sb256 * (sizeof(R2gAv2Filter) + sizeof(LrPacked));
     int rc;
     for (int i = 0; i < 5; i++)
         if ((rc = r2g_dev_alloc(ctx, &f->buf[i], f->buf_bytes)) != R2G_OK) {
@@ -461,34 +461,42 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
         d.gdf_ref_dst_idx = TBL[md < 11 ? md : 11];
     }
 
-    // stage side-info: masks + restoration records, then segmaps (the
-    // deblock kernel applies the reference's bottom-edge crop as it reads
-    // the masks).  Records in page-locked memory are copied straight to the
-    // device when the context overlaps copies (asynchronously: the caller
-    // keeps them unchanged until the frame's work completes); otherwise they
-    // go through the frame's pinned staging buffer, which is reused, so wait
-    // for its previous upload first.
+    // stage side-info: masks, restoration records packed to the fields the
+    // filters read (LrPacked), then segmaps.  The deblock kernel applies the
+    // reference's bottom-edge crop as it reads the masks.  With copy overlap,
+    // masks in page-locked memory go straight to the device (asynchronously:
+    // the caller keeps them unchanged until the frame's work completes);
+    // otherwise they go through the frame's pinned staging buffer, which is
+    // reused, so wait for its previous upload first.
     if (!f->side_done) CK(cudaEventCreateWithFlags(&f->side_done, cudaEventDisableTiming));
     size_t mbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Filter);
-    size_t lbytes = (size_t)f->n_sb256 * sizeof(R2gAv2Restoration);
+    size_t lbytes = (size_t)f->n_sb256 * sizeof(LrPacked);
     bool direct = false;
     if (ctx->overlap) {
-        cudaPointerAttributes am, al;
-        direct = cudaPointerGetAttributes(&am, side->masks) == cudaSuccess && am.type == cudaMemoryTypeHost &&
-                 cudaPointerGetAttributes(&al, side->lr) == cudaSuccess && al.type == cudaMemoryTypeHost;
+        cudaPointerAttributes am;
+        direct = cudaPointerGetAttributes(&am, side->masks) == cudaSuccess && am.type == cudaMemoryTypeHost;
         cudaGetLastError();
     }
+    CK(cudaEventSynchronize(f->side_done));
+    LrPacked *pk = (LrPacked *)((char *)f->side_host + mbytes);
+    for (int i = 0; i < f->n_sb256; i++)
+        for (int pl = 0; pl < 3; pl++)
+            for (int u = 0; u < 16; u++) {
+                const R2gAv2RestorationUnit &src = side->lr[i].lr[pl][u];
+                LrUnitPacked &dst = pk[i].lr[pl][u];
+                dst.type = src.restoration_type;
+                memcpy(dst.f, src.ns_filter[0], sizeof(dst.f));
+                dst.pad = 0;
+            }
     if (direct) {
         CK(cudaMemcpyAsync(f->side_dev, side->masks, mbytes, cudaMemcpyHostToDevice, cs));
-        CK(cudaMemcpyAsync((char *)f->side_dev + mbytes, side->lr, lbytes, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpyAsync((char *)f->side_dev + mbytes, pk, lbytes, cudaMemcpyHostToDevice, cs));
     } else {
-        CK(cudaEventSynchronize(f->side_done));
         memcpy(f->side_host, side->masks, mbytes);
-        memcpy((char *)f->side_host + mbytes, side->lr, lbytes);
         CK(cudaMemcpyAsync(f->side_dev, f->side_host, mbytes + lbytes, cudaMemcpyHostToDevice, cs));
     }
     d.masks = (const R2gAv2Filter *)f->side_dev;
-    d.lr = (const R2gAv2Restoration *)((char *)f->side_dev + mbytes);
+    d.lr = (const LrPacked *)((char *)f->side_dev + mbytes);
     size_t seg_y = side->segmap ? (size_t)side->segmap_stride * d.bh4 : 0;
     size_t seg_uv = side->segmap_uv ? (size_t)side->segmap_uv_stride * (d.bh4 >> 1) : 0;
     if (seg_y + seg_uv) {
