@@ -268,6 +268,27 @@ int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_t y_stride,
 /* Block until every call enqueued on the context has finished. */
 int r2g_sync(R2gCtx *ctx);
 
+/* ---- output formatting and partial downloads ----
+ * r2g_download_y4m: one Y4M frame of the filtered (which 0) or grained
+ * (which 1) picture into `dst`, as rav2d-cli's write_picture / pack_plane
+ * and Y4mWriter::write_frame produce it (crates/rav2d-cli/src/main.rs:114-149,
+ * y4m.rs:36-45): "FRAME\n" then the Y, U and V planes tightly packed,
+ * 16-bit little-endian samples above 8 bits.  out_bitdepth 0 keeps the
+ * frame's depth; 8 on a 10-bit frame reduces samples to 8 bits on the device
+ * ((v + 2) >> 2, clipped; a display option the reference does not have).
+ * The planes are packed by a kernel and copied back in one transfer;
+ * dst_size must be at least r2g_y4m_frame_bytes(...).
+ * r2g_y4m_header: the stream header line rav2d-cli writes (y4m.rs:17-31,
+ * main.rs:98-111 colorspace tags) for a 4:2:0 stream; returns its length.
+ * r2g_download_rows: rows [row0, row0 + nrows) of the luma plane and the
+ * co-located chroma rows (row0 and nrows even), e.g. the band of a reference
+ * frame that the next frame's reconstruction reads. */
+int r2g_download_y4m(R2gCtx *ctx, R2gFrame *f, int which, int out_bitdepth, void *dst, int64_t dst_size);
+int64_t r2g_y4m_frame_bytes(int width, int height, int out_bitdepth);
+int r2g_y4m_header(int width, int height, int fps_num, int fps_den, int bitdepth, char *buf, int cap);
+int r2g_download_rows(R2gCtx *ctx, R2gFrame *f, int which, int row0, int nrows, void *y, int64_t y_stride,
+                      void *u, void *v, int64_t uv_stride);
+
 /* ---- one-call convenience: host recon in, host filtered/grained out ---- */
 int r2g_filter_frame_host(R2gCtx *ctx, const R2gFrameParams *fp, const R2gSideInfo *side,
                           uint32_t inloop_mask, const R2gFilmGrainData *fgd, uint32_t grain_seed,

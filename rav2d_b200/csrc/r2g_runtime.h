@@ -70,6 +70,8 @@ struct R2gFrame {
     bool staged = false;
     void *grain_scratch = nullptr;  // batched film grain (R2G_GRAIN_SCRATCH)
     DevFrame desc{};
+    void *pack_buf = nullptr;  // packed Y4M payload (r2g_download_y4m)
+    size_t pack_bytes = 0;
     // copy-overlap ordering: last upload / staging (up stream), last kernels
     // (context stream), last download (down stream) of this frame
     cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_down = nullptr;

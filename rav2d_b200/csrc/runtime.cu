@@ -199,6 +199,7 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     r2g_dev_free(ctx, f->side_dev, f->side_bytes);
     r2g_dev_free(ctx, f->seg_dev, f->seg_bytes);
     r2g_dev_free(ctx, f->grain_scratch, R2G_GRAIN_SCRATCH);
+    r2g_dev_free(ctx, f->pack_buf, f->pack_bytes);
     if (f->side_host) cudaFreeHost(f->side_host);
     if (f->seg_host) cudaFreeHost(f->seg_host);
     if (f->side_done) cudaEventDestroy(f->side_done);

@@ -23,7 +23,8 @@ SYMBOLS = [
     "r2g_frame_stage", "r2g_frame_run", "r2g_ctx_set_stream", "r2g_ctx_profile", "r2g_ctx_profile_read",
     "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config", "r2g_server_create",
     "r2g_server_submit", "r2g_server_wait", "r2g_server_close_stream", "r2g_server_stats", "r2g_server_destroy",
-    "r2g_ctx_overlap_copies", "r2g_ctx_fence",
+    "r2g_ctx_overlap_copies", "r2g_ctx_fence", "r2g_download_y4m", "r2g_y4m_frame_bytes", "r2g_y4m_header",
+    "r2g_download_rows",
 ]
 
 
@@ -74,6 +75,12 @@ def lib():
         L.r2g_server_destroy.argtypes = [C.c_void_p]
         L.r2g_ctx_overlap_copies.argtypes = [C.c_void_p, C.c_int]
         L.r2g_ctx_fence.argtypes = [C.c_void_p]
+        L.r2g_download_y4m.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64]
+        L.r2g_y4m_frame_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.r2g_y4m_frame_bytes.restype = C.c_int64
+        L.r2g_y4m_header.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
+        L.r2g_download_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64,
+                                        C.c_void_p, C.c_void_p, C.c_int64]
         _lib = L
     return _lib
 
@@ -210,6 +217,22 @@ class Frame:
         self.ctx.check(lib().r2g_frame_filter(self.ctx.h, self.h, C.byref(sf.fp), C.byref(side),
                                               sf.inloop if inloop is None else inloop))
 
+    def download_y4m(self, which=0, out_bitdepth=0):
+        """One Y4M frame ("FRAME\\n" + packed planes) as bytes."""
+        n = lib().r2g_y4m_frame_bytes(self.width, self.height, out_bitdepth or self.bitdepth)
+        buf = np.zeros(n, np.uint8)
+        self.ctx.check(lib().r2g_download_y4m(self.ctx.h, self.h, which, out_bitdepth, _ptr(buf), n))
+        self.ctx.sync()
+        return buf.tobytes()
+
+    def download_rows(self, like, row0, nrows, which=0):
+        """Rows [row0, row0 + nrows) (and the chroma rows under them)."""
+        out = [np.zeros((nrows >> (i > 0), p.shape[1]), p.dtype) for i, p in enumerate(like)]
+        self.ctx.check(lib().r2g_download_rows(self.ctx.h, self.h, which, row0, nrows, _ptr(out[0]),
+                                               out[0].strides[0], _ptr(out[1]), _ptr(out[2]), out[1].strides[0]))
+        self.ctx.sync()
+        return out
+
     def grain(self, fgd, seed):
         self.ctx.check(lib().r2g_frame_grain(self.ctx.h, self.h, C.byref(fgd), seed))
 
@@ -298,3 +321,11 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def y4m_header(width, height, fps_num, fps_den, bitdepth):
+    buf = C.create_string_buffer(128)
+    n = lib().r2g_y4m_header(width, height, fps_num, fps_den, bitdepth, buf, 128)
+    if n < 0:
+        raise R2gError(n, "bad Y4M header parameters")
+    return buf.raw[:n]
