@@ -289,6 +289,47 @@ int r2g_y4m_header(int width, int height, int fps_num, int fps_den, int bitdepth
 int r2g_download_rows(R2gCtx *ctx, R2gFrame *f, int which, int row0, int nrows, void *y, int64_t y_stride,
                       void *u, void *v, int64_t uv_stride);
 
+/* ---- DSP-context slots (crates/rav2d/src/dsp.rs:9-122) ----
+ * Per-block functions for the self-contained slots of the reference's
+ * DSPContext, with the reference functions' argument meaning and order; the
+ * reference declares these slots but never fills or calls them, and the
+ * per-frame entry points above are the performance path.  Each call copies
+ * the block and the neighbours the reference would read to the GPU, runs one
+ * kernel and copies the result back, synchronously, on the current device.
+ * Host buffers hold u8 samples at bitdepth 8, u16 above; strides count
+ * samples.  `top` points at row -2 and `bottom` at row h (column 0) of the
+ * block, both with the block's stride; `left` holds [h][2] samples (columns
+ * -2, -1); edges: 1 left, 2 right, 4 top, 8 bottom available (CDEF_HAVE_*,
+ * cdef.rs:6-9). */
+/* CdefDSPContext.dir: cdef_find_dir_bd (cdef.rs:134-216) on the 8x8 block at
+ * img; returns the direction 0..7 (or < 0 on error), *var its variance. */
+int r2g_dsp_cdef_dir(const void *img, int64_t stride, uint32_t *var, int bitdepth);
+/* CdefDSPContext.fb[0..2]: cdef_filter_block (cdef.rs:320-458) in place on a
+ * w x h block (8x8, 4x8 or 4x4) with cdef_padding's rules (cdef.rs:37-114). */
+int r2g_dsp_cdef_filter(void *dst, int64_t stride, const void *left, const void *top, const void *bottom,
+                        int pri, int sec, int dir, int damping, int w, int h, int edges, int bitdepth);
+/* CcsoDSPContext.prep: ccso_prep (ccso.rs:115-187) of a w x h output block
+ * whose co-located luma region (w << ss_hor) x (h << ss_ver) starts at src;
+ * class / band indices into dst.  Region at most 64 x 32 luma samples. */
+int r2g_dsp_ccso_prep(uint8_t *dst, int64_t dst_stride, const void *src, int64_t stride, const void *left,
+                      const void *top, const void *bottom, int max_band_log2, int ext_filter, int quant_step,
+                      int edge_clf, int bo_only, int edges, int w, int h, int ss_hor, int ss_ver, int bitdepth);
+/* CcsoDSPContext.add: ccso_add (ccso.rs:215-254) in place; offset_idxs[64]
+ * packed offset indices, offset_lut[8], ll_mask [h/4][4] lossless bits.
+ * w, h multiples of 4, at most 64. */
+int r2g_dsp_ccso_add(void *dst, int64_t dst_stride, const uint8_t *idx, int64_t idx_stride,
+                     const uint8_t *offset_idxs, const int8_t *offset_lut, int w, int h, const uint16_t *ll_mask,
+                     int bitdepth);
+/* LoopRestorationDSPContext.gdf_add: the GdfAddFn slot (looprestoration.rs:
+ * 1770-1779; gdf_add :273-329) in place on a w x h block, w, h <= 64. */
+int r2g_dsp_gdf_add(void *p, int64_t stride, const int8_t *err, int64_t err_stride, int w, int h, int scale,
+                    const uint16_t *ll_mask, int bitdepth);
+/* FilmGrainDSPContext.generate_grain_y / generate_grain_uv[1] (filmgrain.rs:
+ * 115-230, 4:2:0): the 82x73 luma template and the two 44x38 chroma templates
+ * (top-left of 82x73 arrays); any buffer may be NULL. */
+int r2g_dsp_generate_grain(int16_t *buf_y, int16_t *buf_u, int16_t *buf_v, const R2gFilmGrainData *fgd,
+                           uint32_t seed, int bitdepth);
+
 /* ---- one-call convenience: host recon in, host filtered/grained out ---- */
 int r2g_filter_frame_host(R2gCtx *ctx, const R2gFrameParams *fp, const R2gSideInfo *side,
                           uint32_t inloop_mask, const R2gFilmGrainData *fgd, uint32_t grain_seed,

@@ -636,6 +636,15 @@ void r2o_ccso_prep(uint8_t *dst, int dst_stride, const uint16_t *src, int64_t sr
                    bottom_off, max_band_log2, ext_filter, quant_step, edge_clf, bo_only != 0, edges, w, h, ss_hor,
                    ss_ver);
 }
+/* cdef.rs:320-458 cdef_filter_block on a block at dst_off of a plane */
+void r2o_cdef_filter_block(uint16_t *dst, int64_t dst_stride, int64_t dst_off, const uint16_t *left_2,
+                           const uint16_t *top, int64_t top_off, const uint16_t *bottom, int64_t bottom_off,
+                           int pri, int sec, int dir, int damping, int w, int h, int edges, int bitdepth) {
+    r2o::BD bd;
+    bd.bitdepth = bitdepth;
+    r2o::cdef_filter_block(bd, dst, dst_stride, dst_off, (const r2o::Left2 *)left_2, top, top_off, bottom, bottom_off,
+                           pri, sec, dir, damping, w, h, edges);
+}
 void r2o_ccso_add(uint16_t *dst, int64_t dst_stride, const uint8_t *idx_buf, int idx_stride,
                   const uint8_t *offset_idxs, const int8_t *offset_lut, int w, int h, const uint16_t *ll_mask_x4,
                   int bitdepth) {

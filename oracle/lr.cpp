@@ -917,6 +917,11 @@ void lr_sbrow_apply(Frame &f, int sby, uint32_t inloop) {
 
 /* ---- known-answer-test hooks (the reference's looprestoration.rs tests) ---- */
 extern "C" {
+/* looprestoration.rs:273-329 gdf_add */
+void r2o_gdf_add(uint16_t *p, int64_t stride, const int8_t *err, int err_stride, int w, int h, int scale,
+                 const uint16_t *ll_mask_x4, int bitdepth) {
+    r2o::gdf_add(p, stride, err, err_stride, w, h, scale, (const uint16_t(*)[4])ll_mask_x4, bitdepth);
+}
 void r2o_backup_row_luma(uint16_t *dst, int o, const uint16_t *src, int64_t src_o, int64_t src_stride, int w,
                          int edges, int ss_hor, int ss_ver, int cfl_ds_flt) {
     r2o::backup_row_luma(dst, o, src, src_o, src_stride, w, edges, ss_hor, ss_ver, cfl_ds_flt);

@@ -471,6 +471,120 @@ __global__ void __launch_bounds__(256, 6) cdef_batch_kernel(BatchArgs a) {
     }
 }
 
+
+// ---- DSP-context slot kernels (r2g_dsp_*): one block per call ----
+// `tile` holds the block and a 2-sample ring around it, (h + 4) x (w + 4),
+// as the caller's buffers provide it; positions whose edge flag is absent
+// are not read.
+
+// cdef_filter_block (cdef.rs:320-458) with cdef_padding (:37-114): absent
+// edges become INT16_MIN.
+__global__ void dsp_cdef_filter_kernel(const uint16_t *tile, int w, int h, int edges, int pri, int sec, int dir,
+                                       int damping, int bitdepth, const DevTables tab, uint16_t *out) {
+    __shared__ int16_t t[12 * 12];
+    __shared__ int off[6];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 144; i += blockDim.x) {
+        const int y = i / 12 - 2, x = i % 12 - 2;
+        int16_t v = (int16_t)INT16_MIN;
+        if (y < h + 2 && x < w + 2) {
+            const bool absent = (y < 0 && !(edges & 4)) || (y >= h && !(edges & 8)) || (x < 0 && !(edges & 1)) ||
+                                (x >= w && !(edges & 2));
+            if (!absent) v = (int16_t)tile[(y + 2) * (w + 4) + x + 2];
+        }
+        t[i] = v;
+    }
+    if (tid < 6) {
+        const int wh = tid >> 1, k = tid & 1;
+        const int which = wh == 0 ? dir + 2 : (wh == 1 ? dir + 4 : dir);
+        int dy, dx;
+        dir_off(tab.CDEF_DIRECTIONS[which * 2 + k], dy, dx);
+        off[tid] = dy * 12 + dx;
+    }
+    __syncthreads();
+    if (tid < w * h) {
+        const int y = tid / w, x = tid % w;
+        int o[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) o[k] = off[k];
+        const int v = cdef_px(&t[(y + 2) * 12 + x + 2], pri, sec, o, damping, bitdepth - 8);
+        out[tid] = (uint16_t)(bitdepth == 8 ? (v & 0xff) : (v & 0xffff));
+    }
+}
+
+// cdef_find_dir_bd (cdef.rs:134-224) on one 8x8 block; out = {dir, var}.
+__global__ void dsp_cdef_dir_kernel(const uint16_t *blk, int bitdepth, uint32_t *out) {
+    __shared__ int16_t b[64];
+    __shared__ uint32_t cost[8];
+    const int tid = threadIdx.x;
+    if (tid < 64) b[tid] = (int16_t)(((int)blk[tid] >> (bitdepth - 8)) - 128);
+    __syncthreads();
+    switch (tid) {
+        case 0: cost[0] = dir_cost<0>(b); break;
+        case 1: cost[1] = dir_cost<1>(b); break;
+        case 2: cost[2] = dir_cost<2>(b); break;
+        case 3: cost[3] = dir_cost<3>(b); break;
+        case 4: cost[4] = dir_cost<4>(b); break;
+        case 5: cost[5] = dir_cost<5>(b); break;
+        case 6: cost[6] = dir_cost<6>(b); break;
+        case 7: cost[7] = dir_cost<7>(b); break;
+        default: break;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t best = cost[0];
+        int dir = 0;
+        for (int d = 1; d < 8; d++)
+            if (cost[d] > best) {
+                best = cost[d];
+                dir = d;
+            }
+        out[0] = (uint32_t)dir;
+        out[1] = (best - cost[dir ^ 4]) >> 10;
+    }
+}
+
+// ccso_prep (ccso.rs:115-187) with ccso_padding (:26-65): coordinates clamp
+// to the available area.  The tile covers the luma region W x H = w << ss_hor
+// by h << ss_ver.
+__global__ void dsp_ccso_prep_kernel(const uint16_t *tile, int w, int h, int ss_hor, int ss_ver, int edges,
+                                     int max_band_log2, int ext, int quant_step, int edge_clf, int bo_only,
+                                     int bitdepth, uint8_t *out) {
+    const int W = w << ss_hor, H = h << ss_ver, tw = W + 4;
+    const int x_min = (edges & 1) ? -2 : 0, x_max = W - 1 + ((edges & 2) ? 2 : 0);
+    const int y_min = (edges & 4) ? -2 : 0, y_max = H - 1 + ((edges & 8) ? 2 : 0);
+    auto px = [&](int yy, int xx) -> int {
+        yy = iclip_(yy, y_min, y_max);
+        xx = iclip_(xx, x_min, x_max);
+        return tile[(yy + 2) * tw + xx + 2];
+    };
+    const int dy = c_ccso_pos[ext][0], dx = c_ccso_pos[ext][1];
+    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
+        const int y = i / w, x = i % w, yl = y << ss_ver, xl = x << ss_hor;
+        const int c = px(yl, xl);
+        const uint8_t band = (uint8_t)((uint32_t)c >> (bitdepth - max_band_log2));
+        if (bo_only) {
+            out[i] = band;
+        } else {
+            const uint32_t c0 = ccso_score(px(yl + dy, xl + dx) - c, quant_step, (uint32_t)edge_clf);
+            const uint32_t c1 = ccso_score(px(yl - dy, xl - dx) - c, quant_step, (uint32_t)edge_clf);
+            out[i] = (uint8_t)((c0 << 5) | (c1 << 3)) | band;
+        }
+    }
+}
+
+// ccso_add (ccso.rs:215-254) on a w x h block.
+__global__ void dsp_ccso_add_kernel(uint16_t *dst, const uint8_t *idx, const uint8_t *offs, const int8_t *lut, int w,
+                                    int h, const uint16_t *llm, int bdmax) {
+    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
+        const int y = i / w, x = i % w;
+        if ((llm[(y >> 2) * 4] >> (x >> 2)) & 1) continue;
+        const int k = idx[i];
+        const int packed = (k >> 1) < 64 ? offs[k >> 1] : 0;
+        dst[i] = (uint16_t)iclip_((int)dst[i] + lut[7 & (packed >> (4 * (k & 1)))], 0, bdmax);
+    }
+}
+
 }  // namespace
 
 void r2g_batch_launch_cdef(const BatchArgs &a, int grid, cudaStream_t s) { cdef_batch_kernel<<<grid, 256, 0, s>>>(a); }
@@ -489,4 +603,21 @@ int r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
     else
         cdef_ccso_kernel<uint8_t><<<grid, 256, 0, s>>>(f);
     return 1;
+}
+
+void r2g_dsp_launch_cdef_filter(const uint16_t *tile, int w, int h, int edges, int pri, int sec, int dir, int damping,
+                                int bitdepth, const DevTables &tab, uint16_t *out) {
+    dsp_cdef_filter_kernel<<<1, 64>>>(tile, w, h, edges, pri, sec, dir, damping, bitdepth, tab, out);
+}
+void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out) {
+    dsp_cdef_dir_kernel<<<1, 64>>>(blk, bitdepth, out);
+}
+void r2g_dsp_launch_ccso_prep(const uint16_t *tile, int w, int h, int ss_hor, int ss_ver, int edges, int max_band_log2,
+                              int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out) {
+    dsp_ccso_prep_kernel<<<1, 256>>>(tile, w, h, ss_hor, ss_ver, edges, max_band_log2, ext, quant_step, edge_clf,
+                                     bo_only, bitdepth, out);
+}
+void r2g_dsp_launch_ccso_add(uint16_t *dst, const uint8_t *idx, const uint8_t *offs, const int8_t *lut, int w, int h,
+                             const uint16_t *llm, int bdmax) {
+    dsp_ccso_add_kernel<<<1, 256>>>(dst, idx, offs, lut, w, h, llm, bdmax);
 }

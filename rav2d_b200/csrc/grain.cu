@@ -611,3 +611,12 @@ extern "C" int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u
         grain_apply_kernel<uint8_t><<<grid, 256, 0, s>>>(d, gp, lut, scaling);
     return cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
 }
+
+// DSP-context slot (r2g_dsp_generate_grain): the three grain templates of a
+// parameter set on the default stream.
+void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    init_lfsr_pow(dev);
+    grain_template_kernel<<<1, 256>>>(gp, tab, lut, scaling);
+}

@@ -694,6 +694,21 @@ __global__ void __launch_bounds__(256, 4) lr_batch_kernel(BatchArgs a) {
     }
 }
 
+
+// ---- DSP-context slot kernel (r2g_dsp_gdf_add): gdf_add
+// (looprestoration.rs:273-329) on a w x h block ----
+__global__ void dsp_gdf_add_kernel(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm,
+                                   int bitdepth) {
+    const int shift = 12 - bitdepth, rnd = (1 << shift) >> 1, bdmax = (1 << bitdepth) - 1;
+    for (int i = threadIdx.x; i < (w & ~3) * (h & ~3); i += blockDim.x) {
+        const int ww = w & ~3, y = i / ww, x = i % ww;
+        if ((llm[(y >> 2) * 4] >> (x >> 2)) & 1) continue;
+        const int diff = err[y * w + x] * scale;
+        const int ad = diff < 0 ? -diff : diff;
+        p[y * w + x] = (uint16_t)iclip_((int)p[y * w + x] + apply_sign_((ad + rnd) >> shift, diff), 0, bdmax);
+    }
+}
+
 }  // namespace
 
 void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s) { lr_batch_kernel<<<grid, 256, 0, s>>>(a); }
@@ -715,4 +730,8 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     else
         lr_kernel<uint8_t><<<n, 256, 0, s>>>(f);
     return 1;
+}
+
+void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth) {
+    dsp_gdf_add_kernel<<<1, 256>>>(p, err, w, h, scale, llm, bitdepth);
 }

@@ -130,3 +130,15 @@ int r2g_launch_cdef(const DevFrame &f, cudaStream_t s);
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s);
 
 struct GrainDev;  // grain.cu
+
+// DSP-context slot launchers (dsp.cu): one block per call, default stream.
+void r2g_dsp_launch_cdef_filter(const uint16_t *tile, int w, int h, int edges, int pri, int sec, int dir, int damping,
+                                int bitdepth, const DevTables &tab, uint16_t *out);
+void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out);
+void r2g_dsp_launch_ccso_prep(const uint16_t *tile, int w, int h, int ss_hor, int ss_ver, int edges, int max_band_log2,
+                              int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out);
+void r2g_dsp_launch_ccso_add(uint16_t *dst, const uint8_t *idx, const uint8_t *offs, const int8_t *lut, int w, int h,
+                             const uint16_t *llm, int bdmax);
+void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth);
+void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling);
+

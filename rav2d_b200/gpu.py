@@ -24,7 +24,8 @@ SYMBOLS = [
     "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config", "r2g_server_create",
     "r2g_server_submit", "r2g_server_wait", "r2g_server_close_stream", "r2g_server_stats", "r2g_server_destroy",
     "r2g_ctx_overlap_copies", "r2g_ctx_fence", "r2g_download_y4m", "r2g_y4m_frame_bytes", "r2g_y4m_header",
-    "r2g_download_rows",
+    "r2g_download_rows", "r2g_dsp_cdef_dir", "r2g_dsp_cdef_filter", "r2g_dsp_ccso_prep", "r2g_dsp_ccso_add",
+    "r2g_dsp_gdf_add", "r2g_dsp_generate_grain",
 ]
 
 
@@ -78,6 +79,13 @@ def lib():
         L.r2g_download_y4m.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64]
         L.r2g_y4m_frame_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
         L.r2g_y4m_frame_bytes.restype = C.c_int64
+        vp, i64, ci = C.c_void_p, C.c_int64, C.c_int
+        L.r2g_dsp_cdef_dir.argtypes = [vp, i64, C.POINTER(C.c_uint32), ci]
+        L.r2g_dsp_cdef_filter.argtypes = [vp, i64, vp, vp, vp] + [ci] * 8
+        L.r2g_dsp_ccso_prep.argtypes = [vp, i64, vp, i64, vp, vp, vp] + [ci] * 11
+        L.r2g_dsp_ccso_add.argtypes = [vp, i64, vp, i64, vp, vp, ci, ci, vp, ci]
+        L.r2g_dsp_gdf_add.argtypes = [vp, i64, vp, i64, ci, ci, ci, vp, ci]
+        L.r2g_dsp_generate_grain.argtypes = [vp, vp, vp, C.POINTER(abi.FilmGrainData), C.c_uint32, ci]
         L.r2g_y4m_header.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
         L.r2g_download_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.c_int64]
