@@ -47,7 +47,7 @@ BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film
 # dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload,
 # from `ncu --set full` (profiles/stages_full_1080p10.md); the outputs were
 # still in L2 when the capture ended, so the write term was 0
-NCU_TRAFFIC = {"deblock": 6605568, "cdef_ccso": 6272768, "loop_restoration": 6915584}
+NCU_TRAFFIC = {"deblock": 6609664, "cdef_ccso": 6291200, "loop_restoration": 6850048}
 
 
 def log(*a):
