@@ -46,9 +46,11 @@ struct BlockParams {
     int y_ll;     // luma lossless rows mask bits for CCSO: bit r>>2 of the block
 };
 
+// constrain (cdef.rs:117-120): min(|d|, max(0, t - (|d| >> s))) equals
+// max(0, min(|d|, t - (|d| >> s))) since |d| >= 0 - one fused min/relu.
 R2G_D int constrain(int diff, int threshold, int shift) {
     int adiff = diff < 0 ? -diff : diff;
-    return apply_sign_(imin_(adiff, imax_(0, threshold - (adiff >> shift))), diff);
+    return apply_sign_(__vimin_s32_relu(adiff, threshold - (adiff >> shift)), diff);
 }
 
 // CDEF_DIRECTIONS entries are offsets in a 12-wide padded block; decode to
@@ -83,14 +85,13 @@ R2G_D int cdef_px(const int16_t *t, int pri, int sec, const int *off, int dampin
                 sum += tk * constrain(p0 - px, pri, pri_shift);
                 sum += tk * constrain(p1 - px, pri, pri_shift);
                 tk = (tk & 3) | 2;
-                mn = imin_(imin_(p0, p1), mn);
-                mx = imax_(imax_(p0, p1), mx);
                 int s0 = t[off[2 + k]], s1 = t[-off[2 + k]], s2 = t[off[4 + k]], s3 = t[-off[4 + k]];
                 int st = 2 - k;
                 sum += st * (constrain(s0 - px, sec, sec_shift) + constrain(s1 - px, sec, sec_shift) +
                              constrain(s2 - px, sec, sec_shift) + constrain(s3 - px, sec, sec_shift));
-                mn = imin_(imin_(imin_(s0, s1), imin_(s2, s3)), mn);
-                mx = imax_(imax_(imax_(s0, s1), imax_(s2, s3)), mx);
+                // the six taps of this k and the running bounds, 3-input min / max
+                mn = __vimin3_s32(__vimin3_s32(p0, p1, s0), __vimin3_s32(s1, s2, s3), mn);
+                mx = __vimax3_s32(__vimax3_s32(p0, p1, s0), __vimax3_s32(s1, s2, s3), mx);
             }
             return iclip_(px + ((sum - (sum < 0) + 8) >> 4), mn, mx);
         }

@@ -543,9 +543,11 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 const int o = TapsY::gdf[k][0] * LW + TapsY::gdf[k][1];
                 const uint2 al = aa[k];
                 const int4 p = wt[k];
-                const uint32_t above = __vmins2(__viaddmax_s16x2(wc[-o] << up, nm, al.y), al.x);
-                const uint32_t below = __vmins2(__viaddmax_s16x2(wc[o] << up, nm, al.y), al.x);
-                const uint32_t v = __vmins2(__viaddmax_s16x2(above, below, 0xfe00fe00u), 0x01ff01ffu);
+                // (min as the fused add-min with 0: one instruction, where a
+                // plain packed min is slower on this part)
+                const uint32_t above = __viaddmin_s16x2(__viaddmax_s16x2(wc[-o] << up, nm, al.y), 0u, al.x);
+                const uint32_t below = __viaddmin_s16x2(__viaddmax_s16x2(wc[o] << up, nm, al.y), 0u, al.x);
+                const uint32_t v = __viaddmin_s16x2(__viaddmax_s16x2(above, below, 0xfe00fe00u), 0u, 0x01ff01ffu);
                 const int v0 = lo16(v), v1 = hi16(v);
                 i0 += v0 * p.x;
                 i1 += v0 * p.y;
