@@ -405,7 +405,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
                            band_) & 0xff;
                 const int bi = idx >> 1;
                 const int packed = bi < 64 ? cp.filter_off[bi] : 0;
-                v = iclip_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], 0, bdmax);
+                v = clip_px_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], bdmax);
             }
             out[k] = v;
         }
@@ -442,7 +442,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
                 }
                 const int bi = idx >> 1;
                 const int packed = bi < 64 ? cpc.filter_off[bi] : 0;
-                v = iclip_(v + f.tab.CCSO_OFFSET[cpc.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], 0, bdmax);
+                v = clip_px_(v + f.tab.CCSO_OFFSET[cpc.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], bdmax);
             }
         }
         Cp[cgy * uvs + cgx] = (P)v;

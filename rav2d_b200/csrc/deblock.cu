@@ -167,11 +167,11 @@ R2G_D void filter_edge(int16_t *e, int along, int across, uint32_t q_thr, uint32
         for (int j = 0; j < 8; j++) {
             if (!neg_ll && j < wn) {
                 int diff = (dn * (wn - j) + (1 << 10)) >> 11;
-                ln[(-j - 1) * across] = (int16_t)iclip_(L[7 - j] + diff, 0, bdmax);
+                ln[(-j - 1) * across] = (int16_t)clip_px_(L[7 - j] + diff, bdmax);
             }
             if (!pos_ll && j < wp) {
                 int diff = (dp * (wp - j) + (1 << 10)) >> 11;
-                ln[j * across] = (int16_t)iclip_(L[8 + j] - diff, 0, bdmax);
+                ln[j * across] = (int16_t)clip_px_(L[8 + j] - diff, bdmax);
             }
         }
     }

@@ -315,7 +315,7 @@ R2G_D void grain_block(const DevFrame &f, const GrainParams &gp, const int16_t *
             int val;
             if (!d.chroma_scaling_from_luma) {
                 int combined = avg * d.uv_luma_mult[uv] + sv * d.uv_mult[uv];
-                val = iclip_((combined >> 6) + d.uv_offset[uv] * (1 << b8), 0, bdmax);
+                val = clip_px_((combined >> 6) + d.uv_offset[uv] * (1 << b8), bdmax);
             } else {
                 val = avg;
             }

@@ -378,7 +378,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                         const int o = TapsY::uvy[k][0] * CWW + TapsY::uvy[k][1];
                         s += (lw_[o] - l) * flt[6 + k];
                     }
-                    v = iclip_((s + 64) >> 7, 0, bdmax);
+                    v = clip_px_((s + 64) >> 7, bdmax);
                 }
                 Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
             }
@@ -658,12 +658,12 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                         s += (w[o] + w[-o] - 2 * m) * flt[k];
                     }
                 }
-                v = iclip_((s + 64) >> 7, 0, bdmax);
+                v = clip_px_((s + 64) >> 7, bdmax);
             }
             if (gdf_on && !ll) {
                 int diff = sm.gerr[y * 64 + x] * gscale;
                 int ad = diff < 0 ? -diff : diff;
-                v = iclip_(v + apply_sign_((ad + grnd) >> gshift, diff), 0, bdmax);
+                v = clip_px_(v + apply_sign_((ad + grnd) >> gshift, diff), bdmax);
             }
             Lp[(int64_t)(g.y0 + ro + y) * stride + g.x0 + x] = (P)v;
         }
@@ -707,7 +707,7 @@ __global__ void dsp_gdf_add_kernel(uint16_t *p, const int8_t *err, int w, int h,
         if ((llm[(y >> 2) * 4] >> (x >> 2)) & 1) continue;
         const int diff = err[y * w + x] * scale;
         const int ad = diff < 0 ? -diff : diff;
-        p[y * w + x] = (uint16_t)iclip_((int)p[y * w + x] + apply_sign_((ad + rnd) >> shift, diff), 0, bdmax);
+        p[y * w + x] = (uint16_t)clip_px_((int)p[y * w + x] + apply_sign_((ad + rnd) >> shift, diff), bdmax);
     }
 }
 

@@ -71,6 +71,8 @@ struct DevFrame {
 R2G_HD int imin_(int a, int b) { return a < b ? a : b; }
 R2G_HD int imax_(int a, int b) { return a > b ? a : b; }
 R2G_HD int iclip_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+// clip to [0, hi] (hi >= 0): max(min(v, hi), 0) as one fused instruction
+R2G_D int clip_px_(int v, int hi) { return __vimin_s32_relu(v, hi); }
 R2G_HD int apply_sign_(int v, int s) { return s < 0 ? -v : v; }
 R2G_D int ulog2_(uint32_t v) { return 31 - __clz((int)v); }
 
