@@ -179,8 +179,9 @@ R2G_D int hi16(uint32_t v) { return (int)v >> 16; }
 // slot sbh is the second stripe that only the last superblock row can have.
 // A luma stripe is split into two 32-row halves (separate CTAs) so that a
 // frame gives twice as many, lighter work items.
-template <typename P>
+template <typename P, int NT>
 R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
+    constexpr int NW = NT / 32;  // warps of the CTA
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
     const int n_luma_units = (f.sbh + 1) * 2 * nux_l;
@@ -237,7 +238,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         // unfiltered unit: copy C -> L in 4-byte words (unit widths are
         // multiples of 4 samples; rows and unit origins are 64-byte aligned)
         const int wpr = g.uw * (int)sizeof(P) / 4;
-        for (int i = tid; i < nr * wpr; i += 256) {
+        for (int i = tid; i < nr * wpr; i += NT) {
             const int r = ro + i / wpr, q = i % wpr;
             const int64_t o = (int64_t)(g.y0 + r) * stride + g.x0;
             reinterpret_cast<uint32_t *>(Lp + o)[q] = __ldg(reinterpret_cast<const uint32_t *>(Cp + o) + q);
@@ -291,7 +292,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     if (chroma) {
         // ---- chroma window: rows -2 .. sh+1, columns -2 .. uw+1 ----
         const int wh = g.sh + 4, ww = g.uw + 4;
-        for (int r = warp; r < wh; r += 8) {
+        for (int r = warp; r < wh; r += NW) {
             int row;
             bool from_d;
             row_src(g, r - 2, row, from_d);
@@ -307,7 +308,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
             const int64_t ls = f.stride[0];
             const int ds = fp.cfl_ds_filter_index;
             const int lw = g.uw << 1, lx0 = g.x0 << 1;
-            for (int r = warp; r < wh; r += 8) {
+            for (int r = warp; r < wh; r += NW) {
                 int rr = r - 2;
                 if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
                 if (!(g.edges & LR_HAVE_BOTTOM) && rr >= g.sh) rr = g.sh - 1;
@@ -358,7 +359,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
 #pragma unroll
             for (int k = 0; k < 18; k++) flt[k] = src[k];
         }
-        for (int y = warp; y < g.sh; y += 8)
+        for (int y = warp; y < g.sh; y += NW)
             for (int x = lane; x < g.uw; x += 32) {
                 const int16_t *w = &sm.u.ch.win[(y + 2) * CWW + x + 2];
                 const int16_t *lw_ = &sm.u.ch.lwin[(y + 2) * CWW + x + 2];
@@ -397,12 +398,12 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         constexpr int NJ = 38, SH = 8 * (int)sizeof(P);
         constexpr uint32_t MK = (1u << SH) - 1;
         const int total = wh * NJ;
-        for (int base = 0; base < total; base += 4 * 256) {
+        for (int base = 0; base < total; base += 4 * NT) {
             uint32_t a[4], nb[4];
             int dst[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int i = base + q * 256 + tid;
+                const int i = base + q * NT + tid;
                 dst[q] = -1;
                 a[q] = nb[q] = 0;
                 if (i < total) {
@@ -433,7 +434,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
             cs0[j] = col_src(g, c - 6);
             cs1[j] = c + 1 < ww ? col_src(g, c - 5) : cs0[j];
         }
-        for (int r = warp; r < wh; r += 8) {
+        for (int r = warp; r < wh; r += NW) {
             int row;
             bool from_d;
             row_src(g, ro + r - 6, row, from_d);
@@ -453,7 +454,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
                                                 : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
         const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
-        for (int i = tid; i < 88; i += 256) {
+        for (int i = tid; i < 88; i += NT) {
             int k = i >> 2, c = i & 3;
             const int a = f.tab.GDF_ALPHA[alpha_base + i];
             sm.s_w[c][k] = make_int4(f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i],
@@ -464,10 +465,10 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 sm.s_aa[c][k] = make_uint2(pa | (pa << 16), na | (na << 16));
             }
         }
-        for (int i = tid; i < nerr; i += 256) sm.s_err[i] = errtab[i];
+        for (int i = tid; i < nerr; i += NT) sm.s_err[i] = errtab[i];
     }
     if (wkind == W_PC)
-        for (int i = tid; i < 64 * 13; i += 256) sm.s_pcf[i] = f.tab.PC_WIENER_FILTERS[f.wiener_idx * 64 * 13 + i];
+        for (int i = tid; i < 64 * 13; i += NT) sm.s_pcf[i] = f.tab.PC_WIENER_FILTERS[f.wiener_idx * 64 * 13 + i];
     __syncthreads();
 
     const int b8 = bitdepth - 8;
@@ -482,7 +483,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         // (compute_gradient_row :114-193); pair (y1, x1) sums cells
         // (y1/2 .. y1/2+1, x1/2 .. x1/2+1)
         const int cj = (nr >> 1) + 1, ci = (g.uw >> 1) + 1;
-        for (int i = tid; i < cj * ci; i += 256) {
+        for (int i = tid; i < cj * ci; i += NT) {
             int j = i / ci, c = i % ci;
             int gs[4] = {0, 0, 0, 0};
 #pragma unroll
@@ -512,7 +513,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         const int b0 = f.tab.GDF_BIAS[bias_idx * 3], b1 = f.tab.GDF_BIAS[bias_idx * 3 + 1],
                   b2 = f.tab.GDF_BIAS[bias_idx * 3 + 2];
         const int npairs = nr * (g.uw >> 1);
-        for (int i = tid; i < npairs; i += 256) {
+        for (int i = tid; i < npairs; i += NT) {
             int y = i / (g.uw >> 1), x1 = (i % (g.uw >> 1)) * 2;
             int j = y >> 1, c = x1 >> 1;
             int gsum[4];
@@ -578,7 +579,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                                      ? f.tab.PC_WIENER_SUB_CLASSIFY + f.wiener_idx * 256
                                      : f.tab.PC_WIENER_SUB_CLASSIFY_NS +
                                            (f.wiener_idx * 7 + (f.ns_ci >= 0 ? imin_(f.ns_ci, 6) : 0)) * 256;
-        for (int i = tid; i < bh4 * bw4; i += 256) {
+        for (int i = tid; i < bh4 * bw4; i += NT) {
             int by = i / bw4, bx = i % bw4;
             int fs0 = 0, fs1 = 0, fs2 = 0;
 #pragma unroll
@@ -632,7 +633,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         for (int k = 0; k < 16; k++) single[k] = src[k];
     }
     const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
-    for (int y = warp; y < nr; y += 8)
+    for (int y = warp; y < nr; y += NW)
         for (int x = lane; x < g.uw; x += 32) {
             const int16_t *w = &W16[2 * ((y + 6) * LW + x + 6)];
             int m = w[0];
@@ -669,18 +670,21 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         }
 }
 
+// Per-frame kernel: one CTA per work item (the hardware hands items to SMs
+// as CTAs finish, which balances light and heavy items).
+constexpr int LR_FRAME_NT = 256;
 template <typename P>
-__global__ void __launch_bounds__(256, 4) lr_kernel(const DevFrame f) {
+__global__ void __launch_bounds__(LR_FRAME_NT, 4) lr_kernel(const DevFrame f) {
     __shared__ LrSmem sm;
-    lr_unit<P>(f, sm, blockIdx.x);
+    lr_unit<P, LR_FRAME_NT>(f, sm, blockIdx.x);
 }
 
 // Persistent kernel over a cross-frame work list: item = frame << 22 |
 // per-frame item index.
 // (one call per sample type, kept out of line so the two instantiations do
 // not share one register allocation)
-__device__ __noinline__ void lr_unit_hbd(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint16_t>(f, sm, b); }
-__device__ __noinline__ void lr_unit_8(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint8_t>(f, sm, b); }
+__device__ __noinline__ void lr_unit_hbd(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint16_t, 256>(f, sm, b); }
+__device__ __noinline__ void lr_unit_8(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint8_t, 256>(f, sm, b); }
 
 __global__ void __launch_bounds__(256, 4) lr_batch_kernel(BatchArgs a) {
     __shared__ LrSmem sm;
@@ -728,9 +732,9 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     if (!f.lr_on) return 0;
     int n = r2g_lr_items(f);
     if (f.bitdepth > 8)
-        lr_kernel<uint16_t><<<n, 256, 0, s>>>(f);
+        lr_kernel<uint16_t><<<n, LR_FRAME_NT, 0, s>>>(f);
     else
-        lr_kernel<uint8_t><<<n, 256, 0, s>>>(f);
+        lr_kernel<uint8_t><<<n, LR_FRAME_NT, 0, s>>>(f);
     return 1;
 }
 
