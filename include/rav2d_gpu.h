@@ -413,9 +413,10 @@ int r2g_server_stats(R2gServer *s, R2gServeStats *st, int reset);
 /* Completes every queued frame, then stops the worker and frees all. */
 int r2g_server_destroy(R2gServer *s);
 
-/* Instrumentation (no counterpart in the reference): the CTAs per SM the
- * last batch used for stages 0 deblock, 1 CDEF+CCSO, 2 loop restoration,
- * 3 film grain (autotuned); returns the SM count. */
+/* Instrumentation (no counterpart in the reference): the grid the last
+ * batch used for stages 0 deblock, 1 CDEF+CCSO, 2 loop restoration, 3 film
+ * grain (autotuned): CTAs per SM of a persistent grid, or 0 for one CTA per
+ * work item; returns the SM count. */
 int r2g_batch_config(R2gCtx *ctx, int32_t *ctas_per_sm, int n);
 
 /* ---- film grain without any device allocation ----

@@ -16,7 +16,7 @@
 // autotuner: on the first batch of a given bit-depth mix it times every
 // occupancy-legal choice per stage and keeps the fastest; the choice is
 // cached per device in a text file ($R2G_TUNE_CACHE, default
-// $HOME/.cache/rav2d_b200/autotune-v1.txt).  R2G_AUTOTUNE=0 skips tuning and
+// $HOME/.cache/rav2d_b200/autotune-v2.txt).  R2G_AUTOTUNE=0 skips tuning and
 // uses the occupancy limit.
 #include <sys/stat.h>
 
@@ -33,6 +33,10 @@ int r2g_grain_ready(int device);
 namespace {
 
 enum { N_BSTAGES = 4 };  // deblock, cdef, lr, grain apply
+// Tuned grid choice meaning "one CTA per work item" (grid = the batch's item
+// count; the hardware then hands items to SMs as CTAs finish) rather than a
+// persistent grid of CTAs-per-SM x SMs.
+constexpr int PER_ITEM = 255;
 
 struct Layout {
     int max_frames = 0;
@@ -88,7 +92,7 @@ static std::string cache_path() {
     const char *p = getenv("R2G_TUNE_CACHE");
     if (p && *p) return p;
     const char *h = getenv("HOME");
-    return std::string(h ? h : "/tmp") + "/.cache/rav2d_b200/autotune-v1.txt";
+    return std::string(h ? h : "/tmp") + "/.cache/rav2d_b200/autotune-v2.txt";
 }
 
 static void load_cache(BatchState &b) {
@@ -100,7 +104,7 @@ static void load_cache(BatchState &b) {
         char name[256];
         int cls, k, v;
         if (sscanf(line, "%255[^|]|%d|%d|%d", name, &cls, &k, &v) == 4 && b.dev_name == name && cls >= 0 &&
-            cls < 3 && k >= 0 && k < N_BSTAGES && v > 0 && v <= b.occ[k])
+            cls < 3 && k >= 0 && k < N_BSTAGES && v > 0 && (v <= b.occ[k] || v == PER_ITEM))
             b.tuned[cls][k] = v;
     }
     fclose(fp);
@@ -193,8 +197,9 @@ static int autotune(R2gCtx *ctx, BatchState &b, const Slot &s, const int *counts
             r2g_batch_launch_grain_template(a, counts[4] < b.num_sms ? counts[4] : b.num_sms, ctx->stream);
         float best = 1e30f;
         int best_v = b.occ[k];
-        for (int v = 1; v <= b.occ[k]; v++) {
-            int grid = v * b.num_sms;
+        for (int v = 1; v <= b.occ[k] + 1; v++) {
+            const int vv = v <= b.occ[k] ? v : PER_ITEM;
+            const int grid = vv == PER_ITEM ? counts[k] : v * b.num_sms;
             launch_stage(k, a, grid, ctx->stream);  // warm
             cudaEventRecord(b.t0, ctx->stream);
             launch_stage(k, a, grid, ctx->stream);
@@ -205,7 +210,7 @@ static int autotune(R2gCtx *ctx, BatchState &b, const Slot &s, const int *counts
             cudaEventElapsedTime(&ms, b.t0, b.t1);
             if (ms < best) {
                 best = ms;
-                best_v = v;
+                best_v = vv;
             }
         }
         b.tuned[cls][k] = best_v;
@@ -214,10 +219,11 @@ static int autotune(R2gCtx *ctx, BatchState &b, const Slot &s, const int *counts
     return cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
 }
 
+// Captures the batch graph with these grids.  An instantiated graph of the
+// slot is updated in place when the topology allows (only grids changed),
+// else re-instantiated.
 static int build_graph(R2gCtx *ctx, BatchState &b, Slot &s, const int *grids, int tpl_grid) {
-    if (s.exec) cudaGraphExecDestroy(s.exec);
     if (s.graph) cudaGraphDestroy(s.graph);
-    s.exec = nullptr;
     s.graph = nullptr;
     BatchArgs a = args_of(s);
     cudaStream_t st = ctx->stream;
@@ -230,7 +236,17 @@ static int build_graph(R2gCtx *ctx, BatchState &b, Slot &s, const int *grids, in
     cudaStreamWaitEvent(st, b.join, 0);
     launch_stage(3, a, grids[3], st);
     if (cudaStreamEndCapture(st, &s.graph) != cudaSuccess) return R2G_E_DEVICE;
-    if (cudaGraphInstantiate(&s.exec, s.graph, 0) != cudaSuccess) return R2G_E_DEVICE;
+    bool updated = false;
+    if (s.exec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(s.exec, s.graph, &info) == cudaSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(s.exec);
+            s.exec = nullptr;
+        }
+    }
+    if (!updated && cudaGraphInstantiate(&s.exec, s.graph, 0) != cudaSuccess) return R2G_E_DEVICE;
     for (int k = 0; k < N_BSTAGES; k++) s.grids[k] = grids[k];
     s.grids[N_BSTAGES] = tpl_grid;
     return R2G_OK;
@@ -363,8 +379,8 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
     int grids[N_BSTAGES];
     for (int k = 0; k < N_BSTAGES; k++) {
         int v = b.tuned[cls][k] > 0 ? b.tuned[cls][k] : b.occ[k];
-        b.last[k] = v;
-        grids[k] = v * b.num_sms;
+        b.last[k] = v == PER_ITEM ? 0 : v;
+        grids[k] = v == PER_ITEM ? (counts[k] > 0 ? counts[k] : 1) : v * b.num_sms;
     }
     const int tpl_grid = b.num_sms;
     bool same = s.exec != nullptr && s.grids[N_BSTAGES] == tpl_grid;

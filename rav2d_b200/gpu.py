@@ -178,7 +178,7 @@ class Context:
         return lib().r2g_wait(self.h, C.c_uint64(ticket), timeout_ms)
 
     def batch_config(self):
-        """(SM count, CTAs per SM of the last batch per stage)."""
+        """(SM count, CTAs per SM of the last batch per stage; 0 = one CTA per item)."""
         v = (C.c_int32 * 4)()
         sms = lib().r2g_batch_config(self.h, v, 4)
         return sms, dict(zip(("deblock", "cdef_ccso", "loop_restoration", "film_grain"), list(v)))

@@ -110,7 +110,7 @@ def test_batch_grows_and_reports_grid(ctx):
     _same(got[2][0], wf, big[2], "4K after growth (filter)")
     _same(got[2][1], wg, big[2], "4K after growth (grain)")
     sms, cfg = ctx.batch_config()
-    assert sms > 0 and all(v >= 1 for v in cfg.values())
+    assert sms > 0 and all(v >= 0 for v in cfg.values())  # 0: one CTA per work item
 
 
 def test_batch_oracle_spot_check(ctx, oracle):
