@@ -450,7 +450,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
 }
 
 template <typename P>
-__global__ void __launch_bounds__(256, 6) cdef_ccso_kernel(const DevFrame f) {
+__global__ void __launch_bounds__(256, 7) cdef_ccso_kernel(const DevFrame f) {
     __shared__ CdefSmem sm;
     cdef_region<P>(f, sm, blockIdx.x, blockIdx.y);
 }
