@@ -205,42 +205,6 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
         else
             sm.toff_y[dir][w * 2 + k] = dy * TW + dx;
     }
-    // ---- stage the region (clamped coordinates) ----
-    for (int r = warp; r < TH; r += 8) {
-        const int ry = gy0 - 2 + r, gy = iclip_(ry, 0, f.h - 1);
-        const bool row_out = ry < 0 || ry >= f.h;
-        const P *row = Dy + gy * ys;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const int c = lane + 32 * j;
-            if (c < TW) {
-                const int rx = gx0 - 2 + c;
-                const int v = __ldg(row + iclip_(rx, 0, f.w - 1));
-                sm.ty[r][c] = (int16_t)v;
-                sm.pty[r][c] = (row_out || rx < 0 || rx >= f.w) ? (int16_t)INT16_MIN : (int16_t)v;
-                const int yy = r - 2, xx = c - 2;
-                if (yy >= 0 && yy < RH && xx >= 0 && xx < 64)
-                    sm.blk[(yy >> 3) * 8 + (xx >> 3)][(yy & 7) * 8 + (xx & 7)] = (int16_t)((v >> bd8) - 128);
-            }
-        }
-    }
-    for (int r2 = warp; r2 < 2 * CH; r2 += 8) {
-        const int pl = r2 / CH, r = r2 % CH;
-        const int ry = cy0 - 2 + r, gy = iclip_(ry, 0, f.ch - 1);
-        const bool row_out = ry < 0 || ry >= f.ch;
-        const P *row = (pl ? Dv : Du) + gy * uvs;
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const int c = lane + 32 * j;
-            if (c < CW) {
-                const int rx = cx0 - 2 + c;
-                const int v = __ldg(row + iclip_(rx, 0, f.cw - 1));
-                sm.tc[pl][r][c] = (int16_t)v;
-                sm.ptc[pl][r][c] = (row_out || rx < 0 || rx >= f.cw) ? (int16_t)INT16_MIN : (int16_t)v;
-            }
-        }
-    }
-
     // ---- phase 1: superblock and per-block parameters (cdef.rs:787-907) ----
     const int sb256x = sbx >> 2, sb64x_idx = sbx & 3;
     const int by0 = gy0 >> 2;  // 4x4 row of the region's top
@@ -296,6 +260,45 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
         }
         sm.bp[b] = p;
     }
+    // the deblocked planes come from the previous kernel on the stream:
+    // wait for it before staging (everything above reads side-info only)
+    pdl_wait();
+    // ---- stage the region (clamped coordinates) ----
+    for (int r = warp; r < TH; r += 8) {
+        const int ry = gy0 - 2 + r, gy = iclip_(ry, 0, f.h - 1);
+        const bool row_out = ry < 0 || ry >= f.h;
+        const P *row = Dy + gy * ys;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int c = lane + 32 * j;
+            if (c < TW) {
+                const int rx = gx0 - 2 + c;
+                const int v = __ldg(row + iclip_(rx, 0, f.w - 1));
+                sm.ty[r][c] = (int16_t)v;
+                sm.pty[r][c] = (row_out || rx < 0 || rx >= f.w) ? (int16_t)INT16_MIN : (int16_t)v;
+                const int yy = r - 2, xx = c - 2;
+                if (yy >= 0 && yy < RH && xx >= 0 && xx < 64)
+                    sm.blk[(yy >> 3) * 8 + (xx >> 3)][(yy & 7) * 8 + (xx & 7)] = (int16_t)((v >> bd8) - 128);
+            }
+        }
+    }
+    for (int r2 = warp; r2 < 2 * CH; r2 += 8) {
+        const int pl = r2 / CH, r = r2 % CH;
+        const int ry = cy0 - 2 + r, gy = iclip_(ry, 0, f.ch - 1);
+        const bool row_out = ry < 0 || ry >= f.ch;
+        const P *row = (pl ? Dv : Du) + gy * uvs;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int c = lane + 32 * j;
+            if (c < CW) {
+                const int rx = cx0 - 2 + c;
+                const int v = __ldg(row + iclip_(rx, 0, f.cw - 1));
+                sm.tc[pl][r][c] = (int16_t)v;
+                sm.ptc[pl][r][c] = (row_out || rx < 0 || rx >= f.cw) ? (int16_t)INT16_MIN : (int16_t)v;
+            }
+        }
+    }
+
     __syncthreads();
 
     // ---- phase 2: direction costs, warp = direction, lane = block ----
@@ -451,6 +454,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
 
 template <typename P>
 __global__ void __launch_bounds__(256, 7) cdef_ccso_kernel(const DevFrame f) {
+    pdl_trigger();
     __shared__ CdefSmem sm;
     cdef_region<P>(f, sm, blockIdx.x, blockIdx.y);
 }
@@ -600,9 +604,9 @@ int r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
     if (!f.cdef_stage_on) return 0;
     dim3 grid((f.w + 63) / 64, (f.h + RH - 1) / RH);
     if (f.bitdepth > 8)
-        cdef_ccso_kernel<uint16_t><<<grid, 256, 0, s>>>(f);
+        r2g_launch_pdl(cdef_ccso_kernel<uint16_t>, grid, dim3(256), s, f);
     else
-        cdef_ccso_kernel<uint8_t><<<grid, 256, 0, s>>>(f);
+        r2g_launch_pdl(cdef_ccso_kernel<uint8_t>, grid, dim3(256), s, f);
     return 1;
 }
 

@@ -447,7 +447,9 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
     __syncthreads();
     run_edges<1>(sm, sm.hl, sm.n[2], sm.hc, sm.n[3], f.bdmax);
     __syncthreads();
-    // ---- write the tile
+    // ---- write the tile (the previous kernel on the stream may still read
+    // this frame's deblocked planes: wait for it first)
+    pdl_wait();
     P *Dy = plane_ptr<P>(f.D[0]);
     for (int i = tid; i < 64 * 16; i += nt) {
         int r = i >> 4, c4 = (i & 15) * 4;
@@ -471,6 +473,7 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
 
 template <typename P>
 __global__ void __launch_bounds__(256, 4) deblock_tile_kernel(const DevFrame f) {
+    pdl_trigger();
     __shared__ DeblockSmem sm;
     deblock_tile<P>(f, sm, blockIdx.x, blockIdx.y);
 }
@@ -508,8 +511,8 @@ int r2g_launch_deblock(const DevFrame &f, cudaStream_t s) {
     if (!f.deblock_on) return 0;
     dim3 grid((f.w + 63) / 64, (f.h + 63) / 64);
     if (f.bitdepth > 8)
-        deblock_tile_kernel<uint16_t><<<grid, 256, 0, s>>>(f);
+        r2g_launch_pdl(deblock_tile_kernel<uint16_t>, grid, dim3(256), s, f);
     else
-        deblock_tile_kernel<uint8_t><<<grid, 256, 0, s>>>(f);
+        r2g_launch_pdl(deblock_tile_kernel<uint8_t>, grid, dim3(256), s, f);
     return 1;
 }

@@ -234,6 +234,9 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && sb256_idx < nsb &&
                         f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
 
+    // C and D come from the previous kernels on the stream: wait for them
+    // (everything above reads side-info only)
+    pdl_wait();
     if (wkind == W_NONE && !gdf_on) {
         // unfiltered unit: copy C -> L in 4-byte words (unit widths are
         // multiples of 4 samples; rows and unit origins are 64-byte aligned)
@@ -675,6 +678,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
 constexpr int LR_FRAME_NT = 256;
 template <typename P>
 __global__ void __launch_bounds__(LR_FRAME_NT, 4) lr_kernel(const DevFrame f) {
+    pdl_trigger();
     __shared__ LrSmem sm;
     lr_unit<P, LR_FRAME_NT>(f, sm, blockIdx.x);
 }
@@ -732,9 +736,9 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     if (!f.lr_on) return 0;
     int n = r2g_lr_items(f);
     if (f.bitdepth > 8)
-        lr_kernel<uint16_t><<<n, LR_FRAME_NT, 0, s>>>(f);
+        r2g_launch_pdl(lr_kernel<uint16_t>, dim3(n), dim3(LR_FRAME_NT), s, f);
     else
-        lr_kernel<uint8_t><<<n, LR_FRAME_NT, 0, s>>>(f);
+        r2g_launch_pdl(lr_kernel<uint8_t>, dim3(n), dim3(LR_FRAME_NT), s, f);
     return 1;
 }
 

@@ -144,3 +144,30 @@ void r2g_dsp_launch_ccso_add(uint16_t *dst, const uint8_t *idx, const uint8_t *o
 void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth);
 void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling);
 
+// ---- programmatic dependent launch (per-frame kernels) ----
+// A per-frame kernel is launched so that it may start while the previous
+// kernel on the stream finishes: it does its prologue (work that reads only
+// side-info, tables or the recon, which no kernel writes), then waits for the
+// previous grid (griddepcontrol.wait: a hardware dependency, complete and
+// memory-visible) before reading or writing any plane a kernel produces.
+// Each of these kernels lets its own dependents launch as soon as all its
+// CTAs are resident.  R2G_PDL=0 in the environment launches them plainly.
+R2G_D void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+R2G_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::); }
+
+bool r2g_pdl_enabled();
+
+template <typename... Exp, typename... Act>
+inline cudaError_t r2g_launch_pdl(void (*kern)(Exp...), dim3 grid, dim3 block, cudaStream_t s, Act &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = r2g_pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<Act &&>(args)...);
+}

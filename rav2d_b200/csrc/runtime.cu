@@ -10,6 +10,7 @@
 // skips it.
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -38,6 +39,14 @@ static void set_err(R2gCtx *ctx, const char *fmt, const char *a = "") {
     } while (0)
 
 extern "C" int r2g_version(void) { return R2G_VERSION; }
+
+bool r2g_pdl_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("R2G_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 extern "C" int r2g_plane_geometry(int width, int height, int bitdepth, int64_t *y_stride, int64_t *uv_stride,
                                   int64_t *y_rows, int64_t *uv_rows) {
