@@ -234,21 +234,6 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && sb256_idx < nsb &&
                         f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
 
-    // C and D come from the previous kernels on the stream: wait for them
-    // (everything above reads side-info only)
-    pdl_wait();
-    if (wkind == W_NONE && !gdf_on) {
-        // unfiltered unit: copy C -> L in 4-byte words (unit widths are
-        // multiples of 4 samples; rows and unit origins are 64-byte aligned)
-        const int wpr = g.uw * (int)sizeof(P) / 4;
-        for (int i = tid; i < nr * wpr; i += NT) {
-            const int r = ro + i / wpr, q = i % wpr;
-            const int64_t o = (int64_t)(g.y0 + r) * stride + g.x0;
-            reinterpret_cast<uint32_t *>(Lp + o)[q] = __ldg(reinterpret_cast<const uint32_t *>(Cp + o) + q);
-        }
-        return;
-    }
-
     // ---- lossless rows of the stripe (looprestoration.rs:2037-2075) ----
     const int ll_rows = imax_(g.sh >> 2, 1) + 1;
     if (tid < 17) {
@@ -291,6 +276,45 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         }
         sm.noskip[tid] = v;
     }
+    // GDF and PC-Wiener parameters of the frame (tables only)
+    if (gdf_on && !chroma) {
+        const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
+        const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
+        const int weight_base = ref_dst_idx * 1584 + qp_idx * 264;
+        const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
+                                                : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
+        const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
+        for (int i = tid; i < 88; i += NT) {
+            int k = i >> 2, c = i & 3;
+            const int a = f.tab.GDF_ALPHA[alpha_base + i];
+            sm.s_w[c][k] = make_int4(f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i],
+                                     f.tab.GDF_WEIGHT[weight_base + 1 * 88 + i],
+                                     f.tab.GDF_WEIGHT[weight_base + 2 * 88 + i], a);
+            if (k < 18) {
+                const uint32_t pa = (uint32_t)a & 0xffff, na = (uint32_t)(-a) & 0xffff;
+                sm.s_aa[c][k] = make_uint2(pa | (pa << 16), na | (na << 16));
+            }
+        }
+        for (int i = tid; i < nerr; i += NT) sm.s_err[i] = errtab[i];
+    }
+    if (wkind == W_PC)
+        for (int i = tid; i < 64 * 13; i += NT) sm.s_pcf[i] = f.tab.PC_WIENER_FILTERS[f.wiener_idx * 64 * 13 + i];
+    // C and D come from the previous kernels on the stream: wait for them
+    // (everything above reads side-info and tables only; a CTA that only
+    // copies has staged a few unused rows and parameters)
+    pdl_wait();
+    if (wkind == W_NONE && !gdf_on) {
+        // unfiltered unit: copy C -> L in 4-byte words (unit widths are
+        // multiples of 4 samples; rows and unit origins are 64-byte aligned)
+        const int wpr = g.uw * (int)sizeof(P) / 4;
+        for (int i = tid; i < nr * wpr; i += NT) {
+            const int r = ro + i / wpr, q = i % wpr;
+            const int64_t o = (int64_t)(g.y0 + r) * stride + g.x0;
+            reinterpret_cast<uint32_t *>(Lp + o)[q] = __ldg(reinterpret_cast<const uint32_t *>(Cp + o) + q);
+        }
+        return;
+    }
+
 
     if (chroma) {
         // ---- chroma window: rows -2 .. sh+1, columns -2 .. uw+1 ----
@@ -450,28 +474,6 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
         }
     }
     const int16_t *W16 = reinterpret_cast<const int16_t *>(sm.u.wp);  // scalar sample i at W16[2 * i]
-    if (gdf_on) {
-        const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
-        const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
-        const int weight_base = ref_dst_idx * 1584 + qp_idx * 264;
-        const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
-                                                : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
-        const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
-        for (int i = tid; i < 88; i += NT) {
-            int k = i >> 2, c = i & 3;
-            const int a = f.tab.GDF_ALPHA[alpha_base + i];
-            sm.s_w[c][k] = make_int4(f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i],
-                                     f.tab.GDF_WEIGHT[weight_base + 1 * 88 + i],
-                                     f.tab.GDF_WEIGHT[weight_base + 2 * 88 + i], a);
-            if (k < 18) {
-                const uint32_t pa = (uint32_t)a & 0xffff, na = (uint32_t)(-a) & 0xffff;
-                sm.s_aa[c][k] = make_uint2(pa | (pa << 16), na | (na << 16));
-            }
-        }
-        for (int i = tid; i < nerr; i += NT) sm.s_err[i] = errtab[i];
-    }
-    if (wkind == W_PC)
-        for (int i = tid; i < 64 * 13; i += NT) sm.s_pcf[i] = f.tab.PC_WIENER_FILTERS[f.wiener_idx * 64 * 13 + i];
     __syncthreads();
 
     const int b8 = bitdepth - 8;
