@@ -462,6 +462,7 @@ __global__ void __launch_bounds__(256, 7) cdef_ccso_kernel(const DevFrame f) {
 // Persistent kernel over a cross-frame work list: item = frame << 22 |
 // region row * sb64w + sbx.
 __global__ void __launch_bounds__(256, 6) cdef_batch_kernel(BatchArgs a) {
+    pdl_trigger();
     __shared__ CdefSmem sm;
     const int n = a.count[1];
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
@@ -592,7 +593,9 @@ __global__ void dsp_ccso_add_kernel(uint16_t *dst, const uint8_t *idx, const uin
 
 }  // namespace
 
-void r2g_batch_launch_cdef(const BatchArgs &a, int grid, cudaStream_t s) { cdef_batch_kernel<<<grid, 256, 0, s>>>(a); }
+void r2g_batch_launch_cdef(const BatchArgs &a, int grid, cudaStream_t s) {
+    r2g_launch_pdl(cdef_batch_kernel, dim3(grid), dim3(256), s, a);
+}
 int r2g_batch_occupancy_cdef() {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cdef_batch_kernel, 256, 0);

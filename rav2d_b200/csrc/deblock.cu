@@ -481,6 +481,7 @@ __global__ void __launch_bounds__(256, 4) deblock_tile_kernel(const DevFrame f) 
 // Persistent kernel over a cross-frame work list: item = frame << 22 | ty *
 // tiles_w + tx.
 __global__ void __launch_bounds__(256, 4) deblock_batch_kernel(BatchArgs a) {
+    pdl_trigger();
     __shared__ DeblockSmem sm;
     const int n = a.count[0];
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
@@ -498,7 +499,7 @@ __global__ void __launch_bounds__(256, 4) deblock_batch_kernel(BatchArgs a) {
 }  // namespace
 
 void r2g_batch_launch_deblock(const BatchArgs &a, int grid, cudaStream_t s) {
-    deblock_batch_kernel<<<grid, 256, 0, s>>>(a);
+    r2g_launch_pdl(deblock_batch_kernel, dim3(grid), dim3(256), s, a);
 }
 int r2g_batch_occupancy_deblock() {
     int nb = 0;

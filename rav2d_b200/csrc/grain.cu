@@ -213,6 +213,9 @@ R2G_D void grain_block(const DevFrame &f, const GrainParams &gp, const int16_t *
         off[which][i][n] = v;
     }
     __syncthreads();
+    // the filtered planes may come from the previous kernel of a batch
+    // graph launched ahead (programmatic dependent launch): wait for it
+    pdl_wait();
     const int b8 = f.bitdepth - 8, bdmax = f.bdmax;
     const int gmin = -(128 << b8), gmax = (128 << b8) - 1;
     const int64_t ys = f.stride[0], uvs = f.stride[1];
@@ -374,7 +377,7 @@ void r2g_batch_launch_grain_template(const BatchArgs &a, int grid, cudaStream_t 
     grain_template_batch_kernel<<<grid, 256, 0, s>>>(a);
 }
 void r2g_batch_launch_grain_apply(const BatchArgs &a, int grid, cudaStream_t s) {
-    grain_apply_batch_kernel<<<grid, 256, 0, s>>>(a);
+    r2g_launch_pdl(grain_apply_batch_kernel, dim3(grid), dim3(256), s, a);
 }
 int r2g_batch_occupancy_grain_apply() {
     int nb = 0;

@@ -693,6 +693,7 @@ __device__ __noinline__ void lr_unit_hbd(const DevFrame &f, LrSmem &sm, int b) {
 __device__ __noinline__ void lr_unit_8(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint8_t, 256>(f, sm, b); }
 
 __global__ void __launch_bounds__(256, 4) lr_batch_kernel(BatchArgs a) {
+    pdl_trigger();
     __shared__ LrSmem sm;
     const int n = a.count[2];
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
@@ -723,7 +724,9 @@ __global__ void dsp_gdf_add_kernel(uint16_t *p, const int8_t *err, int w, int h,
 
 }  // namespace
 
-void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s) { lr_batch_kernel<<<grid, 256, 0, s>>>(a); }
+void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s) {
+    r2g_launch_pdl(lr_batch_kernel, dim3(grid), dim3(256), s, a);
+}
 int r2g_batch_occupancy_lr() {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lr_batch_kernel, 256, 0);
