@@ -57,6 +57,69 @@ struct GrainTplSmem {
     int16_t lc[2][SGH][SGW];
 };
 
+// The auto-regressive filters of generate_grain_y (filmgrain.rs:134-157) and
+// generate_grain_uv (:183-228), specialised on the lag: cell (y, x) reads
+// rows y - LAG .. y - 1 over x - LAG .. x + LAG and row y over x - LAG ..
+// x - 1, so the cells with equal x + 4y (LAG <= 3) only read earlier fronts
+// and one front is computed per step.  The coefficients sit in registers and
+// every tap is an unrolled, independent shared-memory read.
+template <int LAG>
+R2G_D void ar_fronts(const GrainParams &gp, GrainTplSmem &sm, bool gen_u, bool gen_v, int gmin, int gmax) {
+    constexpr int NTAP = 2 * LAG * (LAG + 1);
+    const R2gFilmGrainData &d = gp.d;
+    const int tid = threadIdx.x, ar_shift = (int)d.ar_coeff_shift;
+    // luma: one row per thread (73 rows); lag 0 only clips, cell by cell
+    if (LAG == 0) {
+        for (int i = tid; i < (GH - 3) * (GW - 6); i += blockDim.x) {
+            int16_t &g = sm.ly[3 + i / (GW - 6)][3 + i % (GW - 6)];
+            g = (int16_t)iclip_(g, gmin, gmax);
+        }
+        __syncthreads();
+    } else {
+        int cy[NTAP > 0 ? NTAP : 1];
+#pragma unroll
+        for (int i = 0; i < NTAP; i++) cy[i] = d.ar_coeffs[0][i];
+        const int y = 3 + tid;
+        for (int t = 3 + 4 * 3; t <= (GW - 4) + 4 * (GH - 1); t++) {
+            const int x = t - 4 * y;
+            if (y < GH && x >= 3 && x < GW - 3) {
+                int sum = 0, ci = 0;
+#pragma unroll
+                for (int dy = -LAG; dy <= 0; dy++)
+#pragma unroll
+                    for (int dx = -LAG; dx <= LAG; dx++)
+                        if (dy < 0 || dx < 0) sum += cy[ci++] * sm.ly[y + dy][x + dx];
+                sm.ly[y][x] = (int16_t)iclip_(sm.ly[y][x] + round2(sum, ar_shift), gmin, gmax);
+            }
+            __syncthreads();
+        }
+    }
+    // chroma: threads 0..127 plane U, 128..255 plane V, one row each
+    const int uv = tid >> 7, y = 3 + (tid & 127);
+    int cc[NTAP + 1];
+#pragma unroll
+    for (int i = 0; i <= NTAP; i++) cc[i] = d.ar_coeffs[1 + uv][i];
+    const bool gen = uv ? gen_v : gen_u, with_luma = d.num_points[0] > 0;
+    for (int t = 3 + 4 * 3; t <= (SGW - 4) + 4 * (SGH - 1); t++) {
+        const int x = t - 4 * y;
+        if (gen && y < SGH && x >= 3 && x < SGW - 3) {
+            int sum = 0, ci = 0;
+#pragma unroll
+            for (int dy = -LAG; dy <= 0; dy++)
+#pragma unroll
+                for (int dx = -LAG; dx <= LAG; dx++)
+                    if (dy < 0 || dx < 0) sum += cc[ci++] * sm.lc[uv][y + dy][x + dx];
+            if (with_luma) {
+                const int lx = ((x - 3) << 1) + 3, lyy = ((y - 3) << 1) + 3;
+                const int luma = sm.ly[lyy][lx] + sm.ly[lyy][lx + 1] + sm.ly[lyy + 1][lx] + sm.ly[lyy + 1][lx + 1];
+                sum += round2(luma, 2) * cc[NTAP];
+            }
+            sm.lc[uv][y][x] = (int16_t)iclip_(sm.lc[uv][y][x] + round2(sum, ar_shift), gmin, gmax);
+        }
+        __syncthreads();
+    }
+}
+
 R2G_D void grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling,
                           GrainTplSmem &sm) {
     auto &ly = sm.ly;
@@ -95,42 +158,11 @@ R2G_D void grain_template(const GrainParams &gp, const DevTables &tab, int16_t *
         }
     }
     __syncthreads();
-    const int lag = d.ar_coeff_lag;
-    const int ar_shift = (int)d.ar_coeff_shift;
-    // luma AR wavefront (generate_grain_y :134-157)
-    for (int t = 3 + 4 * 3; t <= (GW - 4) + 4 * (GH - 1); t++) {
-        for (int y = 3 + tid; y < GH; y += 256) {
-            int x = t - 4 * y;
-            if (x < 3 || x >= GW - 3) continue;
-            int sum = 0, ci = 0;
-            for (int dy = y - lag; dy <= y; dy++) {
-                int dx_end = dy == y ? x : x + lag + 1;
-                for (int dx = x - lag; dx < dx_end; dx++) sum += d.ar_coeffs[0][ci++] * ly[dy][dx];
-            }
-            ly[y][x] = (int16_t)iclip_(ly[y][x] + round2(sum, ar_shift), gmin, gmax);
-        }
-        __syncthreads();
-    }
-    // chroma AR wavefront (generate_grain_uv :183-228), both planes
-    for (int t = 3 + 4 * 3; t <= (SGW - 4) + 4 * (SGH - 1); t++) {
-        int uv = tid >> 7;
-        for (int y = 3 + (tid & 127); y < SGH; y += 128) {
-            int x = t - 4 * y;
-            if (x < 3 || x >= SGW - 3) continue;
-            if (!(uv ? gen_v : gen_u)) continue;
-            const int8_t *coeff = d.ar_coeffs[1 + uv];
-            int sum = 0, ci = 0;
-            for (int dy = y - lag; dy < y; dy++)
-                for (int dx = x - lag; dx <= x + lag; dx++) sum += coeff[ci++] * lc[uv][dy][dx];
-            for (int dx = x - lag; dx < x; dx++) sum += coeff[ci++] * lc[uv][y][dx];
-            if (d.num_points[0] > 0) {
-                int lx = ((x - 3) << 1) + 3, lyy = ((y - 3) << 1) + 3;
-                int luma = ly[lyy][lx] + ly[lyy][lx + 1] + ly[lyy + 1][lx] + ly[lyy + 1][lx + 1];
-                sum += round2(luma, 2) * coeff[ci];
-            }
-            lc[uv][y][x] = (int16_t)iclip_(lc[uv][y][x] + round2(sum, ar_shift), gmin, gmax);
-        }
-        __syncthreads();
+    switch (d.ar_coeff_lag) {
+        case 0: ar_fronts<0>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+        case 1: ar_fronts<1>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+        case 2: ar_fronts<2>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+        default: ar_fronts<3>(gp, sm, gen_u, gen_v, gmin, gmax); break;
     }
     // write templates (zero where a plane's template is not generated)
     for (int i = tid; i < GH * GW; i += 256) {
