@@ -304,8 +304,7 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
             g.frame = i;
             g.lut = (int16_t *)f->grain_scratch;
             g.scaling = (uint8_t *)f->grain_scratch + 3 * 73 * 82 * 2;
-            int bs = 16 << items[i].fgd->block_size;
-            counts[3] += ((f->w + bs - 1) / bs) * ((f->h + bs - 1) / bs);
+            counts[3] += r2g_grain_items(f->w, f->h, items[i].fgd->block_size);
             grains.push_back(g);
             f->grain_buf = 4;
         }
@@ -358,8 +357,7 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
         int c3 = 0;
         for (size_t gi = 0; gi < grains.size(); gi++) {
             const DevFrame &f = frames[grains[gi].frame];
-            int bs = 16 << grains[gi].gp.d.block_size;
-            int e = ((f.w + bs - 1) / bs) * ((f.h + bs - 1) / bs);
+            int e = r2g_grain_items(f.w, f.h, grains[gi].gp.d.block_size);
             for (int j = 0; j < e; j++) w3[c3++] = ((uint32_t)gi << 22) | j;
         }
     }

@@ -258,6 +258,7 @@ extern "C" int r2g_dsp_generate_grain(int16_t *buf_y, int16_t *buf_u, int16_t *b
     gp.seed = seed;
     gp.bitdepth = bitdepth;
     gp.has_y = gp.has_u = gp.has_v = 1;
+    gp.vec = 0;
     const size_t plane = 73 * 82;
     int16_t *lut = (int16_t *)d->buf;
     uint8_t *scaling = (uint8_t *)(d->buf + 3 * plane * sizeof(int16_t));

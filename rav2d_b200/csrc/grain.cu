@@ -16,6 +16,7 @@
 // * block offsets of row band r and block b are draws 8b + 4n + 1 of the
 //   band's seed, evaluated directly by jump-ahead in the apply kernel.
 #include <cstring>
+#include <mutex>
 
 #include "r2g_common.cuh"
 #include "r2g_runtime.h"
@@ -24,7 +25,12 @@ namespace {
 
 constexpr int GW = 82, GH = 73, SGW = 44, SGH = 38;
 
-__constant__ uint16_t c_lfsr_pow[14][16];  // columns of M^(2^j)
+// The LFSR of filmgrain.rs:11-16 (taps 16, 15, 13, 4) is maximal-length:
+// every nonzero state lies on one cycle of 65535 states.  g_lfsr_cycle[i] is
+// the state i steps after state 1 and g_lfsr_pos its inverse, so a jump of k
+// steps is two look-ups.  Both are built on the host once per device.
+__device__ uint16_t g_lfsr_cycle[65536];
+__device__ uint16_t g_lfsr_pos[65536];
 
 // one LFSR step (filmgrain.rs:11-16)
 R2G_HD uint32_t lfsr_step(uint32_t r) {
@@ -32,20 +38,13 @@ R2G_HD uint32_t lfsr_step(uint32_t r) {
     return (r >> 1) | (bit << 15);
 }
 
-R2G_D uint32_t apply_mat(const uint16_t *cols, uint32_t s) {
-    uint32_t o = 0;
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        if ((s >> i) & 1) o ^= cols[i];
-    return o;
-}
-
-// state after k steps from s (16-bit state; k < 2^14)
+// state after k steps from s (16-bit state)
 R2G_D uint32_t lfsr_jump(uint32_t s, uint32_t k) {
-    uint32_t st = s & 0xffff;  // seeds are 16-bit (checked at the boundary)
-    for (int j = 0; j < 14; j++)
-        if ((k >> j) & 1) st = apply_mat(c_lfsr_pow[j], st);
-    return st;
+    s &= 0xffff;  // seeds are 16-bit (checked at the boundary)
+    if (!s) return 0;  // the all-zero state stays zero
+    uint32_t i = (uint32_t)__ldg(&g_lfsr_pos[s]) + k % 65535u;
+    if (i >= 65535u) i -= 65535u;
+    return __ldg(&g_lfsr_cycle[i]);
 }
 
 R2G_D int round2(int x, int shift) { return (x + ((1 << shift) >> 1)) >> shift; }
@@ -228,149 +227,262 @@ R2G_D int block_offset(uint32_t in_seed, int row, int i, int b, int n, int block
     return (int)(((uint32_t)(3 - block_size) * ((st >> 7) & 511)) >> 6);
 }
 
-// One CTA per (row band, 32-px block): luma 32x32 (or the frame remainder)
-// and both chroma 16x16 blocks.
-template <typename P>
-R2G_D void grain_block(const DevFrame &f, const GrainParams &gp, const int16_t *lut, const uint8_t *scaling, int row,
-                       int b, int (&off)[2][2][2]) {
+template <int BYTES>
+struct RawRun;
+template <>
+struct RawRun<2> {
+    using T = unsigned short;
+};
+template <>
+struct RawRun<4> {
+    using T = unsigned int;
+};
+template <>
+struct RawRun<8> {
+    using T = uint2;
+};
+
+// N consecutive samples at p: one aligned vector load / store when `vec`,
+// else sample by sample over the first n (the part inside the plane).
+template <typename P, int N>
+R2G_D void load_run(const P *p, int n, bool vec, int (&v)[N]) {
+    if (vec) {
+        using T = typename RawRun<N * sizeof(P)>::T;
+        const T raw = __ldg(reinterpret_cast<const T *>(p));
+        P s[N];
+        memcpy(s, &raw, sizeof(raw));
+#pragma unroll
+        for (int k = 0; k < N; k++) v[k] = s[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; k++) v[k] = k < n ? (int)__ldg(p + k) : 0;
+    }
+}
+
+template <typename P, int N>
+R2G_D void store_run(P *p, int n, bool vec, const int (&v)[N]) {
+    if (vec) {
+        using T = typename RawRun<N * sizeof(P)>::T;
+        P s[N];
+#pragma unroll
+        for (int k = 0; k < N; k++) s[k] = (P)v[k];
+        T raw;
+        memcpy(&raw, s, sizeof(raw));
+        *reinterpret_cast<T *>(p) = raw;
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; k++)
+            if (k < n) p[k] = (P)v[k];
+    }
+}
+
+// Luma samples of a band covered by one CTA (a segment): 4 blocks of 32 or
+// 8 blocks of 16.
+constexpr int SEG_W = 128;
+
+// Offsets (filmgrain.rs:274-305) of blocks b0 - 1 .. b0 + NB - 1 of a
+// segment: v[j][i][n] for block b0 - 1 + j, seed row i, coordinate n.
+template <int BS>
+struct SegOffsets {
+    int v[SEG_W / BS + 1][2][2];
+};
+
+// Overlap blend of two grain values (filmgrain.rs:560-600 / :760-800).
+R2G_D int blend(int a, int wa, int b, int wb, int gmin, int gmax) {
+    return iclip_((a * wa + b * wb + 16) >> 5, gmin, gmax);
+}
+
+// One CTA per segment of a row band: luma BS rows x SEG_W samples and both
+// chroma planes' BS/2 x SEG_W/2 (fgy_32x32xn / fguv_32x32xn, 4:2:0).  Thread
+// t takes luma columns 4 (t % 32) .. +3 over rows (t / 32) * BS/8 .. +BS/8-1
+// and chroma columns 2 (t % 32) .. +1 over rows (t / 32) * BS/16 .. of both
+// planes: the luma samples that chroma scaling averages are the thread's own
+// even rows, a warp moves whole rows, and every plane sample is requested
+// before the first template or scaling look-up.  Overlap: the blend of the
+// first two rows of a band is uniform per warp; the first two columns of a
+// block are a fix-up of the runs that start a block.
+template <typename P, int BS>
+R2G_D void grain_segment(const DevFrame &f, const GrainParams &gp, const int16_t *lut, const uint8_t *scaling, int row,
+                         int seg, SegOffsets<BS> &so) {
+    constexpr int NB = SEG_W / BS, RL = BS / 8, RC = BS / 16, CB = BS / 2;
     const int tid = threadIdx.x;
     const R2gFilmGrainData &d = gp.d;
-    const int bs = 16 << d.block_size;
     const int rows = 1 + (d.overlap_flag && row > 0);
-    if (tid < 8) {
-        int which = tid >> 2, i = (tid >> 1) & 1, n = tid & 1;
-        int v = 0;
-        int bb = b - which;
-        if (i < rows && bb >= 0) v = block_offset(gp.seed, row, i, bb, n, d.block_size);
-        off[which][i][n] = v;
+    const int b0 = seg * NB;
+    if (tid < 4 * (NB + 1)) {
+        const int j = tid >> 2, i = (tid >> 1) & 1, n = tid & 1, bb = b0 - 1 + j;
+        so.v[j][i][n] = (i < rows && bb >= 0) ? block_offset(gp.seed, row, i, bb, n, d.block_size) : 0;
     }
-    __syncthreads();
-    // the filtered planes may come from the previous kernel of a batch
-    // graph launched ahead (programmatic dependent launch): wait for it
+    // the filtered planes may come from the previous kernel (programmatic
+    // dependent launch): wait for it
     pdl_wait();
     const int b8 = f.bitdepth - 8, bdmax = f.bdmax;
     const int gmin = -(128 << b8), gmax = (128 << b8) - 1;
     const int64_t ys = f.stride[0], uvs = f.stride[1];
-    const P *Ly = plane_ptr<const P>(f.L[0]);
+    const bool vec = gp.vec;
+    const int c32 = tid & 31, r0 = tid >> 5;
+    const int bl = (4 * c32) / BS;  // block of the segment
+
+    // ---- plane loads ----
+    const int X = seg * SEG_W + 4 * c32, Y0 = row * BS + r0 * RL;
+    const int bh = imin_(BS, f.h - row * BS);
+    const int ln = f.w - X;  // luma samples of the run inside the plane
+    const P *Ly = plane_ptr<const P>(f.L[0]) + (int64_t)Y0 * ys + X;
+    int sy[RL][4];
+#pragma unroll
+    for (int k = 0; k < RL; k++) {
+        if (ln > 0 && r0 * RL + k < bh)
+            load_run<P, 4>(Ly + k * ys, ln, vec && ln >= 4, sy[k]);
+        else
+            sy[k][0] = sy[k][1] = sy[k][2] = sy[k][3] = 0;
+    }
+    const int CX = seg * (SEG_W / 2) + 2 * c32, CY0 = row * CB + r0 * RC;
+    const int cbh = (bh + 1) >> 1;
+    const int cn = ((f.w + 1) >> 1) - CX;
+    int sc[2][RC][2];
+#pragma unroll
+    for (int uv = 0; uv < 2; uv++) {
+        const P *Lc = plane_ptr<const P>(f.L[1 + uv]) + (int64_t)CY0 * uvs + CX;
+#pragma unroll
+        for (int k = 0; k < RC; k++) {
+            if (cn > 0 && r0 * RC + k < cbh)
+                load_run<P, 2>(Lc + k * uvs, cn, vec && cn >= 2, sc[uv][k]);
+            else
+                sc[uv][k][0] = sc[uv][k][1] = 0;
+        }
+    }
+    __syncthreads();  // offsets
+
+    const int bb = b0 + bl;
+    const bool ovx = d.overlap_flag && bb > 0, ovy = d.overlap_flag && row > 0;
+    const int sshift = d.scaling_shift, srnd = (1 << sshift) >> 1;
+
+    // ---- chroma (uses the luma samples before grain) ----
+    if (cn > 0) {
+        const int cx0 = (2 * c32) % CB;  // block-relative column of the run
+        const int cbw = imin_(CB, ((f.w + 1) >> 1) - bb * CB);
+        const int ystart = ovy ? imin_(1, cbh) : 0;
+        const bool hfix = ovx && cx0 == 0 && cbw >= 1;  // column 0 blends with the block to the left
+        int minv = 0, maxv = bdmax;
+        if (d.clip_to_restricted_range) {
+            minv = 16 << b8;
+            maxv = (d.mc_identity ? 235 : 240) << b8;
+        }
+        int cbase[2][2];  // template index of block-relative (0, 0)
+#pragma unroll
+        for (int bxs = 0; bxs < 2; bxs++)
+#pragma unroll
+            for (int bys = 0; bys < 2; bys++) {
+                const int *of = so.v[bl + 1 - bxs][bys];
+                cbase[bxs][bys] = (3 + (3 + of[0]) + CB * bys) * GW + 3 + (3 + of[1]) + CB * bxs + cx0;
+            }
+#pragma unroll
+        for (int uv = 0; uv < 2; uv++) {
+            const bool has = uv ? gp.has_v : gp.has_u;
+            const int16_t *cl = lut + (1 + uv) * GH * GW;
+            const uint8_t *scl = scaling + (d.chroma_scaling_from_luma ? 0 : (1 + uv)) * 1024;
+            const int lm = d.uv_luma_mult[uv], m = d.uv_mult[uv], o = d.uv_offset[uv] * (1 << b8);
+            P *Gc = plane_ptr<P>(f.G[1 + uv]) + (int64_t)CY0 * uvs + CX;
+#pragma unroll
+            for (int k = 0; k < RC; k++) {
+                const int cy = r0 * RC + k;
+                if (cy >= cbh) continue;
+                int out[2] = {sc[uv][k][0], sc[uv][k][1]};
+                if (has) {
+                    int g[2];
+#pragma unroll
+                    for (int e = 0; e < 2; e++) g[e] = __ldg(&cl[cbase[0][0] + cy * GW + e]);
+                    if (hfix) g[0] = blend(__ldg(&cl[cbase[1][0] + cy * GW]), 23, g[0], 22, gmin, gmax);
+                    if (cy < ystart) {
+                        int t[2];
+#pragma unroll
+                        for (int e = 0; e < 2; e++) t[e] = __ldg(&cl[cbase[0][1] + cy * GW + e]);
+                        if (hfix) t[0] = blend(__ldg(&cl[cbase[1][1] + cy * GW]), 23, t[0], 22, gmin, gmax);
+#pragma unroll
+                        for (int e = 0; e < 2; e++) g[e] = blend(t[e], 23, g[e], 22, gmin, gmax);
+                    }
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        // luma row 2 cy of the band is the thread's row 2 k
+                        const int avg = (sy[2 * k][2 * e] + sy[2 * k][2 * e + 1] + 1) >> 1;
+                        int val = avg;
+                        if (!d.chroma_scaling_from_luma) val = clip_px_(((avg * lm + sc[uv][k][e] * m) >> 6) + o, bdmax);
+                        const int noise = ((int)__ldg(&scl[val]) * g[e] + srnd) >> sshift;
+                        out[e] = iclip_(sc[uv][k][e] + noise, minv, maxv);
+                    }
+                }
+                store_run<P, 2>(Gc + k * uvs, cn, vec && cn >= 2, out);
+            }
+        }
+    }
+
     // ---- luma ----
-    {
-        const int x0 = b * bs, y0 = row * bs;
-        const int bw = imin_(bs, f.w - x0), bh = imin_(bs, f.h - y0);
-        P *Gy = plane_ptr<P>(f.G[0]);
-        const int ystart = (d.overlap_flag && row > 0) ? imin_(2, bh) : 0;
-        const int xstart = (d.overlap_flag && b > 0) ? imin_(2, bw) : 0;
-        int minv, maxv;
+    if (ln > 0) {
+        const int lx0 = (4 * c32) % BS;
+        const int bw = imin_(BS, f.w - bb * BS);
+        const int ystart = ovy ? imin_(2, bh) : 0, xstart = ovx && lx0 == 0 ? imin_(2, bw) : 0;
+        int minv = 0, maxv = bdmax;
         if (d.clip_to_restricted_range) {
             minv = 16 << b8;
             maxv = 235 << b8;
-        } else {
-            minv = 0;
-            maxv = bdmax;
         }
-        const int w[2][2] = {{27, 17}, {17, 27}};
-        for (int i = tid; i < bs * bs; i += 256) {
-            int y = i / bs, x = i % bs;
-            if (y >= bh || x >= bw) continue;
-            int64_t o = (int64_t)(y0 + y) * ys + x0 + x;
-            int sv = Ly[o];
-            if (!gp.has_y) {
-                Gy[o] = (P)sv;
-                continue;
+        int obase[2][2];
+#pragma unroll
+        for (int bxs = 0; bxs < 2; bxs++)
+#pragma unroll
+            for (int bys = 0; bys < 2; bys++) {
+                const int *of = so.v[bl + 1 - bxs][bys];
+                obase[bxs][bys] = (3 + 2 * (3 + of[0]) + BS * bys) * GW + 3 + 2 * (3 + of[1]) + BS * bxs + lx0;
             }
-            auto S = [&](int bxs, int bys) -> int {
-                const int *of = off[bxs][bys];
-                int offx = 3 + 2 * (3 + of[1]), offy = 3 + 2 * (3 + of[0]);
-                return lut[(offy + y + bs * bys) * GW + offx + x + bs * bxs];
-            };
-            int grain;
-            if (y >= ystart) {
-                if (x >= xstart)
-                    grain = S(0, 0);
-                else
-                    grain = iclip_(round2(S(1, 0) * w[x][0] + S(0, 0) * w[x][1], 5), gmin, gmax);
-            } else {
-                if (x >= xstart) {
-                    grain = iclip_(round2(S(0, 1) * w[y][0] + S(0, 0) * w[y][1], 5), gmin, gmax);
-                } else {
-                    int top = iclip_(round2(S(1, 1) * w[x][0] + S(0, 1) * w[x][1], 5), gmin, gmax);
-                    int g = iclip_(round2(S(1, 0) * w[x][0] + S(0, 0) * w[x][1], 5), gmin, gmax);
-                    grain = iclip_(round2(top * w[y][0] + g * w[y][1], 5), gmin, gmax);
+        P *Gy = plane_ptr<P>(f.G[0]) + (int64_t)Y0 * ys + X;
+#pragma unroll
+        for (int k = 0; k < RL; k++) {
+            const int y = r0 * RL + k;
+            if (y >= bh) continue;
+            int out[4] = {sy[k][0], sy[k][1], sy[k][2], sy[k][3]};
+            if (gp.has_y) {
+                int g[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) g[e] = __ldg(&lut[obase[0][0] + y * GW + e]);
+                if (xstart > 0) g[0] = blend(__ldg(&lut[obase[1][0] + y * GW]), 27, g[0], 17, gmin, gmax);
+                if (xstart > 1) g[1] = blend(__ldg(&lut[obase[1][0] + y * GW + 1]), 17, g[1], 27, gmin, gmax);
+                if (y < ystart) {  // uniform per warp
+                    int t[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) t[e] = __ldg(&lut[obase[0][1] + y * GW + e]);
+                    if (xstart > 0) t[0] = blend(__ldg(&lut[obase[1][1] + y * GW]), 27, t[0], 17, gmin, gmax);
+                    if (xstart > 1) t[1] = blend(__ldg(&lut[obase[1][1] + y * GW + 1]), 17, t[1], 27, gmin, gmax);
+                    const int wt = y ? 17 : 27, wc = y ? 27 : 17;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) g[e] = blend(t[e], wt, g[e], wc, gmin, gmax);
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int noise = ((int)__ldg(&scaling[sy[k][e]]) * g[e] + srnd) >> sshift;
+                    out[e] = iclip_(sy[k][e] + noise, minv, maxv);
                 }
             }
-            int noise = round2(scaling[sv] * grain, d.scaling_shift);
-            Gy[o] = (P)iclip_(sv + noise, minv, maxv);
-        }
-    }
-    // ---- chroma (fguv_32x32xn, 4:2:0) ----
-    {
-        const int cbs = bs >> 1;
-        const int x0 = b * cbs, y0 = row * cbs;
-        const int pw = (f.w + 1) >> 1;
-        const int bw = imin_(cbs, pw - x0);
-        const int bh = (imin_(f.h - row * bs, bs) + 1) >> 1;
-        const int ystart = (d.overlap_flag && row > 0) ? imin_(1, bh) : 0;
-        const int xstart = (d.overlap_flag && b > 0) ? imin_(1, bw) : 0;
-        for (int i = tid; i < 2 * cbs * cbs; i += 256) {
-            int uv = i / (cbs * cbs), j = i % (cbs * cbs);
-            int y = j / cbs, x = j % cbs;
-            if (y >= bh || x >= bw) continue;
-            const P *Lc = plane_ptr<const P>(f.L[1 + uv]);
-            P *Gc = plane_ptr<P>(f.G[1 + uv]);
-            int64_t o = (int64_t)(y0 + y) * uvs + x0 + x;
-            int sv = Lc[o];
-            bool has = uv ? gp.has_v : gp.has_u;
-            if (!has) {
-                Gc[o] = (P)sv;
-                continue;
-            }
-            const int16_t *cl = lut + (1 + uv) * GH * GW;
-            auto S = [&](int bxs, int bys) -> int {
-                const int *of = off[bxs][bys];
-                int offx = 3 + (3 + of[1]), offy = 3 + (3 + of[0]);
-                return cl[(offy + y + cbs * bys) * GW + offx + x + cbs * bxs];
-            };
-            int grain;
-            if (y >= ystart) {
-                if (x >= xstart)
-                    grain = S(0, 0);
-                else
-                    grain = iclip_(round2(S(1, 0) * 23 + S(0, 0) * 22, 5), gmin, gmax);
-            } else {
-                if (x >= xstart) {
-                    grain = iclip_(round2(S(0, 1) * 23 + S(0, 0) * 22, 5), gmin, gmax);
-                } else {
-                    int top = iclip_(round2(S(1, 1) * 23 + S(0, 1) * 22, 5), gmin, gmax);
-                    int g = iclip_(round2(S(1, 0) * 23 + S(0, 0) * 22, 5), gmin, gmax);
-                    grain = iclip_(round2(top * 23 + g * 22, 5), gmin, gmax);
-                }
-            }
-            int lx = (x0 + x) << 1, lyy = (y0 + y) << 1;
-            int luma = Ly[(int64_t)lyy * ys + lx];
-            int avg = (luma + Ly[(int64_t)lyy * ys + lx + 1] + 1) >> 1;
-            int val;
-            if (!d.chroma_scaling_from_luma) {
-                int combined = avg * d.uv_luma_mult[uv] + sv * d.uv_mult[uv];
-                val = clip_px_((combined >> 6) + d.uv_offset[uv] * (1 << b8), bdmax);
-            } else {
-                val = avg;
-            }
-            const uint8_t *sc = scaling + (d.chroma_scaling_from_luma ? 0 : (1 + uv)) * 1024;
-            int noise = round2(sc[val] * grain, d.scaling_shift);
-            int minv = 0, maxv = bdmax;
-            if (d.clip_to_restricted_range) {
-                minv = 16 << b8;
-                maxv = (d.mc_identity ? 235 : 240) << b8;
-            }
-            Gc[o] = (P)iclip_(sv + noise, minv, maxv);
+            store_run<P, 4>(Gy + k * ys, ln, vec && ln >= 4, out);
         }
     }
 }
 
-template <typename P>
-__global__ void __launch_bounds__(256) grain_apply_kernel(const DevFrame f, const GrainParams gp, const int16_t *lut,
+template <typename P, int BS>
+__global__ void __launch_bounds__(256, 4) grain_apply_kernel(const DevFrame f, const GrainParams gp, const int16_t *lut,
                                                           const uint8_t *scaling) {
-    __shared__ int off[2][2][2];  // [cur/prev block][seed i][n]
-    grain_block<P>(f, gp, lut, scaling, blockIdx.y, blockIdx.x, off);
+    __shared__ SegOffsets<BS> so;
+    grain_segment<P, BS>(f, gp, lut, scaling, blockIdx.y, blockIdx.x, so);
+}
+
+template <typename P>
+void launch_grain_apply(const DevFrame &d, const GrainParams &gp, const int16_t *lut, const uint8_t *scaling,
+                        cudaStream_t s) {
+    const int bs = 16 << gp.d.block_size;
+    const dim3 grid((d.w + SEG_W - 1) / SEG_W, (d.h + bs - 1) / bs);
+    if (bs == 32)
+        r2g_launch_pdl(grain_apply_kernel<P, 32>, grid, dim3(256), s, d, gp, lut, scaling);
+    else
+        r2g_launch_pdl(grain_apply_kernel<P, 16>, grid, dim3(256), s, d, gp, lut, scaling);
 }
 
 // Persistent kernels of the batched path: one template set per grained
@@ -385,23 +497,34 @@ __global__ void __launch_bounds__(256) grain_template_batch_kernel(BatchArgs a) 
     }
 }
 
-__global__ void __launch_bounds__(256) grain_apply_batch_kernel(BatchArgs a) {
-    __shared__ int off[2][2][2];
+__global__ void __launch_bounds__(256, 3) grain_apply_batch_kernel(BatchArgs a) {
+    __shared__ union {
+        SegOffsets<32> s32;
+        SegOffsets<16> s16;
+    } so;
     const int n = a.count[3];
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
         const uint32_t it = a.work[3][w];
         const GrainBatch &g = a.grain[it >> 22];
         const DevFrame &f = a.frames[g.frame];
-        const int b = it & 0x3fffff, bs = 16 << g.gp.d.block_size, bw = (f.w + bs - 1) / bs;
-        if (f.bitdepth > 8)
-            grain_block<uint16_t>(f, g.gp, g.lut, g.scaling, b / bw, b % bw, off);
-        else
-            grain_block<uint8_t>(f, g.gp, g.lut, g.scaling, b / bw, b % bw, off);
+        const int b = it & 0x3fffff, sw = (f.w + SEG_W - 1) / SEG_W;
+        const bool hbd = f.bitdepth > 8;
+        if (g.gp.d.block_size) {
+            if (hbd)
+                grain_segment<uint16_t, 32>(f, g.gp, g.lut, g.scaling, b / sw, b % sw, so.s32);
+            else
+                grain_segment<uint8_t, 32>(f, g.gp, g.lut, g.scaling, b / sw, b % sw, so.s32);
+        } else {
+            if (hbd)
+                grain_segment<uint16_t, 16>(f, g.gp, g.lut, g.scaling, b / sw, b % sw, so.s16);
+            else
+                grain_segment<uint8_t, 16>(f, g.gp, g.lut, g.scaling, b / sw, b % sw, so.s16);
+        }
         __syncthreads();
     }
 }
 
-bool g_pow_ready[64] = {false};
+bool g_lfsr_ready[64] = {false};
 
 }  // namespace
 
@@ -436,21 +559,30 @@ void r2g_grain_ctx_free(R2gCtx *ctx) {
     ctx->grain = nullptr;
 }
 
-// Columns of M^(2^j) for the LFSR of filmgrain.rs:11, derived by stepping
-// each basis vector.
+// The LFSR cycle and its inverse (see g_lfsr_cycle), for the current device.
 static cudaError_t init_lfsr_pow(int device) {
-    if (device >= 0 && device < 64 && g_pow_ready[device]) return cudaSuccess;
-    uint16_t pw[14][16];
-    for (int i = 0; i < 16; i++) pw[0][i] = (uint16_t)lfsr_step(1u << i);
-    for (int j = 1; j < 14; j++)
-        for (int i = 0; i < 16; i++) {
-            uint32_t v = pw[j - 1][i], o = 0;
-            for (int k = 0; k < 16; k++)
-                if ((v >> k) & 1) o ^= pw[j - 1][k];
-            pw[j][i] = (uint16_t)o;
+    if (device >= 0 && device < 64 && g_lfsr_ready[device]) return cudaSuccess;
+    static uint16_t cyc[65536], pos[65536];
+    static bool built = false;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!built) {
+            uint32_t st = 1;
+            pos[0] = 0;
+            for (uint32_t i = 0; i < 65535u; i++) {
+                cyc[i] = (uint16_t)st;
+                pos[st] = (uint16_t)i;
+                st = lfsr_step(st);
+            }
+            cyc[65535] = 1;
+            if (st != 1) return cudaErrorInvalidValue;  // not one cycle: refuse
+            built = true;
         }
-    cudaError_t e = cudaMemcpyToSymbol(c_lfsr_pow, pw, sizeof(pw));
-    if (e == cudaSuccess && device >= 0 && device < 64) g_pow_ready[device] = true;
+    }
+    cudaError_t e = cudaMemcpyToSymbol(g_lfsr_cycle, cyc, sizeof(cyc));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_lfsr_pos, pos, sizeof(pos));
+    if (e == cudaSuccess && device >= 0 && device < 64) g_lfsr_ready[device] = true;
     return e;
 }
 
@@ -468,9 +600,15 @@ void r2g_grain_params(const R2gFilmGrainData &fgd, uint32_t seed, int bitdepth, 
     g.gp.d = fgd;
     g.gp.seed = seed;
     g.gp.bitdepth = bitdepth;
+    g.gp.vec = 1;
     bool any;
     grain_planes(fgd, g.gp.has_y, g.gp.has_u, g.gp.has_v, any);
     g.any = any;
+}
+
+int r2g_grain_items(int width, int height, int block_size) {
+    const int bs = 16 << block_size;
+    return ((width + SEG_W - 1) / SEG_W) * ((height + bs - 1) / bs);
 }
 
 int r2g_grain_ready(int device) { return init_lfsr_pow(device) == cudaSuccess ? R2G_OK : R2G_E_DEVICE; }
@@ -490,6 +628,7 @@ int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uin
     gp.d = *fgd;
     gp.seed = seed;
     gp.bitdepth = f->bd;
+    gp.vec = 1;  // frames of this library: aligned planes and strides
     bool any;
     grain_planes(*fgd, gp.has_y, gp.has_u, gp.has_v, any);
     DevFrame d = f->desc;
@@ -509,13 +648,13 @@ int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uin
         if (cudaEventRecord(ctx->grain->ready, ctx->side_stream) != cudaSuccess) return R2G_E_DEVICE;
         if (cudaStreamWaitEvent(ctx->stream, ctx->grain->ready, 0) != cudaSuccess) return R2G_E_DEVICE;
     }
-    int bs = 16 << fgd->block_size;
-    dim3 grid((f->w + bs - 1) / bs, (f->h + bs - 1) / bs);
     r2g_prof_stage(ctx, 3, true, 0);
+    // programmatic dependent launch: the block offsets are drawn while the
+    // previous kernel of the frame drains
     if (f->bd > 8)
-        grain_apply_kernel<uint16_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
+        launch_grain_apply<uint16_t>(d, gp, ctx->grain->lut, ctx->grain->scaling, ctx->stream);
     else
-        grain_apply_kernel<uint8_t><<<grid, 256, 0, ctx->stream>>>(d, gp, ctx->grain->lut, ctx->grain->scaling);
+        launch_grain_apply<uint8_t>(d, gp, ctx->grain->lut, ctx->grain->scaling, ctx->stream);
     r2g_prof_stage(ctx, 3, false, 1 + (any ? 1 : 0));
     if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
     if (cudaEventRecord(ctx->grain->freed, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
@@ -563,7 +702,6 @@ extern "C" int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData 
 // * The array holds scaling LUTs of at most 1024 entries, i.e. bit depths up
 //   to 10; larger bit depths are rejected with R2G_E_TOO_LARGE.
 
-#include <mutex>
 
 #define R2G_NOALLOC_LUT_BYTES (3 * GH * GW * 2)
 #define R2G_NOALLOC_SCALING_BYTES (3 * 1024)
@@ -619,6 +757,11 @@ extern "C" int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u
     gp.d = *fgd;
     gp.seed = seed;
     gp.bitdepth = bitdepth;
+    // runs of samples move as one vector access when every plane and stride
+    // is 16-byte aligned; otherwise sample by sample
+    const void *planes[6] = {src_y, src_u, src_v, dst_y, dst_u, dst_v};
+    gp.vec = (y_stride % 16) == 0 && (uv_stride % 16) == 0;
+    for (const void *pl : planes) gp.vec = gp.vec && ((uintptr_t)pl % 16) == 0;
     bool any;
     grain_planes(*fgd, gp.has_y, gp.has_u, gp.has_v, any);
     DevFrame d;
@@ -638,12 +781,10 @@ extern "C" int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u
     d.G[1] = dst_u;
     d.G[2] = dst_v;
     if (any) grain_template_kernel<<<1, 256, 0, s>>>(gp, nd.tab, lut, scaling);
-    int bs = 16 << fgd->block_size;
-    dim3 grid((width + bs - 1) / bs, (height + bs - 1) / bs);
     if (bitdepth > 8)
-        grain_apply_kernel<uint16_t><<<grid, 256, 0, s>>>(d, gp, lut, scaling);
+        launch_grain_apply<uint16_t>(d, gp, lut, scaling, s);
     else
-        grain_apply_kernel<uint8_t><<<grid, 256, 0, s>>>(d, gp, lut, scaling);
+        launch_grain_apply<uint8_t>(d, gp, lut, scaling, s);
     return cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
 }
 

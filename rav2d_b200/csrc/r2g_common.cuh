@@ -94,6 +94,9 @@ struct GrainParams {
     uint32_t seed;
     int bitdepth;
     int has_y, has_u, has_v;
+    // planes 16-byte aligned with 16-byte multiple strides: runs of samples
+    // move with one vector access each
+    int vec;
 };
 // One grained frame of a batch: its parameters, its frame index in the
 // batch and its template / scaling-LUT scratch.
@@ -115,6 +118,8 @@ void r2g_batch_launch_grain_apply(const BatchArgs &a, int grid, cudaStream_t s);
 int r2g_batch_occupancy_grain_apply();
 // Sets the grain fields of a GrainBatch from the frame's parameters.
 void r2g_grain_params(const R2gFilmGrainData &fgd, uint32_t seed, int bitdepth, GrainBatch &g);
+// Work items (band segments of 256 luma columns) of a grained frame.
+int r2g_grain_items(int width, int height, int block_size);
 void r2g_batch_launch_deblock(const BatchArgs &a, int grid, cudaStream_t s);
 void r2g_batch_launch_cdef(const BatchArgs &a, int grid, cudaStream_t s);
 void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s);

@@ -69,6 +69,52 @@ def test_noalloc_grain_matches_frame_grain():
         ctx.close()
 
 
+def test_noalloc_unaligned_planes():
+    """Planes that start off a 16-byte boundary, with strides that are not
+    multiples of 16 bytes, take the sample-by-sample path of the apply kernel;
+    it must agree with the regular entry point (aligned, vector path)."""
+    import torch
+
+    from rav2d_b200 import gpu
+
+    lib = gpu.lib()
+    lib.r2g_film_grain_apply_noalloc.restype = C.c_int
+    ctx = gpu.Context(0)
+    stream = torch.cuda.Stream()
+    try:
+        for sf in (synth.make_frame(328, 136, 8, 0x5EED00A3, chain="db", grain=True),
+                   synth.make_frame(200, 72, 10, 0x5EED00A4, chain="db", grain=True)):
+            filtered, want = gpu.filter_frame(ctx, sf, grain=True)
+            bps = 2 if sf.bitdepth > 8 else 1
+            dt = torch.int16 if bps == 2 else torch.uint8
+            pad, lead = 3, 1  # samples: 3 past each row, 1 before the plane
+            src, dst, strides = [], [], []
+            for pl, p in enumerate(filtered):
+                h, w = sf.height >> (pl > 0), sf.width >> (pl > 0)
+                s = w + pad
+                buf = torch.zeros(lead + h * s, dtype=dt, device="cuda")
+                rows = torch.from_numpy(np.ascontiguousarray(p[:h, :w]).view(np.int16) if bps == 2 else
+                                        np.ascontiguousarray(p[:h, :w])).to(dtype=dt).cuda()
+                buf[lead:].view(h, s)[:, :w] = rows
+                src.append(buf)
+                dst.append(torch.zeros_like(buf))
+                strides.append(s * bps)
+            ptr = [C.c_void_p(t.data_ptr() + lead * bps) for t in src + dst]
+            rc = lib.r2g_film_grain_apply_noalloc(*ptr, C.c_int64(strides[0]), C.c_int64(strides[1]), sf.width,
+                                                  sf.height, sf.bitdepth, C.byref(sf.fgd), C.c_uint32(sf.grain_seed),
+                                                  C.c_void_p(stream.cuda_stream))
+            assert rc == 0
+            torch.cuda.synchronize()
+            for pl in range(3):
+                h, w = sf.height >> (pl > 0), sf.width >> (pl > 0)
+                got = dst[pl][lead:].view(h, strides[pl] // bps)[:, :w].cpu().numpy()
+                if bps == 2:
+                    got = got.view(np.uint16)
+                assert np.array_equal(got, want[pl][:h, :w]), f"plane {pl} differs"
+    finally:
+        ctx.close()
+
+
 def test_noalloc_rejects_oversized_bitdepth():
     from rav2d_b200 import abi, gpu
 
