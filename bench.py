@@ -249,7 +249,7 @@ def run_ours(args, rank, world, device):
     for fr in frames:
         fr.free()
     batch = run_batched(args, ctx, stream, device) if args.batch_steps > 0 else None
-    uhd = run_4k_grain(args, ctx, stream, device) if args.batch_steps > 0 else None
+    uhd = run_4k_grain(args, ctx, stream, device) if args.grain_steps > 0 else None
     ctx.close()
     return {
         "batched": batch, "per_frame_4k_grain": uhd,
@@ -307,7 +307,7 @@ def run_4k_grain(args, ctx, stream, device):
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
-    n = max(3, min(args.steps, 300))
+    n = args.grain_steps
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for i in range(n):
@@ -540,6 +540,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-steps", type=int, default=30, help="timed batches of the 64-frame mix (0 = skip)")
+    ap.add_argument("--grain-steps", type=int, default=300,
+                    help="timed frames of the per-frame 4K 10-bit + film grain block (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="measured serving window (0 = skip)")
     ap.add_argument("--ref-seconds", type=float, default=120.0, help="target duration of --impl reference")
     args = ap.parse_args()
