@@ -7,12 +7,13 @@
 // decode.rs:4641-4775.
 //
 // The reference's serial parts are re-scheduled, not approximated:
-// * the 16-bit LFSR is linear over GF(2), so the state after k steps is
-//   M^k * s; the host derives M from the LFSR taps and tabulates M^(2^j), and
-//   each thread jumps straight to its first draw;
+// * the 16-bit LFSR is maximal-length, so every nonzero state lies on one
+//   cycle of 65535 states; the host tabulates the cycle and each state's
+//   position on it, and a thread jumps k steps with two look-ups;
 // * the auto-regressive filter reads rows y-lag..y-1 at x-lag..x+lag and row
 //   y at x-lag..x-1, so every sample on the line x + 4y = t depends only on
-//   lines < t: the template is filled as a wavefront over t;
+//   lines < t: the template is filled as a wavefront over t, one warp per
+//   plane;
 // * block offsets of row band r and block b are draws 8b + 4n + 1 of the
 //   band's seed, evaluated directly by jump-ahead in the apply kernel.
 #include <cstring>
@@ -54,68 +55,189 @@ R2G_D int round2(int x, int shift) { return (x + ((1 << shift) >> 1)) >> shift; 
 struct GrainTplSmem {
     int16_t ly[GH][GW];
     int16_t lc[2][SGH][SGW];
+    uint32_t sc[3 * 1024 / 4];  // scaling LUTs, built here (zero-initialised) and copied out
 };
 
-// The auto-regressive filters of generate_grain_y (filmgrain.rs:134-157) and
-// generate_grain_uv (:183-228), specialised on the lag: cell (y, x) reads
-// rows y - LAG .. y - 1 over x - LAG .. x + LAG and row y over x - LAG ..
-// x - 1, so the cells with equal x + 4y (LAG <= 3) only read earlier fronts
-// and one front is computed per step.  The coefficients sit in registers and
-// every tap is an unrolled, independent shared-memory read.
+// Barrier of warps 0-2, which run the auto-regressive filters; warps 6-7
+// build the scaling LUTs meanwhile.
+R2G_D void ar_sync() { asm volatile("bar.sync 1, 96;\n" ::: "memory"); }
+
+// One front of the auto-regressive filter of generate_grain_y
+// (filmgrain.rs:134-157) or generate_grain_uv (:183-228), lag >= 1, for the
+// calling lane.  Cell (y, x) reads rows y - LAG .. y - 1 over x - LAG .. x +
+// LAG and row y over x - LAG .. x - 1, so the cells with equal x + 4y (a
+// front) depend only on earlier fronts.  Lane l owns rows 3 + l + 32k; a
+// row is active for 78 fronts and rows 32 apart are 128 fronts apart, so a
+// lane has at most one active cell per front and one set of registers: the
+// windows of the rows above (win) and its own last outputs (own).  At x == 2
+// the lane loads the windows of column 3; at each cell it loads one new value
+// (row y - 1, column x + LAG: the previous front's output of the lane
+// above), finishes the cell and slides the windows.
 template <int LAG>
-R2G_D void ar_fronts(const GrainParams &gp, GrainTplSmem &sm, bool gen_u, bool gen_v, int gmin, int gmax) {
-    constexpr int NTAP = 2 * LAG * (LAG + 1);
-    const R2gFilmGrainData &d = gp.d;
-    const int tid = threadIdx.x, ar_shift = (int)d.ar_coeff_shift;
-    // luma: one row per thread (73 rows); lag 0 only clips, cell by cell
-    if (LAG == 0) {
-        for (int i = tid; i < (GH - 3) * (GW - 6); i += blockDim.x) {
-            int16_t &g = sm.ly[3 + i / (GW - 6)][3 + i % (GW - 6)];
-            g = (int16_t)iclip_(g, gmin, gmax);
+R2G_D void ar_front(int16_t *base, int stride, int nrows, int xlim, int t, const int *cf, int (&win)[LAG][2 * LAG + 1],
+                    int (&own)[LAG], int &g0, int sh, int gmin, int gmax, const int16_t (*luma)[GW], int lcoef) {
+    constexpr int W = 2 * LAG + 1;
+    const int lane = threadIdx.x & 31;
+    const int rel = t - 14 - 4 * lane;  // column - 2 of row 3 + lane at front t
+    if (rel < 0) return;
+    const int k = rel >> 7;
+    const int y = 3 + lane + 32 * k, x = 2 + rel - 128 * k;
+    if (y >= nrows || x >= xlim) return;
+    if (x == 2) {
+#pragma unroll
+        for (int r = 0; r < LAG; r++)
+#pragma unroll
+            for (int j = 0; j < W; j++)
+                if (r < LAG - 1 || j < W - 1) win[r][j] = base[(y - LAG + r) * stride + 3 - LAG + j];
+#pragma unroll
+        for (int j = 0; j < LAG; j++) own[j] = base[y * stride + 3 - LAG + j];
+        g0 = base[y * stride + 3];
+        return;
+    }
+    const int v = base[(y - 1) * stride + x + LAG];
+    int acc0 = 0, acc1 = 0;
+#pragma unroll
+    for (int r = 0; r < LAG; r++)
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            if (r == LAG - 1 && j == W - 1) continue;
+            if ((r * W + j) & 1)
+                acc1 += cf[r * W + j] * win[r][j];
+            else
+                acc0 += cf[r * W + j] * win[r][j];
         }
-        __syncthreads();
-    } else {
-        int cy[NTAP > 0 ? NTAP : 1];
 #pragma unroll
-        for (int i = 0; i < NTAP; i++) cy[i] = d.ar_coeffs[0][i];
-        const int y = 3 + tid;
-        for (int t = 3 + 4 * 3; t <= (GW - 4) + 4 * (GH - 1); t++) {
-            const int x = t - 4 * y;
-            if (y < GH && x >= 3 && x < GW - 3) {
-                int sum = 0, ci = 0;
+    for (int j = 0; j < LAG; j++) acc1 += cf[LAG * W + j] * own[j];
+    int sum = acc0 + acc1 + cf[LAG * W - 1] * v;
+    if (luma) {
+        const int lx = ((x - 3) << 1) + 3, lyy = ((y - 3) << 1) + 3;
+        const int l4 = luma[lyy][lx] + luma[lyy][lx + 1] + luma[lyy + 1][lx] + luma[lyy + 1][lx + 1];
+        sum += ((l4 + 2) >> 2) * lcoef;
+    }
+    const int out = iclip_(g0 + ((sum + ((1 << sh) >> 1)) >> sh), gmin, gmax);
+    base[y * stride + x] = (int16_t)out;
+    if (x + 1 < xlim) {
 #pragma unroll
-                for (int dy = -LAG; dy <= 0; dy++)
+        for (int r = 0; r < LAG; r++) {
 #pragma unroll
-                    for (int dx = -LAG; dx <= LAG; dx++)
-                        if (dy < 0 || dx < 0) sum += cy[ci++] * sm.ly[y + dy][x + dx];
-                sm.ly[y][x] = (int16_t)iclip_(sm.ly[y][x] + round2(sum, ar_shift), gmin, gmax);
+            for (int j = 0; j < W - 1; j++) win[r][j] = win[r][j + 1];
+            if (r < LAG - 1) win[r][W - 1] = base[(y - LAG + r) * stride + x + 1 + LAG];
+        }
+        win[LAG - 1][W - 2] = v;
+#pragma unroll
+        for (int j = 0; j < LAG - 1; j++) own[j] = own[j + 1];
+        own[LAG - 1] = out;
+        g0 = base[y * stride + x + 1];
+    }
+}
+
+// The filters of both templates for lag >= 1: warp 0 luma (fronts 14 ..
+// 381, 8 per round), warp 1 chroma U and warp 2 chroma V (fronts 8 .. 191, 4
+// per round).  Fronts are ordered inside a warp by __syncwarp; a barrier of
+// the three warps ends each round.  Chroma front t reads luma fronts up to
+// 2t - 10 (its luma term); in round r chroma runs fronts 4r + 8 .. 4r + 11,
+// which read luma fronts up to 8r + 12, all finished in rounds before r.
+template <int LAG>
+R2G_D void ar_wave(const GrainParams &gp, GrainTplSmem &sm, bool gen_u, bool gen_v, int gmin, int gmax) {
+    constexpr int W = 2 * LAG + 1, NT = LAG * W + LAG;
+    const R2gFilmGrainData &d = gp.d;
+    const int warp = threadIdx.x >> 5, sh = (int)d.ar_coeff_shift;
+    const bool gen = warp == 0 || (warp == 1 ? gen_u : gen_v);
+    int16_t *base = warp == 0 ? &sm.ly[0][0] : &sm.lc[warp - 1][0][0];
+    const int stride = warp == 0 ? GW : SGW, nrows = warp == 0 ? GH : SGH;
+    const int16_t(*luma)[GW] = (warp > 0 && d.num_points[0] > 0) ? sm.ly : nullptr;
+    int cf[NT + 1];
+#pragma unroll
+    for (int i = 0; i <= NT; i++) cf[i] = d.ar_coeffs[warp][i];
+    int win[LAG][W], own[LAG], g0 = 0;
+#pragma unroll
+    for (int r = 0; r < LAG; r++)
+#pragma unroll
+        for (int j = 0; j < W; j++) win[r][j] = 0;
+#pragma unroll
+    for (int j = 0; j < LAG; j++) own[j] = 0;
+    for (int round = 0; round < 46; round++) {
+        if (warp == 0) {
+            for (int i = 0; i < 8; i++) {
+                ar_front<LAG>(base, stride, nrows, GW - 3, 14 + 8 * round + i, cf, win, own, g0, sh, gmin, gmax,
+                              nullptr, 0);
+                __syncwarp();
             }
-            __syncthreads();
+        } else if (gen) {
+            for (int i = 0; i < 4; i++) {
+                ar_front<LAG>(base, stride, nrows, SGW - 3, 4 * round + 8 + i, cf, win, own, g0, sh, gmin, gmax, luma,
+                              cf[NT]);
+                __syncwarp();
+            }
+        }
+        ar_sync();
+    }
+}
+
+// Lag 0: no neighbour taps.  Luma cells are only clipped; a chroma cell adds
+// the luma term, which reads the finished luma template.
+R2G_D void ar_lag0(const GrainParams &gp, GrainTplSmem &sm, bool gen_u, bool gen_v, int gmin, int gmax) {
+    const R2gFilmGrainData &d = gp.d;
+    const int tid = threadIdx.x, sh = (int)d.ar_coeff_shift, rnd = (1 << sh) >> 1;
+    for (int i = tid; i < (GH - 3) * (GW - 6); i += 96) {
+        int16_t &g = sm.ly[3 + i / (GW - 6)][3 + i % (GW - 6)];
+        g = (int16_t)iclip_(g, gmin, gmax);
+    }
+    ar_sync();
+    const bool with_luma = d.num_points[0] > 0;
+    for (int i = tid; i < 2 * (SGH - 3) * (SGW - 6); i += 96) {
+        const int uv = i / ((SGH - 3) * (SGW - 6)), j = i % ((SGH - 3) * (SGW - 6));
+        if (!(uv ? gen_v : gen_u)) continue;
+        const int y = 3 + j / (SGW - 6), x = 3 + j % (SGW - 6);
+        int sum = 0;
+        if (with_luma) {
+            const int lx = ((x - 3) << 1) + 3, lyy = ((y - 3) << 1) + 3;
+            const int l4 = sm.ly[lyy][lx] + sm.ly[lyy][lx + 1] + sm.ly[lyy + 1][lx] + sm.ly[lyy + 1][lx + 1];
+            sum = ((l4 + 2) >> 2) * d.ar_coeffs[1 + uv][0];
+        }
+        sm.lc[uv][y][x] = (int16_t)iclip_(sm.lc[uv][y][x] + ((sum + rnd) >> sh), gmin, gmax);
+    }
+}
+
+// Scaling LUT of one plane (generate_scaling_8bpc / _hbd, filmgrain.rs:
+// 22-113) into a zeroed shared-memory LUT: the interpolation pass reads back
+// what the first pass wrote, which in shared memory costs a few cycles.
+R2G_D void scaling_lut(const GrainParams &gp, int pl, uint8_t *scaling) {
+    const R2gFilmGrainData &d = gp.d;
+    uint8_t *sc = scaling + pl * 1024;
+    const int size = 1 << gp.bitdepth, sx = gp.bitdepth - 8;
+    const int num = d.num_points[pl];
+    const bool wanted = pl == 0 || !d.chroma_scaling_from_luma;
+    if (!wanted || num == 0) {
+        for (int i = 0; i < size; i++) sc[i] = 0;
+        return;
+    }
+    const uint8_t(*pts)[2] = d.points[pl];
+    for (int i = 0; i < (pts[0][0] << sx); i++) sc[i] = pts[0][1];
+    for (int i = 0; i < num - 1; i++) {
+        int bx = pts[i][0], by = pts[i][1], ex = pts[i + 1][0], ey = pts[i + 1][1];
+        int dx = ex - bx, dyv = ey - by;
+        if (dx <= 0) continue;
+        int delta = dyv * ((0x10000 + (dx >> 1)) / dx);
+        int dd = 0x8000;
+        for (int x = 0; x < dx; x++) {
+            sc[(bx + x) << sx] = (uint8_t)(by + (dd >> 16));
+            dd += delta;
         }
     }
-    // chroma: threads 0..127 plane U, 128..255 plane V, one row each
-    const int uv = tid >> 7, y = 3 + (tid & 127);
-    int cc[NTAP + 1];
-#pragma unroll
-    for (int i = 0; i <= NTAP; i++) cc[i] = d.ar_coeffs[1 + uv][i];
-    const bool gen = uv ? gen_v : gen_u, with_luma = d.num_points[0] > 0;
-    for (int t = 3 + 4 * 3; t <= (SGW - 4) + 4 * (SGH - 1); t++) {
-        const int x = t - 4 * y;
-        if (gen && y < SGH && x >= 3 && x < SGW - 3) {
-            int sum = 0, ci = 0;
-#pragma unroll
-            for (int dy = -LAG; dy <= 0; dy++)
-#pragma unroll
-                for (int dx = -LAG; dx <= LAG; dx++)
-                    if (dy < 0 || dx < 0) sum += cc[ci++] * sm.lc[uv][y + dy][x + dx];
-            if (with_luma) {
-                const int lx = ((x - 3) << 1) + 3, lyy = ((y - 3) << 1) + 3;
-                const int luma = sm.ly[lyy][lx] + sm.ly[lyy][lx + 1] + sm.ly[lyy + 1][lx] + sm.ly[lyy + 1][lx + 1];
-                sum += round2(luma, 2) * cc[NTAP];
+    for (int i = pts[num - 1][0] << sx; i < size; i++) sc[i] = pts[num - 1][1];
+    if (sx > 0) {
+        int pad = 1 << sx, rnd = pad >> 1;
+        for (int i = 0; i < num - 1; i++) {
+            int bx = pts[i][0] << sx, ex = pts[i + 1][0] << sx;
+            for (int x = 0; x < ex - bx; x += pad) {
+                int b0 = sc[bx + x], range = sc[bx + x + pad] - b0, r = rnd;
+                for (int n2 = 1; n2 < pad; n2++) {
+                    r += range;
+                    sc[bx + x + n2] = (uint8_t)(b0 + (r >> sx));
+                }
             }
-            sm.lc[uv][y][x] = (int16_t)iclip_(sm.lc[uv][y][x] + round2(sum, ar_shift), gmin, gmax);
         }
-        __syncthreads();
     }
 }
 
@@ -156,58 +278,26 @@ R2G_D void grain_template(const GrainParams &gp, const DevTables &tab, int16_t *
             }
         }
     }
+    for (int i = tid; i < 3 * 1024 / 4; i += 256) sm.sc[i] = 0;
     __syncthreads();
-    switch (d.ar_coeff_lag) {
-        case 0: ar_fronts<0>(gp, sm, gen_u, gen_v, gmin, gmax); break;
-        case 1: ar_fronts<1>(gp, sm, gen_u, gen_v, gmin, gmax); break;
-        case 2: ar_fronts<2>(gp, sm, gen_u, gen_v, gmin, gmax); break;
-        default: ar_fronts<3>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+    if (tid < 96) {
+        switch (d.ar_coeff_lag) {
+            case 0: ar_lag0(gp, sm, gen_u, gen_v, gmin, gmax); break;
+            case 1: ar_wave<1>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+            case 2: ar_wave<2>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+            default: ar_wave<3>(gp, sm, gen_u, gen_v, gmin, gmax); break;
+        }
+    } else if (tid >= 192 && tid < 195) {
+        scaling_lut(gp, tid - 192, reinterpret_cast<uint8_t *>(sm.sc));
     }
+    __syncthreads();
+    for (int i = tid; i < 3 * 1024 / 4; i += 256) reinterpret_cast<uint32_t *>(scaling)[i] = sm.sc[i];
     // write templates (zero where a plane's template is not generated)
     for (int i = tid; i < GH * GW; i += 256) {
         int y = i / GW, x = i % GW;
         lut[i] = ly[y][x];
         lut[GH * GW + i] = (gen_u && y < SGH && x < SGW) ? lc[0][y][x] : 0;
         lut[2 * GH * GW + i] = (gen_v && y < SGH && x < SGW) ? lc[1][y][x] : 0;
-    }
-    // scaling LUTs (generate_scaling_8bpc / _hbd), one thread per plane
-    if (tid < 3) {
-        int pl = tid;
-        uint8_t *sc = scaling + pl * 1024;
-        int size = 1 << gp.bitdepth, sx = b8;
-        int num = d.num_points[pl];
-        bool wanted = pl == 0 || !d.chroma_scaling_from_luma;
-        if (!wanted || num == 0) {
-            for (int i = 0; i < size; i++) sc[i] = 0;
-        } else {
-            const uint8_t(*pts)[2] = d.points[pl];
-            for (int i = 0; i < (pts[0][0] << sx); i++) sc[i] = pts[0][1];
-            for (int i = 0; i < num - 1; i++) {
-                int bx = pts[i][0], by = pts[i][1], ex = pts[i + 1][0], ey = pts[i + 1][1];
-                int dx = ex - bx, dyv = ey - by;
-                if (dx <= 0) continue;
-                int delta = dyv * ((0x10000 + (dx >> 1)) / dx);
-                int dd = 0x8000;
-                for (int x = 0; x < dx; x++) {
-                    sc[(bx + x) << sx] = (uint8_t)(by + (dd >> 16));
-                    dd += delta;
-                }
-            }
-            for (int i = pts[num - 1][0] << sx; i < size; i++) sc[i] = pts[num - 1][1];
-            if (sx > 0) {
-                int pad = 1 << sx, rnd = pad >> 1;
-                for (int i = 0; i < num - 1; i++) {
-                    int bx = pts[i][0] << sx, ex = pts[i + 1][0] << sx;
-                    for (int x = 0; x < ex - bx; x += pad) {
-                        int base = sc[bx + x], range = sc[bx + x + pad] - base, r = rnd;
-                        for (int n2 = 1; n2 < pad; n2++) {
-                            r += range;
-                            sc[bx + x + n2] = (uint8_t)(base + (r >> sx));
-                        }
-                    }
-                }
-            }
-        }
     }
 }
 
