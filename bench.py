@@ -364,6 +364,7 @@ def run_batched(args, ctx, stream, device):
     pf_ms, pf_l = timed(per_frame, reps)
     b_ms, b_l = timed(batched, reps)
     sms, cfg = ctx.batch_config()
+    tile_rows = ctx.batch_tile_rows()
     for fr in frames:
         fr.free()
     mix = {}
@@ -378,7 +379,7 @@ def run_batched(args, ctx, stream, device):
         "launches_per_batch": b_l,
         "per_frame_value": round(mpix / pf_ms * 1e3, 2), "per_frame_ms": round(pf_ms, 4),
         "per_frame_launches": pf_l,
-        "speedup_vs_per_frame": round(pf_ms / b_ms, 3), "ctas_per_sm": cfg, "sms": sms,
+        "speedup_vs_per_frame": round(pf_ms / b_ms, 3), "ctas_per_sm": cfg, "tile_rows": tile_rows, "sms": sms,
         "l2": f"inputs larger than L2: {round(mpix * 1.5 * 1.5, 0)} MB of recon per batch",
     }
 

@@ -419,6 +419,12 @@ int r2g_server_destroy(R2gServer *s);
  * work item; returns the SM count. */
 int r2g_batch_config(R2gCtx *ctx, int32_t *ctas_per_sm, int n);
 
+/* Instrumentation (no counterpart in the reference): the tile shape the last
+ * batch used per stage, as luma rows per work item (deblock 64, CDEF+CCSO 32,
+ * loop restoration 32 or 16 as autotuned, film grain the grain block size or
+ * 0 without grain); returns the number of stages written. */
+int r2g_batch_tile_rows(R2gCtx *ctx, int32_t *rows, int n);
+
 /* ---- film grain without any device allocation ----
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * a decoder embedded in a framework whose device memory is owned by that

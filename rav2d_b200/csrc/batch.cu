@@ -12,12 +12,14 @@
 // instantiated graph serves every batch that fits the slot's capacity.  Two
 // slots alternate, so the host can stage batch k+1 while batch k runs.
 //
-// The grid of each persistent kernel (CTAs per SM) is chosen by a small
+// The grid of each persistent kernel (CTAs per SM, or one CTA per work
+// item) and the tile shape of the stages that have a choice (loop
+// restoration: 32 or 16 luma rows per work item) are chosen by a small
 // autotuner: on the first batch of a given bit-depth mix it times every
-// occupancy-legal choice per stage and keeps the fastest; the choice is
-// cached per device in a text file ($R2G_TUNE_CACHE, default
-// $HOME/.cache/rav2d_b200/autotune-v2.txt).  R2G_AUTOTUNE=0 skips tuning and
-// uses the occupancy limit.
+// (shape, grid) pair per stage and keeps the fastest; the choice is cached
+// per device in a text file ($R2G_TUNE_CACHE, default
+// $HOME/.cache/rav2d_b200/autotune-v3.txt).  R2G_AUTOTUNE=0 skips tuning and
+// uses the occupancy limit and the default shapes.
 #include <sys/stat.h>
 
 #include <cstdio>
@@ -82,7 +84,9 @@ struct BatchState {
     int num_sms = 0;
     int occ[N_BSTAGES] = {0, 0, 0, 0};
     int tuned[3][N_BSTAGES] = {{0}};  // [8-bit, 10-bit, mixed][stage] CTAs per SM
+    int shape[3][N_BSTAGES] = {{0}};  // tile shape (luma rows per work item; 0: the stage's fixed shape)
     int last[N_BSTAGES] = {0, 0, 0, 0};
+    int last_rows[N_BSTAGES] = {0, 0, 0, 0};  // luma rows per work item of the last batch
     bool cache_loaded = false;
     std::string dev_name;
     cudaEvent_t fork = nullptr, join = nullptr, copied = nullptr, t0 = nullptr, t1 = nullptr;
@@ -92,7 +96,7 @@ static std::string cache_path() {
     const char *p = getenv("R2G_TUNE_CACHE");
     if (p && *p) return p;
     const char *h = getenv("HOME");
-    return std::string(h ? h : "/tmp") + "/.cache/rav2d_b200/autotune-v2.txt";
+    return std::string(h ? h : "/tmp") + "/.cache/rav2d_b200/autotune-v3.txt";
 }
 
 static void load_cache(BatchState &b) {
@@ -102,10 +106,13 @@ static void load_cache(BatchState &b) {
     char line[512];
     while (fgets(line, sizeof(line), fp)) {
         char name[256];
-        int cls, k, v;
-        if (sscanf(line, "%255[^|]|%d|%d|%d", name, &cls, &k, &v) == 4 && b.dev_name == name && cls >= 0 &&
-            cls < 3 && k >= 0 && k < N_BSTAGES && v > 0 && (v <= b.occ[k] || v == PER_ITEM))
+        int cls, k, v, shape;
+        if (sscanf(line, "%255[^|]|%d|%d|%d|%d", name, &cls, &k, &v, &shape) == 5 && b.dev_name == name &&
+            cls >= 0 && cls < 3 && k >= 0 && k < N_BSTAGES && v > 0 && (v <= b.occ[k] || v == PER_ITEM) &&
+            (shape == 0 || (k == 2 && (shape == 16 || shape == 32)))) {
             b.tuned[cls][k] = v;
+            b.shape[cls][k] = shape;
+        }
     }
     fclose(fp);
 }
@@ -119,7 +126,8 @@ static void save_cache(const BatchState &b, int cls) {
     FILE *fp = fopen(path.c_str(), "a");
     if (!fp) return;
     for (int k = 0; k < N_BSTAGES; k++)
-        if (b.tuned[cls][k] > 0) fprintf(fp, "%s|%d|%d|%d\n", b.dev_name.c_str(), cls, k, b.tuned[cls][k]);
+        if (b.tuned[cls][k] > 0)
+            fprintf(fp, "%s|%d|%d|%d|%d\n", b.dev_name.c_str(), cls, k, b.tuned[cls][k], b.shape[cls][k]);
     fclose(fp);
 }
 
@@ -179,9 +187,37 @@ static int ensure_state(R2gCtx *ctx) {
     return R2G_OK;
 }
 
-// Times every legal grid of each stage on the staged batch (stage outputs
-// are pure functions of their inputs, so re-running a stage is harmless).
-static int autotune(R2gCtx *ctx, BatchState &b, const Slot &s, const int *counts, int cls) {
+// Loop-restoration tile shapes the autotuner tries (luma rows per item).
+constexpr int LR_SHAPES[2] = {32, 16};
+
+// Sets every frame's loop-restoration item height to `rows` and rewrites the
+// LR work list and its count in the slot's host blob; returns the count.
+static int stage_lr_shape(Slot &s, std::vector<DevFrame> &frames, int rows, int *counts) {
+    const int n = (int)frames.size();
+    DevFrame *hf = (DevFrame *)(s.host + s.L.off_frames);
+    uint32_t *w2 = (uint32_t *)(s.host + s.L.off_work[2]);
+    int c2 = 0;
+    for (int i = 0; i < n; i++) {
+        frames[i].lr_rows = rows;
+        hf[i].lr_rows = rows;
+        for (int j = 0, e = r2g_lr_items(frames[i]); j < e; j++) w2[c2++] = ((uint32_t)i << 22) | j;
+    }
+    counts[2] = c2;
+    memcpy(s.host, counts, sizeof(int) * 8);
+    return c2;
+}
+
+// Copies the used part of the slot's host blob to the device.
+static int copy_blob(R2gCtx *ctx, const Slot &s, const int *counts) {
+    size_t used = s.L.off_work[N_BSTAGES - 1] + sizeof(uint32_t) * counts[3];
+    return cudaMemcpyAsync(s.dev, s.host, used, cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess ? R2G_OK
+                                                                                                     : R2G_E_DEVICE;
+}
+
+// Times every legal (shape, grid) pair of each stage on the staged batch
+// (stage outputs are pure functions of their inputs, so re-running a stage
+// is harmless).  Leaves the blob staged with the chosen LR shape.
+static int autotune(R2gCtx *ctx, BatchState &b, Slot &s, std::vector<DevFrame> &frames, int *counts, int cls) {
     const char *env = getenv("R2G_AUTOTUNE");
     bool enabled = !(env && env[0] == '0');
     BatchArgs a = args_of(s);
@@ -196,24 +232,38 @@ static int autotune(R2gCtx *ctx, BatchState &b, const Slot &s, const int *counts
         if (k == 3 && counts[4] > 0)
             r2g_batch_launch_grain_template(a, counts[4] < b.num_sms ? counts[4] : b.num_sms, ctx->stream);
         float best = 1e30f;
-        int best_v = b.occ[k];
-        for (int v = 1; v <= b.occ[k] + 1; v++) {
-            const int vv = v <= b.occ[k] ? v : PER_ITEM;
-            const int grid = vv == PER_ITEM ? counts[k] : v * b.num_sms;
-            launch_stage(k, a, grid, ctx->stream);  // warm
-            cudaEventRecord(b.t0, ctx->stream);
-            launch_stage(k, a, grid, ctx->stream);
-            launch_stage(k, a, grid, ctx->stream);
-            cudaEventRecord(b.t1, ctx->stream);
-            if (cudaEventSynchronize(b.t1) != cudaSuccess) return R2G_E_DEVICE;
-            float ms = 0;
-            cudaEventElapsedTime(&ms, b.t0, b.t1);
-            if (ms < best) {
-                best = ms;
-                best_v = vv;
+        int best_v = b.occ[k], best_shape = 0;
+        const int nshapes = k == 2 ? 2 : 1;
+        for (int si = 0; si < nshapes; si++) {
+            const int shape = k == 2 ? LR_SHAPES[si] : 0;
+            if (k == 2) {
+                stage_lr_shape(s, frames, shape, counts);
+                if (copy_blob(ctx, s, counts) != R2G_OK) return R2G_E_DEVICE;
+            }
+            for (int v = 1; v <= b.occ[k] + 1; v++) {
+                const int vv = v <= b.occ[k] ? v : PER_ITEM;
+                const int grid = vv == PER_ITEM ? counts[k] : v * b.num_sms;
+                launch_stage(k, a, grid, ctx->stream);  // warm
+                cudaEventRecord(b.t0, ctx->stream);
+                launch_stage(k, a, grid, ctx->stream);
+                launch_stage(k, a, grid, ctx->stream);
+                cudaEventRecord(b.t1, ctx->stream);
+                if (cudaEventSynchronize(b.t1) != cudaSuccess) return R2G_E_DEVICE;
+                float ms = 0;
+                cudaEventElapsedTime(&ms, b.t0, b.t1);
+                if (ms < best) {
+                    best = ms;
+                    best_v = vv;
+                    best_shape = shape;
+                }
             }
         }
         b.tuned[cls][k] = best_v;
+        b.shape[cls][k] = best_shape;
+        if (k == 2 && best_shape != LR_SHAPES[nshapes - 1]) {
+            stage_lr_shape(s, frames, best_shape, counts);
+            if (copy_blob(ctx, s, counts) != R2G_OK) return R2G_E_DEVICE;
+        }
     }
     if (enabled) save_cache(b, cls);
     return cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
@@ -288,7 +338,6 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
         (f->bd > 8 ? any10 : any8) = true;
         counts[0] += r2g_deblock_items(f->desc);
         counts[1] += r2g_cdef_items(f->desc);
-        counts[2] += r2g_lr_items(f->desc);
         if (items[i].fgd) {
             if (r2g_grain_validate(items[i].fgd, items[i].grain_seed) != R2G_OK) {
                 ctx->err = "film-grain parameters out of range";
@@ -311,17 +360,33 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
     }
     counts[4] = (int)grains.size();
     const int cls = any8 && any10 ? 2 : (any10 ? 1 : 0);
+    // loop-restoration tile shape: the tuned one, else the default; while
+    // the stage is still to be tuned, room for the largest item count
+    const int lr_shape = b.shape[cls][2] > 0 ? b.shape[cls][2] : LR_SHAPES[0];
+    int lr_cap = 0;
+    for (int rows : LR_SHAPES) {
+        int c = 0;
+        for (DevFrame &fr : frames) {
+            fr.lr_rows = rows;
+            c += r2g_lr_items(fr);
+        }
+        if (rows == lr_shape) counts[2] = c;
+        if (b.tuned[cls][2] == 0 && c > lr_cap) lr_cap = c;
+    }
+    for (DevFrame &fr : frames) fr.lr_rows = lr_shape;
 
     // slot and capacity
     Slot &s = b.slot[b.next];
     b.next ^= 1;
     if (s.used && cudaEventSynchronize(s.done) != cudaSuccess) return R2G_E_DEVICE;
+    int need[N_BSTAGES];
+    for (int k = 0; k < N_BSTAGES; k++) need[k] = k == 2 && lr_cap > counts[2] ? lr_cap : counts[k];
     bool fits = n <= s.L.max_frames;
-    for (int k = 0; k < N_BSTAGES; k++) fits = fits && counts[k] <= s.L.max_items[k];
+    for (int k = 0; k < N_BSTAGES; k++) fits = fits && need[k] <= s.L.max_items[k];
     if (!fits) {
         int want_items[N_BSTAGES];
         for (int k = 0; k < N_BSTAGES; k++)
-            want_items[k] = counts[k] > s.L.max_items[k] ? counts[k] + counts[k] / 2 + 64 : s.L.max_items[k];
+            want_items[k] = need[k] > s.L.max_items[k] ? need[k] + need[k] / 2 + 64 : s.L.max_items[k];
         Layout L = make_layout(n > s.L.max_frames ? n + n / 2 + 4 : s.L.max_frames, want_items);
         if (s.host) cudaFreeHost(s.host);
         if (s.dev) r2g_dev_free(ctx, s.dev, s.L.bytes);
@@ -368,13 +433,19 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
             cudaStreamWaitEvent(ctx->stream, b.copied, 0) != cudaSuccess)
             return R2G_E_DEVICE;
     }
-    size_t used = s.L.off_work[N_BSTAGES - 1] + sizeof(uint32_t) * counts[3];
-    if (cudaMemcpyAsync(s.dev, s.host, used, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
+    rc = copy_blob(ctx, s, counts);
+    if (rc != R2G_OK) return rc;
 
-    // grid choice (autotuned per bit-depth mix), graph (re)build, launch
-    rc = autotune(ctx, b, s, counts, cls);
+    // grid and tile-shape choice (autotuned per bit-depth mix), graph
+    // (re)build, launch
+    rc = autotune(ctx, b, s, frames, counts, cls);
     if (rc != R2G_OK) return rc;
     int grids[N_BSTAGES];
+    b.last_rows[0] = 64;
+    b.last_rows[1] = 32;
+    b.last_rows[2] = frames.empty() ? 0 : frames[0].lr_rows;
+    b.last_rows[3] = 0;
+    for (const GrainBatch &g : grains) b.last_rows[3] = 16 << g.gp.d.block_size;
     for (int k = 0; k < N_BSTAGES; k++) {
         int v = b.tuned[cls][k] > 0 ? b.tuned[cls][k] : b.occ[k];
         b.last[k] = v == PER_ITEM ? 0 : v;
@@ -412,6 +483,13 @@ extern "C" int r2g_batch_submit(R2gCtx *ctx, const R2gBatchItem *items, int n, u
     int rc = r2g_batch_enqueue(ctx, items, n, nullptr);
     if (rc != R2G_OK) return rc;
     return r2g_ticket_record(ctx, ticket);
+}
+
+extern "C" int r2g_batch_tile_rows(R2gCtx *ctx, int32_t *rows, int n) {
+    if (!ctx || !rows) return R2G_E_INVALID;
+    if (!ctx->batch) return 0;
+    for (int k = 0; k < n && k < N_BSTAGES; k++) rows[k] = ctx->batch->last_rows[k];
+    return N_BSTAGES;
 }
 
 extern "C" int r2g_batch_config(R2gCtx *ctx, int32_t *ctas_per_sm, int n) {

@@ -153,25 +153,29 @@ R2G_D void filter_edge(int16_t *e, int along, int across, uint32_t q_thr, uint32
     int wn = imin_(width, mwn), wp = width;
     int clampv = (int)q_thr * c_q_thresh_mults[width - 1];
     int mneg = c_w_mult[wn - 1], mpos = c_w_mult[wp - 1];
-    // lines are independent once the width is chosen: one at a time keeps
-    // only 16 samples live
+    // lines are independent once the width is chosen: two at a time, both
+    // loaded before either is written
 #pragma unroll 1
-    for (int l = 0; l < 4; l++) {
-        int16_t *ln = e + l * along;
-        int L[16];
+    for (int l = 0; l < 4; l += 2) {
+        int16_t *ln0 = e + l * along, *ln1 = ln0 + along;
+        int L0[16], L1[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) L[j] = ln[(j - 8) * across];
-        int delta = iclip_(4 * (3 * (L[8] - L[7]) - (L[9] - L[6])), -clampv, clampv);
-        int dn = delta * mneg, dp = delta * mpos;
+        for (int j = 0; j < 16; j++) {
+            L0[j] = ln0[(j - 8) * across];
+            L1[j] = ln1[(j - 8) * across];
+        }
+        const int delta0 = iclip_(4 * (3 * (L0[8] - L0[7]) - (L0[9] - L0[6])), -clampv, clampv);
+        const int delta1 = iclip_(4 * (3 * (L1[8] - L1[7]) - (L1[9] - L1[6])), -clampv, clampv);
+        const int dn0 = delta0 * mneg, dp0 = delta0 * mpos, dn1 = delta1 * mneg, dp1 = delta1 * mpos;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             if (!neg_ll && j < wn) {
-                int diff = (dn * (wn - j) + (1 << 10)) >> 11;
-                ln[(-j - 1) * across] = (int16_t)clip_px_(L[7 - j] + diff, bdmax);
+                ln0[(-j - 1) * across] = (int16_t)clip_px_(L0[7 - j] + ((dn0 * (wn - j) + (1 << 10)) >> 11), bdmax);
+                ln1[(-j - 1) * across] = (int16_t)clip_px_(L1[7 - j] + ((dn1 * (wn - j) + (1 << 10)) >> 11), bdmax);
             }
             if (!pos_ll && j < wp) {
-                int diff = (dp * (wp - j) + (1 << 10)) >> 11;
-                ln[j * across] = (int16_t)clip_px_(L[8 + j] - diff, bdmax);
+                ln0[j * across] = (int16_t)clip_px_(L0[8 + j] - ((dp0 * (wp - j) + (1 << 10)) >> 11), bdmax);
+                ln1[j * across] = (int16_t)clip_px_(L1[8 + j] - ((dp1 * (wp - j) + (1 << 10)) >> 11), bdmax);
             }
         }
     }

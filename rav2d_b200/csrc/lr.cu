@@ -174,24 +174,26 @@ R2G_D int lo16(uint32_t v) { return (int)(int16_t)(v & 0xffff); }
 R2G_D int hi16(uint32_t v) { return (int)v >> 16; }
 
 // One (plane, stripe, 64-wide unit) work item; b is the per-frame item index:
-// luma items first (stripe slot, 32-row half, unit), then U, then V (stripe
+// luma items first (stripe slot, row part, unit), then U, then V (stripe
 // slot, unit).  Slots 0 .. sbh-1 are the superblock rows' first stripes;
 // slot sbh is the second stripe that only the last superblock row can have.
-// A luma stripe is split into two 32-row halves (separate CTAs) so that a
-// frame gives twice as many, lighter work items.
+// A luma stripe is split into parts of f.lr_rows rows (32: two halves, or
+// 16: four quarters; separate CTAs) so that a frame gives more, lighter work
+// items.
 template <typename P, int NT>
 R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     constexpr int NW = NT / 32;  // warps of the CTA
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
-    const int n_luma_units = (f.sbh + 1) * 2 * nux_l;
-    int plane, sby, sub, ux, half = 0;
+    const int nparts = 64 / f.lr_rows;
+    const int n_luma_units = (f.sbh + 1) * nparts * nux_l;
+    int plane, sby, sub, ux, part = 0;
     if (b < n_luma_units) {
         plane = 0;
         ux = b % nux_l;
         b /= nux_l;
-        half = b & 1;
-        b >>= 1;
+        part = b % nparts;
+        b /= nparts;
     } else {
         b -= n_luma_units;
         const int per = (f.sbh + 1) * nux_c;
@@ -207,8 +209,8 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     if (g.sh <= 0) return;
     const int chroma = plane != 0;
     // rows [ro, ro + nr) of the stripe are this item's output rows (luma: one
-    // 32-row half; chroma: the whole stripe)
-    const int ro = half * 32, nr = chroma ? g.sh : imin_(32, g.sh - ro);
+    // part of f.lr_rows rows; chroma: the whole stripe)
+    const int ro = part * f.lr_rows, nr = chroma ? g.sh : imin_(f.lr_rows, g.sh - ro);
     if (nr <= 0) return;
     const int64_t stride = f.stride[chroma];
     const P *Cp = plane_ptr<const P>(f.C[plane]);
@@ -734,7 +736,7 @@ int r2g_batch_occupancy_lr() {
 }
 int r2g_lr_items(const DevFrame &f) {
     if (!f.lr_on) return 0;
-    return (f.sbh + 1) * 2 * ((f.w + 63) >> 6) + 2 * (f.sbh + 1) * ((f.cw + 63) >> 6);
+    return (f.sbh + 1) * (64 / f.lr_rows) * ((f.w + 63) >> 6) + 2 * (f.sbh + 1) * ((f.cw + 63) >> 6);
 }
 
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {

@@ -64,6 +64,9 @@ struct DevFrame {
     uint32_t inloop;
     int deblock_on, cdef_stage_on, ccso_on, cdef_on, lr_on, any_lossless;
     int restore_planes, base_q, wiener_idx, ns_ci, gdf_ref_dst_idx;
+    // tile shape of the loop-restoration work items: luma rows per item (32,
+    // or 16 for four lighter items per stripe); set by the batch autotuner
+    int lr_rows;
     DevTables tab;
     R2gFrameParams fp;
 };

@@ -449,6 +449,7 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
                        ((fp->restoration[1].restoration_type != R2G_RESTORE_NONE) << 1) |
                        ((fp->restoration[2].restoration_type != R2G_RESTORE_NONE) << 2);
     d.lr_on = d.restore_planes != 0 && (inloop & (R2G_INLOOP_WIENER | R2G_INLOOP_GDF));
+    d.lr_rows = 32;
     d.base_q = 0;
     d.wiener_idx = 0;
     d.ns_ci = -1;

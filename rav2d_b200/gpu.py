@@ -21,7 +21,7 @@ SYMBOLS = [
     "r2g_last_error", "r2g_frame_alloc", "r2g_frame_free", "r2g_frame_upload_recon", "r2g_frame_filter",
     "r2g_frame_grain", "r2g_download", "r2g_sync", "r2g_filter_frame_host", "r2g_batch_submit", "r2g_wait",
     "r2g_frame_stage", "r2g_frame_run", "r2g_ctx_set_stream", "r2g_ctx_profile", "r2g_ctx_profile_read",
-    "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config", "r2g_server_create",
+    "r2g_ctx_launch_count", "r2g_film_grain_apply_noalloc", "r2g_batch_config", "r2g_batch_tile_rows", "r2g_server_create",
     "r2g_server_submit", "r2g_server_wait", "r2g_server_close_stream", "r2g_server_stats", "r2g_server_destroy",
     "r2g_ctx_overlap_copies", "r2g_ctx_fence", "r2g_download_y4m", "r2g_y4m_frame_bytes", "r2g_y4m_header",
     "r2g_download_rows", "r2g_dsp_cdef_dir", "r2g_dsp_cdef_filter", "r2g_dsp_ccso_prep", "r2g_dsp_ccso_add",
@@ -68,6 +68,7 @@ def lib():
         L.r2g_ctx_launch_count.argtypes = [C.c_void_p]
         L.r2g_ctx_launch_count.restype = C.c_int64
         L.r2g_batch_config.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int]
+        L.r2g_batch_tile_rows.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int]
         L.r2g_server_create.argtypes = [C.c_void_p, C.POINTER(abi.ServeConfig), C.POINTER(C.c_void_p)]
         L.r2g_server_submit.argtypes = [C.c_void_p, C.POINTER(abi.ServeRequest), C.POINTER(C.c_uint64)]
         L.r2g_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(abi.ServeResult)]
@@ -182,6 +183,12 @@ class Context:
         v = (C.c_int32 * 4)()
         sms = lib().r2g_batch_config(self.h, v, 4)
         return sms, dict(zip(("deblock", "cdef_ccso", "loop_restoration", "film_grain"), list(v)))
+
+    def batch_tile_rows(self):
+        """Luma rows per work item of the last batch per stage (the tile shape)."""
+        v = (C.c_int32 * 4)()
+        lib().r2g_batch_tile_rows(self.h, v, 4)
+        return dict(zip(("deblock", "cdef_ccso", "loop_restoration", "film_grain"), list(v)))
 
 
 class Frame:

@@ -119,3 +119,36 @@ def test_batch_oracle_spot_check(ctx, oracle):
     want = oracle.filter_frame(sf)
     _same(f, want, sf, "batch vs oracle (filter)")
     _same(g, oracle.apply_grain(sf, want), sf, "batch vs oracle (grain)")
+
+
+@pytest.mark.parametrize("rows", [16, 32])
+def test_batch_lr_tile_shape(tmp_path, monkeypatch, rows):
+    """The loop-restoration tile shape (luma rows per work item) the autotuner
+    may pick gives the same output as the per-frame path (32 rows): a tune
+    cache that pins the shape forces it for a mixed batch."""
+    import torch
+
+    from rav2d_b200 import gpu
+
+    name = torch.cuda.get_device_name(0)
+    cache = tmp_path / "tune.txt"
+    lines = []
+    for cls in range(3):
+        for k in range(4):
+            lines.append(f"{name}|{cls}|{k}|1|{rows if k == 2 else 0}")
+    cache.write_text("\n".join(lines) + "\n")
+    monkeypatch.setenv("R2G_TUNE_CACHE", str(cache))
+    c = gpu.Context(0)
+    try:
+        sfs = _frames([(640, 360, 10, "full", True), (1280, 720, 8, "full", False), (200, 136, 10, "full", False),
+                       (1920, 1080, 10, "full", True)])
+        got = _batch(c, sfs)
+        assert c.batch_tile_rows()["loop_restoration"] == rows
+        for (f, g), sf in zip(got, sfs):
+            wf = _per_frame(c, sf, sf.fgd is not None)
+            if sf.fgd is not None:
+                wf, wg = wf
+                _same(g, wg, sf, f"lr rows {rows} (grain)")
+            _same(f, wf, sf, f"lr rows {rows} (filter)")
+    finally:
+        c.close()
