@@ -408,9 +408,8 @@ int r2g_validate(R2gCtx *ctx, const R2gFrame *f, const R2gFrameParams *fp, const
         set_err(ctx, "restoration unit size out of range");
         return R2G_E_INVALID;
     }
-    if (fp->seg_enabled && (!side->segmap)) {
-        // segmentation with no map: every block is segment 0
-    }
+    // segmentation enabled without a map is accepted: the kernels read
+    // segment 0 for every block when the map pointer is NULL
     return R2G_OK;
 }
 
