@@ -45,8 +45,8 @@ MPIX = W_ * H_ / 1e6
 # pass over the frame, so its minimum is one read and one write.
 BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film_grain": 8.0}
 # dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload,
-# from `ncu --set full` (profiles/stages_full_1080p10.md); the outputs were
-# still in L2 when the capture ended, so the write term was 0
+# from one `ncu --set full` capture of each kernel (the outputs were still in
+# L2 when the capture ended, so the write term was 0)
 NCU_TRAFFIC = {"deblock": 6609664, "cdef_ccso": 6291200, "loop_restoration": 6850048}
 
 
@@ -180,7 +180,7 @@ def run_ours(args, rank, world, device):
     launches = ctx.launch_count() - l0
     ms = ev0.elapsed_time(ev1)
     barrier()
-    ms_max = replicas.max_over_ranks(ms, f"cuda:{device}")
+    units, ms_max, n_ranks = replicas.aggregate(MPIX * args.steps, ms, f"cuda:{device}")
 
     # ---- profiled pass: per-stage kernel durations from CUDA events ----
     ctx.profile(True)
@@ -236,11 +236,12 @@ def run_ours(args, rank, world, device):
         ctx.sync()
         ms = e0.elapsed_time(e1)
         ctx.overlap_copies(False)
-        return replicas.max_over_ranks(ms, f"cuda:{device}")
+        u, ms_max, _ = replicas.aggregate(MPIX * n, ms, f"cuda:{device}")
+        return u / (ms_max / 1e3)
 
     n_e2e = min(args.steps, 400)
-    e2e_ms_max = e2e_run(n_e2e, True)
-    e2e_serial_ms = e2e_run(min(n_e2e, 200), False)
+    e2e_rate = e2e_run(n_e2e, True)
+    e2e_serial_rate = e2e_run(min(n_e2e, 200), False)
     recon_bytes = int(W_ * H_ * 1.5 * 2)
     # side-info crosses PCIe as the masks plus the restoration records packed
     # to 960 bytes per SB256 (the library packs them while staging)
@@ -253,8 +254,8 @@ def run_ours(args, rank, world, device):
     ctx.close()
     return {
         "batched": batch, "per_frame_4k_grain": uhd,
-        "ms": ms_max, "launches": launches, "prof": prof, "nprof": nprof, "e2e_ms": e2e_ms_max, "n_e2e": n_e2e,
-        "e2e_serial_ms": e2e_serial_ms, "n_e2e_serial": min(n_e2e, 200),
+        "ms": ms_max, "units": units, "n_ranks": n_ranks, "launches": launches, "prof": prof, "nprof": nprof,
+        "e2e_rate": e2e_rate, "n_e2e": n_e2e, "e2e_serial_rate": e2e_serial_rate,
         "clocks": clk.summary(),
         "h2d": recon_bytes + side_bytes, "d2h": recon_bytes,
     }
@@ -549,6 +550,7 @@ def main():
     args.warmup = max(args.warmup, 3)
     from rav2d_b200 import replicas
 
+    replicas.check_world(args.gpus)
     rank, world, local = replicas.env()
     config = {"workload": "per-frame 1920x1080 10-bit 4:2:0, deblock+CDEF+CCSO+LR(NS/PC-Wiener+GDF), no grain",
               "frames_per_step": 1, "width": W_, "height": H_, "bitdepth": BD_, "inloop_mask": 31,
@@ -569,10 +571,10 @@ def main():
     replicas.finish()
     if rank != 0:
         return
-    n = args.gpus
+    n = res["n_ranks"]
     ms_step = res["ms"] / args.steps
-    value = replicas.aggregate_rate(MPIX * args.steps, res["ms"], n)
-    e2e = replicas.aggregate_rate(MPIX * res["n_e2e"], res["e2e_ms"], n)
+    value = res["units"] / (res["ms"] / 1e3)
+    e2e = res["e2e_rate"]
     prof = res["prof"]
     dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
     dom_ms, dom_n = prof[dom]
@@ -591,7 +593,7 @@ def main():
                 "d2h_bytes_per_step": res["d2h"], "steps": res["n_e2e"],
                 "path": "r2g_frame_upload_recon + r2g_frame_stage + r2g_frame_run + r2g_download, pinned host, "
                         "copies overlapped with kernels (r2g_ctx_overlap_copies)",
-                "serial_value": round(replicas.aggregate_rate(MPIX * res["n_e2e_serial"], res["e2e_serial_ms"], n), 2)},
+                "serial_value": round(res["e2e_serial_rate"], 2)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": NCU_TRAFFIC.get(dom),
                      "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum, one launch",

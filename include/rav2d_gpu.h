@@ -295,7 +295,11 @@ int r2g_download_rows(R2gCtx *ctx, R2gFrame *f, int which, int row0, int nrows, 
  * reference declares these slots but never fills or calls them, and the
  * per-frame entry points above are the performance path.  Each call copies
  * the block and the neighbours the reference would read to the GPU, runs one
- * kernel and copies the result back, synchronously, on the current device.
+ * kernel and copies the result back, synchronously, on the current device:
+ * on a non-blocking stream the library owns, so a call neither waits for nor
+ * delays work queued on the caller's streams.  Calls are serialised with each
+ * other (they share a small per-device scratch buffer, allocated on a
+ * device's first DSP call).
  * Host buffers hold u8 samples at bitdepth 8, u16 above; strides count
  * samples.  `top` points at row -2 and `bottom` at row h (column 0) of the
  * block, both with the block's stride; `left` holds [h][2] samples (columns
@@ -439,7 +443,10 @@ int r2g_batch_tile_rows(R2gCtx *ctx, int32_t *rows, int n);
  * up the array's address and should come before any stream capture.  All
  * calls share the array, so calls whose GPU work overlaps race; serialise
  * them (one stream).  Bit depths above 10 exceed the array's LUT capacity and
- * return R2G_E_TOO_LARGE; other bad arguments return R2G_E_INVALID. */
+ * return R2G_E_TOO_LARGE; other bad arguments (including film-grain fields
+ * outside the ranges the reference's parser admits) return R2G_E_INVALID.
+ * The array's address is looked up once per device and kept for the life of
+ * the process: the library does not support cudaDeviceReset between calls. */
 int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u, const void *src_v, void *dst_y,
                                  void *dst_u, void *dst_v, int64_t y_stride, int64_t uv_stride, int width,
                                  int height, int bitdepth, const R2gFilmGrainData *fgd, uint32_t seed,

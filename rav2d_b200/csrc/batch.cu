@@ -302,11 +302,17 @@ static int build_graph(R2gCtx *ctx, BatchState &b, Slot &s, const int *grids, in
     return R2G_OK;
 }
 
+// The ranges the reference's parser admits (obu.rs:272-325): at most 14
+// scaling points per plane (the kernels index points[pl][num - 1]), shifts
+// from their 2-bit fields, a 16-bit seed.
 int r2g_grain_validate(const R2gFilmGrainData *fgd, uint32_t seed) {
-    return (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
-            fgd->scaling_shift < 8 || fgd->scaling_shift > 11 || seed > 0xffff)
-               ? R2G_E_INVALID
-               : R2G_OK;
+    if (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
+        fgd->scaling_shift < 8 || fgd->scaling_shift > 11 || fgd->ar_coeff_shift < 6 || fgd->ar_coeff_shift > 9 ||
+        fgd->grain_scale_shift < 0 || fgd->grain_scale_shift > 3 || seed > 0xffff)
+        return R2G_E_INVALID;
+    for (int pl = 0; pl < 3; pl++)
+        if (fgd->num_points[pl] < 0 || fgd->num_points[pl] > 14) return R2G_E_INVALID;
+    return R2G_OK;
 }
 
 int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_t copy_stream) {

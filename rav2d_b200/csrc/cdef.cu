@@ -614,18 +614,19 @@ int r2g_launch_cdef(const DevFrame &f, cudaStream_t s) {
 }
 
 void r2g_dsp_launch_cdef_filter(const uint16_t *tile, int w, int h, int edges, int pri, int sec, int dir, int damping,
-                                int bitdepth, const DevTables &tab, uint16_t *out) {
-    dsp_cdef_filter_kernel<<<1, 64>>>(tile, w, h, edges, pri, sec, dir, damping, bitdepth, tab, out);
+                                int bitdepth, const DevTables &tab, uint16_t *out, cudaStream_t s) {
+    dsp_cdef_filter_kernel<<<1, 64, 0, s>>>(tile, w, h, edges, pri, sec, dir, damping, bitdepth, tab, out);
 }
-void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out) {
-    dsp_cdef_dir_kernel<<<1, 64>>>(blk, bitdepth, out);
+void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out, cudaStream_t s) {
+    dsp_cdef_dir_kernel<<<1, 64, 0, s>>>(blk, bitdepth, out);
 }
 void r2g_dsp_launch_ccso_prep(const uint16_t *tile, int w, int h, int ss_hor, int ss_ver, int edges, int max_band_log2,
-                              int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out) {
-    dsp_ccso_prep_kernel<<<1, 256>>>(tile, w, h, ss_hor, ss_ver, edges, max_band_log2, ext, quant_step, edge_clf,
+                              int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out,
+                              cudaStream_t s) {
+    dsp_ccso_prep_kernel<<<1, 256, 0, s>>>(tile, w, h, ss_hor, ss_ver, edges, max_band_log2, ext, quant_step, edge_clf,
                                      bo_only, bitdepth, out);
 }
 void r2g_dsp_launch_ccso_add(uint16_t *dst, const uint8_t *idx, const uint8_t *offs, const int8_t *lut, int w, int h,
-                             const uint16_t *llm, int bdmax) {
-    dsp_ccso_add_kernel<<<1, 256>>>(dst, idx, offs, lut, w, h, llm, bdmax);
+                             const uint16_t *llm, int bdmax, cudaStream_t s) {
+    dsp_ccso_add_kernel<<<1, 256, 0, s>>>(dst, idx, offs, lut, w, h, llm, bdmax);
 }

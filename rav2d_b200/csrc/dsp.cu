@@ -8,8 +8,10 @@
 // caller (or a test) can drive one block at a time: each call copies the
 // block and the neighbour samples the reference would read to the GPU, runs
 // one small kernel that applies the reference's padding rule and arithmetic,
-// and copies the result back (synchronously, on the default stream of the
-// current device).  Host buffers hold u8 samples for bitdepth 8 and u16
+// and copies the result back.  Each call is synchronous on a non-blocking
+// stream the library owns on the current device, so it neither waits for nor
+// delays work the caller has queued on other streams; calls are serialised
+// with one another by a mutex (they share that device's scratch).  Host buffers hold u8 samples for bitdepth 8 and u16
 // samples otherwise; strides count samples.
 #include <cstring>
 #include <mutex>
@@ -24,6 +26,7 @@ namespace {
 struct DspDevice {
     bool ready = false;
     char *buf = nullptr;
+    cudaStream_t st = nullptr;  // non-blocking: no implicit sync with the legacy stream
     DevTables tab{};
 };
 constexpr size_t kScratch = 64 * 1024;
@@ -37,7 +40,8 @@ int dsp_device(DspDevice **out) {
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return R2G_E_DEVICE;
     DspDevice &d = g_dsp[dev];
     if (!d.ready) {
-        if (cudaMalloc((void **)&d.buf, kScratch) != cudaSuccess || r2g_get_tables(&d.tab) != cudaSuccess) {
+        if (cudaMalloc((void **)&d.buf, kScratch) != cudaSuccess || r2g_get_tables(&d.tab) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&d.st, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
             return R2G_E_DEVICE;
         }
@@ -89,9 +93,9 @@ void store_block(P *dst, int64_t stride, const std::vector<uint16_t> &v, int w, 
 
 bool ok_bd(int bd) { return bd == 8 || bd == 10; }
 
-int finish(int rc) {
+int finish(const DspDevice *d, int rc) {
     if (rc != R2G_OK) return rc;
-    return cudaDeviceSynchronize() == cudaSuccess && cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
+    return cudaStreamSynchronize(d->st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
 }
 
 }  // namespace
@@ -109,10 +113,10 @@ extern "C" int r2g_dsp_cdef_dir(const void *img, int64_t stride, uint32_t *var, 
         load_block(blk, (const uint8_t *)img, stride, 8, 8);
     uint16_t *dblk = (uint16_t *)d->buf;
     uint32_t *dout = (uint32_t *)(d->buf + 256);
-    if (cudaMemcpy(dblk, blk.data(), 128, cudaMemcpyHostToDevice) != cudaSuccess) return R2G_E_DEVICE;
-    r2g_dsp_launch_cdef_dir(dblk, bitdepth, dout);
+    if (cudaMemcpyAsync(dblk, blk.data(), 128, cudaMemcpyHostToDevice, d->st) != cudaSuccess) return R2G_E_DEVICE;
+    r2g_dsp_launch_cdef_dir(dblk, bitdepth, dout, d->st);
     uint32_t out[2];
-    if (cudaMemcpy(out, dout, sizeof(out), cudaMemcpyDeviceToHost) != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaMemcpyAsync(out, dout, sizeof(out), cudaMemcpyDeviceToHost, d->st) != cudaSuccess) return R2G_E_DEVICE;
     *var = out[1];
     return (int)out[0];
 }
@@ -134,15 +138,15 @@ extern "C" int r2g_dsp_cdef_filter(void *dst, int64_t stride, const void *left, 
         gather(tile, w, h, (const uint8_t *)dst, stride, (const uint8_t *)left, (const uint8_t *)top,
                (const uint8_t *)bottom, edges);
     uint16_t *dtile = (uint16_t *)d->buf, *dout = (uint16_t *)(d->buf + 1024);
-    if (cudaMemcpy(dtile, tile.data(), tile.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) return R2G_E_DEVICE;
-    r2g_dsp_launch_cdef_filter(dtile, w, h, edges, pri, sec, dir, damping, bitdepth, d->tab, dout);
+    if (cudaMemcpyAsync(dtile, tile.data(), tile.size() * 2, cudaMemcpyHostToDevice, d->st) != cudaSuccess) return R2G_E_DEVICE;
+    r2g_dsp_launch_cdef_filter(dtile, w, h, edges, pri, sec, dir, damping, bitdepth, d->tab, dout, d->st);
     std::vector<uint16_t> out((size_t)w * h);
-    if (cudaMemcpy(out.data(), dout, out.size() * 2, cudaMemcpyDeviceToHost) != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaMemcpyAsync(out.data(), dout, out.size() * 2, cudaMemcpyDeviceToHost, d->st) != cudaSuccess) return R2G_E_DEVICE;
     if (bitdepth > 8)
         store_block((uint16_t *)dst, stride, out, w, h);
     else
         store_block((uint8_t *)dst, stride, out, w, h);
-    return finish(R2G_OK);
+    return finish(d, R2G_OK);
 }
 
 extern "C" int r2g_dsp_ccso_prep(uint8_t *dst, int64_t dst_stride, const void *src, int64_t stride, const void *left,
@@ -167,13 +171,13 @@ extern "C" int r2g_dsp_ccso_prep(uint8_t *dst, int64_t dst_stride, const void *s
                (const uint8_t *)bottom, edges);
     uint16_t *dtile = (uint16_t *)d->buf;
     uint8_t *dout = (uint8_t *)(d->buf + 32 * 1024);
-    if (cudaMemcpy(dtile, tile.data(), tile.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaMemcpyAsync(dtile, tile.data(), tile.size() * 2, cudaMemcpyHostToDevice, d->st) != cudaSuccess) return R2G_E_DEVICE;
     r2g_dsp_launch_ccso_prep(dtile, w, h, ss_hor, ss_ver, edges, max_band_log2, ext_filter, quant_step, edge_clf,
-                             bo_only, bitdepth, dout);
+                             bo_only, bitdepth, dout, d->st);
     std::vector<uint8_t> out((size_t)w * h);
-    if (cudaMemcpy(out.data(), dout, out.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return R2G_E_DEVICE;
+    if (cudaMemcpyAsync(out.data(), dout, out.size(), cudaMemcpyDeviceToHost, d->st) != cudaSuccess) return R2G_E_DEVICE;
     for (int y = 0; y < h; y++) memcpy(dst + y * dst_stride, &out[(size_t)y * w], (size_t)w);
-    return finish(R2G_OK);
+    return finish(d, R2G_OK);
 }
 
 extern "C" int r2g_dsp_ccso_add(void *dst, int64_t dst_stride, const uint8_t *idx, int64_t idx_stride,
@@ -197,19 +201,19 @@ extern "C" int r2g_dsp_ccso_add(void *dst, int64_t dst_stride, const uint8_t *id
     uint8_t *did = (uint8_t *)(d->buf + 8192), *doffs = (uint8_t *)(d->buf + 12288);
     int8_t *dlut = (int8_t *)(d->buf + 12416);
     uint16_t *dllm = (uint16_t *)(d->buf + 12544);
-    if (cudaMemcpy(dpx, px.data(), px.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(did, id.data(), id.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(doffs, offset_idxs, 64, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(dlut, offset_lut, 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(dllm, ll_mask, (size_t)(h / 4) * 4 * sizeof(uint16_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(dpx, px.data(), px.size() * 2, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(did, id.data(), id.size(), cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(doffs, offset_idxs, 64, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(dlut, offset_lut, 8, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(dllm, ll_mask, (size_t)(h / 4) * 4 * sizeof(uint16_t), cudaMemcpyHostToDevice, d->st) != cudaSuccess)
         return R2G_E_DEVICE;
-    r2g_dsp_launch_ccso_add(dpx, did, doffs, dlut, w, h, dllm, (1 << bitdepth) - 1);
-    if (cudaMemcpy(px.data(), dpx, px.size() * 2, cudaMemcpyDeviceToHost) != cudaSuccess) return R2G_E_DEVICE;
+    r2g_dsp_launch_ccso_add(dpx, did, doffs, dlut, w, h, dllm, (1 << bitdepth) - 1, d->st);
+    if (cudaMemcpyAsync(px.data(), dpx, px.size() * 2, cudaMemcpyDeviceToHost, d->st) != cudaSuccess) return R2G_E_DEVICE;
     if (bitdepth > 8)
         store_block((uint16_t *)dst, dst_stride, px, w, h);
     else
         store_block((uint8_t *)dst, dst_stride, px, w, h);
-    return finish(R2G_OK);
+    return finish(d, R2G_OK);
 }
 
 extern "C" int r2g_dsp_gdf_add(void *p, int64_t stride, const int8_t *err, int64_t err_stride, int w, int h,
@@ -229,17 +233,17 @@ extern "C" int r2g_dsp_gdf_add(void *p, int64_t stride, const int8_t *err, int64
     uint16_t *dpx = (uint16_t *)d->buf;
     int8_t *derr = (int8_t *)(d->buf + 8192);
     uint16_t *dllm = (uint16_t *)(d->buf + 12288);
-    if (cudaMemcpy(dpx, px.data(), px.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(derr, e.data(), e.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(dllm, ll_mask, (size_t)(h / 4) * 4 * sizeof(uint16_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(dpx, px.data(), px.size() * 2, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(derr, e.data(), e.size(), cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(dllm, ll_mask, (size_t)(h / 4) * 4 * sizeof(uint16_t), cudaMemcpyHostToDevice, d->st) != cudaSuccess)
         return R2G_E_DEVICE;
-    r2g_dsp_launch_gdf_add(dpx, derr, w, h, scale, dllm, bitdepth);
-    if (cudaMemcpy(px.data(), dpx, px.size() * 2, cudaMemcpyDeviceToHost) != cudaSuccess) return R2G_E_DEVICE;
+    r2g_dsp_launch_gdf_add(dpx, derr, w, h, scale, dllm, bitdepth, d->st);
+    if (cudaMemcpyAsync(px.data(), dpx, px.size() * 2, cudaMemcpyDeviceToHost, d->st) != cudaSuccess) return R2G_E_DEVICE;
     if (bitdepth > 8)
         store_block((uint16_t *)p, stride, px, w, h);
     else
         store_block((uint8_t *)p, stride, px, w, h);
-    return finish(R2G_OK);
+    return finish(d, R2G_OK);
 }
 
 extern "C" int r2g_dsp_generate_grain(int16_t *buf_y, int16_t *buf_u, int16_t *buf_v, const R2gFilmGrainData *fgd,
@@ -262,11 +266,11 @@ extern "C" int r2g_dsp_generate_grain(int16_t *buf_y, int16_t *buf_u, int16_t *b
     const size_t plane = 73 * 82;
     int16_t *lut = (int16_t *)d->buf;
     uint8_t *scaling = (uint8_t *)(d->buf + 3 * plane * sizeof(int16_t));
-    r2g_dsp_launch_grain_template(gp, d->tab, lut, scaling);
+    r2g_dsp_launch_grain_template(gp, d->tab, lut, scaling, d->st);
     int16_t *dst[3] = {buf_y, buf_u, buf_v};
     for (int pl = 0; pl < 3; pl++)
-        if (dst[pl] && cudaMemcpy(dst[pl], lut + pl * plane, plane * sizeof(int16_t), cudaMemcpyDeviceToHost) !=
+        if (dst[pl] && cudaMemcpyAsync(dst[pl], lut + pl * plane, plane * sizeof(int16_t), cudaMemcpyDeviceToHost, d->st) !=
                            cudaSuccess)
             return R2G_E_DEVICE;
-    return finish(R2G_OK);
+    return finish(d, R2G_OK);
 }

@@ -17,6 +17,7 @@
 // * block offsets of row band r and block b are draws 8b + 4n + 1 of the
 //   band's seed, evaluated directly by jump-ahead in the apply kernel.
 #include <cstring>
+#include <atomic>
 #include <mutex>
 
 #include "r2g_common.cuh"
@@ -614,7 +615,9 @@ __global__ void __launch_bounds__(256, 3) grain_apply_batch_kernel(BatchArgs a) 
     }
 }
 
-bool g_lfsr_ready[64] = {false};
+// per device: the LFSR cycle tables have been copied (set with release
+// order after the copies, read with acquire order)
+std::atomic<bool> g_lfsr_ready[64];
 
 }  // namespace
 
@@ -650,29 +653,32 @@ void r2g_grain_ctx_free(R2gCtx *ctx) {
 }
 
 // The LFSR cycle and its inverse (see g_lfsr_cycle), for the current device.
+// Host threads may reach this concurrently (contexts, batches, the DSP slot
+// and the allocation-free entry point): the check-and-copy runs under one
+// mutex, and the per-device flag is atomic for the lock-free fast path.
 static cudaError_t init_lfsr_pow(int device) {
-    if (device >= 0 && device < 64 && g_lfsr_ready[device]) return cudaSuccess;
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    if (g_lfsr_ready[device].load(std::memory_order_acquire)) return cudaSuccess;
     static uint16_t cyc[65536], pos[65536];
     static bool built = false;
     static std::mutex mu;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (!built) {
-            uint32_t st = 1;
-            pos[0] = 0;
-            for (uint32_t i = 0; i < 65535u; i++) {
-                cyc[i] = (uint16_t)st;
-                pos[st] = (uint16_t)i;
-                st = lfsr_step(st);
-            }
-            cyc[65535] = 1;
-            if (st != 1) return cudaErrorInvalidValue;  // not one cycle: refuse
-            built = true;
+    std::lock_guard<std::mutex> lk(mu);
+    if (g_lfsr_ready[device].load(std::memory_order_relaxed)) return cudaSuccess;
+    if (!built) {
+        uint32_t st = 1;
+        pos[0] = 0;
+        for (uint32_t i = 0; i < 65535u; i++) {
+            cyc[i] = (uint16_t)st;
+            pos[st] = (uint16_t)i;
+            st = lfsr_step(st);
         }
+        cyc[65535] = 1;
+        if (st != 1) return cudaErrorInvalidValue;  // not one cycle: refuse
+        built = true;
     }
     cudaError_t e = cudaMemcpyToSymbol(g_lfsr_cycle, cyc, sizeof(cyc));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_lfsr_pos, pos, sizeof(pos));
-    if (e == cudaSuccess && device >= 0 && device < 64) g_lfsr_ready[device] = true;
+    if (e == cudaSuccess) g_lfsr_ready[device].store(true, std::memory_order_release);
     return e;
 }
 
@@ -759,8 +765,7 @@ extern "C" int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData 
         ctx->err = "frame not filtered";
         return R2G_E_INVALID;
     }
-    if (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
-        fgd->scaling_shift < 8 || fgd->scaling_shift > 11 || seed > 0xffff) {
+    if (r2g_grain_validate(fgd, seed) != R2G_OK) {
         ctx->err = "film-grain parameters out of range";
         return R2G_E_INVALID;
     }
@@ -817,10 +822,8 @@ extern "C" int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u
     if (!src_y || !src_u || !src_v || !dst_y || !dst_u || !dst_v || !fgd) return R2G_E_INVALID;
     if (bitdepth > 10) return R2G_E_TOO_LARGE;  // scaling LUTs would not fit the scratch
     if (bitdepth != 8 && bitdepth != 10) return R2G_E_INVALID;
-    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || seed > 0xffff) return R2G_E_INVALID;
-    if (fgd->block_size < 0 || fgd->block_size > 1 || fgd->ar_coeff_lag < 0 || fgd->ar_coeff_lag > 3 ||
-        fgd->scaling_shift < 8 || fgd->scaling_shift > 11)
-        return R2G_E_INVALID;
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1)) return R2G_E_INVALID;
+    if (r2g_grain_validate(fgd, seed) != R2G_OK) return R2G_E_INVALID;
     const int bps = bitdepth > 8 ? 2 : 1;
     if (y_stride < (int64_t)width * bps || uv_stride < (int64_t)((width + 1) >> 1) * bps || (y_stride % bps) ||
         (uv_stride % bps))
@@ -879,10 +882,11 @@ extern "C" int r2g_film_grain_apply_noalloc(const void *src_y, const void *src_u
 }
 
 // DSP-context slot (r2g_dsp_generate_grain): the three grain templates of a
-// parameter set on the default stream.
-void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling) {
+// parameter set on stream `s`.
+void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling,
+                                   cudaStream_t s) {
     int dev = 0;
     cudaGetDevice(&dev);
     init_lfsr_pow(dev);
-    grain_template_kernel<<<1, 256>>>(gp, tab, lut, scaling);
+    grain_template_kernel<<<1, 256, 0, s>>>(gp, tab, lut, scaling);
 }

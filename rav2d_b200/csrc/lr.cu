@@ -749,6 +749,7 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     return 1;
 }
 
-void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth) {
-    dsp_gdf_add_kernel<<<1, 256>>>(p, err, w, h, scale, llm, bitdepth);
+void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth,
+                            cudaStream_t s) {
+    dsp_gdf_add_kernel<<<1, 256, 0, s>>>(p, err, w, h, scale, llm, bitdepth);
 }

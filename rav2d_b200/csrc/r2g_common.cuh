@@ -141,16 +141,19 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s);
 
 struct GrainDev;  // grain.cu
 
-// DSP-context slot launchers (dsp.cu): one block per call, default stream.
+// DSP-context slot launchers (dsp.cu): one block per call, on stream `s`.
 void r2g_dsp_launch_cdef_filter(const uint16_t *tile, int w, int h, int edges, int pri, int sec, int dir, int damping,
-                                int bitdepth, const DevTables &tab, uint16_t *out);
-void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out);
+                                int bitdepth, const DevTables &tab, uint16_t *out, cudaStream_t s);
+void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out, cudaStream_t s);
 void r2g_dsp_launch_ccso_prep(const uint16_t *tile, int w, int h, int ss_hor, int ss_ver, int edges, int max_band_log2,
-                              int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out);
+                              int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out,
+                              cudaStream_t s);
 void r2g_dsp_launch_ccso_add(uint16_t *dst, const uint8_t *idx, const uint8_t *offs, const int8_t *lut, int w, int h,
-                             const uint16_t *llm, int bdmax);
-void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth);
-void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling);
+                             const uint16_t *llm, int bdmax, cudaStream_t s);
+void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth,
+                            cudaStream_t s);
+void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling,
+                                   cudaStream_t s);
 
 // ---- programmatic dependent launch (per-frame kernels) ----
 // A per-frame kernel is launched so that it may start while the previous

@@ -54,7 +54,26 @@ def shard(items, rank, world):
     return items[rank::world]
 
 
-def aggregate_rate(units_per_rank, ms_max, world):
-    """Whole-job throughput: every rank processed `units_per_rank` in at
-    most `ms_max` milliseconds (units per second)."""
-    return world * units_per_rank / (ms_max / 1e3)
+def aggregate(units, ms, device="cpu"):
+    """Whole-job totals of one timed region: (units summed over the ranks,
+    the largest elapsed milliseconds of any rank, the number of ranks that
+    reported).  Every rank contributes what it actually processed, so the
+    job's rate is units / (ms / 1e3) whatever the number of ranks."""
+    if not (dist.is_initialized() and dist.get_world_size() > 1):
+        return float(units), float(ms), 1
+    t = torch.tensor([float(units), 1.0], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    m = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    return float(t[0].item()), float(m[0].item()), int(round(t[1].item()))
+
+
+def check_world(requested):
+    """The number of processes must be the number of GPUs asked for: one
+    process per GPU, started by torchrun.  A single process asked for N > 1
+    GPUs is an error (it would otherwise report one GPU's work as N's)."""
+    _, world, _ = env()
+    if world != requested:
+        raise SystemExit(f"--gpus {requested} needs {requested} processes (one per GPU, e.g. "
+                         f"python -m torch.distributed.run --nproc-per-node {requested} bench.py --gpus {requested}); "
+                         f"WORLD_SIZE is {world}")

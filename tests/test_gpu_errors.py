@@ -99,9 +99,16 @@ def test_call_order_and_grain_ranges(gpu, ctx):
             fr.grain(sf.fgd, sf.grain_seed)
         assert _code(e) == abi.R2G_E_INVALID
         fr.filter(sf)
-        for field, value in (("ar_coeff_lag", 4), ("block_size", 2), ("scaling_shift", 12)):
+        # the ranges the reference's parser admits (obu.rs:272-325)
+        for field, value in (("ar_coeff_lag", 4), ("block_size", 2), ("scaling_shift", 12), ("ar_coeff_shift", 5),
+                             ("ar_coeff_shift", 10), ("grain_scale_shift", 4), ("grain_scale_shift", -1),
+                             ("num_points", (15, 0, 0)), ("num_points", (8, -1, 0)), ("num_points", (8, 0, 99))):
             fgd = type(sf.fgd).from_buffer_copy(sf.fgd)
-            setattr(fgd, field, value)
+            if field == "num_points":
+                for i, v in enumerate(value):
+                    fgd.num_points[i] = v
+            else:
+                setattr(fgd, field, value)
             with pytest.raises(gpu.R2gError) as e:
                 fr.grain(fgd, sf.grain_seed)
             assert _code(e) == abi.R2G_E_INVALID, field

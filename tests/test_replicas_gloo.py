@@ -41,7 +41,8 @@ def _replica(rank, world, port, q):
     ms = 100.0 + 50.0 * r  # rank 1 is the slow one
     mx = replicas.max_over_ranks(ms)
     mpix = sum(a * b for a, b in mine) / 1e6
-    q.put((r, w, mine, mx, replicas.aggregate_rate(mpix, mx, w)))
+    units, ms_max, nrep = replicas.aggregate(mpix, ms)
+    q.put((r, w, mine, mx, units / (ms_max / 1e3), nrep))
     replicas.finish()
 
 
@@ -72,13 +73,16 @@ def test_two_gloo_replicas_share_and_time():
     for p in ps:
         p.join(60)
         assert p.exitcode == 0
-    (r0, w0, s0, mx0, v0), (r1, w1, s1, mx1, v1) = out
+    (r0, w0, s0, mx0, v0, n0), (r1, w1, s1, mx1, v1, n1) = out
     assert (r0, r1, w0, w1) == (0, 1, 2, 2)
     assert mx0 == mx1 == 150.0  # max over ranks, seen by both
     assert sorted(s0 + s1) == sorted([(640, 360), (1280, 720), (1920, 1080), (3840, 2160)] * 3)
     assert len(s0) == len(s1) == 6
-    mpix = sum(a * b for a, b in s0) / 1e6
-    assert v0 == pytest.approx(2 * mpix / 0.150)
+    # the job's rate: the units every rank processed over the slowest rank's
+    # time, with the number of ranks that reported (the bench's n_gpus)
+    assert n0 == n1 == 2
+    mpix = sum(a * b for a, b in s0 + s1) / 1e6
+    assert v0 == v1 == pytest.approx(mpix / 0.150)
 
 
 def test_missing_rank_fails_fast():
@@ -101,3 +105,16 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--steps", "3", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_bench_refuses_more_gpus_than_processes():
+    """`bench.py --gpus 2` started as one process must fail, not print one
+    process's rate as two GPUs' (the driver starts one process per GPU)."""
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--steps", "3", "--warmup", "3"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert r.stdout.strip() == ""
+    assert "WORLD_SIZE is 1" in r.stderr
