@@ -261,6 +261,11 @@ int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp,
 /* Film grain on the filtered frame into the frame's display copy; replaces
  * `apply_grain_to_picture_mt` (decode.rs:4672). */
 int r2g_frame_grain(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed);
+/* No counterpart in the reference (its filters cannot fail).  Waits for the
+ * context's stream and returns in *count how many bounded device-side waits
+ * of the stage kernels ran out (0 in a healthy run; a kernel whose wait ran
+ * out stops its work item and leaves its output incomplete). */
+int r2g_ctx_device_faults(R2gCtx *ctx, uint32_t *count);
 /* Copy the filtered planes (which = 0) or the grained display copy
  * (which = 1) into host memory; enqueued, complete after r2g_sync. */
 int r2g_download(R2gCtx *ctx, R2gFrame *f, int which, void *y, int64_t y_stride, void *u,

@@ -22,30 +22,58 @@ static const uint8_t UV_DIRS[2][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {7, 0, 2, 4, 5, 
 
 typedef pixel Left2[2];
 
+/* cdef.rs:122-128 fill: INT16_MIN over a w x h rectangle */
+static void fill(int16_t *tmp, ptrdiff_t stride, int w, int h) {
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) tmp[y * stride + x] = INT16_MIN;
+}
+
+/* cdef.rs:218-220 cdef_pri_tap */
+static int cdef_pri_tap(int pri_strength) { return 4 - (pri_strength & 1); }
+
+/* cdef.rs:243-262 backup2lines_plane: the last 2 rows of a `height`-row
+ * block (for a negative stride, the rows as the reference addresses them) */
+static void backup2lines_plane(pixel *dst, ptrdiff_t dst_off, const pixel *src, ptrdiff_t src_off, ptrdiff_t stride,
+                               int height) {
+    ptrdiff_t abs_stride = stride < 0 ? -stride : stride, len = 2 * abs_stride;
+    if (stride < 0)
+        memcpy(dst + dst_off + stride, src + src_off + (height - 1) * stride, sizeof(pixel) * len);
+    else
+        memcpy(dst + dst_off, src + src_off + (height - 2) * abs_stride, sizeof(pixel) * len);
+}
+
+/* cdef.rs:265-280 backup2x8_plane: columns x_off-2, x_off-1 of `rows` rows */
+static void backup2x8_plane(Left2 *dst, const pixel *src, ptrdiff_t src_off, ptrdiff_t stride, ptrdiff_t x_off,
+                            int rows) {
+    ptrdiff_t off = src_off;
+    for (int y = 0; y < rows; y++) {
+        ptrdiff_t s = off + x_off - 2;
+        dst[y][0] = src[s];
+        dst[y][1] = src[s + 1];
+        off += stride;
+    }
+}
+
 /* cdef.rs:37-112 cdef_padding */
 static void cdef_padding(int16_t *tmp, int tmp_stride, const pixel *src, ptrdiff_t src_stride,
                          ptrdiff_t src_off, const Left2 *left, const pixel *top, ptrdiff_t top_off,
                          const pixel *bottom, ptrdiff_t bottom_off, int w, int h, int edges) {
     int o = 2 * tmp_stride + 2;
     int x_start = -2, x_end = w + 2, y_start = -2, y_end = h + 2;
-    auto fill = [&](int base, int fw, int fh) {
-        for (int y = 0; y < fh; y++)
-            for (int x = 0; x < fw; x++) tmp[base + y * tmp_stride + x] = INT16_MIN;
-    };
     if (!(edges & HAVE_TOP)) {
-        fill(o - 2 - 2 * tmp_stride, w + 4, 2);
+        fill(tmp + o - 2 - 2 * tmp_stride, tmp_stride, w + 4, 2);
         y_start = 0;
     }
     if (!(edges & HAVE_BOTTOM)) {
-        fill(o + h * tmp_stride - 2, w + 4, 2);
+        fill(tmp + o + h * tmp_stride - 2, tmp_stride, w + 4, 2);
         y_end -= 2;
     }
     if (!(edges & HAVE_LEFT)) {
-        fill(o + y_start * tmp_stride - 2, 2, y_end - y_start);
+        fill(tmp + o + y_start * tmp_stride - 2, tmp_stride, 2, y_end - y_start);
         x_start = 0;
     }
     if (!(edges & HAVE_RIGHT)) {
-        fill(o + y_start * tmp_stride + w, 2, y_end - y_start);
+        fill(tmp + o + y_start * tmp_stride + w, tmp_stride, 2, y_end - y_start);
         x_end -= 2;
     }
     ptrdiff_t toff = top_off;
@@ -320,15 +348,9 @@ static void backup2lines_bank(std::vector<pixel> bank[3], Frame &f, ptrdiff_t y_
     memcpy(bank[2].data(), f.p[2] + s, sizeof(pixel) * 2 * uvs);
 }
 
-/* cdef.rs:649-663 cdef_backup2x8 */
+/* cdef.rs:649-663 cdef_backup2x8: backup2x8_plane with a positive stride */
 static void backup2x8(Left2 *dst, const pixel *src, ptrdiff_t base, ptrdiff_t stride, int x_off, int rows) {
-    ptrdiff_t off = base;
-    for (int r = 0; r < rows; r++) {
-        ptrdiff_t s = off + x_off - 2;
-        dst[r][0] = src[s];
-        dst[r][1] = src[s + 1];
-        off += stride;
-    }
+    backup2x8_plane(dst, src, base, stride, x_off, rows);
 }
 
 struct CcsoPlaneCfg {
@@ -635,6 +657,31 @@ void r2o_ccso_prep(uint8_t *dst, int dst_stride, const uint16_t *src, int64_t sr
     r2o::ccso_prep(bd, dst, dst_stride, src, src_stride, src_off, (const r2o::Left2 *)left_2, top, top_off, bottom,
                    bottom_off, max_band_log2, ext_filter, quant_step, edge_clf, bo_only != 0, edges, w, h, ss_hor,
                    ss_ver);
+}
+/* ccso.rs:5-13 CCSO_POS entry [i][k] */
+int r2o_ccso_pos(int i, int k) { return r2o::CCSO_POS[i][k]; }
+int r2o_ccso_pos_len(void) { return (int)(sizeof(r2o::CCSO_POS) / sizeof(r2o::CCSO_POS[0])); }
+/* cdef.rs:122-128, 218-224, 243-280: the helpers the reference tests */
+void r2o_cdef_fill(int16_t *tmp, int64_t stride, int w, int h) { r2o::fill(tmp, stride, w, h); }
+int r2o_cdef_pri_tap(int pri) { return r2o::cdef_pri_tap(pri); }
+/* cdef.rs:222-224 cdef_apply_constrain */
+int r2o_cdef_apply_constrain(int px, int p0, int p1, int strength, int shift, int tap) {
+    return tap * r2o::constrain(p0 - px, strength, shift) + tap * r2o::constrain(p1 - px, strength, shift);
+}
+void r2o_backup2lines_plane(uint16_t *dst, int64_t dst_off, const uint16_t *src, int64_t src_off, int64_t stride,
+                            int height) {
+    r2o::backup2lines_plane(dst, dst_off, src, src_off, stride, height);
+}
+void r2o_backup2x8_plane(uint16_t *dst_x2, const uint16_t *src, int64_t src_off, int64_t stride, int64_t x_off,
+                         int rows) {
+    r2o::backup2x8_plane((r2o::Left2 *)dst_x2, src, src_off, stride, x_off, rows);
+}
+/* cdef.rs:37-112 cdef_padding into a tmp_stride-wide i16 buffer */
+void r2o_cdef_padding(int16_t *tmp, int tmp_stride, const uint16_t *src, int64_t src_stride, int64_t src_off,
+                      const uint16_t *left_2, const uint16_t *top, int64_t top_off, const uint16_t *bottom,
+                      int64_t bottom_off, int w, int h, int edges) {
+    r2o::cdef_padding(tmp, tmp_stride, src, src_stride, src_off, (const r2o::Left2 *)left_2, top, top_off, bottom,
+                      bottom_off, w, h, edges);
 }
 /* cdef.rs:320-458 cdef_filter_block on a block at dst_off of a plane */
 void r2o_cdef_filter_block(uint16_t *dst, int64_t dst_stride, int64_t dst_off, const uint16_t *left_2,

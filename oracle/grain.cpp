@@ -386,6 +386,30 @@ int r2o_apply_grain(const R2gFilmGrainData *fgd, uint32_t seed, int w, int h, in
     return 0;
 }
 
+/* Single-function hooks for the reference's filmgrain.rs unit tests
+ * (:943-1342).  Templates are 73 x 82 int16 arrays (GrainLut). */
+void r2o_generate_grain_y(int16_t *buf, const R2gFilmGrainData *fgd, uint32_t seed, int bitdepth) {
+    generate_grain_y(*(GrainLut *)buf, *fgd, seed, bitdepth);
+}
+void r2o_generate_grain_uv(int16_t *buf, const int16_t *buf_y, const R2gFilmGrainData *fgd, uint32_t seed, int uv,
+                           int subx, int suby, int bitdepth) {
+    generate_grain_uv(*(GrainLut *)buf, *(const GrainLut *)buf_y, *fgd, seed, uv, subx != 0, suby != 0, bitdepth);
+}
+/* offsets: [bx][by][n] as 8 ints */
+int r2o_sample_lut(const int16_t *lut, int bs, const int *offsets, int subx, int suby, int bx, int by, int x, int y) {
+    return sample_lut(*(const GrainLut *)lut, bs, (const int(*)[2][2])offsets, subx, suby, bx, by, x, y);
+}
+void r2o_fgy_32x32xn(uint16_t *dst, const uint16_t *src, int64_t stride, const R2gFilmGrainData *fgd, uint32_t seed,
+                     int pw, const uint8_t *scaling, const int16_t *lut, int bh, int row_num, int bitdepth) {
+    fgy_32x32xn(dst, src, stride, *fgd, seed, pw, scaling, *(const GrainLut *)lut, bh, row_num, bitdepth);
+}
+void r2o_fguv_32x32xn(uint16_t *dst, const uint16_t *src, int64_t stride, const R2gFilmGrainData *fgd, uint32_t seed,
+                      int pw, const uint8_t *scaling, const int16_t *lut, int bh, int row_num, const uint16_t *luma,
+                      int64_t luma_stride, int uv, int is_id, int sx, int sy, int bitdepth) {
+    fguv_32x32xn(dst, src, stride, *fgd, seed, pw, scaling, *(const GrainLut *)lut, bh, row_num, luma, luma_stride, uv,
+                 is_id != 0, sx, sy, bitdepth);
+}
+
 uint32_t r2o_get_random_number(uint32_t bits, uint32_t *state) { return get_random_number(bits, state); }
 int r2o_round2(int x, uint32_t shift) { return round2(x, shift); }
 int r2o_generate_scaling(int bitdepth, const uint8_t *points, int num, uint8_t *scaling) {

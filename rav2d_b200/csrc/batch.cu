@@ -140,9 +140,14 @@ static void launch_stage(int k, const BatchArgs &a, int grid, cudaStream_t s) {
     }
 }
 
-static BatchArgs args_of(const Slot &s) {
+// The first 256 bytes of a slot's blob: item counts (ints 0..7), then the
+// stage kernels' work counters at byte 64 (zeroed with each batch's upload;
+// the kernels leave them zero after every launch).
+static BatchArgs args_of(const R2gCtx *ctx, const Slot &s) {
     BatchArgs a;
     a.count = (const int *)s.dev;
+    a.sched = (StageSched *)(s.dev + 64);
+    a.fault = ctx->fault;
     a.frames = (const DevFrame *)(s.dev + s.L.off_frames);
     a.grain = (const GrainBatch *)(s.dev + s.L.off_grain);
     for (int k = 0; k < N_BSTAGES; k++) a.work[k] = (const uint32_t *)(s.dev + s.L.off_work[k]);
@@ -220,7 +225,7 @@ static int copy_blob(R2gCtx *ctx, const Slot &s, const int *counts) {
 static int autotune(R2gCtx *ctx, BatchState &b, Slot &s, std::vector<DevFrame> &frames, int *counts, int cls) {
     const char *env = getenv("R2G_AUTOTUNE");
     bool enabled = !(env && env[0] == '0');
-    BatchArgs a = args_of(s);
+    BatchArgs a = args_of(ctx, s);
     for (int k = 0; k < N_BSTAGES; k++) {
         if (b.tuned[cls][k] > 0) continue;
         if (!enabled || counts[k] == 0) {
@@ -275,7 +280,7 @@ static int autotune(R2gCtx *ctx, BatchState &b, Slot &s, std::vector<DevFrame> &
 static int build_graph(R2gCtx *ctx, BatchState &b, Slot &s, const int *grids, int tpl_grid) {
     if (s.graph) cudaGraphDestroy(s.graph);
     s.graph = nullptr;
-    BatchArgs a = args_of(s);
+    BatchArgs a = args_of(ctx, s);
     cudaStream_t st = ctx->stream;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return R2G_E_DEVICE;
     cudaEventRecord(b.fork, st);

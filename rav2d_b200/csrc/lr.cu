@@ -14,8 +14,25 @@
 //     copy_db (D); rows further out repeat the outermost saved row;
 //   at the frame top / bottom: the stripe's first / last row repeated;
 //   at the frame left / right: the row's first / last sample repeated.
-// Each CTA materialises exactly that window for one (plane, stripe, 64-wide
-// unit) in shared memory and evaluates every restoration tap from it.
+//
+// Work items are (plane, stripe, 64-wide unit, row part): luma parts of
+// f.lr_rows (32 or 16) rows, chroma parts of 16 rows.  The kernel is
+// persistent and warp-specialised:
+//   * one producer warp takes items (blockIdx.x first, then a shared atomic
+//     counter), decodes their geometry, unit kind, lossless and no-skip rows
+//     from the side-info, and stages every source row of the item's window
+//     (C or D by the rule above; the unit's width plus a 16-byte margin on
+//     each side) into one of two shared-memory slots, one bulk copy
+//     (cp.async.bulk) per row completing on the slot's "full" mbarrier;
+//   * eight consumer warps take the slots in turn: they turn the raw rows
+//     into the filter window (edge replication at the frame's left / right
+//     border; each position holds its sample and the right neighbour as a
+//     16x2 pair), release the slot through its "empty" mbarrier, and filter
+//     (GDF gradient cells and PC classes, then per pixel pair: GDF error,
+//     FIR, GDF add, one 2-sample store).
+// So the producer loads items k+1 and k+2 while the consumers filter item
+// k, and a frame's GDF / PC-Wiener tables are staged once per CTA.
+#include <atomic>
 #include <type_traits>
 
 #include "r2g_common.cuh"
@@ -23,17 +40,34 @@
 namespace {
 
 enum { LR_HAVE_LEFT = 1, LR_HAVE_RIGHT = 2, LR_HAVE_TOP = 4, LR_HAVE_BOTTOM = 8 };
+enum { W_NONE = 0, W_NS_SINGLE = 1, W_NS_MULTI = 2, W_PC = 3 };
 
-constexpr int LW = 76;   // luma window width: -6 .. 69
-constexpr int LH = 44;   // luma window height: -6 .. 37 (a work item has <= 32 rows)
-constexpr int CWW = 68;  // chroma window width: -2 .. 65
-constexpr int CWH = 36;  // chroma window height: -2 .. 33 (stripe <= 32 rows)
+constexpr int NCW = 8;           // consumer warps
+constexpr int NCT = NCW * 32;    // consumer threads
+constexpr int LR_NT = NCT + 32;  // plus the producer warp
+constexpr int CROWS = 16;        // chroma rows per work item
+constexpr int LW = 76, LH = 44;  // luma window: columns -6 .. 69, rows -6 .. nr + 5 (nr <= 32)
+constexpr int CW2 = 68, CH2 = 20;  // chroma windows: columns -2 .. 65, rows -2 .. 17
+constexpr int RAW_BYTES = 14720;   // one staging slot (largest item: 10-bit chroma with its CfL luma)
+
+// Raw staging rows start 16 bytes left of the unit origin (every copy is
+// 16-byte aligned) and hold the unit's 64 samples plus 16 bytes on each
+// side; the CfL luma rows of a chroma item hold 128 luma samples plus the
+// same margins.
+template <typename P>
+struct RawGeom {
+    static constexpr int XO = 16 / (int)sizeof(P);                // margin in samples
+    static constexpr int RB = (64 + 2 * XO) * (int)sizeof(P);    // bytes per raw row
+    static constexpr int LRB = (128 + 2 * XO) * (int)sizeof(P);  // bytes per raw CfL luma row
+    static constexpr int LOFF = CH2 * RB;                         // offset of the CfL luma rows
+};
+static_assert(LH * RawGeom<uint16_t>::RB <= RAW_BYTES, "luma window slot");
+static_assert(RawGeom<uint16_t>::LOFF + 2 * CH2 * RawGeom<uint16_t>::LRB <= RAW_BYTES, "chroma slot");
+static_assert(RawGeom<uint8_t>::LOFF + 2 * CH2 * RawGeom<uint8_t>::LRB <= RAW_BYTES, "chroma slot");
 
 __constant__ uint16_t c_pcw_norm[4] = {3739, 3273, 3074, 7};
 __constant__ int16_t c_mode_weights[4][3] = {{-527, 15325, 321}, {26436, -17705, 17905}, {366, -147, -194}, {202, -267, -179}};
 __constant__ int16_t c_mode_offsets[4] = {-547, -21565, -573, -680};
-
-enum { W_NONE = 0, W_NS_SINGLE = 1, W_NS_MULTI = 2, W_PC = 3 };
 
 struct UnitGeom {
     int plane, x0, uw, y0, sh, edges, valid;
@@ -51,11 +85,12 @@ R2G_D int get_qval(int qstep, int tskip, int i, int b8) {
     return 255 * (c_mode_offsets[i] + qval);
 }
 
-// Work item -> geometry, following lr_sbrow_apply / lr_sbrow_plane /
-// lr_stripe for one tile row (sb128 = 0).  A superblock row's LR call covers
-// [y_call, row_h); its first stripe is 56 (luma) rows high on superblock row
-// 0 and 64 otherwise, so a call holds one stripe, or two when the frame
-// height is a multiple of 64 and this is the last superblock row.
+// Stripe geometry and unit selection, following lr_sbrow_apply /
+// lr_sbrow_plane / lr_stripe for one tile row (sb128 = 0).  A superblock
+// row's LR call covers [y_call, row_h); its first stripe is 56 (luma) rows
+// high on superblock row 0 and 64 otherwise, so a call holds one stripe, or
+// two when the frame height is a multiple of 64 and this is the last
+// superblock row.
 R2G_D void unit_geom(const DevFrame &f, int plane, int sby, int sub, int ux, UnitGeom &g) {
     const int chroma = plane != 0;
     const int ss = chroma;  // 4:2:0: ss_hor = ss_ver = 1 for chroma
@@ -125,10 +160,11 @@ R2G_D void row_src(const UnitGeom &g, int r, int &row, bool &from_d) {
     }
 }
 
-R2G_D int col_src(const UnitGeom &g, int c) {
-    if (c < 0 && !(g.edges & LR_HAVE_LEFT)) return g.x0;
-    if (c >= g.uw && !(g.edges & LR_HAVE_RIGHT)) return g.x0 + g.uw - 1;
-    return g.x0 + c;
+// Window column x (unit-relative) -> the column whose sample it holds.
+R2G_D int col_clamp(int x, int uw, int edges) {
+    if (x < 0 && !(edges & LR_HAVE_LEFT)) return 0;
+    if (x >= uw && !(edges & LR_HAVE_RIGHT)) return uw - 1;
+    return x;
 }
 
 // Compile-time tap tables (the reference's WIENER_NS_CONFIG_Y :389,
@@ -146,84 +182,190 @@ __device__ constexpr int8_t uvy[12][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 
                                           {-1, 1}, {1, -1}, {2, 0}, {-2, 0}, {0, 2}, {0, -2}};
 }  // namespace TapsY
 
+// One work item as the producer publishes it to the consumers.
+struct LrDesc {
+    int b;   // per-frame item index; -1: no more items
+    int fi;  // frame of the batch (0 in a per-frame launch)
+    int plane, x0, y0, sh, ro, nr, uw, edges, kind, gdf, copy;
+    int c0, c1;           // single-class FIR constants (sums of the taps)
+    int8_t f[20];         // single-class NS-Wiener taps (the unit's or the frame's)
+    uint16_t llm[18];     // lossless 4x4 bits per 4 rows of the stripe
+    uint16_t noskip[18];  // no-skip 4x4 bits per 4 rows of the stripe (multi-class)
+};
+
 struct LrSmem {
+    uint64_t full[2], empty[2];
+    LrDesc desc[2];
+    alignas(16) unsigned char raw[2][RAW_BYTES];
     union {
-        // luma: every window position holds the sample and its right
-        // neighbour as a signed 16x2 pair, so GDF can work on two adjacent
-        // pixels (which share a GDF class) with one 32-bit load per tap;
-        // a scalar sample is the low half (16-bit loads at a 4-byte stride)
+        // luma: every window position holds its sample and the right
+        // neighbour as a 16x2 pair (low half = the sample), so a pixel pair
+        // (x, x + 1) reads one tap of both pixels with one 32-bit load
         uint32_t wp[LH * LW];
         struct {
-            int16_t win[CWH * CWW];   // chroma window
-            int16_t lwin[CWH * CWW];  // downsampled luma window
+            uint32_t win[CH2 * CW2];   // chroma window, same pairing
+            uint32_t lwin[CH2 * CW2];  // downsampled luma window, same pairing
         } ch;
     } u;
     uint16_t gcell[17 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
-    int8_t gerr[32 * 64];
-    int8_t s_err[4096];
-    uint2 s_aa[4][18];   // per class and tap: (alpha, alpha), (-alpha, -alpha) as s16x2
-    int4 s_w[4][22];     // per class and tap / feature: weights 0..2, alpha
-    int16_t s_pcf[64 * 13];  // PC-Wiener filters of this frame's wiener_idx
     uint8_t classes[8][16];
+    // consumer-side copies of the item's row data (the slot is released
+    // before filtering)
+    int8_t f[20];
+    uint16_t llm[18];
     uint16_t noskip[18];
-    uint16_t llm[17];
+    // frame tables and the parameters they were staged for (-1: none)
+    int gdf_key, pc_key, nsm_key;
+    int bias[3];
+    uint2 s_aa[4][18];       // per class and tap: (alpha, alpha), (-alpha, -alpha) as s16x2
+    int4 s_w[4][22];         // per class and tap / feature: weights 0..2, alpha
+    int16_t s_pcf[64 * 13];  // PC-Wiener filters of the frame's wiener_idx
+    int8_t s_nsm[16][16];    // multi-class NS-Wiener filters of the frame
+    int s_nsm_c0[16];
+    int8_t s_err[4096];
 };
 
-// Sign-extended low / high halves of a 16x2 pair.
+// Sign-extended low / high halves of a 16x2 pair; unsigned halves.
 R2G_D int lo16(uint32_t v) { return (int)(int16_t)(v & 0xffff); }
 R2G_D int hi16(uint32_t v) { return (int)v >> 16; }
+R2G_D int ulo(uint32_t v) { return (int)(v & 0xffff); }
+R2G_D int uhi(uint32_t v) { return (int)(v >> 16); }
 
-// One (plane, stripe, 64-wide unit) work item; b is the per-frame item index:
-// luma items first (stripe slot, row part, unit), then U, then V (stripe
-// slot, unit).  Slots 0 .. sbh-1 are the superblock rows' first stripes;
-// slot sbh is the second stripe that only the last superblock row can have.
-// A luma stripe is split into parts of f.lr_rows rows (32: two halves, or
-// 16: four quarters; separate CTAs) so that a frame gives more, lighter work
-// items.
-template <typename P, int NT>
-R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
-    constexpr int NW = NT / 32;  // warps of the CTA
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// Per-frame item index b -> geometry (luma items first: stripe slot, row
+// part, unit; then U, then V: stripe slot, row part, unit).  Slots
+// 0 .. sbh-1 are the superblock rows' first stripes; slot sbh is the second
+// stripe only the last superblock row can have.  False: an empty item.
+R2G_D bool item_geom(const DevFrame &f, int b, UnitGeom &g, int &ro, int &nr) {
     const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
     const int nparts = 64 / f.lr_rows;
-    const int n_luma_units = (f.sbh + 1) * nparts * nux_l;
-    int plane, sby, sub, ux, part = 0;
-    if (b < n_luma_units) {
+    const int n_luma = (f.sbh + 1) * nparts * nux_l;
+    int plane, ux, part, slot;
+    if (b < n_luma) {
         plane = 0;
         ux = b % nux_l;
         b /= nux_l;
         part = b % nparts;
-        b /= nparts;
+        slot = b / nparts;
     } else {
-        b -= n_luma_units;
-        const int per = (f.sbh + 1) * nux_c;
+        b -= n_luma;
+        const int per = (f.sbh + 1) * 2 * nux_c;
         plane = 1 + b / per;
         b %= per;
         ux = b % nux_c;
         b /= nux_c;
+        part = b & 1;
+        slot = b >> 1;
     }
-    sub = b >= f.sbh;
-    sby = sub ? f.sbh - 1 : b;
-    UnitGeom g;
-    unit_geom(f, plane, sby, sub, ux, g);
-    if (g.sh <= 0) return;
-    const int chroma = plane != 0;
-    // rows [ro, ro + nr) of the stripe are this item's output rows (luma: one
-    // part of f.lr_rows rows; chroma: the whole stripe)
-    const int ro = part * f.lr_rows, nr = chroma ? g.sh : imin_(f.lr_rows, g.sh - ro);
-    if (nr <= 0) return;
-    const int64_t stride = f.stride[chroma];
-    const P *Cp = plane_ptr<const P>(f.C[plane]);
-    const P *Dp = plane_ptr<const P>(f.D[plane]);
-    P *Lp = plane_ptr<P>(f.L[plane]);
-    const R2gFrameParams &fp = f.fp;
-    const int bitdepth = f.bitdepth, bdmax = f.bdmax;
+    const int sub = slot >= f.sbh;
+    unit_geom(f, plane, sub ? f.sbh - 1 : slot, sub, ux, g);
+    const int rows = plane ? CROWS : f.lr_rows;
+    ro = part * rows;
+    nr = imin_(rows, g.sh - ro);
+    return g.sh > 0 && nr > 0;
+}
 
+// ---------------------------------------------------------------- producer
+// Issues (issue = true) or only sizes the bulk copies of one item's raw
+// rows, spread over the warp's lanes; returns this lane's bytes.
+template <typename P>
+R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int ro, int nr, int kind, bool copy,
+                           unsigned char *raw, uint64_t *bar, int lane, bool issue) {
+    typedef RawGeom<P> RG;
+    constexpr int bps = (int)sizeof(P);
+    const int64_t stride = f.stride[plane != 0];
+    const char *Cp = (const char *)f.C[plane];
+    const char *Dp = (const char *)f.D[plane];
+    uint32_t total = 0;
+    if (copy) {
+        // unfiltered unit: its output rows only, from the unit origin
+        const uint32_t bytes = (uint32_t)((g.uw * bps + 15) & ~15);
+        for (int r = lane; r < nr; r += 32) {
+            if (issue)
+                bulk_g2s(raw + r * RG::RB, Cp + ((int64_t)(g.y0 + ro + r) * stride + g.x0) * bps, bytes, bar);
+            total += bytes;
+        }
+        return total;
+    }
+    // window columns [x0 - XO, x0 + 64 + XO), clipped to the plane row
+    int cs = g.x0 - RG::XO, doff = 0;
+    if (cs < 0) {
+        doff = -cs * bps;
+        cs = 0;
+    }
+    const int ce = imin_(g.x0 + 64 + RG::XO, (int)stride);
+    const uint32_t bytes = (uint32_t)((ce - cs) * bps);
+    const int halo = plane ? 2 : 6;
+    const int wrows = nr + 2 * halo;
+    for (int r = lane; r < wrows; r += 32) {
+        int row;
+        bool from_d;
+        row_src(g, ro + r - halo, row, from_d);
+        if (issue) bulk_g2s(raw + r * RG::RB + doff, (from_d ? Dp : Cp) + ((int64_t)row * stride + cs) * bps, bytes, bar);
+        total += bytes;
+    }
+    if (plane && kind == W_NS_SINGLE) {
+        // CfL luma rows (backup_row_luma with ns_wiener_single_uv's row
+        // selection, looprestoration.rs:1207-1350): two luma rows per window
+        // row, C inside the stripe, D at the stripe boundaries
+        const int64_t ls = f.stride[0];
+        const char *Cy = (const char *)f.C[0];
+        const char *Dy = (const char *)f.D[0];
+        int lcs = 2 * g.x0 - RG::XO, ldoff = 0;
+        if (lcs < 0) {
+            ldoff = -lcs * bps;
+            lcs = 0;
+        }
+        const int lce = imin_(2 * g.x0 + 128 + RG::XO, (int)ls);
+        const uint32_t lbytes = (uint32_t)((lce - lcs) * bps);
+        for (int q = lane; q < 2 * wrows; q += 32) {
+            int rr = ro + (q >> 1) - 2;
+            if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
+            if (!(g.edges & LR_HAVE_BOTTOM) && rr >= g.sh) rr = g.sh - 1;
+            const char *src;
+            int ra, rb;
+            if (rr == -2) {
+                src = Dy;
+                ra = rb = 2 * g.y0 - 2;
+            } else if (rr == -1) {
+                src = Dy;
+                ra = 2 * g.y0 - 2;
+                rb = 2 * g.y0 - 1;
+            } else if (rr == g.sh) {
+                src = Dy;
+                ra = 2 * (g.y0 + g.sh);
+                rb = ra + 1;
+            } else if (rr == g.sh + 1) {
+                src = Dy;
+                ra = rb = 2 * (g.y0 + g.sh) + 1;
+            } else {
+                src = Cy;
+                ra = 2 * (g.y0 + rr);
+                rb = ra + 1;
+            }
+            const int lrow = (q & 1) ? rb : ra;
+            if (issue)
+                bulk_g2s(raw + RG::LOFF + q * RG::LRB + ldoff, src + ((int64_t)lrow * ls + lcs) * bps, lbytes, bar);
+            total += lbytes;
+        }
+    }
+    return total;
+}
+
+// Produces one work item into slot k & 1, after waiting for the slot's
+// release when it was used before.  Returns 0 for an empty item (nothing
+// published), 1 when published, -1 when a wait ran out.
+template <typename P>
+R2G_D int produce_item(const DevFrame &f, int fi, int b, LrSmem &sm, int k, int lane, bool &waited) {
+    UnitGeom g;
+    int ro, nr;
+    if (!item_geom(f, b, g, ro, nr)) return 0;
+    const int plane = g.plane, chroma = plane != 0;
+    const R2gFrameParams &fp = f.fp;
     // ---- kernel selection (looprestoration.rs:1880-1920) ----
     int wkind = W_NONE;
-    bool plane_on = (f.restore_planes >> plane) & 1;
+    const bool plane_on = (f.restore_planes >> plane) & 1;
     if (plane_on && g.valid) {
-        int wt = (f.inloop & R2G_INLOOP_WIENER) ? g.unit->type : 0;
+        const int wt = (f.inloop & R2G_INLOOP_WIENER) ? g.unit->type : 0;
         const R2gRestorationPlane &pd = fp.restoration[plane];
         if (wt == R2G_RESTORE_NS_WIENER)
             wkind = (pd.frame_filters_on && pd.num_classes != 1) ? W_NS_MULTI : W_NS_SINGLE;
@@ -235,59 +377,182 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
     const int nsb = f.sb256w * f.sb256h;
     const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && sb256_idx < nsb &&
                         f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
-
-    // ---- lossless rows of the stripe (looprestoration.rs:2037-2075) ----
-    const int ll_rows = imax_(g.sh >> 2, 1) + 1;
-    if (tid < 17) {
-        uint16_t v = 0;
-        if (tid < ll_rows && sb256_idx < nsb) {
-            const R2gAv2Filter &m = f.masks[sb256_idx];
-            int y4 = ((g.y0 << chroma) & 255) >> 2;
-            if (plane == 0) {
-                int yy = y4 + tid;
-                if (yy < 64) v = m.lossless_mask_y[yy][g.sb64x_idx];
-            } else {
-                int init_y = g.y0 >> 2, end_y = (g.y0 + g.sh) >> 2;
-                int base = y4 >> 1;
-                if (init_y + tid < end_y) {
-                    int sy = base + tid;
-                    if (sy < 64) {
-                        uint16_t lo = m.lossless_mask_uv[sy][g.sb64x_idx];
-                        uint16_t hi = g.sb64x_idx + 1 < 4 ? m.lossless_mask_uv[sy][g.sb64x_idx + 1] : 0;
-                        v = (uint16_t)((lo & 0xff) | ((hi & 0xff) << 8));
+    const bool copy = wkind == W_NONE && !gdf_on;
+    // ---- per-lane side-info: lossless rows (looprestoration.rs:2037-2075),
+    // multi-class no-skip rows (:1922-1944), single-class taps ----
+    uint16_t llm = 0, nsk = 0;
+    int tap = 0;
+    if (!copy) {
+        if (lane < 17) {
+            const int ll_rows = imax_(g.sh >> 2, 1) + 1;
+            if (lane < ll_rows && sb256_idx < nsb) {
+                const R2gAv2Filter &m = f.masks[sb256_idx];
+                const int y4 = ((g.y0 << chroma) & 255) >> 2;
+                if (plane == 0) {
+                    const int yy = y4 + lane;
+                    if (yy < 64) llm = m.lossless_mask_y[yy][g.sb64x_idx];
+                } else {
+                    const int init_y = g.y0 >> 2, end_y = (g.y0 + g.sh) >> 2;
+                    const int sy = (y4 >> 1) + lane;
+                    if (init_y + lane < end_y && sy < 64) {
+                        const uint16_t lo = m.lossless_mask_uv[sy][g.sb64x_idx];
+                        const uint16_t hi = g.sb64x_idx + 1 < 4 ? m.lossless_mask_uv[sy][g.sb64x_idx + 1] : 0;
+                        llm = (uint16_t)((lo & 0xff) | ((hi & 0xff) << 8));
                     }
                 }
             }
         }
-        sm.llm[tid] = v;
-    }
-    // ---- multi-class noskip rows (looprestoration.rs:1922-1944) ----
-    if ((wkind == W_NS_MULTI || wkind == W_PC) && tid < 18) {
-        uint16_t v = 0;
-        int by = (g.y0 >> 2) + tid;
-        if (by < ((g.y0 + g.sh) >> 2)) {
-            int sidx = f.sb256w * (by >> 6) + g.sb256x;
-            if (sidx < nsb) {
-                v = f.masks[sidx].lr_noskip_mask[by & 63][g.sb64x_idx];
-                if (!(g.edges & LR_HAVE_RIGHT) && (g.uw & 63) != 0) {
-                    int sh = ((g.uw >> 2) & 15) - 1;
-                    uint16_t eb = (uint16_t)(v >> sh);
-                    v = (uint16_t)(v | (uint16_t)(eb << (sh + 1)));
+        if ((wkind == W_NS_MULTI || wkind == W_PC) && lane < 18) {
+            const int by = (g.y0 >> 2) + lane;
+            if (by < ((g.y0 + g.sh) >> 2)) {
+                const int sidx = f.sb256w * (by >> 6) + g.sb256x;
+                if (sidx < nsb) {
+                    uint16_t v = f.masks[sidx].lr_noskip_mask[by & 63][g.sb64x_idx];
+                    if (!(g.edges & LR_HAVE_RIGHT) && (g.uw & 63) != 0) {
+                        const int s = ((g.uw >> 2) & 15) - 1;
+                        const uint16_t eb = (uint16_t)(v >> s);
+                        v = (uint16_t)(v | (uint16_t)(eb << (s + 1)));
+                    }
+                    nsk = v;
                 }
             }
         }
-        sm.noskip[tid] = v;
+        if (wkind == W_NS_SINGLE && lane < 18) {
+            const R2gRestorationPlane &pd = fp.restoration[plane];
+            tap = pd.frame_filters_on ? pd.filter[0][lane] : g.unit->f[lane];
+        }
     }
-    // GDF and PC-Wiener parameters of the frame (tables only)
-    if (gdf_on && !chroma) {
-        const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
+    // single-class FIR constants: s = m * c0 + sum (a + b) f [- l * c1 + sum l' f]
+    // equals the reference's (m << 7) + sum (a + b - 2m) f [+ sum (l' - l) f]
+    const int nsym = chroma ? 6 : 16;
+    const int fsym = __reduce_add_sync(0xffffffffu, lane < nsym ? tap : 0);
+    const int fcc = __reduce_add_sync(0xffffffffu, (chroma && lane >= 6 && lane < 18) ? tap : 0);
+
+    // C and D (and L, which the consumers write) belong to the previous
+    // kernels on the stream: wait for them before the first copy
+    if (!waited) {
+        pdl_wait();
+        waited = true;
+    }
+    const int s = k & 1;
+    if (k >= 2 && !mbar_wait(&sm.empty[s], ((k >> 1) - 1) & 1)) return -1;
+    LrDesc &d = sm.desc[s];
+    if (lane == 0) {
+        d.b = b;
+        d.fi = fi;
+        d.plane = plane;
+        d.x0 = g.x0;
+        d.y0 = g.y0;
+        d.sh = g.sh;
+        d.ro = ro;
+        d.nr = nr;
+        d.uw = g.uw;
+        d.edges = g.edges;
+        d.kind = wkind;
+        d.gdf = gdf_on;
+        d.copy = copy;
+        d.c0 = 128 - 2 * fsym;
+        d.c1 = fcc;
+    }
+    if (lane < 18) {
+        d.llm[lane] = llm;
+        d.noskip[lane] = nsk;
+        d.f[lane] = (int8_t)tap;
+    }
+    const uint32_t total =
+        __reduce_add_sync(0xffffffffu, item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane,
+                                                      false));
+    // the consumers' reads of this slot (ordered before by the empty
+    // barrier) precede the copies' writes
+    fence_proxy_async();
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(&sm.full[s], total);
+    __syncwarp();
+    item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane, true);
+    return 1;
+}
+
+template <int HB>
+R2G_D bool is_hbd(const DevFrame &f) {
+    return HB == 1 || (HB == 2 && f.bitdepth > 8);
+}
+
+// The producer warp: work-list positions blockIdx.x, then
+// gridDim.x + atomicAdd(next), until the list is exhausted.
+template <int HB, typename Src>
+R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
+    const int n = src.count();
+    StageSched *sched = src.sched();
+    int k = 0;  // items published
+    int w = blockIdx.x;
+    bool waited = false, ok = true;
+    while (w < n) {
+        int fi, b;
+        src.item(w, fi, b);
+        const DevFrame &f = src.frame(fi);
+        const int rc = is_hbd<HB>(f) ? produce_item<uint16_t>(f, fi, b, sm, k, lane, waited)
+                                     : produce_item<uint8_t>(f, fi, b, sm, k, lane, waited);
+        if (rc < 0) {
+            ok = false;
+            break;
+        }
+        k += rc;
+        if (!waited) {
+            pdl_wait();
+            waited = true;
+        }
+        int nx = 0;
+        if (lane == 0) nx = (int)(gridDim.x + atomicAdd(&sched->next, 1u));
+        w = __shfl_sync(0xffffffffu, nx, 0);
+    }
+    if (!waited) pdl_wait();
+    if (ok) {
+        // no more items: publish the stop marker
+        const int s = k & 1;
+        if (k >= 2 && !mbar_wait(&sm.empty[s], ((k >> 1) - 1) & 1)) {
+            ok = false;
+        } else {
+            if (lane == 0) {
+                sm.desc[s].b = -1;
+                mbar_arrive_expect_tx(&sm.full[s], 0);
+            }
+            __syncwarp();
+        }
+    }
+    if (!ok && lane == 0) {
+        // a wait ran out: record it, and let this CTA's copies in flight land
+        // before the CTA (and its shared memory) goes away
+        atomicAdd(src.fault(), 1u);
+        for (int s = 0; s < 2; s++) {
+            const int uses = (k + 1 - s) / 2;
+            if (uses > 0) mbar_wait(&sm.full[s], (uses - 1) & 1);
+        }
+    }
+    __syncwarp();
+    if (lane == 0) sched_retire(sched);
+}
+
+// ---------------------------------------------------------------- consumers
+// Stages the frame tables an item needs (GDF alpha / weights / bias / error
+// LUT of the frame's ref_dst_idx and qp_idx; PC-Wiener filters of its
+// wiener_idx; multi-class NS-Wiener filters).  Uniform over the consumers.
+// Returns what it staged; after a consumer barrier, commit_tables records it
+// (the keys are read by every consumer before any of them may change them).
+R2G_D int stage_tables(const DevFrame &f, int fi, LrSmem &sm, bool gdf, bool pc, bool nsm, int tid) {
+    const R2gFrameParams &fp = f.fp;
+    const int ref_dst_idx = f.gdf_ref_dst_idx, qp_idx = fp.gdf_qp_idx;
+    const int gkey = ref_dst_idx * 8 + qp_idx;
+    const bool do_gdf = gdf && sm.gdf_key != gkey;
+    const bool do_pc = pc && sm.pc_key != f.wiener_idx;
+    const bool do_nsm = nsm && sm.nsm_key != fi;
+    if (do_gdf) {
         const int alpha_base = ref_dst_idx * 528 + qp_idx * 88;
         const int weight_base = ref_dst_idx * 1584 + qp_idx * 264;
         const int8_t *errtab = ref_dst_idx == 0 ? f.tab.GDF_INTRA_ERROR + qp_idx * 4096
                                                 : f.tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
         const int nerr = ref_dst_idx == 0 ? 4096 : 1000;
-        for (int i = tid; i < 88; i += NT) {
-            int k = i >> 2, c = i & 3;
+        for (int i = tid; i < 88; i += NCT) {
+            const int k = i >> 2, c = i & 3;
             const int a = f.tab.GDF_ALPHA[alpha_base + i];
             sm.s_w[c][k] = make_int4(f.tab.GDF_WEIGHT[weight_base + 0 * 88 + i],
                                      f.tab.GDF_WEIGHT[weight_base + 1 * 88 + i],
@@ -297,201 +562,214 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 sm.s_aa[c][k] = make_uint2(pa | (pa << 16), na | (na << 16));
             }
         }
-        for (int i = tid; i < nerr; i += NT) sm.s_err[i] = errtab[i];
+        if (tid < 3) sm.bias[tid] = f.tab.GDF_BIAS[(ref_dst_idx * 6 + qp_idx) * 3 + tid];
+#pragma unroll 4
+        for (int i = tid; i < nerr; i += NCT) sm.s_err[i] = __ldg(errtab + i);
     }
-    if (wkind == W_PC)
-        for (int i = tid; i < 64 * 13; i += NT) sm.s_pcf[i] = f.tab.PC_WIENER_FILTERS[f.wiener_idx * 64 * 13 + i];
-    // C and D come from the previous kernels on the stream: wait for them
-    // (everything above reads side-info and tables only; a CTA that only
-    // copies has staged a few unused rows and parameters)
-    pdl_wait();
-    if (wkind == W_NONE && !gdf_on) {
-        // unfiltered unit: copy C -> L in 4-byte words (unit widths are
-        // multiples of 4 samples; rows and unit origins are 64-byte aligned)
-        const int wpr = g.uw * (int)sizeof(P) / 4;
-        for (int i = tid; i < nr * wpr; i += NT) {
-            const int r = ro + i / wpr, q = i % wpr;
-            const int64_t o = (int64_t)(g.y0 + r) * stride + g.x0;
-            reinterpret_cast<uint32_t *>(Lp + o)[q] = __ldg(reinterpret_cast<const uint32_t *>(Cp + o) + q);
+    if (do_pc)
+        for (int i = tid; i < 64 * 13; i += NCT) sm.s_pcf[i] = __ldg(f.tab.PC_WIENER_FILTERS + f.wiener_idx * 64 * 13 + i);
+    if (do_nsm) {
+        sm.s_nsm[tid >> 4][tid & 15] = fp.restoration[0].filter[tid >> 4][tid & 15];
+        if (tid < 16) {
+            int s = 0;
+            for (int k = 0; k < 16; k++) s += fp.restoration[0].filter[tid][k];
+            sm.s_nsm_c0[tid] = 128 - 2 * s;
         }
-        return;
     }
+    return (do_gdf ? 1 : 0) | (do_pc ? 2 : 0) | (do_nsm ? 4 : 0);
+}
+R2G_D void commit_tables(const DevFrame &f, int fi, LrSmem &sm, int staged) {
+    if (staged & 1) sm.gdf_key = f.gdf_ref_dst_idx * 8 + f.fp.gdf_qp_idx;
+    if (staged & 2) sm.pc_key = f.wiener_idx;
+    if (staged & 4) sm.nsm_key = fi;
+}
 
+template <typename P>
+R2G_D int raw_at(const unsigned char *row, int x) {
+    return (int)reinterpret_cast<const P *>(row)[x];
+}
 
-    if (chroma) {
-        // ---- chroma window: rows -2 .. sh+1, columns -2 .. uw+1 ----
-        const int wh = g.sh + 4, ww = g.uw + 4;
-        for (int r = warp; r < wh; r += NW) {
-            int row;
-            bool from_d;
-            row_src(g, r - 2, row, from_d);
-            const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
-            for (int c = lane; c < ww; c += 32) sm.u.ch.win[r * CWW + c] = (int16_t)src[col_src(g, c - 2)];
-        }
-        if (wkind == W_NS_SINGLE) {
-            // downsampled luma for chroma rows -2 .. sh+1 at chroma columns
-            // -2 .. uw+1 (backup_row_luma with the ns_wiener_single_uv row
-            // selection, looprestoration.rs:1207-1350)
-            const P *Cy = plane_ptr<const P>(f.C[0]);
-            const P *Dy = plane_ptr<const P>(f.D[0]);
-            const int64_t ls = f.stride[0];
-            const int ds = fp.cfl_ds_filter_index;
-            const int lw = g.uw << 1, lx0 = g.x0 << 1;
-            for (int r = warp; r < wh; r += NW) {
-                int rr = r - 2;
-                if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
-                if (!(g.edges & LR_HAVE_BOTTOM) && rr >= g.sh) rr = g.sh - 1;
-                const P *src;
-                int ra, rb;
-                if (rr == -2) {
-                    src = Dy;
-                    ra = rb = 2 * g.y0 - 2;
-                } else if (rr == -1) {
-                    src = Dy;
-                    ra = 2 * g.y0 - 2;
-                    rb = 2 * g.y0 - 1;
-                } else if (rr == g.sh) {
-                    src = Dy;
-                    ra = 2 * (g.y0 + g.sh);
-                    rb = ra + 1;
-                } else if (rr == g.sh + 1) {
-                    src = Dy;
-                    ra = rb = 2 * (g.y0 + g.sh) + 1;
-                } else {
-                    src = Cy;
-                    ra = 2 * (g.y0 + rr);
-                    rb = ra + 1;
-                }
-                const P *rowa = src + (int64_t)ra * ls + lx0;
-                const P *rowb = src + (int64_t)rb * ls + lx0;
-                for (int j = lane; j < ww; j += 32) {
-                    int pos = 2 * (j - 2);
-                    if (pos < 0 && !(g.edges & LR_HAVE_LEFT)) pos = 0;
-                    if (pos >= lw && !(g.edges & LR_HAVE_RIGHT)) pos = lw - 2;
-                    int v;
-                    if (ds == 0)
-                        v = ((int)rowa[pos] + rowb[pos] + rowa[pos + 1] + rowb[pos + 1]) >> 2;
-                    else if (ds == 1)
-                        v = ((int)rowa[pos] + rowb[pos]) >> 1;
-                    else
-                        v = rowa[pos];
-                    sm.u.ch.lwin[r * CWW + j] = (int16_t)v;
-                }
+// Raw rows -> luma pair window (window column c holds source column c - 6),
+// replicating the frame's left / right edge samples.
+template <typename P>
+R2G_D void build_luma_window(LrSmem &sm, const unsigned char *raw, int nr, int uw, int edges, int tid) {
+    typedef RawGeom<P> RG;
+    const int wh = nr + 12;
+    if ((edges & LR_HAVE_LEFT) && (edges & LR_HAVE_RIGHT)) {
+        // interior unit (uw == 64): four window columns 4q .. 4q + 3 per
+        // step, from raw samples 4q + 2 .. 4q + 6 (u16) / 4q + 10 .. 4q + 14 (u8)
+        for (int i = tid; i < wh * 19; i += NCT) {
+            const int r = i / 19, q = i - r * 19;
+            const unsigned char *row = raw + r * RG::RB;
+            uint4 o;
+            if (sizeof(P) == 2) {
+                const uint32_t w0 = *reinterpret_cast<const uint32_t *>(row + 8 * q + 4);
+                const uint32_t w1 = *reinterpret_cast<const uint32_t *>(row + 8 * q + 8);
+                const uint32_t s4 = *reinterpret_cast<const uint16_t *>(row + 8 * q + 12);
+                o = make_uint4(w0, __byte_perm(w0, w1, 0x5432), w1, __byte_perm(w1, s4, 0x5432));
+            } else {
+                const uint32_t w0 = *reinterpret_cast<const uint32_t *>(row + 4 * q + 8);
+                const uint32_t w1 = *reinterpret_cast<const uint32_t *>(row + 4 * q + 12);
+                const uint32_t e0 = __byte_perm(w0, 0, 0x4342), e1 = __byte_perm(w1, 0, 0x4140),
+                               e2 = __byte_perm(w1, 0, 0x4442);
+                o = make_uint4(e0, __byte_perm(e0, e1, 0x5432), e1, __byte_perm(e1, e2, 0x5432));
             }
-        }
-        __syncthreads();
-        // ---- chroma NS-Wiener with cross-component luma taps (:1145-1430) ----
-        int8_t flt[18];
-        if (wkind == W_NS_SINGLE) {
-            const int8_t *src = fp.restoration[plane].frame_filters_on ? fp.restoration[plane].filter[0]
-                                                                       : g.unit->f;
-#pragma unroll
-            for (int k = 0; k < 18; k++) flt[k] = src[k];
-        }
-        for (int y = warp; y < g.sh; y += NW)
-            for (int x = lane; x < g.uw; x += 32) {
-                const int16_t *w = &sm.u.ch.win[(y + 2) * CWW + x + 2];
-                const int16_t *lw_ = &sm.u.ch.lwin[(y + 2) * CWW + x + 2];
-                int m = w[0];
-                int v = m;
-                bool ll = (sm.llm[y >> 2] >> (x >> 2)) & 1;
-                if (!ll && wkind == W_NS_SINGLE) {
-                    int s = m << 7;
-#pragma unroll
-                    for (int k = 0; k < 6; k++) {
-                        const int o = TapsY::uv[k][0] * CWW + TapsY::uv[k][1];
-                        s += (w[o] + w[-o] - 2 * m) * flt[k];
-                    }
-                    int l = lw_[0];
-#pragma unroll
-                    for (int k = 0; k < 12; k++) {
-                        const int o = TapsY::uvy[k][0] * CWW + TapsY::uvy[k][1];
-                        s += (lw_[o] - l) * flt[6 + k];
-                    }
-                    v = clip_px_((s + 64) >> 7, bdmax);
-                }
-                Lp[(int64_t)(g.y0 + y) * stride + g.x0 + x] = (P)v;
-            }
-        return;
-    }
-
-    // ---- luma window: rows ro-6 .. ro+nr+5 of the stripe, columns -6 .. uw+5 ----
-    const int wh = nr + 12, ww = g.uw + 12;
-    if ((g.edges & LR_HAVE_LEFT) && (g.edges & LR_HAVE_RIGHT) && g.uw == 64) {
-        // interior unit: window columns are source columns x0-6 .. x0+69, all
-        // inside the frame.  Read them as 2-sample words U_j (samples
-        // x0-6+2j, x0-5+2j): pair 2j is U_j, pair 2j+1 joins U_j's second
-        // sample with U_{j+1}'s first.  Each thread issues four words' loads
-        // before storing any pair.
-        typedef typename std::conditional<sizeof(P) == 2, uint32_t, uint16_t>::type U;
-        constexpr int NJ = 38, SH = 8 * (int)sizeof(P);
-        constexpr uint32_t MK = (1u << SH) - 1;
-        const int total = wh * NJ;
-        for (int base = 0; base < total; base += 4 * NT) {
-            uint32_t a[4], nb[4];
-            int dst[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int i = base + q * NT + tid;
-                dst[q] = -1;
-                a[q] = nb[q] = 0;
-                if (i < total) {
-                    const int r = i / NJ, j = i - r * NJ;
-                    int row;
-                    bool from_d;
-                    row_src(g, ro + r - 6, row, from_d);
-                    const U *src = reinterpret_cast<const U *>((from_d ? Dp : Cp) + (int64_t)row * stride + g.x0 - 6);
-                    a[q] = __ldg(src + j);
-                    nb[q] = __ldg(src + j + 1);
-                    dst[q] = r * LW + 2 * j;
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (dst[q] >= 0) {
-                    const uint32_t s0 = a[q] & MK, s1 = a[q] >> SH, t0 = nb[q] & MK;
-                    sm.u.wp[dst[q]] = s0 | (s1 << 16);
-                    sm.u.wp[dst[q] + 1] = s1 | (t0 << 16);
-                }
+            *reinterpret_cast<uint4 *>(&sm.u.wp[r * LW + 4 * q]) = o;
         }
     } else {
-        // source columns of this lane's window columns (the same on every row)
-        int cs0[3], cs1[3];
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const int c = lane + 32 * j;
-            cs0[j] = col_src(g, c - 6);
-            cs1[j] = c + 1 < ww ? col_src(g, c - 5) : cs0[j];
-        }
-        for (int r = warp; r < wh; r += NW) {
-            int row;
-            bool from_d;
-            row_src(g, ro + r - 6, row, from_d);
-            const P *src = (from_d ? Dp : Cp) + (int64_t)row * stride;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const int c = lane + 32 * j;
-                if (c < ww) sm.u.wp[r * LW + c] = (uint32_t)src[cs0[j]] | ((uint32_t)src[cs1[j]] << 16);
-            }
+        const int ww = uw + 12;
+        for (int i = tid; i < wh * ww; i += NCT) {
+            const int r = i / ww, c = i - r * ww;
+            const unsigned char *row = raw + r * RG::RB;
+            const int a = raw_at<P>(row, col_clamp(c - 6, uw, edges) + RG::XO);
+            const int b = raw_at<P>(row, col_clamp(c - 5, uw, edges) + RG::XO);
+            sm.u.wp[r * LW + c] = (uint32_t)a | ((uint32_t)b << 16);
         }
     }
-    const int16_t *W16 = reinterpret_cast<const int16_t *>(sm.u.wp);  // scalar sample i at W16[2 * i]
-    __syncthreads();
+}
 
-    const int b8 = bitdepth - 8;
-    const int bh4 = nr >> 2, bw4 = g.uw >> 2, sbh4 = g.sh >> 2;
-    // ---- GDF prep (looprestoration.rs:1432-1640) ----
-    if (gdf_on) {
-        // GDF works in a 10-bit domain (looprestoration.rs:1450-1453): 8-bit
-        // samples shift up by 2; 12-bit (not accepted at the boundary) would
-        // shift down by 2.
-        constexpr int down = 0, up = sizeof(P) == 1 ? 2 : 0;
-        // gradient cell (j, i): rows 2j-1, 2j; columns 2i-1, 2i
-        // (compute_gradient_row :114-193); pair (y1, x1) sums cells
-        // (y1/2 .. y1/2+1, x1/2 .. x1/2+1)
-        const int cj = (nr >> 1) + 1, ci = (g.uw >> 1) + 1;
-        for (int i = tid; i < cj * ci; i += NT) {
-            int j = i / ci, c = i % ci;
+// Raw rows -> chroma pair window and (CfL) downsampled luma pair window
+// (window column j holds chroma column j - 2).
+template <typename P>
+R2G_D void build_chroma_windows(LrSmem &sm, const unsigned char *raw, int nr, int uw, int edges, bool cfl, int ds,
+                                int tid) {
+    typedef RawGeom<P> RG;
+    const int wh = nr + 4, ww = uw + 4;
+    for (int i = tid; i < wh * ww; i += NCT) {
+        const int r = i / ww, j = i - r * ww;
+        const unsigned char *row = raw + r * RG::RB;
+        const int a = raw_at<P>(row, col_clamp(j - 2, uw, edges) + RG::XO);
+        const int b = raw_at<P>(row, col_clamp(j - 1, uw, edges) + RG::XO);
+        sm.u.ch.win[r * CW2 + j] = (uint32_t)a | ((uint32_t)b << 16);
+    }
+    if (!cfl) return;
+    const int lw = uw << 1;
+    for (int i = tid; i < wh * ww; i += NCT) {
+        const int r = i / ww, j = i - r * ww;
+        const unsigned char *ra = raw + RG::LOFF + (2 * r) * RG::LRB;
+        const unsigned char *rb = ra + RG::LRB;
+        int l[2];
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            int pos = 2 * (j + t - 2);
+            if (pos < 0 && !(edges & LR_HAVE_LEFT)) pos = 0;
+            if (pos >= lw && !(edges & LR_HAVE_RIGHT)) pos = lw - 2;
+            pos += RG::XO;
+            if (ds == 0)
+                l[t] = (raw_at<P>(ra, pos) + raw_at<P>(rb, pos) + raw_at<P>(ra, pos + 1) + raw_at<P>(rb, pos + 1)) >> 2;
+            else if (ds == 1)
+                l[t] = (raw_at<P>(ra, pos) + raw_at<P>(rb, pos)) >> 1;
+            else
+                l[t] = raw_at<P>(ra, pos);
+        }
+        sm.u.ch.lwin[r * CW2 + j] = (uint32_t)l[0] | ((uint32_t)l[1] << 16);
+    }
+}
+
+// An unfiltered unit: staged rows -> L, 16 bytes per store.
+template <typename P>
+R2G_D void copy_unit(const DevFrame &f, const unsigned char *raw, int plane, int x0, int y, int nr, int uw, int tid) {
+    typedef RawGeom<P> RG;
+    const int bytes = uw * (int)sizeof(P);
+    const int nch = (bytes + 15) >> 4;
+    const int64_t stride = f.stride[plane != 0] * (int64_t)sizeof(P);
+    char *L = (char *)f.L[plane] + (int64_t)y * stride + (int64_t)x0 * sizeof(P);
+    for (int i = tid; i < nr * nch; i += NCT) {
+        const int r = i / nch, q = i - r * nch;
+        const unsigned char *src = raw + r * RG::RB + 16 * q;
+        char *dst = L + r * stride + 16 * q;
+        const int left = bytes - 16 * q;
+        if (left >= 16) {
+            *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
+        } else if (left >= 8) {
+            *reinterpret_cast<uint2 *>(dst) = *reinterpret_cast<const uint2 *>(src);
+            if (left >= 12) *reinterpret_cast<uint32_t *>(dst + 8) = *reinterpret_cast<const uint32_t *>(src + 8);
+        } else {
+            *reinterpret_cast<uint32_t *>(dst) = *reinterpret_cast<const uint32_t *>(src);
+        }
+    }
+}
+
+// GDF error of a luma pixel pair (x1, x1 + 1), x1 even, window row y
+// (gdf_prep, looprestoration.rs:1540-1640): both pixels share the 2x2
+// gradient cell and so the class; their 18 clipped symmetric differences run
+// as 16x2 pairs.
+template <typename P>
+R2G_D void gdf_pair(const DevFrame &f, const LrSmem &sm, const uint32_t *wc, int y, int x1, int uw, int &e0, int &e1) {
+    constexpr int up = sizeof(P) == 1 ? 2 : 0;  // the 10-bit internal domain
+    const int ci = (uw >> 1) + 1;
+    const int j = y >> 1, c = x1 >> 1;
+    int gsum[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++)
+        gsum[d] = sm.gcell[(j * ci + c) * 4 + d] + sm.gcell[(j * ci + c + 1) * 4 + d] +
+                  sm.gcell[((j + 1) * ci + c) * 4 + d] + sm.gcell[((j + 1) * ci + c + 1) * 4 + d];
+    const int cls = (gsum[0] <= gsum[1]) | ((gsum[2] <= gsum[3]) << 1);
+    const int4 *wt = sm.s_w[cls];
+    const uint2 *aa = sm.s_aa[cls];
+    int sh0 = sm.bias[0], sh1 = sm.bias[1], sh2 = sm.bias[2];
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const int4 p = wt[18 + d];
+        const int v = imin_(gsum[d] >> (4 - up), p.w);
+        sh0 += v * p.x;
+        sh1 += v * p.y;
+        sh2 += v * p.z;
+    }
+    const uint32_t mm = wc[0] << up;  // samples < 2^10: no carry between the halves
+    const uint32_t nm = __vneg2(mm);
+    int i0 = sh0, i1 = sh1, i2 = sh2, j0 = sh0, j1 = sh1, j2 = sh2;
+#pragma unroll
+    for (int k = 0; k < 18; k++) {
+        const int o = TapsY::gdf[k][0] * LW + TapsY::gdf[k][1];
+        const uint2 al = aa[k];
+        const int4 p = wt[k];
+        // clip(a - m, -alpha, alpha) as the fused add-max / add-min
+        const uint32_t above = __viaddmin_s16x2(__viaddmax_s16x2(wc[-o] << up, nm, al.y), 0u, al.x);
+        const uint32_t below = __viaddmin_s16x2(__viaddmax_s16x2(wc[o] << up, nm, al.y), 0u, al.x);
+        const uint32_t v = __viaddmin_s16x2(__viaddmax_s16x2(above, below, 0xfe00fe00u), 0u, 0x01ff01ffu);
+        const int v0 = lo16(v), v1 = hi16(v);
+        i0 += v0 * p.x;
+        i1 += v0 * p.y;
+        i2 += v0 * p.z;
+        j0 += v1 * p.x;
+        j1 += v1 * p.y;
+        j2 += v1 * p.z;
+    }
+    const int scale = f.gdf_ref_dst_idx == 0 ? 8 : 5;
+    int full0 = 0, full1 = 0;
+    const int iv0[3] = {i0, i1, i2}, iv1[3] = {j0, j1, j2};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        int sv = iv0[q] * scale;
+        int v = apply_sign_(((sv < 0 ? -sv : sv) + (1 << 14)) >> 15, sv);
+        full0 = full0 * (scale * 2) + iclip_(v, -scale, scale - 1) + scale;
+        sv = iv1[q] * scale;
+        v = apply_sign_(((sv < 0 ? -sv : sv) + (1 << 14)) >> 15, sv);
+        full1 = full1 * (scale * 2) + iclip_(v, -scale, scale - 1) + scale;
+    }
+    e0 = sm.s_err[full0];
+    e1 = sm.s_err[full1];
+}
+
+// Filters one staged luma item (everything after the window is built).
+template <typename P>
+R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, int ro, int nr, int uw, int kind,
+                       bool gdf, int c0, int tid) {
+    const int warp = tid >> 5, lane = tid & 31;
+    const R2gFrameParams &fp = f.fp;
+    const int16_t *W16 = reinterpret_cast<const int16_t *>(sm.u.wp);  // scalar sample i at W16[2 * i]
+    const int bh4 = nr >> 2, bw4 = uw >> 2, sbh4 = sh >> 2;
+    const int b8 = f.bitdepth - 8;
+    // ---- phase 1: GDF gradient cells (compute_gradient_row :114-193) and
+    // multi-class 4x4 classes (get_class_lut_idx :195-271, :870-896) ----
+    if (gdf) {
+        // cell (j, i): window rows 2j-1, 2j; columns 2i-1, 2i; pair (y, x1)
+        // sums cells (y/2 .. y/2+1, x1/2 .. x1/2+1)
+        constexpr int down = 0;
+        const int cj = (nr >> 1) + 1, ci = (uw >> 1) + 1;
+        for (int i = tid; i < cj * ci; i += NCT) {
+            const int j = i / ci, c = i - j * ci;
             int gs[4] = {0, 0, 0, 0};
 #pragma unroll
             for (int yy = 0; yy < 2; yy++)
@@ -499,7 +777,7 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 for (int xx = 0; xx < 2; xx++) {
                     const int16_t *w = &W16[2 * ((2 * j - 1 + yy + 6) * LW + 2 * c - 1 + xx + 6)];
                     constexpr int R = 2 * LW, C1 = 2;
-                    int bv = w[0] >> down;
+                    const int bv = w[0] >> down;
                     int t;
                     t = 2 * bv - (w[-R] >> down) - (w[R] >> down);
                     gs[0] += t < 0 ? -t : t;
@@ -510,84 +788,17 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                     t = 2 * bv - (w[R - C1] >> down) - (w[-R + C1] >> down);
                     gs[3] += t < 0 ? -t : t;
                 }
-#pragma unroll
-            for (int d = 0; d < 4; d++) sm.gcell[i * 4 + d] = (uint16_t)gs[d];
-        }
-        __syncthreads();
-        const int ref_dst_idx = f.gdf_ref_dst_idx;
-        const int bias_idx = ref_dst_idx * 6 + fp.gdf_qp_idx;
-        const int scale = ref_dst_idx == 0 ? 8 : 5;
-        const int b0 = f.tab.GDF_BIAS[bias_idx * 3], b1 = f.tab.GDF_BIAS[bias_idx * 3 + 1],
-                  b2 = f.tab.GDF_BIAS[bias_idx * 3 + 2];
-        const int npairs = nr * (g.uw >> 1);
-        for (int i = tid; i < npairs; i += NT) {
-            int y = i / (g.uw >> 1), x1 = (i % (g.uw >> 1)) * 2;
-            int j = y >> 1, c = x1 >> 1;
-            int gsum[4];
-#pragma unroll
-            for (int d = 0; d < 4; d++)
-                gsum[d] = sm.gcell[(j * ci + c) * 4 + d] + sm.gcell[(j * ci + c + 1) * 4 + d] +
-                          sm.gcell[((j + 1) * ci + c) * 4 + d] + sm.gcell[((j + 1) * ci + c + 1) * 4 + d];
-            int cls = (gsum[0] <= gsum[1]) | ((gsum[2] <= gsum[3]) << 1);
-            const int4 *wt = sm.s_w[cls];
-            const uint2 *aa = sm.s_aa[cls];
-            int sh0 = b0, sh1 = b1, sh2 = b2;
-#pragma unroll
-            for (int d = 0; d < 4; d++) {
-                int4 p = wt[18 + d];
-                int v = imin_(gsum[d] >> (4 - up), p.w);
-                sh0 += v * p.x;
-                sh1 += v * p.y;
-                sh2 += v * p.z;
-            }
-            // the 18 clipped symmetric differences of both pixels at once,
-            // as signed 16x2 pairs: (pixel x, pixel x + 1)
-            const uint32_t *wc = &sm.u.wp[(y + 6) * LW + x1 + 6];
-            const uint32_t mm = wc[0] << up;  // samples < 2^10: no carry between halves
-            const uint32_t nm = __vneg2(mm);
-            int i0 = sh0, i1 = sh1, i2 = sh2, j0 = sh0, j1 = sh1, j2 = sh2;
-#pragma unroll
-            for (int k = 0; k < 18; k++) {
-                const int o = TapsY::gdf[k][0] * LW + TapsY::gdf[k][1];
-                const uint2 al = aa[k];
-                const int4 p = wt[k];
-                // (min as the fused add-min with 0: one instruction, where a
-                // plain packed min is slower on this part)
-                const uint32_t above = __viaddmin_s16x2(__viaddmax_s16x2(wc[-o] << up, nm, al.y), 0u, al.x);
-                const uint32_t below = __viaddmin_s16x2(__viaddmax_s16x2(wc[o] << up, nm, al.y), 0u, al.x);
-                const uint32_t v = __viaddmin_s16x2(__viaddmax_s16x2(above, below, 0xfe00fe00u), 0u, 0x01ff01ffu);
-                const int v0 = lo16(v), v1 = hi16(v);
-                i0 += v0 * p.x;
-                i1 += v0 * p.y;
-                i2 += v0 * p.z;
-                j0 += v1 * p.x;
-                j1 += v1 * p.y;
-                j2 += v1 * p.z;
-            }
-#pragma unroll
-            for (int x2 = 0; x2 < 2; x2++) {
-                const int iv[3] = {x2 ? j0 : i0, x2 ? j1 : i1, x2 ? j2 : i2};
-                int full = 0;
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    int sv = iv[q] * scale;
-                    int asv = sv < 0 ? -sv : sv;
-                    int v = apply_sign_((asv + (1 << 14)) >> 15, sv);
-                    int subi = iclip_(v, -scale, scale - 1) + scale;
-                    full = full * (scale * 2) + subi;
-                }
-                sm.gerr[y * 64 + x1 + x2] = sm.s_err[full];
-            }
+            *reinterpret_cast<uint2 *>(&sm.gcell[i * 4]) =
+                make_uint2((uint32_t)gs[0] | ((uint32_t)gs[1] << 16), (uint32_t)gs[2] | ((uint32_t)gs[3] << 16));
         }
     }
-    // ---- classification for PC-Wiener / NS-multi (:195-271, :870-896) ----
-    if (wkind == W_NS_MULTI || wkind == W_PC) {
-        const uint8_t *sub_lut = wkind == W_PC
+    if (kind == W_NS_MULTI || kind == W_PC) {
+        const uint8_t *sub_lut = kind == W_PC
                                      ? f.tab.PC_WIENER_SUB_CLASSIFY + f.wiener_idx * 256
                                      : f.tab.PC_WIENER_SUB_CLASSIFY_NS +
                                            (f.wiener_idx * 7 + (f.ns_ci >= 0 ? imin_(f.ns_ci, 6) : 0)) * 256;
-        for (int i = tid; i < bh4 * bw4; i += NT) {
-            int by = i / bw4, bx = i % bw4;
+        for (int i = tid; i < bh4 * bw4; i += NCT) {
+            const int by = i / bw4, bx = i - by * bw4;
             int fs0 = 0, fs1 = 0, fs2 = 0;
 #pragma unroll
             for (int dy = -1; dy <= 4; dy++)
@@ -595,10 +806,10 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 for (int dx = -1; dx <= 4; dx++) {
                     const int16_t *w = &W16[2 * ((by * 4 + dy + 6) * LW + bx * 4 + dx + 6)];
                     constexpr int R = 2 * LW, C1 = 2;
-                    int m2 = 2 * w[0];
-                    int vert = w[-R] - m2 + w[R];
-                    int anti = w[-R + C1] - m2 + w[R - C1];
-                    int diag = w[-R - C1] - m2 + w[R + C1];
+                    const int m2 = 2 * w[0];
+                    const int vert = w[-R] - m2 + w[R];
+                    const int anti = w[-R + C1] - m2 + w[R - C1];
+                    const int diag = w[-R - C1] - m2 + w[R + C1];
                     fs0 += vert < 0 ? -vert : vert;
                     fs1 += anti < 0 ? -anti : anti;
                     fs2 += diag < 0 ? -diag : diag;
@@ -609,12 +820,12 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
             for (int dy = -1; dy <= 1; dy++)
 #pragma unroll
                 for (int dx = -1; dx <= 1; dx++) {
-                    int e = (dy != 0) + (dx != 0);
-                    int fx = iclip_((bx & 15) + dx, 0, 15);
-                    int fy = iclip_((ro >> 2) + by + dy, 0, sbh4 - 1);
+                    const int e = (dy != 0) + (dx != 0);
+                    const int fx = iclip_((bx & 15) + dx, 0, 15);
+                    const int fy = iclip_((ro >> 2) + by + dy, 0, sbh4 - 1);
                     s += np[e] * (((sm.noskip[fy] >> fx) & 1) == 0);
                 }
-            int rnd = (1 << b8) >> 1;
+            const int rnd = (1 << b8) >> 1;
             int fs[3] = {fs0, fs1, fs2};
 #pragma unroll
             for (int k = 0; k < 3; k++) fs[k] = (int)((uint32_t)fs[k] * (uint32_t)c_pcw_norm[k] + (uint32_t)rnd) >> b8;
@@ -628,87 +839,255 @@ R2G_D void lr_unit(const DevFrame &f, LrSmem &sm, int b) {
                 qv = imin_(qv, 255) >> 5;
                 lut_idx |= qv << (3 * (2 - k));
             }
-            sm.classes[by][bx] = sub_lut[f.tab.PC_WIENER_LUT_TO_CLASS[lut_idx]];
+            sm.classes[by][bx] = __ldg(sub_lut + __ldg(f.tab.PC_WIENER_LUT_TO_CLASS + lut_idx));
         }
     }
-    __syncthreads();
-    // ---- Wiener FIR + GDF add, one output sample per iteration ----
-    int8_t single[16];
-    if (wkind == W_NS_SINGLE) {
-        const int8_t *src = fp.restoration[0].frame_filters_on ? fp.restoration[0].filter[0] : g.unit->f;
-#pragma unroll
-        for (int k = 0; k < 16; k++) single[k] = src[k];
-    }
-    const int gshift = 12 - bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
-    for (int y = warp; y < nr; y += NW)
-        for (int x = lane; x < g.uw; x += 32) {
-            const int16_t *w = &W16[2 * ((y + 6) * LW + x + 6)];
-            int m = w[0];
-            int v = m;
-            bool ll = (sm.llm[(ro + y) >> 2] >> (x >> 2)) & 1;
-            if (!ll && wkind != W_NONE) {
-                int s;
-                if (wkind == W_PC) {
-                    const int16_t *flt = sm.s_pcf + sm.classes[y >> 2][x >> 2] * 13;
-                    s = m * flt[12];
+    if (gdf || kind == W_NS_MULTI || kind == W_PC) bar_sync_n(NCT);
+    // ---- phase 2: per pixel pair: GDF error, FIR, GDF add, store ----
+    const int bdmax = f.bdmax;
+    const int gshift = 12 - f.bitdepth, grnd = (1 << gshift) >> 1, gscale = fp.gdf_scale;
+    const int64_t stride = f.stride[0];
+    P *Lp = plane_ptr<P>(f.L[0]) + (int64_t)(y0 + ro) * stride + x0;
+    const int x1 = 2 * lane;
+    if (x1 >= uw) return;
+    for (int y = warp; y < nr; y += NCW) {
+        const uint32_t *wc = &sm.u.wp[(y + 6) * LW + x1 + 6];
+        const uint32_t mm = wc[0];
+        int v0 = ulo(mm), v1 = uhi(mm);
+        const bool ll = (sm.llm[(ro + y) >> 2] >> (x1 >> 2)) & 1;
+        if (!ll) {
+            int e0 = 0, e1 = 0;
+            if (gdf) gdf_pair<P>(f, sm, wc, y, x1, uw, e0, e1);
+            if (kind != W_NONE) {
+                int s0, s1;
+                if (kind == W_PC) {
+                    const int16_t *flt = sm.s_pcf + sm.classes[y >> 2][x1 >> 2] * 13;
+                    s0 = v0 * flt[12];
+                    s1 = v1 * flt[12];
 #pragma unroll
                     for (int k = 0; k < 12; k++) {
-                        const int o = 2 * (TapsY::pc[k][0] * LW + TapsY::pc[k][1]);
-                        s += (w[o] + w[-o]) * flt[k];
+                        const int o = TapsY::pc[k][0] * LW + TapsY::pc[k][1];
+                        const uint32_t t = wc[o] + wc[-o];  // both halves < 2^11: no carry
+                        const int fk = flt[k];
+                        s0 += ulo(t) * fk;
+                        s1 += uhi(t) * fk;
                     }
                 } else {
-                    const int8_t *flt =
-                        wkind == W_NS_SINGLE ? single : fp.restoration[0].filter[sm.classes[y >> 2][x >> 2]];
-                    s = m << 7;
+                    const int8_t *flt;
+                    int cc;
+                    if (kind == W_NS_SINGLE) {
+                        flt = sm.f;
+                        cc = c0;
+                    } else {
+                        const int cls = sm.classes[y >> 2][x1 >> 2];
+                        flt = sm.s_nsm[cls];
+                        cc = sm.s_nsm_c0[cls];
+                    }
+                    s0 = v0 * cc;
+                    s1 = v1 * cc;
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
-                        const int o = 2 * (TapsY::ns[k][0] * LW + TapsY::ns[k][1]);
-                        s += (w[o] + w[-o] - 2 * m) * flt[k];
+                        const int o = TapsY::ns[k][0] * LW + TapsY::ns[k][1];
+                        const uint32_t t = wc[o] + wc[-o];
+                        const int fk = flt[k];
+                        s0 += ulo(t) * fk;
+                        s1 += uhi(t) * fk;
                     }
                 }
-                v = clip_px_((s + 64) >> 7, bdmax);
+                v0 = clip_px_((s0 + 64) >> 7, bdmax);
+                v1 = clip_px_((s1 + 64) >> 7, bdmax);
             }
-            if (gdf_on && !ll) {
-                int diff = sm.gerr[y * 64 + x] * gscale;
-                int ad = diff < 0 ? -diff : diff;
-                v = clip_px_(v + apply_sign_((ad + grnd) >> gshift, diff), bdmax);
+            if (gdf) {
+                int diff = e0 * gscale;
+                v0 = clip_px_(v0 + apply_sign_(((diff < 0 ? -diff : diff) + grnd) >> gshift, diff), bdmax);
+                diff = e1 * gscale;
+                v1 = clip_px_(v1 + apply_sign_(((diff < 0 ? -diff : diff) + grnd) >> gshift, diff), bdmax);
             }
-            Lp[(int64_t)(g.y0 + ro + y) * stride + g.x0 + x] = (P)v;
         }
-}
-
-// Per-frame kernel: one CTA per work item (the hardware hands items to SMs
-// as CTAs finish, which balances light and heavy items).
-constexpr int LR_FRAME_NT = 256;
-template <typename P>
-__global__ void __launch_bounds__(LR_FRAME_NT, 4) lr_kernel(const DevFrame f) {
-    pdl_trigger();
-    __shared__ LrSmem sm;
-    lr_unit<P, LR_FRAME_NT>(f, sm, blockIdx.x);
-}
-
-// Persistent kernel over a cross-frame work list: item = frame << 22 |
-// per-frame item index.
-// (one call per sample type, kept out of line so the two instantiations do
-// not share one register allocation)
-__device__ __noinline__ void lr_unit_hbd(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint16_t, 256>(f, sm, b); }
-__device__ __noinline__ void lr_unit_8(const DevFrame &f, LrSmem &sm, int b) { lr_unit<uint8_t, 256>(f, sm, b); }
-
-__global__ void __launch_bounds__(256, 4) lr_batch_kernel(BatchArgs a) {
-    pdl_trigger();
-    __shared__ LrSmem sm;
-    const int n = a.count[2];
-    for (int w = blockIdx.x; w < n; w += gridDim.x) {
-        const uint32_t it = a.work[2][w];
-        const DevFrame &f = a.frames[it >> 22];
-        if (f.bitdepth > 8)
-            lr_unit_hbd(f, sm, it & 0x3fffff);
+        if (sizeof(P) == 2)
+            *reinterpret_cast<uint32_t *>(Lp + (int64_t)y * stride + x1) = (uint32_t)v0 | ((uint32_t)v1 << 16);
         else
-            lr_unit_8(f, sm, it & 0x3fffff);
-        __syncthreads();
+            *reinterpret_cast<uint16_t *>(Lp + (int64_t)y * stride + x1) = (uint16_t)(v0 | (v1 << 8));
     }
 }
 
+// Filters one staged chroma item: NS-Wiener with 6 chroma taps and 12
+// cross-component taps on the downsampled luma (ns_wiener_single_uv
+// :1145-1430).
+template <typename P>
+R2G_D void filter_chroma(const DevFrame &f, LrSmem &sm, int plane, int x0, int y0, int ro, int nr, int uw, int c0,
+                         int c1, int tid) {
+    const int warp = tid >> 5, lane = tid & 31;
+    const int bdmax = f.bdmax;
+    const int64_t stride = f.stride[1];
+    P *Lp = plane_ptr<P>(f.L[plane]) + (int64_t)(y0 + ro) * stride + x0;
+    const int x = 2 * lane;
+    if (x >= uw) return;
+    for (int y = warp; y < nr; y += NCW) {
+        const uint32_t *w = &sm.u.ch.win[(y + 2) * CW2 + x + 2];
+        const uint32_t *l = &sm.u.ch.lwin[(y + 2) * CW2 + x + 2];
+        const uint32_t mm = w[0];
+        int v0 = ulo(mm), v1 = uhi(mm);
+        const bool ll = (sm.llm[(ro + y) >> 2] >> (x >> 2)) & 1;
+        if (!ll) {
+            const uint32_t lm = l[0];
+            int s0 = v0 * c0 - ulo(lm) * c1, s1 = v1 * c0 - uhi(lm) * c1;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const int o = TapsY::uv[k][0] * CW2 + TapsY::uv[k][1];
+                const uint32_t t = w[o] + w[-o];
+                const int fk = sm.f[k];
+                s0 += ulo(t) * fk;
+                s1 += uhi(t) * fk;
+            }
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const int o = TapsY::uvy[k][0] * CW2 + TapsY::uvy[k][1];
+                const uint32_t t = l[o];
+                const int fk = sm.f[6 + k];
+                s0 += ulo(t) * fk;
+                s1 += uhi(t) * fk;
+            }
+            v0 = clip_px_((s0 + 64) >> 7, bdmax);
+            v1 = clip_px_((s1 + 64) >> 7, bdmax);
+        }
+        if (sizeof(P) == 2)
+            *reinterpret_cast<uint32_t *>(Lp + (int64_t)y * stride + x) = (uint32_t)v0 | ((uint32_t)v1 << 16);
+        else
+            *reinterpret_cast<uint16_t *>(Lp + (int64_t)y * stride + x) = (uint16_t)(v0 | (v1 << 8));
+    }
+}
+
+// One consumed item: tables, window, slot release, filtering.
+template <typename P>
+R2G_D void consume_item(const DevFrame &f, LrSmem &sm, int s, int tid) {
+    const LrDesc &d = sm.desc[s];
+    const int fi = d.fi, plane = d.plane, x0 = d.x0, y0 = d.y0, sh = d.sh, ro = d.ro, nr = d.nr, uw = d.uw;
+    const int edges = d.edges, kind = d.kind, c0 = d.c0, c1 = d.c1;
+    const bool gdf = d.gdf, copy = d.copy;
+    const unsigned char *raw = sm.raw[s];
+    if (copy) {
+        copy_unit<P>(f, raw, plane, x0, y0 + ro, nr, uw, tid);
+        __syncwarp();
+        if ((tid & 31) == 0) mbar_arrive(&sm.empty[s]);
+        return;
+    }
+    const int staged = stage_tables(f, fi, sm, gdf, kind == W_PC, kind == W_NS_MULTI, tid);
+    if (tid < 18) {
+        sm.llm[tid] = d.llm[tid];
+        sm.noskip[tid] = d.noskip[tid];
+        sm.f[tid] = d.f[tid];
+    }
+    if (plane == 0)
+        build_luma_window<P>(sm, raw, nr, uw, edges, tid);
+    else
+        build_chroma_windows<P>(sm, raw, nr, uw, edges, kind == W_NS_SINGLE, f.fp.cfl_ds_filter_index, tid);
+    __syncwarp();
+    if ((tid & 31) == 0) mbar_arrive(&sm.empty[s]);
+    bar_sync_n(NCT);
+    if (tid == 0 && staged) commit_tables(f, fi, sm, staged);
+    if (plane == 0)
+        filter_luma<P>(f, sm, x0, y0, sh, ro, nr, uw, kind, gdf, c0, tid);
+    else
+        filter_chroma<P>(f, sm, plane, x0, y0, ro, nr, uw, c0, c1, tid);
+}
+
+// The consumer warps: slots in publication order until the stop marker.
+template <int HB, typename Src>
+R2G_D void lr_consumers(const Src &src, LrSmem &sm, int tid) {
+    for (int k = 0;; k++) {
+        const int s = k & 1;
+        const bool got = mbar_wait(&sm.full[s], (k >> 1) & 1);
+        // one vote per item: the previous item is finished by every consumer
+        // and all of them saw the slot (or all stop)
+        if (bar_or(!got, NCT)) {
+            if (tid == 0) atomicAdd(src.fault(), 1u);
+            return;
+        }
+        if (sm.desc[s].b < 0) return;
+        const DevFrame &f = src.frame(sm.desc[s].fi);
+        if (is_hbd<HB>(f))
+            consume_item<uint16_t>(f, sm, s, tid);
+        else
+            consume_item<uint8_t>(f, sm, s, tid);
+    }
+}
+
+template <int HB, typename Src>
+R2G_D void lr_run(const Src &src, LrSmem &sm) {
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&sm.full[0], 1);
+        mbar_init(&sm.full[1], 1);
+        mbar_init(&sm.empty[0], NCW);
+        mbar_init(&sm.empty[1], NCW);
+        sm.gdf_key = sm.pc_key = sm.nsm_key = -1;
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid >= NCT) {
+        lr_producer<HB>(src, sm, tid & 31);
+    } else {
+        src.prologue(sm, tid);
+        pdl_wait();
+        lr_consumers<HB>(src, sm, tid);
+    }
+}
+
+// Work sources: one frame (kernel parameter) or a batch's LR work list.
+struct FrameSrc {
+    const DevFrame *f;
+    int n;
+    R2G_D int count() const { return n; }
+    R2G_D const DevFrame &frame(int) const { return *f; }
+    R2G_D void item(int w, int &fi, int &b) const {
+        fi = 0;
+        b = w;
+    }
+    R2G_D StageSched *sched() const { return f->sched + 2; }
+    R2G_D unsigned *fault() const { return f->fault; }
+    // the frame's tables, staged before the dependency wait
+    R2G_D void prologue(LrSmem &sm, int tid) const {
+        const bool gdf = (f->inloop & R2G_INLOOP_GDF) && f->fp.gdf_enabled;
+        const int rt = f->fp.restoration[0].restoration_type;
+        const bool pc = (f->inloop & R2G_INLOOP_WIENER) && (rt == R2G_RESTORE_PC_WIENER || rt == R2G_RESTORE_SWITCHABLE);
+        const bool nsm = (f->inloop & R2G_INLOOP_WIENER) && f->fp.restoration[0].frame_filters_on &&
+                         f->fp.restoration[0].num_classes != 1;
+        const int staged = stage_tables(*f, 0, sm, gdf, pc, nsm, tid);
+        bar_sync_n(NCT);
+        if (tid == 0 && staged) commit_tables(*f, 0, sm, staged);
+    }
+};
+struct BatchSrc {
+    const BatchArgs *a;
+    R2G_D int count() const { return a->count[2]; }
+    R2G_D const DevFrame &frame(int fi) const { return a->frames[fi]; }
+    R2G_D void item(int w, int &fi, int &b) const {
+        const uint32_t it = a->work[2][w];
+        fi = (int)(it >> 22);
+        b = (int)(it & 0x3fffff);
+    }
+    R2G_D StageSched *sched() const { return a->sched + 2; }
+    R2G_D unsigned *fault() const { return a->fault; }
+    R2G_D void prologue(LrSmem &, int) const {}
+};
+
+template <typename P>
+__global__ void __launch_bounds__(LR_NT, 3) lr_kernel(const __grid_constant__ DevFrame f, int n) {
+    pdl_trigger();
+    extern __shared__ __align__(128) unsigned char lr_smem[];
+    LrSmem &sm = *reinterpret_cast<LrSmem *>(lr_smem);
+    FrameSrc src{&f, n};
+    lr_run<sizeof(P) == 2 ? 1 : 0>(src, sm);
+}
+
+__global__ void __launch_bounds__(LR_NT, 3) lr_batch_kernel(const __grid_constant__ BatchArgs a) {
+    pdl_trigger();
+    extern __shared__ __align__(128) unsigned char lr_smem[];
+    LrSmem &sm = *reinterpret_cast<LrSmem *>(lr_smem);
+    BatchSrc src{&a};
+    lr_run<2>(src, sm);
+}
 
 // ---- DSP-context slot kernel (r2g_dsp_gdf_add): gdf_add
 // (looprestoration.rs:273-329) on a w x h block ----
@@ -724,28 +1103,56 @@ __global__ void dsp_gdf_add_kernel(uint16_t *p, const int8_t *err, int w, int h,
     }
 }
 
+// Per device: dynamic shared memory opted in, SM count and CTAs per SM.
+struct LrLaunchInfo {
+    std::atomic<int> ready{0};
+    int sms = 0, occ[3] = {0, 0, 0};
+};
+LrLaunchInfo g_lr_info[64];
+
+const LrLaunchInfo &lr_info() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    LrLaunchInfo &li = g_lr_info[dev & 63];
+    if (!li.ready.load(std::memory_order_acquire)) {
+        const int bytes = (int)sizeof(LrSmem);
+        cudaFuncSetAttribute(lr_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(lr_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(lr_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaDeviceGetAttribute(&li.sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&li.occ[0], lr_kernel<uint8_t>, LR_NT, bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&li.occ[1], lr_kernel<uint16_t>, LR_NT, bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&li.occ[2], lr_batch_kernel, LR_NT, bytes);
+        for (int &o : li.occ)
+            if (o < 1) o = 1;
+        li.ready.store(1, std::memory_order_release);
+    }
+    return li;
+}
+
 }  // namespace
 
 void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s) {
-    r2g_launch_pdl(lr_batch_kernel, dim3(grid), dim3(256), s, a);
+    lr_info();
+    r2g_launch_pdl_smem(lr_batch_kernel, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, a);
 }
-int r2g_batch_occupancy_lr() {
-    int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lr_batch_kernel, 256, 0);
-    return nb;
-}
+int r2g_batch_occupancy_lr() { return lr_info().occ[2]; }
 int r2g_lr_items(const DevFrame &f) {
     if (!f.lr_on) return 0;
-    return (f.sbh + 1) * (64 / f.lr_rows) * ((f.w + 63) >> 6) + 2 * (f.sbh + 1) * ((f.cw + 63) >> 6);
+    return (f.sbh + 1) * (64 / f.lr_rows) * ((f.w + 63) >> 6) + 2 * (f.sbh + 1) * 2 * ((f.cw + 63) >> 6);
 }
 
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     if (!f.lr_on) return 0;
-    int n = r2g_lr_items(f);
-    if (f.bitdepth > 8)
-        r2g_launch_pdl(lr_kernel<uint16_t>, dim3(n), dim3(LR_FRAME_NT), s, f);
+    const LrLaunchInfo &li = lr_info();
+    const int n = r2g_lr_items(f);
+    const int hbd = f.bitdepth > 8;
+    int grid = li.sms * li.occ[hbd];
+    if (grid > n) grid = n;
+    if (hbd)
+        r2g_launch_pdl_smem(lr_kernel<uint16_t>, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, f, n);
     else
-        r2g_launch_pdl(lr_kernel<uint8_t>, dim3(n), dim3(LR_FRAME_NT), s, f);
+        r2g_launch_pdl_smem(lr_kernel<uint8_t>, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, f, n);
     return 1;
 }
 

@@ -9,6 +9,14 @@
 #define R2G_HD __host__ __device__ __forceinline__
 #define R2G_D __device__ __forceinline__
 
+// Per-stage work counters of the persistent stage kernels (two words: the
+// next dynamic item, and CTAs finished).  A CTA takes blockIdx.x first, then
+// gridDim.x + atomicAdd(next); the last CTA to finish resets both words, so
+// every launch starts from zero without a memset.
+struct StageSched {
+    unsigned next, done;
+};
+
 // Device addresses of the AV2 constant tables (defined once in tables.cu).
 struct DevTables {
     const int8_t *CDEF_DIRECTIONS;          // [12][2]
@@ -67,6 +75,11 @@ struct DevFrame {
     // tile shape of the loop-restoration work items: luma rows per item (32,
     // or 16 for four lighter items per stripe); set by the batch autotuner
     int lr_rows;
+    // per-stage work counters of the persistent kernels (per-frame launches;
+    // the batched path keeps its own) and the context's device fault word
+    // (bounded waits that ran out)
+    StageSched *sched;
+    unsigned *fault;
     DevTables tab;
     R2gFrameParams fp;
 };
@@ -115,6 +128,8 @@ struct BatchArgs {
     const uint32_t *work[4];
     const int *count;  // [0..3] items per stage, [4] grained frames
     const GrainBatch *grain;
+    StageSched *sched;  // [4] work counters of the batch's stage kernels
+    unsigned *fault;
 };
 void r2g_batch_launch_grain_template(const BatchArgs &a, int grid, cudaStream_t s);
 void r2g_batch_launch_grain_apply(const BatchArgs &a, int grid, cudaStream_t s);
@@ -155,6 +170,89 @@ void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int sc
 void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling,
                                    cudaStream_t s);
 
+// ---- asynchronous staging: bulk copies (TMA engine) + mbarriers ----
+// A producer warp copies each work item's rows from global memory into
+// shared memory with cp.async.bulk (one instruction per row, 16-byte aligned
+// addresses and sizes), completing on an mbarrier that counts the bytes;
+// consumer warps wait on that barrier and release the buffer through a
+// second one.  Every wait is bounded (R2G_WAIT_NS): a wait that runs out
+// reports failure so the kernel can record a fault and stop instead of
+// spinning forever.
+constexpr unsigned long long R2G_WAIT_NS = 1000000000ull;  // 1 s
+
+R2G_D uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+R2G_D void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// makes the initialised barriers visible to the other threads and to the
+// asynchronous proxy (before the CTA-wide barrier that follows it)
+R2G_D void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+R2G_D void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+R2G_D void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+R2G_D bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+R2G_D uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Waits for the phase of `bar` with the given parity to complete; false when
+// it has not completed within R2G_WAIT_NS.
+R2G_D bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 32; i++)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > R2G_WAIT_NS) return false;
+    }
+}
+// global -> shared bulk copy of `bytes` (multiple of 16; both addresses
+// 16-byte aligned) completing on `bar`; never multicast
+R2G_D void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// orders this thread's earlier shared-memory accesses before its later
+// asynchronous-proxy (bulk copy) accesses
+R2G_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// barrier among the first `n` threads (the consumer warps) on named barrier
+// 1; returns whether `pred` was true in any of them
+R2G_D bool bar_or(int pred, int n) {
+    uint32_t any;
+    asm volatile(
+        "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.or.pred q, 1, %2, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(any)
+        : "r"(pred), "r"(n)
+        : "memory");
+    return any != 0;
+}
+R2G_D void bar_sync_n(int n) { asm volatile("bar.sync 1, %0;\n" ::"r"(n) : "memory"); }
+
+// (StageSched: see the definition near DevFrame.)
+R2G_D void sched_retire(StageSched *s) {
+    __threadfence();
+    if (atomicAdd(&s->done, 1u) == gridDim.x - 1) {
+        atomicExch(&s->next, 0u);
+        atomicExch(&s->done, 0u);
+    }
+}
+
 // ---- programmatic dependent launch (per-frame kernels) ----
 // A per-frame kernel is launched so that it may start while the previous
 // kernel on the stream finishes: it does its prologue (work that reads only
@@ -167,6 +265,22 @@ R2G_D void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 R2G_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::); }
 
 bool r2g_pdl_enabled();
+
+template <typename... Exp, typename... Act>
+inline cudaError_t r2g_launch_pdl_smem(void (*kern)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                       Act &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = r2g_pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<Act &&>(args)...);
+}
 
 template <typename... Exp, typename... Act>
 inline cudaError_t r2g_launch_pdl(void (*kern)(Exp...), dim3 grid, dim3 block, cudaStream_t s, Act &&...args) {

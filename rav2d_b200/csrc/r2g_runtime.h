@@ -49,7 +49,13 @@ struct R2gCtx {
     std::vector<ProfRun> prof;
     double prof_ms[R2G_N_STAGES] = {0};
     int64_t prof_launches[R2G_N_STAGES] = {0};
+    // device control block: work counters of the per-frame persistent stage
+    // kernels, then the fault word (bounded waits that ran out)
+    StageSched *sched = nullptr;
+    unsigned *fault = nullptr;
 };
+// bytes of the context's device control block
+#define R2G_CTL_BYTES 256
 
 struct R2gFrame {
     int w = 0, h = 0, bd = 8;

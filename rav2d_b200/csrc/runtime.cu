@@ -93,7 +93,26 @@ extern "C" int r2g_ctx_create(int device, int64_t mem_budget, R2gCtx **out) {
         delete ctx;
         return R2G_E_DEVICE;
     }
+    void *ctl = nullptr;
+    if (cudaMalloc(&ctl, R2G_CTL_BYTES) != cudaSuccess || cudaMemset(ctl, 0, R2G_CTL_BYTES) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctl) cudaFree(ctl);
+        cudaStreamDestroy(ctx->stream);
+        cudaStreamDestroy(ctx->side_stream);
+        delete ctx;
+        return R2G_E_DEVICE;
+    }
+    ctx->sched = (StageSched *)ctl;
+    ctx->fault = (unsigned *)((char *)ctl + 128);
     *out = ctx;
+    return R2G_OK;
+}
+
+extern "C" int r2g_ctx_device_faults(R2gCtx *ctx, uint32_t *count) {
+    if (!ctx || !count) return R2G_E_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess ||
+        cudaMemcpy(count, ctx->fault, sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return R2G_E_DEVICE;
     return R2G_OK;
 }
 
@@ -116,6 +135,7 @@ extern "C" int r2g_ctx_destroy(R2gCtx *ctx) {
         if (e) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->own_stream ? ctx->own_stream : ctx->stream);
     cudaStreamDestroy(ctx->side_stream);
+    if (ctx->sched) cudaFree(ctx->sched);
     delete ctx;
     return R2G_OK;
 }
@@ -359,6 +379,13 @@ extern "C" int r2g_sync(R2gCtx *ctx) {
     CK(cudaStreamSynchronize(ctx->stream));
     for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
         if (st) CK(cudaStreamSynchronize(st));
+    // a stage kernel whose bounded wait ran out left its work incomplete
+    uint32_t faults = 0;
+    CK(cudaMemcpy(&faults, ctx->fault, sizeof(faults), cudaMemcpyDeviceToHost));
+    if (faults) {
+        set_err(ctx, "%s", (std::to_string(faults) + " device-side waits ran out; the filtered output is incomplete").c_str());
+        return R2G_E_DEVICE;
+    }
     return R2G_OK;
 }
 
@@ -436,6 +463,8 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
     d.stride[1] = f->stride[1] / bps;
     d.fp = *fp;
     d.tab = ctx->tab;
+    d.sched = ctx->sched;
+    d.fault = ctx->fault;
     d.inloop = inloop;
     d.deblock_on = (inloop & R2G_INLOOP_DEBLOCK) && (fp->deblock_level_y[0] || fp->deblock_level_y[1]);
     d.cdef_stage_on = fp->seq_cdef && (inloop & (R2G_INLOOP_CDEF | R2G_INLOOP_CCSO));

@@ -65,6 +65,7 @@ def lib():
         L.r2g_ctx_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         L.r2g_ctx_profile.argtypes = [C.c_void_p, C.c_int]
         L.r2g_ctx_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
+        L.r2g_ctx_device_faults.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
         L.r2g_ctx_launch_count.argtypes = [C.c_void_p]
         L.r2g_ctx_launch_count.restype = C.c_int64
         L.r2g_batch_config.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int]
@@ -152,6 +153,12 @@ class Context:
 
     def launch_count(self):
         return lib().r2g_ctx_launch_count(self.h)
+
+    def device_faults(self):
+        """Bounded device-side waits that ran out so far (0 when healthy)."""
+        n = C.c_uint32()
+        self.check(lib().r2g_ctx_device_faults(self.h, C.byref(n)))
+        return n.value
 
     def frame(self, width, height, bitdepth):
         return Frame(self, width, height, bitdepth)
