@@ -915,8 +915,96 @@ void lr_sbrow_apply(Frame &f, int sby, uint32_t inloop) {
 
 }  // namespace r2o
 
+namespace r2o {
+/* looprestoration.rs:1820-1839 backup_nxu: the n samples left of src_off on
+ * each of u rows into columns 6-n .. 5 of [6]-wide rows (bounds-checked as
+ * the reference does) */
+static void backup_nxu(Left6 *dst, size_t dst_len, const pixel *src, size_t src_len, size_t src_off,
+                       ptrdiff_t src_stride, int u, size_t n) {
+    size_t abs_stride = (size_t)(src_stride < 0 ? -src_stride : src_stride);
+    size_t di = 0, si = src_off;
+    while (u > 0) {
+        if (di < dst_len && si >= n && si + n <= src_len)
+            for (size_t i = 0; i < n; i++) dst[di][6 - n + i] = src[si - n + i];
+        di++;
+        si += abs_stride;
+        u--;
+    }
+}
+/* looprestoration.rs:1841-1845 copy_n_lines */
+static void copy_n_lines(pixel *dst, size_t dst_len, const pixel *src, size_t src_len, ptrdiff_t stride, size_t n) {
+    size_t len = (size_t)(stride < 0 ? -stride : stride) * n;
+    size_t copy_len = len < dst_len ? len : dst_len;
+    if (src_len < copy_len) copy_len = src_len;
+    memcpy(dst, src, sizeof(pixel) * copy_len);
+}
+}  // namespace r2o
+
 /* ---- known-answer-test hooks (the reference's looprestoration.rs tests) ---- */
 extern "C" {
+/* Constant tables and flags by name: which = 0 PC_WIENER_NORMALIZER[i],
+ * 1 WIENER_NS_CONFIG_Y[i][k], 2 WIENER_NS_CONFIG_UV[i][k],
+ * 3 WIENER_NS_CONFIG_UV_FROM_Y[i][k], 4 PC_WIENER_CONFIG[i][k],
+ * 5 GDF_COORDS[i][k], 6 LR_HAVE_* flag i (0 left .. 3 bottom), 7 MODE_OFFSETS[i];
+ * i = -1 returns the table's length. */
+int r2o_lr_const(int which, int i, int k) {
+    using namespace r2o;
+    switch (which) {
+        case 0: return i < 0 ? 4 : PC_WIENER_NORMALIZER[i];
+        case 1: return i < 0 ? 16 : WIENER_NS_CONFIG_Y[i][k];
+        case 2: return i < 0 ? 6 : WIENER_NS_CONFIG_UV[i][k];
+        case 3: return i < 0 ? 12 : WIENER_NS_CONFIG_UV_FROM_Y[i][k];
+        case 4: return i < 0 ? 12 : PC_WIENER_CONFIG[i][k];
+        case 5: return i < 0 ? 18 : GDF_COORDS[i][k];
+        case 6: {
+            static const int fl[4] = {LR_HAVE_LEFT, LR_HAVE_RIGHT, LR_HAVE_TOP, LR_HAVE_BOTTOM};
+            return i < 0 ? 4 : fl[i];
+        }
+        case 7: return i < 0 ? 4 : MODE_OFFSETS[i];
+    }
+    return 0;
+}
+void r2o_backup_row(uint16_t *dst, int o, const uint16_t *src, int64_t src_o, const uint16_t *left, int left_off,
+                    int w, int edge_len, int edges) {
+    r2o::backup_row(dst, o, src, src_o, left, left_off, w, edge_len, edges);
+}
+void r2o_backup_row_lpf(uint16_t *dst, int o, const uint16_t *src, int64_t src_o, int w, int edge_len, int edges) {
+    r2o::backup_row_lpf(dst, o, src, src_o, w, edge_len, edges);
+}
+/* rows: an array of row pointers, as the reference's &[&[P]] */
+void r2o_compute_gradient_row(uint16_t *dst_x4, const uint16_t *const *rows, int row_off, int col_off, int w,
+                              uint32_t shift) {
+    r2o::compute_gradient_row((uint16_t(*)[4])dst_x4, rows, row_off, col_off, w, shift);
+}
+int r2o_get_class_lut_idx(const uint16_t *const *rows, int row_center, int col_off, const uint16_t *noskip_mask,
+                          int base_q, int bx, int by, int bh, int bitdepth_min_8) {
+    return r2o::get_class_lut_idx(rows, row_center, col_off, noskip_mask, base_q, bx, by, bh, bitdepth_min_8);
+}
+void r2o_ns_wiener_single_uv(uint16_t *p, int64_t p_off, int64_t stride, const uint16_t *left_6, const uint16_t *lpf,
+                             int64_t lpf_off, const uint16_t *lpf_bottom, int64_t lpf_bottom_off, int w, int h,
+                             const int8_t *filter18, const uint16_t *luma, int64_t luma_off, int64_t lstride,
+                             const uint16_t *luma_top, int64_t luma_top_off, const uint16_t *luma_bottom,
+                             int64_t luma_bottom_off, int ss_hor, int ss_ver, int ds_flt, int edges,
+                             const uint16_t *ll_mask_x4, int bitdepth) {
+    r2o::ns_wiener_single_uv(p, p_off, stride, (const r2o::Left6 *)left_6, lpf, lpf_off, lpf_bottom, lpf_bottom_off,
+                             w, h, filter18, luma, luma_off, lstride, luma_top, luma_top_off, luma_bottom,
+                             luma_bottom_off, ss_hor, ss_ver, ds_flt, edges, (const uint16_t(*)[4])ll_mask_x4,
+                             bitdepth);
+}
+void r2o_gdf_prep(int8_t *dst, int dst_stride, const uint16_t *p, int64_t p_off, int64_t stride,
+                  const uint16_t *left_6, const uint16_t *lpf, int64_t lpf_off, const uint16_t *lpf_bottom,
+                  int64_t lpf_bottom_off, int w, int h, int ref_dst_idx, int qp_idx, int edges, int bitdepth) {
+    r2o::gdf_prep(dst, dst_stride, p, p_off, stride, (const r2o::Left6 *)left_6, lpf, lpf_off, lpf_bottom,
+                  lpf_bottom_off, w, h, ref_dst_idx, qp_idx, edges, bitdepth);
+}
+void r2o_backup_nxu(uint16_t *dst_x6, int64_t dst_len, const uint16_t *src, int64_t src_len, int64_t src_off,
+                    int64_t src_stride, int u, int64_t n) {
+    r2o::backup_nxu((r2o::Left6 *)dst_x6, dst_len, src, src_len, src_off, src_stride, u, n);
+}
+void r2o_copy_n_lines(uint16_t *dst, int64_t dst_len, const uint16_t *src, int64_t src_len, int64_t stride,
+                      int64_t n) {
+    r2o::copy_n_lines(dst, dst_len, src, src_len, stride, n);
+}
 /* looprestoration.rs:273-329 gdf_add */
 void r2o_gdf_add(uint16_t *p, int64_t stride, const int8_t *err, int err_stride, int w, int h, int scale,
                  const uint16_t *ll_mask_x4, int bitdepth) {
