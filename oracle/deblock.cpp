@@ -568,19 +568,22 @@ void deblock_sbrow_rows(Frame &f, size_t mask_row, int sby) {
     }
 }
 
-/* deblock.rs:688-729 backup_db (n_tc == 1) */
+/* deblock.rs:688-729 backup_db (the filter pass runs it with n_tc = 1) */
 void backup_db(pixel *dst, const pixel *src, ptrdiff_t stride, int ss_ver, bool sb128, int row,
-               int row_h, int w, bool lr_backup) {
+               int row_h, int w, bool lr_backup, int n_tc) {
     int cdef_backup = !lr_backup;
     int sb128_i = sb128;
     int stripe_h = ((64 << (cdef_backup & sb128_i)) - 8 * (row == 0)) >> ss_ver;
     ptrdiff_t src_off = (ptrdiff_t)(stripe_h - 2) * stride;
     ptrdiff_t dst_off = 0;
-    if (row > 0) {
-        int top = 4 << sb128_i;
-        for (int i = 0; i < 4; i++) memmove(dst + dst_off + i * stride, dst + dst_off + (top + i) * stride, w * sizeof(pixel));
+    if (n_tc == 1) {
+        if (row > 0) {
+            int top = 4 << sb128_i;
+            for (int i = 0; i < 4; i++)
+                memmove(dst + dst_off + i * stride, dst + dst_off + (top + i) * stride, w * sizeof(pixel));
+        }
+        dst_off += 4 * stride;
     }
-    dst_off += 4 * stride;
     while (row + stripe_h <= row_h) {
         for (int i = 0; i < 4; i++) {
             memcpy(dst + dst_off, src + src_off, w * sizeof(pixel));
@@ -604,7 +607,7 @@ void copy_db(Frame &f, int sby) {
     bool lr_backup = f.restore_planes != 0;
     if (y_stripe < row_h)
         backup_db(f.lr_db_line[0].data(), f.p[0] + (ptrdiff_t)y_stripe * f.stride[0], f.stride[0], 0,
-                  sb128, y_stripe, row_h, w, lr_backup);
+                  sb128, y_stripe, row_h, w, lr_backup, 1);
     if (f.stride[1] != 0) {
         int cw = w >> SS_HOR;
         int ch = (f.bh * 4) >> SS_VER;
@@ -614,9 +617,9 @@ void copy_db(Frame &f, int sby) {
         if (cy_stripe < crow_h) {
             ptrdiff_t o = (ptrdiff_t)cy_stripe * f.stride[1];
             backup_db(f.lr_db_line[1].data(), f.p[1] + o, f.stride[1], SS_VER, sb128, cy_stripe,
-                      crow_h, cw, lr_backup);
+                      crow_h, cw, lr_backup, 1);
             backup_db(f.lr_db_line[2].data(), f.p[2] + o, f.stride[1], SS_VER, sb128, cy_stripe,
-                      crow_h, cw, lr_backup);
+                      crow_h, cw, lr_backup, 1);
         }
     }
 }
@@ -632,8 +635,55 @@ void r2o_setup_thr_cols(uint16_t *q_thr, uint16_t *side_thr, const uint8_t *segm
                         (const uint32_t(*)[16])thr_lut_2x16, left_q, left_side, y64, ss_ver, w4, h4);
 }
 void r2o_backup_db(uint16_t *dst, const uint16_t *src, int64_t stride, int ss_ver, int sb128, int row, int row_h,
-                   int w, int lr_backup) {
-    r2o::backup_db(dst, src, stride, ss_ver, sb128 != 0, row, row_h, w, lr_backup != 0);
+                   int w, int lr_backup, int n_tc) {
+    r2o::backup_db(dst, src, stride, ss_ver, sb128 != 0, row, row_h, w, lr_backup != 0, n_tc);
+}
+/* deblock.rs:6-11 constant tables: which 0 MAX_WIDTH_Y, 1 MAX_WIDTH_UV,
+ * 2 Q_FIRST, 3 Q_THRESH_MULTS, 4 W_MULT; i = -1 gives the length */
+int r2o_deblock_const(int which, int i) {
+    using namespace r2o;
+    switch (which) {
+        case 0: return i < 0 ? 4 : MAX_WIDTH_Y[i];
+        case 1: return i < 0 ? 3 : MAX_WIDTH_UV[i];
+        case 2: return i < 0 ? 3 : Q_FIRST[i];
+        case 3: return i < 0 ? 8 : Q_THRESH_MULTS[i];
+        case 4: return i < 0 ? 8 : W_MULT[i];
+    }
+    return 0;
+}
+/* deblock.rs:13-33 / :35-57: lut [2][16] (y) or [2][2][16] (uv) */
+void r2o_init_deblock_thr_lut_y(const R2gFrameParams *fp, int hbd, int dir, int qidx, uint32_t *lut) {
+    r2o::Frame f;
+    f.fp = fp;
+    f.hbd = hbd;
+    r2o::init_lut_y(f, dir, qidx, (uint32_t(*)[16])lut);
+}
+void r2o_init_deblock_thr_lut_uv(const R2gFrameParams *fp, int hbd, int qidx, uint32_t *lut) {
+    r2o::Frame f;
+    f.fp = fp;
+    f.hbd = hbd;
+    r2o::init_lut_uv(f, qidx, (uint32_t(*)[2][16])lut);
+}
+/* deblock.rs:303-548 deblock_{h,v}_sb64{y,uv}_bd: luma/chroma, vert = the
+ * h (vertical edge) variants */
+void r2o_deblock_sb64(uint16_t *dst, int64_t dst_off, int64_t stride, const uint16_t *vmask, const uint16_t *ll_mask,
+                      const uint16_t *q_thr, const uint16_t *side_thr, int edge, int luma, int vert, int bitdepth) {
+    r2o::BD bd;
+    bd.bitdepth = bitdepth;
+    r2o::deblock_sb64(bd, dst, dst_off, stride, vmask, ll_mask, q_thr, side_thr, edge != 0, luma != 0, vert != 0);
+}
+/* lf_mask.rs:344-358 transpose_lossless_mask; src is [rows][4] */
+void r2o_transpose_lossless_mask(uint16_t *dst17, const uint16_t *src_x4, int x64, int ss_hor, int ss_ver) {
+    r2o::transpose_lossless_mask(dst17, (const uint16_t(*)[4])src_x4, x64, ss_hor, ss_ver);
+}
+/* deblock.rs:1519-1567 setup_thr_rows (dst stride 16); above_lut NULL: no
+ * row above; its segment ids are read at seg_off - seg_stride */
+void r2o_setup_thr_rows(uint16_t *q_thr, uint16_t *side_thr, const uint8_t *segmap, int64_t seg_off,
+                        int64_t seg_stride, const uint16_t *mask_x4_5_4, const uint32_t *thr_lut_2x16,
+                        const uint32_t *above_lut_2x16, int sb64x, int ss_hor, int w4, int h4) {
+    r2o::setup_thr_rows(q_thr, side_thr, segmap, seg_off, seg_stride, (const uint16_t(*)[5][4])mask_x4_5_4, 0,
+                        (const uint32_t(*)[16])thr_lut_2x16, (const uint32_t(*)[16])above_lut_2x16,
+                        above_lut_2x16 ? segmap : nullptr, seg_off - seg_stride, sb64x, ss_hor, w4, h4);
 }
 void r2o_deblock(uint16_t *dst, int64_t off, uint32_t q_thr, uint32_t side_thr, int64_t stridea, int64_t strideb,
                  int mwp, int mwn, int pos_ll, int neg_ll, int bitdepth) {

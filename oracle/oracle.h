@@ -86,7 +86,7 @@ void deblock_sbrow_cols(Frame &f, size_t mask_row, int sby);
 void deblock_sbrow_rows(Frame &f, size_t mask_row, int sby);
 void copy_db(Frame &f, int sby);
 void backup_db(pixel *dst, const pixel *src, ptrdiff_t stride, int ss_ver, bool sb128, int row,
-               int row_h, int w, bool lr_backup);
+               int row_h, int w, bool lr_backup, int n_tc);
 
 /* cdef.cpp */
 int cdef_find_dir(const pixel *img, ptrdiff_t stride, uint32_t *var, int bd8);

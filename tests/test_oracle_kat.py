@@ -119,7 +119,7 @@ def test_backup_db_first_row_single_thread(oracle):
     for i in range(4):
         src[(54 + i) * stride:(54 + i) * stride + w] = 10 + i
     dst = np.zeros(stride * 64, np.uint16)
-    oracle.lib().r2o_backup_db(p(dst), p(src), C.c_int64(stride), 0, 0, 0, 56, w, 0)
+    oracle.lib().r2o_backup_db(p(dst), p(src), C.c_int64(stride), 0, 0, 0, 56, w, 0, 1)
     for i in range(4):
         assert (dst[(4 + i) * stride:(4 + i) * stride + w] == 10 + i).all()
 
@@ -133,7 +133,7 @@ def test_backup_db_not_first_row(oracle):
     dst = np.zeros(stride * 64, np.uint16)
     for i in range(4):
         dst[(4 + i) * stride:(4 + i) * stride + w] = 50 + i
-    oracle.lib().r2o_backup_db(p(dst), p(src), C.c_int64(stride), 0, 0, 56, 120, w, 0)
+    oracle.lib().r2o_backup_db(p(dst), p(src), C.c_int64(stride), 0, 0, 56, 120, w, 0, 1)
     assert (dst[0:w] == 50).all() and (dst[3 * stride:3 * stride + w] == 53).all()
     assert (dst[4 * stride:4 * stride + w] == 20).all() and (dst[7 * stride:7 * stride + w] == 23).all()
 
