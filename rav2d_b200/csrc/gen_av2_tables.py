@@ -40,7 +40,18 @@ TABLES = [
     ("gdf_tables.rs", "GDF_BIAS", "int16_t"),
     ("gdf_tables.rs", "GDF_INTRA_ERROR", "int8_t"),
     ("gdf_tables.rs", "GDF_INTER_ERROR", "int8_t"),
+    # block / transform geometry read by the deblock mask builder
+    # (lf_mask.rs create_db_mask, mask_edges_part)
+    ("tables.rs", "BLOCK_DIMENSIONS", "uint8_t"),
+    ("tables.rs", "TXFM_DIMENSIONS", "uint8_t"),
+    ("tables.rs", "MAX_TXFM_SIZE_FOR_BS", "uint8_t"),
+    ("tables.rs", "TX_PART_TBL", "int8_t"),
 ]
+
+# Named array lengths and struct element sizes used in the tables' Rust types
+# (levels.rs N_BS_SIZES / N_RECT_TX_SIZES; tables.rs TxfmInfo has 8 u8 fields).
+CONSTS = {"N_BS_SIZES": 31, "N_RECT_TX_SIZES": 25}
+STRUCT_FIELDS = {"TxfmInfo": 8}
 
 
 def parse_table(src: str, name: str):
@@ -68,8 +79,11 @@ def parse_table(src: str, name: str):
     t = rust_type.strip()
     while t.startswith("["):
         inner, _, n = t[1:-1].rpartition(";")
-        dims.append(int(n.strip()))
+        n = n.strip()
+        dims.append(CONSTS[n] if n in CONSTS else int(n))
         t = inner.strip()
+    if t in STRUCT_FIELDS:
+        dims.append(STRUCT_FIELDS[t])
     count = 1
     for d in dims:
         count *= d
