@@ -333,6 +333,55 @@ int r2g_dsp_ccso_add(void *dst, int64_t dst_stride, const uint8_t *idx, int64_t 
  * 1770-1779; gdf_add :273-329) in place on a w x h block, w, h <= 64. */
 int r2g_dsp_gdf_add(void *p, int64_t stride, const int8_t *err, int64_t err_stride, int w, int h, int scale,
                     const uint16_t *ll_mask, int bitdepth);
+/* WienerParamsC (looprestoration.rs:1716-1740): the per-call parameters of
+ * the WienerFilterFn slots.  Sample pointers are u8 at bitdepth 8, u16
+ * above; strides count samples. */
+typedef struct R2gWienerParamsSingle {
+    const int8_t *filter;    /* 16 taps (luma) or 6 + 12 taps (chroma) */
+    const void *luma;        /* chroma: co-located pre-LR luma at the block origin */
+    const void *luma_top;    /* chroma: the 2 saved deblocked luma rows above */
+    const void *luma_bottom; /* chroma: the 2 saved deblocked luma rows below */
+    int64_t stride;          /* luma stride */
+    int32_t ss_ver, ss_hor, ds_flt;
+} R2gWienerParamsSingle;
+typedef struct R2gWienerParamsMulti {
+    const void *filters;         /* NS multi: int8_t[class][18]; PC: int16_t[class][13] */
+    const uint8_t *subclass_lut; /* PC_WIENER_LUT_TO_CLASS class -> filter class */
+    const uint16_t *noskip_mask; /* one 16-bit row mask per 4 rows */
+    int32_t base_q;
+} R2gWienerParamsMulti;
+typedef union R2gWienerParams {
+    R2gWienerParamsSingle single;
+    R2gWienerParamsMulti multi;
+} R2gWienerParams;
+
+/* LoopRestorationDSPContext.ns_wiener_single[0] / [1], .ns_wiener_multi,
+ * .pc_wiener: the WienerFilterFn slot (looprestoration.rs:1742-1753;
+ * ns_wiener_single_y :524, ns_wiener_single_uv :1145, ns_wiener_multi
+ * :1061, pc_wiener :1102) in place on a w x h block of one stripe (w <= 64,
+ * h <= 64, multiples of 4).  `left` holds [h][6] samples (the unit to the
+ * left's pre-filter border), `top` the 2 saved deblocked rows above the
+ * stripe (row -2 first, column 0, stride dst_stride), `bottom` the 2 below
+ * (row h first); `ll_mask` [h/4 + 1][4] lossless 4x4 bits; edges as
+ * LR_HAVE_* (1 left, 2 right, 4 top, 8 bottom). */
+int r2g_dsp_ns_wiener_single_y(void *dst, int64_t dst_stride, const void *left, const void *top, const void *bottom,
+                               int w, int h, const R2gWienerParams *params, int edges, const uint16_t *ll_mask,
+                               int bitdepth);
+int r2g_dsp_ns_wiener_single_uv(void *dst, int64_t dst_stride, const void *left, const void *top,
+                                const void *bottom, int w, int h, const R2gWienerParams *params, int edges,
+                                const uint16_t *ll_mask, int bitdepth);
+int r2g_dsp_ns_wiener_multi(void *dst, int64_t dst_stride, const void *left, const void *top, const void *bottom,
+                            int w, int h, const R2gWienerParams *params, int edges, const uint16_t *ll_mask,
+                            int bitdepth);
+int r2g_dsp_pc_wiener(void *dst, int64_t dst_stride, const void *left, const void *top, const void *bottom, int w,
+                      int h, const R2gWienerParams *params, int edges, const uint16_t *ll_mask, int bitdepth);
+/* LoopRestorationDSPContext.gdf_prep: the GdfPrepFn slot (looprestoration.rs:
+ * 1755-1768; gdf_prep :1432-1640): the GDF error of every sample of the w x h
+ * luma block at p (w, h <= 64, even) into dst, with the same left / top /
+ * bottom conventions (6 left columns, 2 saved rows each side). */
+int r2g_dsp_gdf_prep(int8_t *dst, int64_t dst_stride, const void *p, int64_t stride, const void *left,
+                     const void *top, const void *bottom, int w, int h, int ref_dst_idx, int qp_idx, int edges,
+                     int bitdepth);
 /* FilmGrainDSPContext.generate_grain_y / generate_grain_uv[1] (filmgrain.rs:
  * 115-230, 4:2:0): the 82x73 luma template and the two 44x38 chroma templates
  * (top-left of 82x73 arrays); any buffer may be NULL. */

@@ -193,6 +193,24 @@ class ServeStats(C.Structure):
     ]
 
 
+class WienerParamsSingle(C.Structure):
+    """R2gWienerParamsSingle (WienerParamsSingle, looprestoration.rs:1716-1726)."""
+    _fields_ = [("filter", C.c_void_p), ("luma", C.c_void_p), ("luma_top", C.c_void_p),
+                ("luma_bottom", C.c_void_p), ("stride", C.c_int64), ("ss_ver", C.c_int32), ("ss_hor", C.c_int32),
+                ("ds_flt", C.c_int32)]
+
+
+class WienerParamsMulti(C.Structure):
+    """R2gWienerParamsMulti (WienerParamsMulti, looprestoration.rs:1728-1734)."""
+    _fields_ = [("filters", C.c_void_p), ("subclass_lut", C.c_void_p), ("noskip_mask", C.c_void_p),
+                ("base_q", C.c_int32)]
+
+
+class WienerParams(C.Union):
+    """R2gWienerParams (WienerParamsC, looprestoration.rs:1736-1740)."""
+    _fields_ = [("single", WienerParamsSingle), ("multi", WienerParamsMulti)]
+
+
 # order of r2g_struct_sizes()
 STRUCT_SIZES = [
     ("R2gAv2Filter", AV2_FILTER_DTYPE.itemsize),
@@ -206,6 +224,7 @@ STRUCT_SIZES = [
     ("R2gServeRequest", C.sizeof(ServeRequest)),
     ("R2gServeResult", C.sizeof(ServeResult)),
     ("R2gServeStats", C.sizeof(ServeStats)),
+    ("R2gWienerParams", C.sizeof(WienerParams)),
 ]
 
 

@@ -29,7 +29,7 @@ struct DspDevice {
     cudaStream_t st = nullptr;  // non-blocking: no implicit sync with the legacy stream
     DevTables tab{};
 };
-constexpr size_t kScratch = 64 * 1024;
+constexpr size_t kScratch = 128 * 1024;
 DspDevice g_dsp[64];
 std::mutex g_dsp_mu;
 
@@ -273,4 +273,430 @@ extern "C" int r2g_dsp_generate_grain(int16_t *buf_y, int16_t *buf_u, int16_t *b
                            cudaSuccess)
             return R2G_E_DEVICE;
     return finish(d, R2G_OK);
+}
+
+// ---------------------------------------------------------------------------
+// Typed loop-restoration slots (WienerFilterFn / GdfPrepFn,
+// looprestoration.rs:1716-1768).  The reference's per-block functions keep a
+// ring of backed-up rows (each row with edge_len samples of left / right
+// context, filled from `left`, the unit to the right, the saved deblocked
+// rows or by replication) and move ring pointers as they walk down the
+// block.  The host stages every row the ring would hold, in the order the
+// reference builds them, and records which staged row each ring slot points
+// at for every output row; the GPU then does all the arithmetic.
+
+namespace {
+
+enum { LRE_LEFT = 1, LRE_RIGHT = 2, LRE_TOP = 4, LRE_BOTTOM = 8 };
+
+// Staged rows: `n` rows of (w + 2e) samples, column 0 of the block at e.
+struct RowStage {
+    int w = 0, e = 0, rs = 0, n = 0;
+    std::vector<uint16_t> data;
+    RowStage(int w_, int e_) : w(w_), e(e_), rs(w_ + 2 * e_) {}
+    int add() {
+        data.resize(data.size() + rs, 0);
+        return n++;
+    }
+    uint16_t *row(int id) { return &data[(size_t)id * rs + e]; }
+};
+
+// backup_row (looprestoration.rs:54-80): src row at column 0, left[6]
+template <typename P>
+int stage_row(RowStage &st, const P *src, const P *left6, int edge_len, int edges) {
+    const int id = st.add();
+    uint16_t *d = st.row(id);
+    for (int x = 0; x < edge_len; x++) d[x - edge_len] = (edges & LRE_LEFT) ? left6[6 - edge_len + x] : src[0];
+    for (int x = 0; x < st.w; x++) d[x] = src[x];
+    for (int x = 0; x < edge_len; x++) d[st.w + x] = (edges & LRE_RIGHT) ? src[st.w + x] : src[st.w - 1];
+    return id;
+}
+
+// backup_row_lpf (:85-108): a saved row, its own left / right context
+template <typename P>
+int stage_row_lpf(RowStage &st, const P *src, int edge_len, int edges) {
+    const int id = st.add();
+    uint16_t *d = st.row(id);
+    for (int x = 0; x < edge_len; x++) d[x - edge_len] = (edges & LRE_LEFT) ? src[x - edge_len] : src[0];
+    for (int x = 0; x < st.w; x++) d[x] = src[x];
+    for (int x = 0; x < edge_len; x++) d[st.w + x] = (edges & LRE_RIGHT) ? src[st.w + x] : src[st.w - 1];
+    return id;
+}
+
+// backup_row_luma (:408-522, 4:2:0 and 4:4:4 arms): one downsampled luma
+// row from rows src and src + src_stride (st.w = the luma width)
+template <typename P>
+int stage_row_luma(RowStage &st, const P *src, int64_t src_stride, int edges, int ss_hor, int ss_ver, int ds) {
+    if (ss_ver == 0) return stage_row_lpf(st, src, 4, edges);
+    const int id = st.add();
+    uint16_t *d = st.row(id);
+    const int w = st.w;
+    const P *s2 = src + src_stride;
+    auto sample = [&](int x) -> int {
+        if (ds == 0) return ((int)src[x] + s2[x] + src[x + 1] + s2[x + 1]) >> 2;
+        if (ds == 1) return ((int)src[x] + s2[x]) >> 1;
+        return src[x];
+    };
+    if (ds == 0) {
+        for (int x = 0; x < w; x += 1 + ss_hor) d[x] = (uint16_t)sample(x);
+    } else {
+        for (int x = 0; x < w; x++) d[x] = (uint16_t)sample(x);
+    }
+    for (int i = 0; i < 4; i++) d[i - 4] = (edges & LRE_LEFT) ? (uint16_t)sample(i - 4) : d[0];
+    for (int i = 0; i < 4; i++) d[w + i] = (edges & LRE_RIGHT) ? (uint16_t)sample(w + i) : d[w - 2];
+    return id;
+}
+
+// ns_wiener_single_y / wiener_multi row walk (:524-713, :715-1059): FIR
+// ring slots [h][9] and, for the multi-class kinds, the classification
+// slots [h/4][10].
+template <typename P>
+void stage_wiener_y(RowStage &st, const P *p, int64_t stride, const P *left, const P *top, const P *bottom, int h,
+                    int edges, bool multi, std::vector<int> &ref, std::vector<int> &cref) {
+    auto row = [&](int y) { return stage_row(st, p + y * stride, left + 6 * y, 4, edges); };
+    int ptrs[10] = {0};
+    ptrs[4] = row(0);
+    if (edges & LRE_TOP) {
+        ptrs[2] = stage_row_lpf(st, top, 4, edges);
+        ptrs[3] = stage_row_lpf(st, top + stride, 4, edges);
+        ptrs[0] = ptrs[1] = ptrs[2];
+    } else {
+        ptrs[0] = ptrs[1] = ptrs[2] = ptrs[3] = ptrs[4];
+    }
+    ptrs[5] = row(1);
+    ptrs[6] = row(2);
+    ptrs[7] = row(3);
+    ref.assign((size_t)h * 9, 0);
+    cref.assign((size_t)(h >> 2) * 10, 0);
+    auto fir_row = [&](int y) {
+        if (y + 4 < h)
+            ptrs[8] = row(y + 4);
+        else if (y + 2 < h && (edges & LRE_BOTTOM))
+            ptrs[8] = stage_row_lpf(st, bottom + (y + 4 - h) * stride, 4, edges);
+        else
+            ptrs[8] = ptrs[7];
+        for (int i = 0; i < 9; i++) ref[(size_t)y * 9 + i] = ptrs[i];
+        for (int r = 0; r < 8; r++) ptrs[r] = ptrs[r + 1];
+    };
+    if (!multi) {
+        for (int y = 0; y < h; y++) fir_row(y);
+        return;
+    }
+    const int bh = h >> 2;
+    for (int by = 0; by < bh; by++) {
+        const int by4 = by << 2;
+        if (by + 1 < bh) {
+            ptrs[8] = row(by4 + 4);
+            ptrs[9] = row(by4 + 5);
+        } else if (edges & LRE_BOTTOM) {
+            ptrs[8] = stage_row_lpf(st, bottom, 4, edges);
+            ptrs[9] = stage_row_lpf(st, bottom + stride, 4, edges);
+        } else {
+            ptrs[8] = ptrs[9] = ptrs[7];
+        }
+        for (int i = 0; i < 10; i++) cref[(size_t)by * 10 + i] = ptrs[i];
+        for (int y = by4; y < by4 + 4; y++) fir_row(y);
+    }
+}
+
+// gdf_prep row walk (:1456-1560): gradient events (the initial one, then one
+// per even row) and per output row slots [h][13]
+template <typename P>
+void stage_gdf(RowStage &st, const P *p, int64_t stride, const P *left, const P *top, const P *bottom, int h,
+               int edges, std::vector<int> &gref, std::vector<int> &pref) {
+    auto row = [&](int y) { return stage_row(st, p + y * stride, left + 6 * y, 6, edges); };
+    int ptrs[13] = {0};
+    ptrs[6] = row(0);
+    if (edges & LRE_TOP) {
+        ptrs[4] = stage_row_lpf(st, top, 6, edges);
+        ptrs[5] = stage_row_lpf(st, top + stride, 6, edges);
+        ptrs[0] = ptrs[1] = ptrs[2] = ptrs[3] = ptrs[4];
+    } else {
+        for (int n = 0; n < 6; n++) ptrs[n] = ptrs[6];
+    }
+    for (int y = 1; y < 6; y++) ptrs[6 + y] = row(y);
+    gref.assign(ptrs, ptrs + 13);
+    pref.assign((size_t)h * 13, 0);
+    for (int y = 0; y < h; y++) {
+        if (y + 6 < h)
+            ptrs[12] = row(y + 6);
+        else if (y + 4 < h && (edges & LRE_BOTTOM))
+            ptrs[12] = stage_row_lpf(st, bottom + (y + 6 - h) * stride, 6, edges);
+        else
+            ptrs[12] = ptrs[11];
+        if ((y & 1) == 0) gref.insert(gref.end(), ptrs, ptrs + 13);
+        for (int i = 0; i < 13; i++) pref[(size_t)y * 13 + i] = ptrs[i];
+        for (int r = 0; r < 12; r++) ptrs[r] = ptrs[r + 1];
+    }
+}
+
+// ns_wiener_single_uv row walk (:1145-1430): chroma slots and downsampled
+// luma slots [h][5]
+template <typename P>
+void stage_wiener_uv(RowStage &cs, RowStage &ls, const P *p, int64_t stride, const P *left, const P *top,
+                     const P *bottom, int h, int edges, const R2gWienerParamsSingle &sp, std::vector<int> &cref,
+                     std::vector<int> &lref) {
+    const P *luma = (const P *)sp.luma, *ltop = (const P *)sp.luma_top, *lbot = (const P *)sp.luma_bottom;
+    const int64_t lstride = sp.stride;
+    const int ssh = sp.ss_hor, ssv = sp.ss_ver, ds = sp.ds_flt;
+    auto crow = [&](int y) { return stage_row(cs, p + y * stride, left + 6 * y, 2, edges); };
+    auto lrow = [&](const P *src, int64_t s2) { return stage_row_luma(ls, src, s2, edges, ssh, ssv, ds); };
+    int c[5] = {0}, l[5] = {0};
+    c[2] = crow(0);
+    if (edges & LRE_TOP) {
+        c[0] = stage_row_lpf(cs, top, 2, edges);
+        c[1] = stage_row_lpf(cs, top + stride, 2, edges);
+    } else {
+        c[0] = c[1] = c[2];
+    }
+    c[3] = crow(1);
+    l[2] = lrow(luma, lstride);
+    if (edges & LRE_TOP) {
+        l[0] = lrow(ltop, 0);
+        l[1] = lrow(ltop, lstride);
+    } else {
+        l[0] = l[1] = l[2];
+    }
+    l[3] = lrow(luma + ((int64_t)1 << ssv) * lstride, lstride);
+    cref.assign((size_t)h * 5, 0);
+    lref.assign((size_t)h * 5, 0);
+    int64_t luma_pos = 0;
+    for (int y = 0; y < h; y++) {
+        if (y + 2 < h)
+            c[4] = crow(y + 2);
+        else if (edges & LRE_BOTTOM)
+            c[4] = stage_row_lpf(cs, bottom + (y + 2 - h) * stride, 2, edges);
+        else
+            c[4] = c[3];
+        if (c[4] == c[3])
+            l[4] = l[3];
+        else if (y + 2 == h)
+            l[4] = lrow(lbot, lstride);
+        else if (y + 1 == h)
+            l[4] = lrow(lbot + lstride, 0);
+        else
+            l[4] = lrow(luma + luma_pos + ((int64_t)2 << ssv) * lstride, lstride);
+        for (int i = 0; i < 5; i++) {
+            cref[(size_t)y * 5 + i] = c[i];
+            lref[(size_t)y * 5 + i] = l[i];
+        }
+        for (int r = 0; r < 4; r++) {
+            c[r] = c[r + 1];
+            l[r] = l[r + 1];
+        }
+        luma_pos += lstride << ssv;
+    }
+}
+
+// Device scratch layout of one typed-LR call, 256-byte aligned pieces.
+struct Scratch {
+    char *base;
+    size_t off = 0, cap;
+    template <typename T>
+    T *take(size_t n) {
+        T *p = (T *)(base + off);
+        off = (off + n * sizeof(T) + 255) & ~(size_t)255;
+        return off <= cap ? p : nullptr;
+    }
+};
+
+bool lr_dims_ok(int w, int h, int wmul, int hmin) {
+    return w >= 4 && h >= hmin && w <= 64 && h <= 64 && (w % wmul) == 0 && (h & 1) == 0;
+}
+
+template <typename P>
+void load_rect(std::vector<uint16_t> &v, const P *src, int64_t stride, int w, int h) {
+    v.resize((size_t)w * h);
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) v[(size_t)y * w + x] = src[y * stride + x];
+}
+
+// Common path of the three luma Wiener slots.
+template <typename P>
+int wiener_y(DspDevice *d, void *dst, int64_t stride, const void *left, const void *top, const void *bottom, int w,
+             int h, const R2gWienerParams *params, int edges, const uint16_t *ll_mask, int bitdepth, int kind) {
+    RowStage st(w, 4);
+    std::vector<int> ref, cref;
+    stage_wiener_y<P>(st, (const P *)dst, stride, (const P *)left, (const P *)top, (const P *)bottom, h, edges,
+                      kind != 1, ref, cref);
+    const int bh = h >> 2;
+    // classes the multi-class kinds can select: the largest value in the
+    // subclass LUT bounds the caller's filter table
+    int nclass = 1;
+    std::vector<uint8_t> lut(256, 0);
+    std::vector<uint16_t> noskip(bh, 0);
+    if (kind != 1) {
+        memcpy(lut.data(), params->multi.subclass_lut, 256);
+        for (uint8_t v : lut) nclass = v + 1 > nclass ? v + 1 : nclass;
+        memcpy(noskip.data(), params->multi.noskip_mask, sizeof(uint16_t) * bh);
+    }
+    Scratch sc{d->buf, 0, kScratch};
+    uint16_t *drows = sc.take<uint16_t>(st.data.size());
+    int *dref = sc.take<int>(ref.size()), *dcref = sc.take<int>(cref.size() + 1);
+    int8_t *dtaps = sc.take<int8_t>(16 * 18);
+    int16_t *dpcf = sc.take<int16_t>(64 * 13);
+    uint8_t *dlut = sc.take<uint8_t>(256);
+    uint16_t *dns = sc.take<uint16_t>(bh + 1), *dllm = sc.take<uint16_t>((bh + 1) * 4);
+    uint16_t *dout = sc.take<uint16_t>((size_t)w * h);
+    if (!dout) return R2G_E_TOO_LARGE;
+    int taps_stride = 18;
+    cudaStream_t s = d->st;
+    bool ok = cudaMemcpyAsync(drows, st.data.data(), st.data.size() * 2, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+              cudaMemcpyAsync(dref, ref.data(), ref.size() * 4, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+              cudaMemcpyAsync(dllm, ll_mask, (bh + 1) * 4 * 2, cudaMemcpyHostToDevice, s) == cudaSuccess;
+    if (kind == 1) {
+        ok = ok && cudaMemcpyAsync(dtaps, params->single.filter, 16, cudaMemcpyHostToDevice, s) == cudaSuccess;
+    } else {
+        ok = ok && cudaMemcpyAsync(dcref, cref.data(), cref.size() * 4, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+             cudaMemcpyAsync(dlut, lut.data(), 256, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+             cudaMemcpyAsync(dns, noskip.data(), bh * 2, cudaMemcpyHostToDevice, s) == cudaSuccess;
+        if (kind == 2)
+            ok = ok && nclass <= 16 &&
+                 cudaMemcpyAsync(dtaps, params->multi.filters, (size_t)nclass * 18, cudaMemcpyHostToDevice, s) ==
+                     cudaSuccess;
+        else
+            ok = ok && nclass <= 64 &&
+                 cudaMemcpyAsync(dpcf, params->multi.filters, (size_t)nclass * 13 * 2, cudaMemcpyHostToDevice, s) ==
+                     cudaSuccess;
+    }
+    if (!ok) return R2G_E_INVALID;
+    r2g_dsp_launch_wiener_y(drows, st.rs, st.e, dref, dcref, w, h, kind, dtaps, taps_stride, dpcf, dlut, dns,
+                            kind == 1 ? 0 : params->multi.base_q, dllm, bitdepth, d->tab, dout, s);
+    std::vector<uint16_t> out((size_t)w * h);
+    if (cudaMemcpyAsync(out.data(), dout, out.size() * 2, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return R2G_E_DEVICE;
+    store_block((P *)dst, stride, out, w, h);
+    return R2G_OK;
+}
+
+template <typename P>
+int wiener_uv(DspDevice *d, void *dst, int64_t stride, const void *left, const void *top, const void *bottom, int w,
+              int h, const R2gWienerParams *params, int edges, const uint16_t *ll_mask, int bitdepth) {
+    const R2gWienerParamsSingle &sp = params->single;
+    RowStage cs(w, 2), ls(w << sp.ss_hor, 4);
+    std::vector<int> cref, lref;
+    stage_wiener_uv<P>(cs, ls, (const P *)dst, stride, (const P *)left, (const P *)top, (const P *)bottom, h, edges,
+                       sp, cref, lref);
+    const int bh = h >> 2;
+    Scratch sc{d->buf, 0, kScratch};
+    uint16_t *dc = sc.take<uint16_t>(cs.data.size()), *dl = sc.take<uint16_t>(ls.data.size());
+    int *dcr = sc.take<int>(cref.size()), *dlr = sc.take<int>(lref.size());
+    int8_t *df = sc.take<int8_t>(18);
+    uint16_t *dllm = sc.take<uint16_t>((bh + 1) * 4), *dout = sc.take<uint16_t>((size_t)w * h);
+    if (!dout) return R2G_E_TOO_LARGE;
+    cudaStream_t s = d->st;
+    if (cudaMemcpyAsync(dc, cs.data.data(), cs.data.size() * 2, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dl, ls.data.data(), ls.data.size() * 2, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dcr, cref.data(), cref.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dlr, lref.data(), lref.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(df, sp.filter, 18, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dllm, ll_mask, (bh + 1) * 4 * 2, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return R2G_E_INVALID;
+    r2g_dsp_launch_wiener_uv(dc, cs.rs, dl, ls.rs, dcr, dlr, w, h, sp.ss_hor, df, dllm, bitdepth, dout, s);
+    std::vector<uint16_t> out((size_t)w * h);
+    if (cudaMemcpyAsync(out.data(), dout, out.size() * 2, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return R2G_E_DEVICE;
+    store_block((P *)dst, stride, out, w, h);
+    return R2G_OK;
+}
+
+template <typename P>
+int gdf_prep(DspDevice *d, int8_t *dst, int64_t dst_stride, const void *p, int64_t stride, const void *left,
+             const void *top, const void *bottom, int w, int h, int ref_dst_idx, int qp_idx, int edges, int bitdepth) {
+    RowStage st(w, 6);
+    std::vector<int> gref, pref;
+    stage_gdf<P>(st, (const P *)p, stride, (const P *)left, (const P *)top, (const P *)bottom, h, edges, gref, pref);
+    const int ng = (int)(gref.size() / 13);
+    Scratch sc{d->buf, 0, kScratch};
+    uint16_t *drows = sc.take<uint16_t>(st.data.size());
+    int *dg = sc.take<int>(gref.size()), *dp = sc.take<int>(pref.size());
+    int8_t *dout = sc.take<int8_t>((size_t)w * h);
+    if (!dout) return R2G_E_TOO_LARGE;
+    cudaStream_t s = d->st;
+    if (cudaMemcpyAsync(drows, st.data.data(), st.data.size() * 2, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dg, gref.data(), gref.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dp, pref.data(), pref.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return R2G_E_DEVICE;
+    r2g_dsp_launch_gdf_prep(drows, st.rs, st.e, dg, ng, dp, w, h, ref_dst_idx, qp_idx, bitdepth, d->tab, dout, s);
+    std::vector<int8_t> out((size_t)w * h);
+    if (cudaMemcpyAsync(out.data(), dout, out.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return R2G_E_DEVICE;
+    for (int y = 0; y < h; y++) memcpy(dst + y * dst_stride, &out[(size_t)y * w], (size_t)w);
+    return R2G_OK;
+}
+
+bool lr_edges_ok(int edges) { return (edges & ~15) == 0; }
+
+int wiener_y_entry(void *dst, int64_t stride, const void *left, const void *top, const void *bottom, int w, int h,
+                   const R2gWienerParams *params, int edges, const uint16_t *ll_mask, int bitdepth, int kind) {
+    if (!dst || !params || !ll_mask || !ok_bd(bitdepth) || !lr_dims_ok(w, h, 4, 4) || (h & 3) ||
+        !lr_edges_ok(edges) || ((edges & LRE_LEFT) && !left) || ((edges & LRE_TOP) && !top) ||
+        ((edges & LRE_BOTTOM) && !bottom))
+        return R2G_E_INVALID;
+    if (kind == 1 ? !params->single.filter
+                  : (!params->multi.filters || !params->multi.subclass_lut || !params->multi.noskip_mask))
+        return R2G_E_INVALID;
+    std::lock_guard<std::mutex> lk(g_dsp_mu);
+    DspDevice *d;
+    int rc = dsp_device(&d);
+    if (rc != R2G_OK) return rc;
+    rc = bitdepth > 8 ? wiener_y<uint16_t>(d, dst, stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth, kind)
+                      : wiener_y<uint8_t>(d, dst, stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth, kind);
+    return finish(d, rc);
+}
+
+}  // namespace
+
+extern "C" int r2g_dsp_ns_wiener_single_y(void *dst, int64_t dst_stride, const void *left, const void *top,
+                                          const void *bottom, int w, int h, const R2gWienerParams *params, int edges,
+                                          const uint16_t *ll_mask, int bitdepth) {
+    return wiener_y_entry(dst, dst_stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth, 1);
+}
+extern "C" int r2g_dsp_ns_wiener_multi(void *dst, int64_t dst_stride, const void *left, const void *top,
+                                       const void *bottom, int w, int h, const R2gWienerParams *params, int edges,
+                                       const uint16_t *ll_mask, int bitdepth) {
+    return wiener_y_entry(dst, dst_stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth, 2);
+}
+extern "C" int r2g_dsp_pc_wiener(void *dst, int64_t dst_stride, const void *left, const void *top, const void *bottom,
+                                 int w, int h, const R2gWienerParams *params, int edges, const uint16_t *ll_mask,
+                                 int bitdepth) {
+    return wiener_y_entry(dst, dst_stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth, 3);
+}
+extern "C" int r2g_dsp_ns_wiener_single_uv(void *dst, int64_t dst_stride, const void *left, const void *top,
+                                           const void *bottom, int w, int h, const R2gWienerParams *params, int edges,
+                                           const uint16_t *ll_mask, int bitdepth) {
+    if (!dst || !params || !ll_mask || !ok_bd(bitdepth) || !lr_dims_ok(w, h, 4, 2) || !lr_edges_ok(edges) ||
+        ((edges & LRE_LEFT) && !left) || ((edges & LRE_TOP) && (!top || !params->single.luma_top)) ||
+        ((edges & LRE_BOTTOM) && (!bottom || !params->single.luma_bottom)) || !params->single.filter ||
+        !params->single.luma || params->single.ss_hor < 0 || params->single.ss_hor > 1 ||
+        params->single.ss_ver < 0 || params->single.ss_ver > 1 || params->single.ds_flt < 0 ||
+        params->single.ds_flt > 2)
+        return R2G_E_INVALID;
+    std::lock_guard<std::mutex> lk(g_dsp_mu);
+    DspDevice *d;
+    int rc = dsp_device(&d);
+    if (rc != R2G_OK) return rc;
+    rc = bitdepth > 8 ? wiener_uv<uint16_t>(d, dst, dst_stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth)
+                      : wiener_uv<uint8_t>(d, dst, dst_stride, left, top, bottom, w, h, params, edges, ll_mask, bitdepth);
+    return finish(d, rc);
+}
+extern "C" int r2g_dsp_gdf_prep(int8_t *dst, int64_t dst_stride, const void *p, int64_t stride, const void *left,
+                                const void *top, const void *bottom, int w, int h, int ref_dst_idx, int qp_idx,
+                                int edges, int bitdepth) {
+    if (!dst || !p || !ok_bd(bitdepth) || !lr_dims_ok(w, h, 2, 6) || !lr_edges_ok(edges) || ref_dst_idx < 0 ||
+        ref_dst_idx > 5 || qp_idx < 0 || qp_idx > 5 || ((edges & LRE_LEFT) && !left) || ((edges & LRE_TOP) && !top) ||
+        ((edges & LRE_BOTTOM) && !bottom))
+        return R2G_E_INVALID;
+    std::lock_guard<std::mutex> lk(g_dsp_mu);
+    DspDevice *d;
+    int rc = dsp_device(&d);
+    if (rc != R2G_OK) return rc;
+    rc = bitdepth > 8 ? gdf_prep<uint16_t>(d, dst, dst_stride, p, stride, left, top, bottom, w, h, ref_dst_idx, qp_idx,
+                                           edges, bitdepth)
+                      : gdf_prep<uint8_t>(d, dst, dst_stride, p, stride, left, top, bottom, w, h, ref_dst_idx, qp_idx,
+                                          edges, bitdepth);
+    return finish(d, rc);
 }

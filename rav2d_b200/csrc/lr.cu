@@ -1103,6 +1103,188 @@ __global__ void dsp_gdf_add_kernel(uint16_t *p, const int8_t *err, int w, int h,
     }
 }
 
+// ---- DSP-context slot kernels for the typed LR slots (WienerFilterFn,
+// GdfPrepFn).  The host (dsp.cu) stages the block's rows as the reference's
+// row rings hold them: `rows` is a table of staged rows of `rs` samples
+// (column 0 of the block at index e), and per output row (and per
+// classification row / gradient event) the row ids each ring slot points at.
+// One CTA computes the block; results go to `out` ([h][w]).
+
+R2G_D int trow(const uint16_t *rows, int rs, int e, int id, int x) { return (int)rows[(size_t)id * rs + e + x]; }
+
+// ns_wiener_single_y / ns_wiener_multi / pc_wiener (looprestoration.rs
+// :524-1143): ref [h][9] FIR rows (ring slot 4 = the output row), cref
+// [h/4][10] classification rows.  kind: 1 single, 2 NS multi, 3 PC.
+__global__ void dsp_wiener_y_kernel(const uint16_t *rows, int rs, int e, const int *ref, const int *cref, int w, int h,
+                                    int kind, const int8_t *taps, int taps_stride, const int16_t *pcf,
+                                    const uint8_t *sub_lut, const uint16_t *noskip, int base_q, const uint16_t *llm,
+                                    int bitdepth, const DevTables tab, uint16_t *out) {
+    __shared__ uint8_t classes[16][16];
+    const int tid = threadIdx.x, bh = h >> 2, bw = w >> 2, b8 = bitdepth - 8, bdmax = (1 << bitdepth) - 1;
+    if (kind != W_NS_SINGLE) {
+        // get_class_lut_idx (:195-271) with the ring rows of block row by
+        for (int i = tid; i < bh * bw; i += blockDim.x) {
+            const int by = i / bw, bx = i % bw;
+            const int *r = cref + by * 10;
+            int f0 = 0, f1 = 0, f2 = 0;
+            for (int dy = -1; dy <= 4; dy++)
+                for (int dx = -1; dx <= 4; dx++) {
+                    const int x = bx * 4 + dx, y = 4 + dy;
+                    const int m2 = 2 * trow(rows, rs, e, r[y], x);
+                    int t = trow(rows, rs, e, r[y - 1], x) - m2 + trow(rows, rs, e, r[y + 1], x);
+                    f0 += t < 0 ? -t : t;
+                    t = trow(rows, rs, e, r[y - 1], x + 1) - m2 + trow(rows, rs, e, r[y + 1], x - 1);
+                    f1 += t < 0 ? -t : t;
+                    t = trow(rows, rs, e, r[y - 1], x - 1) - m2 + trow(rows, rs, e, r[y + 1], x + 1);
+                    f2 += t < 0 ? -t : t;
+                }
+            const int np[3] = {16, 4, 1};
+            int s = 0;
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int fx = iclip_((bx & 15) + dx, 0, 15), fy = iclip_(by + dy, 0, bh - 1);
+                    s += np[(dy != 0) + (dx != 0)] * (((noskip[fy] >> fx) & 1) == 0);
+                }
+            const int rnd = (1 << b8) >> 1;
+            int fs[3] = {f0, f1, f2};
+            for (int k = 0; k < 3; k++) fs[k] = (int)((uint32_t)fs[k] * (uint32_t)c_pcw_norm[k] + (uint32_t)rnd) >> b8;
+            s *= c_pcw_norm[3];
+            int qv = (imax_(0, get_qval(base_q, s, 0, b8)) + (1 << 13)) >> 14;
+            int lut_idx = (imin_(qv, 255) >> 5) << 9;
+            for (int k = 0; k < 3; k++) {
+                qv = (imax_(0, fs[k] + get_qval(base_q, s, k + 1, b8)) + (1 << 13)) >> 14;
+                lut_idx |= (imin_(qv, 255) >> 5) << (3 * (2 - k));
+            }
+            classes[by][bx] = sub_lut[tab.PC_WIENER_LUT_TO_CLASS[lut_idx]];
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < w * h; i += blockDim.x) {
+        const int y = i / w, x = i % w;
+        const int *r = ref + y * 9;
+        const int m = trow(rows, rs, e, r[4], x);
+        int v = m;
+        if (!((llm[(y >> 2) * 4] >> (x >> 2)) & 1)) {
+            int s;
+            if (kind == W_PC) {
+                const int16_t *flt = pcf + classes[y >> 2][x >> 2] * 13;
+                s = m * flt[12];
+                for (int k = 0; k < 12; k++) {
+                    const int dy = TapsY::pc[k][0], dx = TapsY::pc[k][1];
+                    s += (trow(rows, rs, e, r[4 + dy], x + dx) + trow(rows, rs, e, r[4 - dy], x - dx)) * flt[k];
+                }
+            } else {
+                const int8_t *flt = kind == W_NS_SINGLE ? taps : taps + classes[y >> 2][x >> 2] * taps_stride;
+                s = m << 7;
+                for (int k = 0; k < 16; k++) {
+                    const int dy = TapsY::ns[k][0], dx = TapsY::ns[k][1];
+                    s += (trow(rows, rs, e, r[4 + dy], x + dx) + trow(rows, rs, e, r[4 - dy], x - dx) - 2 * m) * flt[k];
+                }
+            }
+            v = iclip_((s + 64) >> 7, 0, bdmax);
+        }
+        out[i] = (uint16_t)v;
+    }
+}
+
+// ns_wiener_single_uv (:1145-1430): chroma rows (margin 2) and downsampled
+// luma rows (margin 4, luma columns); cref / lref [h][5], slot 2 = the
+// output row.
+__global__ void dsp_wiener_uv_kernel(const uint16_t *crows, int crs, const uint16_t *lrows, int lrs, const int *cref,
+                                     const int *lref, int w, int h, int ss_hor, const int8_t *f, const uint16_t *llm,
+                                     int bitdepth, uint16_t *out) {
+    const int bdmax = (1 << bitdepth) - 1;
+    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
+        const int y = i / w, x = i % w;
+        const int *cr = cref + y * 5, *lr = lref + y * 5;
+        const int m = trow(crows, crs, 2, cr[2], x);
+        int v = m;
+        if (!((llm[(y >> 2) * 4] >> (x >> 2)) & 1)) {
+            int s = m << 7;
+            for (int k = 0; k < 6; k++) {
+                const int dy = TapsY::uv[k][0], dx = TapsY::uv[k][1];
+                s += (trow(crows, crs, 2, cr[2 + dy], x + dx) + trow(crows, crs, 2, cr[2 - dy], x - dx) - 2 * m) * f[k];
+            }
+            const int l = trow(lrows, lrs, 4, lr[2], x << ss_hor);
+            for (int k = 0; k < 12; k++) {
+                const int dy = TapsY::uvy[k][0], dx = TapsY::uvy[k][1];
+                s += (trow(lrows, lrs, 4, lr[2 + dy], (x + dx) * (1 << ss_hor)) - l) * f[6 + k];
+            }
+            v = iclip_((s + 64) >> 7, 0, bdmax);
+        }
+        out[i] = (uint16_t)v;
+    }
+}
+
+// gdf_prep (:1432-1640): gradient events gref [ng][13] (event 0 with row
+// offset 6, the others with 8), per output row pref [h][13] (slot 6 = the
+// output row).
+__global__ void dsp_gdf_prep_kernel(const uint16_t *rows, int rs, int e, const int *gref, int ng, const int *pref, int w,
+                                    int h, int ref_dst_idx, int qp_idx, int bitdepth, const DevTables tab,
+                                    int8_t *out) {
+    __shared__ uint16_t cells[33][34][4];
+    const int up = bitdepth == 8 ? 2 : 0;
+    const int nc = (w + 2 + 1) >> 1;
+    // compute_gradient_row (:114-193) per event and cell
+    for (int i = threadIdx.x; i < ng * nc; i += blockDim.x) {
+        const int g = i / nc, c = i % nc, x1 = 2 * c;
+        const int *r = gref + g * 13;
+        const int row_off = g == 0 ? 6 : 8;
+        const int offs[4][2] = {{1, 0}, {0, 1}, {1, 1}, {-1, 1}};
+        for (int d = 0; d < 4; d++) {
+            int grad = 0;
+            for (int x2 = 0; x2 < 2; x2++)
+                for (int yy = 0; yy < 2; yy++) {
+                    const int dy = offs[d][0], dx = offs[d][1], ry = row_off + yy, x = x1 + x2;
+                    const int a = trow(rows, rs, e, r[ry - 1 - dy], x - 1 - dx);
+                    const int b = trow(rows, rs, e, r[ry - 1], x - 1);
+                    const int cc = trow(rows, rs, e, r[ry - 1 + dy], x - 1 + dx);
+                    const int t = b * 2 - a - cc;
+                    grad += t < 0 ? -t : t;
+                }
+            cells[g][c][d] = (uint16_t)grad;
+        }
+    }
+    __syncthreads();
+    const int alpha_base = ref_dst_idx * 528 + qp_idx * 88, weight_base = ref_dst_idx * 1584 + qp_idx * 264;
+    const int bias_idx = ref_dst_idx * 6 + qp_idx;
+    const int scale = ref_dst_idx == 0 ? 8 : 5;
+    const int8_t *errtab = ref_dst_idx == 0 ? tab.GDF_INTRA_ERROR + qp_idx * 4096
+                                            : tab.GDF_INTER_ERROR + (ref_dst_idx - 1) * 6000 + qp_idx * 1000;
+    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
+        const int y = i / w, x = i % w, x1 = x & ~1, hx = x1 >> 1;
+        const int k1 = (y >> 1) + 1, k0 = k1 - 1;  // the two gradient rows in use at row y
+        int gs[4];
+        for (int d = 0; d < 4; d++)
+            gs[d] = cells[k0][hx][d] + cells[k0][hx + 1][d] + cells[k1][hx][d] + cells[k1][hx + 1][d];
+        const int cls = (gs[0] <= gs[1]) | ((gs[2] <= gs[3]) << 1);
+        int iv[3];
+        for (int q = 0; q < 3; q++) iv[q] = tab.GDF_BIAS[bias_idx * 3 + q];
+        for (int d = 0; d < 4; d++) {
+            const int k = d + 18;
+            const int v = imin_(gs[d] >> (4 - up), tab.GDF_ALPHA[alpha_base + k * 4 + cls]);
+            for (int q = 0; q < 3; q++) iv[q] += v * tab.GDF_WEIGHT[weight_base + q * 88 + k * 4 + cls];
+        }
+        const int *r = pref + y * 13;
+        const int m = trow(rows, rs, e, r[6], x);
+        for (int k = 0; k < 18; k++) {
+            const int alpha = tab.GDF_ALPHA[alpha_base + k * 4 + cls];
+            const int dy = TapsY::gdf[k][0], dx = TapsY::gdf[k][1];
+            const int a = trow(rows, rs, e, r[6 - dy], x - dx), b = trow(rows, rs, e, r[6 + dy], x + dx);
+            const int above = iclip_((a - m) << up, -alpha, alpha), below = iclip_((b - m) << up, -alpha, alpha);
+            const int v = iclip_(above + below, -512, 511);
+            for (int q = 0; q < 3; q++) iv[q] += v * tab.GDF_WEIGHT[weight_base + q * 88 + k * 4 + cls];
+        }
+        int full = 0;
+        for (int q = 0; q < 3; q++) {
+            const int sv = iv[q] * scale;
+            const int v = apply_sign_(((sv < 0 ? -sv : sv) + (1 << 14)) >> 15, sv);
+            full = full * (scale * 2) + iclip_(v, -scale, scale - 1) + scale;
+        }
+        out[i] = errtab[full];
+    }
+}
+
 // Per device: dynamic shared memory opted in, SM count and CTAs per SM.
 struct LrLaunchInfo {
     std::atomic<int> ready{0};
@@ -1159,4 +1341,22 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
 void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int scale, const uint16_t *llm, int bitdepth,
                             cudaStream_t s) {
     dsp_gdf_add_kernel<<<1, 256, 0, s>>>(p, err, w, h, scale, llm, bitdepth);
+}
+
+void r2g_dsp_launch_wiener_y(const uint16_t *rows, int rs, int e, const int *ref, const int *cref, int w, int h,
+                             int kind, const int8_t *taps, int taps_stride, const int16_t *pcf, const uint8_t *sub_lut,
+                             const uint16_t *noskip, int base_q, const uint16_t *llm, int bitdepth,
+                             const DevTables &tab, uint16_t *out, cudaStream_t s) {
+    dsp_wiener_y_kernel<<<1, 256, 0, s>>>(rows, rs, e, ref, cref, w, h, kind, taps, taps_stride, pcf, sub_lut, noskip,
+                                          base_q, llm, bitdepth, tab, out);
+}
+void r2g_dsp_launch_wiener_uv(const uint16_t *crows, int crs, const uint16_t *lrows, int lrs, const int *cref,
+                              const int *lref, int w, int h, int ss_hor, const int8_t *f, const uint16_t *llm,
+                              int bitdepth, uint16_t *out, cudaStream_t s) {
+    dsp_wiener_uv_kernel<<<1, 256, 0, s>>>(crows, crs, lrows, lrs, cref, lref, w, h, ss_hor, f, llm, bitdepth, out);
+}
+void r2g_dsp_launch_gdf_prep(const uint16_t *rows, int rs, int e, const int *gref, int ng, const int *pref, int w,
+                             int h, int ref_dst_idx, int qp_idx, int bitdepth, const DevTables &tab, int8_t *out,
+                             cudaStream_t s) {
+    dsp_gdf_prep_kernel<<<1, 256, 0, s>>>(rows, rs, e, gref, ng, pref, w, h, ref_dst_idx, qp_idx, bitdepth, tab, out);
 }

@@ -169,6 +169,17 @@ void r2g_dsp_launch_gdf_add(uint16_t *p, const int8_t *err, int w, int h, int sc
                             cudaStream_t s);
 void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, int16_t *lut, uint8_t *scaling,
                                    cudaStream_t s);
+// Typed LR slots: staged row tables (see dsp.cu) -> one block.
+void r2g_dsp_launch_wiener_y(const uint16_t *rows, int rs, int e, const int *ref, const int *cref, int w, int h,
+                             int kind, const int8_t *taps, int taps_stride, const int16_t *pcf, const uint8_t *sub_lut,
+                             const uint16_t *noskip, int base_q, const uint16_t *llm, int bitdepth,
+                             const DevTables &tab, uint16_t *out, cudaStream_t s);
+void r2g_dsp_launch_wiener_uv(const uint16_t *crows, int crs, const uint16_t *lrows, int lrs, const int *cref,
+                              const int *lref, int w, int h, int ss_hor, const int8_t *f, const uint16_t *llm,
+                              int bitdepth, uint16_t *out, cudaStream_t s);
+void r2g_dsp_launch_gdf_prep(const uint16_t *rows, int rs, int e, const int *gref, int ng, const int *pref, int w,
+                             int h, int ref_dst_idx, int qp_idx, int bitdepth, const DevTables &tab, int8_t *out,
+                             cudaStream_t s);
 
 // ---- asynchronous staging: bulk copies (TMA engine) + mbarriers ----
 // A producer warp copies each work item's rows from global memory into

@@ -69,7 +69,7 @@ extern "C" int r2g_struct_sizes(int32_t *sizes, int n) {
                          (int32_t)sizeof(R2gFilmGrainData), (int32_t)sizeof(R2gSideInfo),
                          (int32_t)sizeof(R2gBatchItem), (int32_t)sizeof(R2gServeConfig),
                          (int32_t)sizeof(R2gServeRequest), (int32_t)sizeof(R2gServeResult),
-                         (int32_t)sizeof(R2gServeStats)};
+                         (int32_t)sizeof(R2gServeStats), (int32_t)sizeof(R2gWienerParams)};
     int m = (int)(sizeof(v) / sizeof(v[0]));
     for (int i = 0; i < n && i < m; i++) sizes[i] = v[i];
     return m;

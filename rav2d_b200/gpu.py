@@ -88,6 +88,11 @@ def lib():
         L.r2g_dsp_ccso_add.argtypes = [vp, i64, vp, i64, vp, vp, ci, ci, vp, ci]
         L.r2g_dsp_gdf_add.argtypes = [vp, i64, vp, i64, ci, ci, ci, vp, ci]
         L.r2g_dsp_generate_grain.argtypes = [vp, vp, vp, C.POINTER(abi.FilmGrainData), C.c_uint32, ci]
+        wp = C.POINTER(abi.WienerParams)
+        for n in ("r2g_dsp_ns_wiener_single_y", "r2g_dsp_ns_wiener_single_uv", "r2g_dsp_ns_wiener_multi",
+                  "r2g_dsp_pc_wiener"):
+            getattr(L, n).argtypes = [vp, i64, vp, vp, vp, ci, ci, wp, ci, vp, ci]
+        L.r2g_dsp_gdf_prep.argtypes = [vp, i64, vp, i64, vp, vp, vp] + [ci] * 6
         L.r2g_y4m_header.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
         L.r2g_download_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.c_int64]

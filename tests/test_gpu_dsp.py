@@ -143,3 +143,158 @@ def test_generate_grain(L, oracle, bd):
         assert L.r2g_dsp_generate_grain(p(got[0]), p(got[1]), p(got[2]), C.byref(fgd), sf.grain_seed, bd) == 0
         for pl in range(3):
             assert np.array_equal(got[pl], want[pl]), pl
+
+
+# ---- typed loop-restoration slots (WienerFilterFn / GdfPrepFn) ----
+# One plane holds the block (at row R0, column C0), its right-hand context and
+# the saved rows above / below (rows R0-2, R0-1 and R0+h, R0+h+1 stand in for
+# the deblocked lines); `left` is a separate [h][6] array.  The oracle runs
+# the reference's function on the same buffers (in place on a copy).
+R0, C0, S = 12, 16, 112
+
+
+def _plane(rng, bd, rows=112, cols=S):
+    yy, xx = np.mgrid[0:rows, 0:cols]
+    base = ((1 << bd) // 2 + ((1 << bd) // 5) * np.sin(xx / 7.0 + yy / 11.0)).astype(np.int64)
+    return np.clip(base + rng.integers(-(1 << bd) // 16, (1 << bd) // 16 + 1, (rows, cols)), 0,
+                   (1 << bd) - 1).astype(np.uint16)
+
+
+def _ptr(a, off):
+    return C.c_void_p(a.ctypes.data + off * a.itemsize)
+
+
+def _ll(rng, h, p_ll):
+    return ((rng.random((h // 4 + 1, 4)) < p_ll) * rng.integers(0, 1 << 16, (h // 4 + 1, 4))).astype(np.uint16)
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+@pytest.mark.parametrize("kind", ["single", "multi", "pc"])
+def test_wiener_y_slots(L, oracle, bd, kind):
+    """ns_wiener_single_y / ns_wiener_multi / pc_wiener (looprestoration.rs
+    :524-1143) through r2g_dsp_ns_wiener_single_y / _multi / r2g_dsp_pc_wiener."""
+    from rav2d_b200 import abi
+
+    rng = np.random.default_rng(31 * bd + len(kind))
+    for it in range(40):
+        w = int(rng.choice([8, 16, 32, 60, 64]))
+        h = int(rng.choice([4, 8, 12, 32, 56, 64]))
+        edges = it % 16
+        plane = _plane(rng, bd)
+        left = rng.integers(0, 1 << bd, (h, 6)).astype(np.uint16)
+        ll = _ll(rng, h, 0.2)
+        ref = plane.copy().ravel()
+        fu = rng.integers(-8, 8, (16, 18)).astype(np.int8)
+        fpt = rng.integers(-40, 40, (64, 13)).astype(np.int16)
+        fpt[:, 12] += 128
+        lut = rng.integers(0, 16 if kind == "multi" else 64, 256).astype(np.uint8)
+        noskip = rng.integers(0, 1 << 16, h // 4 + 1).astype(np.uint16)
+        base_q = int(rng.integers(4, 1200))
+        single = fu[0, :16].copy()
+        o = R0 * S + C0
+        if kind == "single":
+            oracle.lib().r2o_ns_wiener_single_y(p(ref), C.c_int64(o), C.c_int64(S), p(left), p(ref),
+                                                C.c_int64(o - 2 * S), p(ref), C.c_int64(o + h * S), w, h, p(single),
+                                                edges, p(ll), bd)
+        else:
+            oracle.lib().r2o_wiener_multi(p(ref), C.c_int64(o), C.c_int64(S), p(left), p(ref), C.c_int64(o - 2 * S),
+                                          p(ref), C.c_int64(o + h * S), w, h, p(fu) if kind == "multi" else None,
+                                          p(fpt) if kind == "pc" else None, p(lut), p(noskip), base_q, edges, p(ll),
+                                          bd)
+        got = _st(plane, bd).copy().ravel()
+        gl = _st(left, bd)
+        prm = abi.WienerParams()
+        if kind == "single":
+            prm.single.filter = single.ctypes.data
+            fn = L.r2g_dsp_ns_wiener_single_y
+        else:
+            prm.multi.filters = (fu if kind == "multi" else fpt).ctypes.data
+            prm.multi.subclass_lut = lut.ctypes.data
+            prm.multi.noskip_mask = noskip.ctypes.data
+            prm.multi.base_q = base_q
+            fn = L.r2g_dsp_ns_wiener_multi if kind == "multi" else L.r2g_dsp_pc_wiener
+        rc = fn(_ptr(got, o), S, p(gl), _ptr(got, o - 2 * S), _ptr(got, o + h * S), w, h, C.byref(prm), edges,
+                p(ll), bd)
+        assert rc == 0
+        assert np.array_equal(got.astype(np.uint16), ref), (kind, w, h, edges)
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+@pytest.mark.parametrize("ds", [0, 1, 2])
+def test_wiener_uv_slot(L, oracle, bd, ds):
+    """ns_wiener_single_uv (looprestoration.rs:1145-1430) through
+    r2g_dsp_ns_wiener_single_uv, 4:2:0 with each CfL downsample filter."""
+    from rav2d_b200 import abi
+
+    rng = np.random.default_rng(17 * bd + ds)
+    LS = 200
+    for it in range(32):
+        w = int(rng.choice([8, 16, 28, 32, 64]))
+        h = int(rng.choice([2, 4, 8, 16, 28, 32]))
+        edges = it % 16
+        plane = _plane(rng, bd)
+        luma = _plane(rng, bd, rows=180, cols=LS)
+        left = rng.integers(0, 1 << bd, (h, 6)).astype(np.uint16)
+        ll = _ll(rng, h, 0.15)
+        f = np.concatenate([rng.integers(-16, 16, 6), rng.integers(-8, 8, 12)]).astype(np.int8)
+        o = R0 * S + C0
+        lo, lto, lbo = 24 * LS + 16, 8 * LS + 16, (24 + 2 * h + 8) * LS + 16
+        ref = plane.copy().ravel()
+        lref = luma.ravel()
+        oracle.lib().r2o_ns_wiener_single_uv(p(ref), C.c_int64(o), C.c_int64(S), p(left), p(ref), C.c_int64(o - 2 * S),
+                                             p(ref), C.c_int64(o + h * S), w, h, p(f), p(lref), C.c_int64(lo),
+                                             C.c_int64(LS), p(lref), C.c_int64(lto), p(lref), C.c_int64(lbo), 1, 1, ds,
+                                             edges, p(ll), bd)
+        got = _st(plane, bd).copy().ravel()
+        gluma = _st(luma, bd).ravel()
+        prm = abi.WienerParams()
+        sp = prm.single
+        sp.filter = f.ctypes.data
+        sp.luma, sp.luma_top, sp.luma_bottom = (gluma.ctypes.data + k * gluma.itemsize for k in (lo, lto, lbo))
+        sp.stride, sp.ss_ver, sp.ss_hor, sp.ds_flt = LS, 1, 1, ds
+        rc = L.r2g_dsp_ns_wiener_single_uv(_ptr(got, o), S, p(_st(left, bd)), _ptr(got, o - 2 * S),
+                                           _ptr(got, o + h * S), w, h, C.byref(prm), edges, p(ll), bd)
+        assert rc == 0
+        assert np.array_equal(got.astype(np.uint16), ref), (w, h, edges)
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+def test_gdf_prep_slot(L, oracle, bd):
+    """gdf_prep (looprestoration.rs:1432-1640) through r2g_dsp_gdf_prep, intra
+    and inter tables."""
+    rng = np.random.default_rng(53 * bd)
+    for it in range(40):
+        w = int(rng.choice([8, 16, 32, 62, 64]))
+        h = int(rng.choice([6, 8, 16, 32, 56, 64]))
+        edges = it % 16
+        rd, qp = int(rng.integers(0, 6)), int(rng.integers(0, 6))
+        plane = _plane(rng, bd)
+        left = rng.integers(0, 1 << bd, (h, 6)).astype(np.uint16)
+        o = R0 * S + C0
+        want = np.zeros((h, w), np.int8)
+        oracle.lib().r2o_gdf_prep(p(want), w, p(plane), C.c_int64(o), C.c_int64(S), p(left), p(plane),
+                                  C.c_int64(o - 2 * S), p(plane), C.c_int64(o + h * S), w, h, rd, qp, edges, bd)
+        got = np.full((h, w), 99, np.int8)
+        g = _st(plane, bd).ravel()
+        rc = L.r2g_dsp_gdf_prep(p(got), w, _ptr(g, o), S, p(_st(left, bd)), _ptr(g, o - 2 * S), _ptr(g, o + h * S),
+                                w, h, rd, qp, edges, bd)
+        assert rc == 0
+        assert np.array_equal(got, want), (w, h, edges, rd, qp)
+
+
+def test_lr_slots_reject_bad_arguments(L):
+    from rav2d_b200 import abi
+
+    buf = np.zeros(64 * 64, np.uint8)
+    prm = abi.WienerParams()
+    f = np.zeros(18, np.int8)
+    prm.single.filter = f.ctypes.data
+    ll = np.zeros((17, 4), np.uint16)
+    for w, h, edges in ((6, 8, 0), (68, 8, 0), (8, 66, 0), (8, 8, 16), (8, 8, 32)):
+        assert L.r2g_dsp_ns_wiener_single_y(p(buf), 64, None, None, None, w, h, C.byref(prm), edges, p(ll),
+                                            8) == abi.R2G_E_INVALID
+    assert L.r2g_dsp_ns_wiener_single_y(p(buf), 64, None, None, None, 8, 8, C.byref(prm), 1, p(ll),
+                                        8) == abi.R2G_E_INVALID  # left context without `left`
+    e = np.zeros(64, np.int8)
+    assert L.r2g_dsp_gdf_prep(p(e), 8, p(buf), 64, None, None, None, 8, 4, 0, 0, 0, 8) == abi.R2G_E_INVALID
+    assert L.r2g_dsp_gdf_prep(p(e), 8, p(buf), 64, None, None, None, 8, 8, 6, 0, 0, 8) == abi.R2G_E_INVALID
