@@ -368,6 +368,7 @@ def run_batched(args, ctx, stream, device):
     tile_rows = ctx.batch_tile_rows()
     for fr in frames:
         fr.free()
+    by_class = run_batched_by_class(args, ctx, timed, reps)
     mix = {}
     for sf in sfs:
         k = f"{sf.width}x{sf.height}/{sf.bitdepth}bit{'+grain' if sf.fgd is not None else ''}"
@@ -382,7 +383,49 @@ def run_batched(args, ctx, stream, device):
         "per_frame_launches": pf_l,
         "speedup_vs_per_frame": round(pf_ms / b_ms, 3), "ctas_per_sm": cfg, "tile_rows": tile_rows, "sms": sms,
         "l2": f"inputs larger than L2: {round(mpix * 1.5 * 1.5, 0)} MB of recon per batch",
+        "by_class": by_class,
     }
+
+
+# frames per batch of each (resolution, bit depth) class: about 15 Mpix each
+CLASS_FRAMES = {(640, 360): 64, (1280, 720): 16, (1920, 1080): 8, (3840, 2160): 2}
+
+
+def run_batched_by_class(args, ctx, timed, reps):
+    """Batched vs per-frame for one resolution and bit depth at a time (full
+    filter chain, no grain): where batching can win is the small frames,
+    whose per-frame grids fill a fraction of the GPU."""
+    from rav2d_b200 import synth
+
+    out = {}
+    for (w, h), n in CLASS_FRAMES.items():
+        for bd in (8, 10):
+            sf = synth.make_frame(w, h, bd, 0x5EED3000 + w + bd, chain="full")
+            frames = []
+            for _ in range(n):
+                fr = ctx.frame(w, h, bd)
+                fr.upload(sf.planes)
+                fr.stage(sf)
+                frames.append(fr)
+            ctx.sync()
+            items = [(fr, sf) for fr in frames]
+
+            def per_frame():
+                for fr in frames:
+                    fr.run()
+
+            def batched():
+                ctx.batch_submit(items, staged=True)
+
+            pf_ms, _ = timed(per_frame, reps)
+            b_ms, _ = timed(batched, reps)
+            for fr in frames:
+                fr.free()
+            mpix = n * w * h / 1e6
+            out[f"{w}x{h}/{bd}bit"] = {"frames": n, "per_frame_mpix_s": round(mpix / pf_ms * 1e3, 1),
+                                       "batched_mpix_s": round(mpix / b_ms * 1e3, 1),
+                                       "speedup": round(pf_ms / b_ms, 3)}
+    return out
 
 
 def run_serving(args, device):

@@ -25,7 +25,8 @@ SYMBOLS = [
     "r2g_server_submit", "r2g_server_wait", "r2g_server_close_stream", "r2g_server_stats", "r2g_server_destroy",
     "r2g_ctx_overlap_copies", "r2g_ctx_fence", "r2g_download_y4m", "r2g_y4m_frame_bytes", "r2g_y4m_header",
     "r2g_download_rows", "r2g_dsp_cdef_dir", "r2g_dsp_cdef_filter", "r2g_dsp_ccso_prep", "r2g_dsp_ccso_add",
-    "r2g_dsp_gdf_add", "r2g_dsp_generate_grain",
+    "r2g_dsp_gdf_add", "r2g_dsp_generate_grain", "r2g_dsp_ns_wiener_single_y", "r2g_dsp_ns_wiener_single_uv",
+    "r2g_dsp_ns_wiener_multi", "r2g_dsp_pc_wiener", "r2g_dsp_gdf_prep", "r2g_ctx_device_faults",
 ]
 
 
