@@ -181,44 +181,6 @@ R2G_D void filter_edge(int16_t *e, int along, int across, uint32_t q_thr, uint32
     }
 }
 
-R2G_D bool ll_y(const R2gAv2Filter &m, int x4, int y4) {
-    return (m.lossless_mask_y[y4 & 63][(x4 >> 4) & 3] >> (x4 & 15)) & 1;
-}
-R2G_D bool ll_uv(const R2gAv2Filter &m, int cx4, int cy4) {
-    return (m.lossless_mask_uv[cy4 & 31][(cx4 >> 3) & 3] >> (cx4 & 7)) & 1;
-}
-R2G_D int seg_y(const DevFrame &f, int x4, int y4) {
-    return f.segmap ? f.segmap[(int64_t)y4 * f.segmap_stride + x4] : 0;
-}
-R2G_D int seg_uv(const DevFrame &f, int cx4, int cy4) {
-    return f.segmap_uv ? f.segmap_uv[(int64_t)cy4 * f.segmap_uv_stride + cx4] : 0;
-}
-
-// Edge-threshold pair for a 4x4 and its neighbour (setup_thr_* :1477/:1520):
-// the neighbour is the 4x4 to the left (vertical edge) or above.
-R2G_D void luma_thr(const DevFrame &f, int dir, int x4, int y4, int nx4, int ny4, bool subpu, uint32_t &q,
-                    uint32_t &s) {
-    const R2gAv2Filter &mc = f.masks[(y4 >> 6) * f.sb256w + (x4 >> 6)];
-    const R2gAv2Filter &mn = f.masks[(ny4 >> 6) * f.sb256w + (nx4 >> 6)];
-    int cq, cs, pq, ps;
-    thr_of(f, dir, mc.qidx[((x4 >> 4) & 3) + (((y4 >> 4) & 3) << 2)], seg_y(f, x4, y4), cq, cs);
-    thr_of(f, dir, mn.qidx[((nx4 >> 4) & 3) + (((ny4 >> 4) & 3) << 2)], seg_y(f, nx4, ny4), pq, ps);
-    int sh = subpu ? 3 : 0;
-    q = (uint32_t)(uint16_t)(edge_thr(cq, pq) >> sh);
-    s = (uint32_t)(uint16_t)(edge_thr(cs, ps) >> sh);
-}
-R2G_D void chroma_thr(const DevFrame &f, int pl, int cx4, int cy4, int nx4, int ny4, bool subpu, uint32_t &q,
-                      uint32_t &s) {
-    const R2gAv2Filter &mc = f.masks[(cy4 >> 5) * f.sb256w + (cx4 >> 5)];
-    const R2gAv2Filter &mn = f.masks[(ny4 >> 5) * f.sb256w + (nx4 >> 5)];
-    int cq, cs, pq, ps;
-    thr_of(f, 2 + pl, mc.qidx[((cx4 >> 3) & 3) + (((cy4 >> 3) & 3) << 2)], seg_uv(f, cx4, cy4), cq, cs);
-    thr_of(f, 2 + pl, mn.qidx[((nx4 >> 3) & 3) + (((ny4 >> 3) & 3) << 2)], seg_uv(f, nx4, ny4), pq, ps);
-    int sh = subpu ? 3 : 0;
-    q = (uint32_t)(uint16_t)(edge_thr(cq, pq) >> sh);
-    s = (uint32_t)(uint16_t)(edge_thr(cs, ps) >> sh);
-}
-
 template <typename P>
 struct Vec4;
 template <>
@@ -266,11 +228,31 @@ struct EdgeDesc {
 // Per-tile edge lists (upper bounds: every segment position of the span).
 constexpr int NVL = 19 * 22, NVC = 2 * 9 * 12, NHL = 19 * 16, NHC = 2 * 9 * 8;
 
+// The side-info one tile's edges read, staged once per tile with independent
+// loads (so resolving an edge touches shared memory only).  Coordinates in
+// 4x4 units; tile origin (X0, Y0) luma, (CX0, CY0) chroma.
+//   vy[j][s][k]: vertical luma edge masks of column X0-1+j, 16-row segment
+//                s of rows Y0-3 .., level k (4 = sub-PU)
+//   hy[i][k]:    horizontal luma edge masks of row Y0-1+i (columns X0..X0+15)
+//   vc, hc:      the chroma twins (columns CX0+j, rows CY0-2.. / CY0+i)
+//   lly[r][g]:   luma lossless bits of row Y0-4+r, 16-column group X0/16-1+g
+//   llc[r][g]:   chroma lossless bits of row CY0-3+r, 8-column group tx-1+g
+//   thr[kind][b][seg]: q_thr | side_thr << 16 of 64x64 block b (3x3 around
+//                the tile), kind 0/1 luma dir 0/1, 2 U, 3 V
+//   segy / segc: segment ids (when the frame has a segment map)
+struct DbSide {
+    uint16_t vy[19][3][5], hy[19][5], vc[9][2][5], hc[9][5];
+    uint16_t lly[23][3], llc[13][3];
+    uint32_t thr[4][9][8];
+    uint8_t segy[23][20], segc[13][10];
+};
+
 struct DeblockSmem {
     int16_t y[LT * LP];
     int16_t uv[2][CT * CP];
     EdgeDesc vl[NVL], vc[NVC], hl[NHL], hc[NHC];  // vertical / horizontal, luma / chroma
     int n[4];  // list lengths: vl, vc, hl, hc
+    DbSide side;
 };
 
 R2G_D void push_edge(DeblockSmem &sm, int list, EdgeDesc d) {
@@ -283,21 +265,127 @@ R2G_D uint32_t pack_geo(int x, int y, int mwp, int mwn, bool pos_ll, bool neg_ll
            ((uint32_t)pos_ll << 24) | ((uint32_t)neg_ll << 25);
 }
 
+// Stages the tile's side-info (all loads independent, spread over the CTA).
+R2G_D void stage_side(const DevFrame &f, DbSide &sd, int tx, int ty, int tid, int nt) {
+    const int X0 = tx * 16, Y0 = ty * 16, CX0 = tx * 8, CY0 = ty * 8;
+    const int bw4 = f.bw4, bh4 = f.bh4, cbw4 = bw4 >> 1, cbh4 = bh4 >> 1;
+    const int nsb = f.sb256w * f.sb256h;
+    auto mask_at = [&](int sbrow, int sbcol) -> const R2gAv2Filter * {
+        const int i = sbrow * f.sb256w + sbcol;
+        return (sbrow >= 0 && sbcol >= 0 && sbcol < f.sb256w && i < nsb) ? &f.masks[i] : nullptr;
+    };
+    const int gy0 = (Y0 - 3) >> 4, gc0 = (CY0 - 2) >> 4;
+    constexpr int NV = 19 * 3 * 5, NH = 19 * 5, NVCW = 9 * 2 * 5, NHCW = 9 * 5, NLY = 23 * 3, NLC = 13 * 3;
+    constexpr int NQ = 9, NSY = 23 * 20, NSC = 13 * 10;
+    const bool segs = f.segmap != nullptr, segsc = f.segmap_uv != nullptr;
+    const int total = NV + NH + NVCW + NHCW + NLY + NLC + NQ + (segs ? NSY : 0) + (segsc ? NSC : 0);
+    __shared__ uint16_t q64[9];
+    for (int i = tid; i < total; i += nt) {
+        int j = i;
+        if (j < NV) {
+            const int c = j / 15, s = (j / 5) % 3, k = j % 5;
+            const int x4 = X0 - 1 + c, g = gy0 + s;
+            const R2gAv2Filter *m = (x4 >= 0 && x4 < bw4 && g >= 0 && 16 * g < bh4) ? mask_at(g >> 2, x4 >> 6) : nullptr;
+            sd.vy[c][s][k] = m ? m->filter_y[0][x4 & 63][k][g & 3] : 0;
+            continue;
+        }
+        j -= NV;
+        if (j < NH) {
+            const int r = j / 5, k = j % 5;
+            const int y4 = Y0 - 1 + r;
+            const R2gAv2Filter *m = (y4 >= 0 && y4 < bh4 && X0 < bw4) ? mask_at(y4 >> 6, X0 >> 6) : nullptr;
+            sd.hy[r][k] = m ? m->filter_y[1][y4 & 63][k][(X0 >> 4) & 3] : 0;
+            continue;
+        }
+        j -= NH;
+        if (j < NVCW) {
+            const int c = j / 10, s = (j / 5) % 2, k = j % 5;
+            const int cx4 = CX0 + c, g = gc0 + s;
+            const R2gAv2Filter *m =
+                (cx4 < cbw4 && g >= 0 && 16 * g < cbh4) ? mask_at(g >> 1, cx4 >> 5) : nullptr;
+            sd.vc[c][s][k] = m ? m->filter_uv[0][cx4 & 31][k][g & 1] : 0;
+            continue;
+        }
+        j -= NVCW;
+        if (j < NHCW) {
+            const int r = j / 5, k = j % 5;
+            const int cy4 = CY0 + r;
+            const R2gAv2Filter *m = (cy4 < cbh4 && CX0 < cbw4) ? mask_at(cy4 >> 5, CX0 >> 5) : nullptr;
+            sd.hc[r][k] = m ? m->filter_uv[1][cy4 & 31][k][(CX0 & 31) >> 4] : 0;
+            continue;
+        }
+        j -= NHCW;
+        if (j < NLY) {
+            const int r = j / 3, g = X0 / 16 - 1 + j % 3, y4 = Y0 - 4 + r;
+            const R2gAv2Filter *m = (y4 >= 0 && y4 < bh4 && g >= 0 && 16 * g < bw4) ? mask_at(y4 >> 6, g >> 2) : nullptr;
+            sd.lly[r][j % 3] = m ? m->lossless_mask_y[y4 & 63][g & 3] : 0;
+            continue;
+        }
+        j -= NLY;
+        if (j < NLC) {
+            const int r = j / 3, g = tx - 1 + j % 3, cy4 = CY0 - 3 + r;
+            const R2gAv2Filter *m =
+                (cy4 >= 0 && cy4 < cbh4 && g >= 0 && 8 * g < cbw4) ? mask_at(cy4 >> 5, g >> 2) : nullptr;
+            sd.llc[r][j % 3] = m ? m->lossless_mask_uv[cy4 & 31][g & 3] : 0;
+            continue;
+        }
+        j -= NLC;
+        if (j < NQ) {
+            const int bx = tx - 1 + j % 3, by = ty - 1 + j / 3;
+            const R2gAv2Filter *m = (bx >= 0 && by >= 0 && 16 * bx < bw4 && 16 * by < bh4) ? mask_at(by >> 2, bx >> 2)
+                                                                                          : nullptr;
+            q64[j] = m ? m->qidx[(bx & 3) + ((by & 3) << 2)] : 0;
+            continue;
+        }
+        j -= NQ;
+        if (segs && j < NSY) {
+            const int r = j / 20, c = j % 20, y4 = Y0 - 4 + r, x4 = X0 - 2 + c;
+            sd.segy[r][c] =
+                (x4 >= 0 && y4 >= 0 && x4 < bw4 && y4 < bh4) ? f.segmap[(int64_t)y4 * f.segmap_stride + x4] : 0;
+            continue;
+        }
+        if (segs) j -= NSY;
+        const int r = j / 10, c = j % 10, cy4 = CY0 - 3 + r, cx4 = CX0 - 1 + c;
+        sd.segc[r][c] = (cx4 >= 0 && cy4 >= 0 && cx4 < cbw4 && cy4 < cbh4)
+                            ? f.segmap_uv[(int64_t)cy4 * f.segmap_uv_stride + cx4]
+                            : 0;
+    }
+    __syncthreads();
+    // thresholds of every (kind, block, segment id < 8) the tile can use
+    // (thr_of gives 0 for ids the frame's segmentation does not define)
+    for (int i = tid; i < 4 * 9 * 8; i += nt) {
+        const int kind = i / 72, b = (i / 8) % 9, seg = i % 8;
+        int q, s;
+        thr_of(f, kind, q64[b], seg, q, s);
+        sd.thr[kind][b][seg] = (uint32_t)q | ((uint32_t)s << 16);
+    }
+    __syncthreads();
+}
+
+// Threshold pair (setup_thr_*, deblock.rs:1477-1567) of a 4x4 and its
+// neighbour (left for vertical edges, above for horizontal ones), from the
+// staged table: block index relative to the 3x3 around the tile.
+R2G_D uint32_t edge_q_s(const DbSide &sd, int kind, int bc, int sc, int bn, int sn, bool subpu) {
+    const uint32_t c = sc < 8 ? sd.thr[kind][bc][sc] : 0, n = sn < 8 ? sd.thr[kind][bn][sn] : 0;
+    const int sh = subpu ? 3 : 0;
+    const uint32_t q = (uint32_t)(uint16_t)(edge_thr((int)(c & 0xffff), (int)(n & 0xffff)) >> sh);
+    const uint32_t s = (uint32_t)(uint16_t)(edge_thr((int)(c >> 16), (int)(n >> 16)) >> sh);
+    return q | (s << 16);
+}
+
 // Resolve one luma edge segment (masks, class, widths, thresholds, lossless
 // sides) into the tile's list.  dir 0: vertical edge at column x, rows
 // y..y+3; dir 1: horizontal edge at row y, columns x..x+3.  (x, y) are frame
 // coordinates; `sx`/`sy` the origin of the staged span.
-R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, int sx, int sy) {
+R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, int sx, int sy, int tx, int ty) {
+    const DbSide &sd = sm.side;
     const int x4 = x >> 2, y4 = y >> 2;
     if (x4 >= f.bw4 || y4 >= f.bh4 || x < 0 || y < 0) return;
     if ((dir == 0 ? x4 : y4) == 0) return;
-    const R2gAv2Filter &m = f.masks[(y4 >> 6) * f.sb256w + (x4 >> 6)];
-    const int pos = dir == 0 ? (x4 & 63) : (y4 & 63);
-    const int idx = dir == 0 ? ((y4 >> 4) & 3) : ((x4 >> 4) & 3);
+    const int X0 = tx * 16, Y0 = ty * 16;
+    const uint16_t *km = dir == 0 ? sd.vy[x4 - X0 + 1][(y4 >> 4) - ((Y0 - 3) >> 4)] : sd.hy[y4 - Y0 + 1];
     const int bit = dir == 0 ? (y4 & 15) : (x4 & 15);
-    const uint16_t(*km)[4] = m.filter_y[dir][pos];
-    int k3 = (km[3][idx] >> bit) & 1, k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1,
-        k0 = (km[0][idx] >> bit) & 1;
+    int k3 = (km[3] >> bit) & 1, k2 = (km[2] >> bit) & 1, k1 = (km[1] >> bit) & 1, k0 = (km[0] >> bit) & 1;
     if (dir == 1) {
         // deblock_crop_bottom_edge (deblock.rs:1572-1606), applied as the
         // masks are read: in a 64-row band that overhangs the frame bottom
@@ -310,47 +398,48 @@ R2G_D void luma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int x, int y, 
         }
     }
     if (!(k0 | k1 | k2 | k3)) return;
-    int cls = k3 ? 3 : k2 ? 2 : k1;
-    int mwp = c_max_width_y[cls];
-    int mwn = (dir == 1 && (y4 & 15) == 0) ? imin_(6, mwp) : mwp;
-    bool subpu = (km[4][idx] >> bit) & 1;
-    int nx4 = dir == 0 ? x4 - 1 : x4, ny4 = dir == 0 ? y4 : y4 - 1;
-    uint32_t q, s;
-    luma_thr(f, dir, x4, y4, nx4, ny4, subpu, q, s);
-    const R2gAv2Filter &mn = f.masks[(ny4 >> 6) * f.sb256w + (nx4 >> 6)];
-    bool pos_ll = ll_y(m, x4, y4), neg_ll = ll_y(mn, nx4, ny4);
-    push_edge(sm, dir == 0 ? 0 : 2, EdgeDesc{q | (s << 16), pack_geo(x - sx, y - sy, mwp, mwn, pos_ll, neg_ll)});
+    const int cls = k3 ? 3 : k2 ? 2 : k1;
+    const int mwp = c_max_width_y[cls];
+    const int mwn = (dir == 1 && (y4 & 15) == 0) ? imin_(6, mwp) : mwp;
+    const bool subpu = (km[4] >> bit) & 1;
+    const int nx4 = dir == 0 ? x4 - 1 : x4, ny4 = dir == 0 ? y4 : y4 - 1;
+    auto blk = [&](int a4, int b4) { return ((b4 >> 4) - ty + 1) * 3 + ((a4 >> 4) - tx + 1); };
+    auto seg = [&](int a4, int b4) { return f.segmap ? (int)sd.segy[b4 - Y0 + 4][a4 - X0 + 2] : 0; };
+    auto ll = [&](int a4, int b4) { return (sd.lly[b4 - Y0 + 4][(a4 >> 4) - tx + 1] >> (a4 & 15)) & 1; };
+    const uint32_t qs = edge_q_s(sd, dir, blk(x4, y4), seg(x4, y4), blk(nx4, ny4), seg(nx4, ny4), subpu);
+    push_edge(sm, dir == 0 ? 0 : 2,
+              EdgeDesc{qs, pack_geo(x - sx, y - sy, mwp, mwn, ll(x4, y4) != 0, ll(nx4, ny4) != 0)});
 }
 
 // One chroma edge segment position: a descriptor per enabled plane (U and V
 // share masks and widths; thresholds differ); plane 1 (V) is flagged by
 // bit 26 of the geometry word.
-R2G_D void chroma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int cx, int cy, int sx, int sy) {
+R2G_D void chroma_edge(const DevFrame &f, DeblockSmem &sm, int dir, int cx, int cy, int sx, int sy, int tx, int ty) {
+    const DbSide &sd = sm.side;
     const R2gFrameParams &fp = f.fp;
     const int cx4 = cx >> 2, cy4 = cy >> 2;
     const int cbw4 = f.bw4 >> 1, cbh4 = f.bh4 >> 1;
     if (cx4 >= cbw4 || cy4 >= cbh4 || cx < 0 || cy < 0) return;
     if ((dir == 0 ? cx4 : cy4) == 0) return;
-    const R2gAv2Filter &m = f.masks[(cy4 >> 5) * f.sb256w + (cx4 >> 5)];
-    const int pos = dir == 0 ? (cx4 & 31) : (cy4 & 31);
-    const int idx = dir == 0 ? ((cy4 & 31) >> 4) : ((cx4 & 31) >> 4);
+    const int CX0 = tx * 8, CY0 = ty * 8;
+    const uint16_t *km = dir == 0 ? sd.vc[cx4 - CX0][(cy4 >> 4) - ((CY0 - 2) >> 4)] : sd.hc[cy4 - CY0];
     const int bit = dir == 0 ? (cy4 & 15) : (cx4 & 15);
-    const uint16_t(*km)[4] = m.filter_uv[dir][pos];
-    int k2 = (km[2][idx] >> bit) & 1, k1 = (km[1][idx] >> bit) & 1, k0 = (km[0][idx] >> bit) & 1;
+    const int k2 = (km[2] >> bit) & 1, k1 = (km[1] >> bit) & 1, k0 = (km[0] >> bit) & 1;
     if (!(k0 | k1 | k2)) return;
-    int cls = k2 ? 2 : k1;
-    int mwp = c_max_width_uv[cls];
-    int mwn = (dir == 1 && (cy4 & 7) == 0) ? imin_(2, mwp) : mwp;
-    bool subpu = (km[4][idx] >> bit) & 1;
-    int nx4 = dir == 0 ? cx4 - 1 : cx4, ny4 = dir == 0 ? cy4 : cy4 - 1;
-    const R2gAv2Filter &mn = f.masks[(ny4 >> 5) * f.sb256w + (nx4 >> 5)];
-    bool pos_ll = ll_uv(m, cx4, cy4), neg_ll = ll_uv(mn, nx4, ny4);
+    const int cls = k2 ? 2 : k1;
+    const int mwp = c_max_width_uv[cls];
+    const int mwn = (dir == 1 && (cy4 & 7) == 0) ? imin_(2, mwp) : mwp;
+    const bool subpu = (km[4] >> bit) & 1;
+    const int nx4 = dir == 0 ? cx4 - 1 : cx4, ny4 = dir == 0 ? cy4 : cy4 - 1;
+    auto blk = [&](int a4, int b4) { return ((b4 >> 3) - ty + 1) * 3 + ((a4 >> 3) - tx + 1); };
+    auto seg = [&](int a4, int b4) { return f.segmap_uv ? (int)sd.segc[b4 - CY0 + 3][a4 - CX0 + 1] : 0; };
+    auto ll = [&](int a4, int b4) { return (sd.llc[b4 - CY0 + 3][(a4 >> 3) - tx + 1] >> (a4 & 7)) & 1; };
+    const bool pos_ll = ll(cx4, cy4), neg_ll = ll(nx4, ny4);
     for (int pl = 0; pl < 2; pl++) {
         if (!(pl ? fp.deblock_level_v : fp.deblock_level_u)) continue;
-        uint32_t q, s;
-        chroma_thr(f, pl, cx4, cy4, nx4, ny4, subpu, q, s);
+        const uint32_t qs = edge_q_s(sd, 2 + pl, blk(cx4, cy4), seg(cx4, cy4), blk(nx4, ny4), seg(nx4, ny4), subpu);
         push_edge(sm, dir == 0 ? 1 : 3,
-                  EdgeDesc{q | (s << 16), pack_geo(cx - sx, cy - sy, mwp, mwn, pos_ll, neg_ll) | ((uint32_t)pl << 26)});
+                  EdgeDesc{qs, pack_geo(cx - sx, cy - sy, mwp, mwn, pos_ll, neg_ll) | ((uint32_t)pl << 26)});
     }
 }
 
@@ -414,8 +503,9 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
         }
         for (int k = 0; k < 4; k++) sm.uv[pl][r * CP + c4 + k] = (int16_t)v[k];
     }
-    // (no barrier: resolving the edges reads only the masks, so it overlaps
-    // the staging loads; the barrier below covers both)
+    // the tile's side-info (its loads are in flight together with the
+    // sample loads above); stage_side ends with a barrier
+    stage_side(f, sm.side, tx, ty, tid, nt);
     const bool do_y_v = fp.deblock_level_y[0] != 0, do_y_h = fp.deblock_level_y[1] != 0;
     const bool do_uv = fp.deblock_level_u || fp.deblock_level_v;
     // ---- resolve every edge segment that can matter into the tile's lists:
@@ -429,21 +519,21 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
         for (int i = tid; i < nlv + ncv + nlh + nch; i += nt) {
             int j = i;
             if (j < nlv) {
-                luma_edge(f, sm, 0, x0 - 4 + 4 * (j % 19), lsy + 4 * (j / 19), lsx, lsy);
+                luma_edge(f, sm, 0, x0 - 4 + 4 * (j % 19), lsy + 4 * (j / 19), lsx, lsy, tx, ty);
                 continue;
             }
             j -= nlv;
             if (j < ncv) {
-                chroma_edge(f, sm, 0, cx0 + 4 * (j % 9), csy + 4 * (j / 9), csx, csy);
+                chroma_edge(f, sm, 0, cx0 + 4 * (j % 9), csy + 4 * (j / 9), csx, csy, tx, ty);
                 continue;
             }
             j -= ncv;
             if (j < nlh) {
-                luma_edge(f, sm, 1, x0 + 4 * (j % 16), y0 - 4 + 4 * (j / 16), lsx, lsy);
+                luma_edge(f, sm, 1, x0 + 4 * (j % 16), y0 - 4 + 4 * (j / 16), lsx, lsy, tx, ty);
                 continue;
             }
             j -= nlh;
-            chroma_edge(f, sm, 1, cx0 + 4 * (j % 8), cy0 + 4 * (j / 8), csx, csy);
+            chroma_edge(f, sm, 1, cx0 + 4 * (j % 8), cy0 + 4 * (j / 8), csx, csy, tx, ty);
         }
     }
     __syncthreads();
