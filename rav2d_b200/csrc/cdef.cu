@@ -9,11 +9,13 @@
 // that is expressed directly: the kernel reads D and writes C.
 //
 // One CTA covers a 64x32 luma region of a 64-wide superblock column (32
-// 8x8 blocks) plus the co-located 32x16 chroma region.  The region and a
-// 2-sample halo are staged in shared memory (coordinates clamped to the
-// frame, which is CCSO's padding; CDEF substitutes INT16_MIN for taps outside
-// the frame, its padding), plus a block-major copy of the region's luma for
-// the direction search.
+// 8x8 blocks) plus the co-located 32x16 chroma region.  The region and its
+// halo are staged in shared memory in aligned 8-sample chunks (one 8- or
+// 16-byte load each; columns -8 .. 71 luma, -8 .. 39 chroma, rows -2 .. +1
+// beyond the region): coordinates clamped to the frame, which is CCSO's
+// padding, and a copy with INT16_MIN for taps outside the frame, CDEF's
+// padding; plus a block-major copy of the region's luma for the direction
+// search.
 //   phase 1: warp 0 decodes each block's strengths and skip / lossless state
 //            (lane = block);
 //   phase 2: warp d computes direction d's cost for every block (lane =
@@ -28,11 +30,18 @@ namespace {
 
 constexpr int RH = 32;   // luma rows per CTA region
 constexpr int NB = 32;   // 8x8 blocks per region (8 wide, 4 high)
-constexpr int TW = 68;   // luma tile width  (-2 .. 65)
+constexpr int XO = 8;    // tile column of the region's first sample
+// Tile pitches: TW / 2 = 4 (mod 8) words puts the 8 rows a warp reads in the
+// filter phase (4 lanes per row, 4 consecutive words) on 32 distinct banks;
+// CW = 56 does the same for the 2 planes x 4 rows of the chroma lanes.
+constexpr int TW = 88;   // luma tile pitch (columns -8 .. 71 used)
 constexpr int TH = RH + 4;   // luma tile height (-2 .. RH+1)
-constexpr int CW = 36;   // chroma tile width (-2 .. 33)
+constexpr int TCH = 10;  // 8-sample chunks per luma tile row
+constexpr int CW = 56;   // chroma tile pitch (columns -8 .. 39 used)
 constexpr int CH = RH / 2 + 4;  // chroma tile height
+constexpr int CCH = 6;   // 8-sample chunks per chroma tile row
 constexpr int BKP = 66;  // block-major pitch (int16): conflict-free per-lane reads
+constexpr int NCHUNK = TH * TCH + 2 * CH * CCH;
 
 __constant__ int8_t c_ccso_pos[7][2] = {{-1, 0}, {0, -1}, {-1, -1}, {-1, 1}, {-1, -2}, {1, -2}, {0, 2}};
 __constant__ uint8_t c_uv_dirs[8] = {0, 1, 2, 3, 4, 5, 6, 7};
@@ -170,16 +179,55 @@ R2G_D uint32_t dir_cost(const int16_t *b) {
 }
 
 struct CdefSmem {
-    int16_t ty[TH][TW];   // clamped to the frame (CCSO padding)
-    int16_t tc[2][CH][CW];
-    int16_t pty[TH][TW];  // INT16_MIN outside the frame (CDEF padding)
-    int16_t ptc[2][CH][CW];
+    alignas(16) int16_t ty[TH][TW];  // clamped to the frame (CCSO padding)
+    alignas(16) int16_t tc[2][CH][CW];
+    alignas(16) int16_t pty[TH][TW];  // INT16_MIN outside the frame (CDEF padding)
+    alignas(16) int16_t ptc[2][CH][CW];
     int16_t blk[NB][BKP]; // per block: (px >> bd8) - 128, raster order
     uint32_t cost[8][NB];
     BlockParams bp[NB];
     int toff_y[8][6], toff_c[8][6];  // tap offsets per direction (tile pitches)
     int s_ccso[3];
 };
+
+// Eight consecutive samples x0 .. x0+7 of one row as four int16 pairs (low
+// half = even sample), clamped to [0, w).  A chunk inside the row is one
+// 8-byte (8-bit) or 16-byte (16-bit) load: plane rows start 64-byte aligned
+// and x0 is a multiple of 8.  Chunks crossing a frame edge clamp per sample.
+template <typename P>
+R2G_D void load_chunk(const P *row, int x0, int w, uint32_t (&v)[4]) {
+    if (x0 >= 0 && x0 + 8 <= w) {
+        if (sizeof(P) == 1) {
+            const uint2 q = __ldg(reinterpret_cast<const uint2 *>(row + x0));
+            v[0] = __byte_perm(q.x, 0, 0x4140);
+            v[1] = __byte_perm(q.x, 0, 0x4342);
+            v[2] = __byte_perm(q.y, 0, 0x4140);
+            v[3] = __byte_perm(q.y, 0, 0x4342);
+        } else {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(row + x0));
+            v[0] = q.x;
+            v[1] = q.y;
+            v[2] = q.z;
+            v[3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            v[k] = (uint32_t)__ldg(row + iclip_(x0 + 2 * k, 0, w - 1)) |
+                   ((uint32_t)__ldg(row + iclip_(x0 + 2 * k + 1, 0, w - 1)) << 16);
+    }
+}
+
+// The same chunk with CDEF's padding (cdef_padding, cdef.rs:37): INT16_MIN
+// for samples outside the frame.
+R2G_D void pad_chunk(const uint32_t (&v)[4], bool row_out, int x0, int w, uint32_t (&pv)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const bool lo = !row_out && x0 + 2 * k >= 0 && x0 + 2 * k < w;
+        const bool hi = !row_out && x0 + 2 * k + 1 >= 0 && x0 + 2 * k + 1 < w;
+        pv[k] = (lo ? (v[k] & 0xffffu) : 0x8000u) | (hi ? (v[k] & 0xffff0000u) : 0x80000000u);
+    }
+}
 
 // One 64x32 region (superblock column sbx, region row rr) of the frame; the
 // work of one CTA, shared by the per-frame and the batched kernels.
@@ -263,38 +311,39 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
     // the deblocked planes come from the previous kernel on the stream:
     // wait for it before staging (everything above reads side-info only)
     pdl_wait();
-    // ---- stage the region (clamped coordinates) ----
-    for (int r = warp; r < TH; r += 8) {
-        const int ry = gy0 - 2 + r, gy = iclip_(ry, 0, f.h - 1);
-        const bool row_out = ry < 0 || ry >= f.h;
-        const P *row = Dy + gy * ys;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const int c = lane + 32 * j;
-            if (c < TW) {
-                const int rx = gx0 - 2 + c;
-                const int v = __ldg(row + iclip_(rx, 0, f.w - 1));
-                sm.ty[r][c] = (int16_t)v;
-                sm.pty[r][c] = (row_out || rx < 0 || rx >= f.w) ? (int16_t)INT16_MIN : (int16_t)v;
-                const int yy = r - 2, xx = c - 2;
-                if (yy >= 0 && yy < RH && xx >= 0 && xx < 64)
-                    sm.blk[(yy >> 3) * 8 + (xx >> 3)][(yy & 7) * 8 + (xx & 7)] = (int16_t)((v >> bd8) - 128);
+    // ---- stage the region and its halo, one 8-sample chunk per thread ----
+    for (int i = tid; i < NCHUNK; i += blockDim.x) {
+        uint32_t v[4], pv[4];
+        uint32_t *dt, *dp;
+        int yy = -1, bc = 0;
+        if (i < TH * TCH) {
+            const int r = i / TCH, k = i - r * TCH;
+            const int ry = gy0 - 2 + r, x0 = gx0 - XO + 8 * k;
+            load_chunk(Dy + iclip_(ry, 0, f.h - 1) * ys, x0, f.w, v);
+            pad_chunk(v, ry < 0 || ry >= f.h, x0, f.w, pv);
+            dt = reinterpret_cast<uint32_t *>(&sm.ty[r][8 * k]);
+            dp = reinterpret_cast<uint32_t *>(&sm.pty[r][8 * k]);
+            if (r >= 2 && r < RH + 2 && k >= 1 && k <= 8) {
+                yy = r - 2;
+                bc = k - 1;
             }
+        } else {
+            const int j = i - TH * TCH, pl = j / (CH * CCH), j2 = j - pl * (CH * CCH);
+            const int r = j2 / CCH, k = j2 - r * CCH;
+            const int ry = cy0 - 2 + r, x0 = cx0 - XO + 8 * k;
+            load_chunk((pl ? Dv : Du) + iclip_(ry, 0, f.ch - 1) * uvs, x0, f.cw, v);
+            pad_chunk(v, ry < 0 || ry >= f.ch, x0, f.cw, pv);
+            dt = reinterpret_cast<uint32_t *>(&sm.tc[pl][r][8 * k]);
+            dp = reinterpret_cast<uint32_t *>(&sm.ptc[pl][r][8 * k]);
         }
-    }
-    for (int r2 = warp; r2 < 2 * CH; r2 += 8) {
-        const int pl = r2 / CH, r = r2 % CH;
-        const int ry = cy0 - 2 + r, gy = iclip_(ry, 0, f.ch - 1);
-        const bool row_out = ry < 0 || ry >= f.ch;
-        const P *row = (pl ? Dv : Du) + gy * uvs;
+        *reinterpret_cast<uint4 *>(dt) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4 *>(dp) = make_uint4(pv[0], pv[1], pv[2], pv[3]);
+        if (yy >= 0) {
+            uint32_t *d = reinterpret_cast<uint32_t *>(&sm.blk[(yy >> 3) * 8 + bc][(yy & 7) * 8]);
 #pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const int c = lane + 32 * j;
-            if (c < CW) {
-                const int rx = cx0 - 2 + c;
-                const int v = __ldg(row + iclip_(rx, 0, f.cw - 1));
-                sm.tc[pl][r][c] = (int16_t)v;
-                sm.ptc[pl][r][c] = (row_out || rx < 0 || rx >= f.cw) ? (int16_t)INT16_MIN : (int16_t)v;
+            for (int q = 0; q < 4; q++) {
+                const int lo = (int)((v[q] & 0xffffu) >> bd8) - 128, hi = (int)((v[q] >> 16) >> bd8) - 128;
+                d[q] = ((uint32_t)lo & 0xffffu) | ((uint32_t)hi << 16);
             }
         }
     }
@@ -389,11 +438,11 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const int c = c0 + k;
-            const int16_t *t = &sm.ty[2 + r][2 + c];
+            const int16_t *t = &sm.ty[2 + r][XO + c];
             const int px = t[0];
             int v = px;
             if (p.active && p.y_on) {
-                v = cdef_px(&sm.pty[2 + r][2 + c], p.y_pri, p.y_sec, yoff, damping, bd8);
+                v = cdef_px(&sm.pty[2 + r][XO + c], p.y_pri, p.y_sec, yoff, damping, bd8);
                 v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
             }
             if (sm.s_ccso[0] && lossy_row) {
@@ -412,16 +461,19 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
             }
             out[k] = v;
         }
-        Cy[gy * ys + gx0 + c0] = (P)out[0];
-        Cy[gy * ys + gx0 + c0 + 1] = (P)out[1];
+        // the pair is 2-sample aligned (c0 even, 64-aligned region): one store
+        if (sizeof(P) == 1)
+            *reinterpret_cast<uint16_t *>(Cy + gy * ys + gx0 + c0) = (uint16_t)(out[0] | (out[1] << 8));
+        else
+            *reinterpret_cast<uint32_t *>(Cy + gy * ys + gx0 + c0) = (uint32_t)out[0] | ((uint32_t)out[1] << 16);
         // chroma: lane -> plane lane/16, row (lane%16)/4, column lane%4
         const int pl = lane >> 4, cr = br * 4 + ((lane & 15) >> 2), cc = bc * 4 + (lane & 3);
         const int cgy = cy0 + cr, cgx = cx0 + cc;
         P *Cp = plane_ptr<P>(f.C[1 + pl]);
-        const int px = sm.tc[pl][2 + cr][2 + cc];
+        const int px = sm.tc[pl][2 + cr][XO + cc];
         int v = px;
         if (p.active && p.uv_on) {
-            v = cdef_px(&sm.ptc[pl][2 + cr][2 + cc], p.uv_pri, p.uv_sec, uvoff, damping - 1, bd8);
+            v = cdef_px(&sm.ptc[pl][2 + cr][XO + cc], p.uv_pri, p.uv_sec, uvoff, damping - 1, bd8);
             v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
         }
         if (sm.s_ccso[1 + pl]) {
@@ -430,7 +482,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
             const bool ll = f.any_lossless && ((m.lossless_mask_uv[by_idx][sb64x_idx] >> (cc >> 2)) & 1);
             if (!ll) {
                 // co-located luma of the chroma sample (ccso_prep, 4:2:0)
-                const int16_t *t = &sm.ty[2 + 2 * cr][2 + 2 * cc];
+                const int16_t *t = &sm.ty[2 + 2 * cr][XO + 2 * cc];
                 const int cl = t[0];
                 const int band_ = (int)((uint32_t)cl >> (bitdepth - cpc.max_band_log2));
                 int idx;
