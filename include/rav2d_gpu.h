@@ -186,6 +186,7 @@ typedef struct R2gFrame R2gFrame;
  * (internal.rs:152-167) after Phase A: n_sb256 = sb256w * sb256h masks in
  * raster order, the same count of restoration records, and the optional
  * segment maps (b4 granularity; NULL = all segment 0). */
+struct R2gDbMaskInput;
 typedef struct R2gSideInfo {
     const R2gAv2Filter *masks;
     const R2gAv2Restoration *lr;
@@ -194,7 +195,51 @@ typedef struct R2gSideInfo {
     int32_t segmap_stride;
     const uint8_t *segmap_uv;
     int32_t segmap_uv_stride;
+    /* Optional (NULL = the masks' filter_y / filter_uv are used as given):
+     * the deblock edge masks are built on the device from the decoder's
+     * create_db_mask calls instead, and only the other Av2Filter fields
+     * are uploaded (filter_y / filter_uv of `masks` are not read). */
+    const struct R2gDbMaskInput *db_masks;
 } R2gSideInfo;
+
+/* One create_db_mask call of the decoder (decode.rs:7869-7912 for a coded
+ * block, :12893-12928 for a TIP superblock; lf_mask.rs:399-503): the
+ * Av2Block fields the mask builders read, for the luma call (bs, bx, by)
+ * or the chroma call (cbs, cbx, cby) of the block.  sizeof == 12. */
+typedef struct R2gDbBlock {
+    uint16_t bx, by;     /* frame position in luma 4x4 units */
+    uint8_t bs;          /* BlockSize (levels.rs) */
+    uint8_t flags;       /* R2G_DBB_* */
+    uint8_t tx_part;     /* TxPartition of the luma transform split */
+    uint8_t seg_id;
+    uint8_t inter_mode;  /* data.inter.inter_mode */
+    uint8_t comp_type;   /* data.inter.comp_type */
+    int8_t ref0, ref1;   /* ref_pair.r */
+} R2gDbBlock;
+#define R2G_DBB_CHROMA (1u << 0)    /* the chroma call (filter_uv) */
+#define R2G_DBB_INTRA (1u << 1)     /* is_intra */
+#define R2G_DBB_SKIP_TXFM (1u << 2) /* skip_txfm */
+#define R2G_DBB_TX_LL (1u << 3)     /* tx_size_ll (lossless luma transform) */
+#define R2G_DBB_REFINE_MV (1u << 4) /* data.inter.refine_mv */
+
+/* The frame's create_db_mask calls with the header fields they read
+ * (subpu_flt_lvl, lf_mask.rs:367-397) and the tile grid, whose starts reset
+ * the edge-level contexts (decode.rs:207 reset_context: the left context at
+ * every tile column of every superblock row, the above context at every
+ * tile row).  Blocks may come in any order: a block's context is the level
+ * its left / above neighbour left there, which is what the decoder's walk
+ * (neighbours first) reads. */
+typedef struct R2gDbMaskInput {
+    const R2gDbBlock *blocks;
+    int32_t n_blocks;
+    uint8_t sub_pu;            /* frame_hdr.deblock.sub_pu */
+    uint8_t tip_frame_mode;    /* frame_hdr.tip.frame_mode */
+    uint8_t tip_subpel_filter; /* frame_hdr.tip.subpel_filter */
+    uint8_t tip_refine_mv;     /* seq_hdr.tip_refine_mv */
+    int32_t n_tile_cols, n_tile_rows;
+    uint16_t tile_col_start4[64]; /* luma 4x4 units; [0] == 0, increasing */
+    uint16_t tile_row_start4[64];
+} R2gDbMaskInput;
 
 /* ---- version / capability ---- */
 int r2g_version(void);
@@ -252,6 +297,11 @@ int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2
 /* Run the filter stages of a staged frame on its uploaded recon (the recon
  * buffer is left unchanged, so a staged frame can be run again). */
 int r2g_frame_run(R2gCtx *ctx, R2gFrame *f);
+/* Copy a staged frame's SB256 records back as the stage kernels read them
+ * (with R2gSideInfo.db_masks: filter_y / filter_uv as the device built them
+ * from the block records).  `n` must be the frame's SB256 count.  No
+ * counterpart in the reference; for inspection and tests. */
+int r2g_frame_read_masks(R2gCtx *ctx, R2gFrame *f, R2gAv2Filter *out, int n);
 /* Run every enabled stage for the whole frame (r2g_frame_stage followed by
  * r2g_frame_run).  Equivalent to calling the
  * reference's `filter_sbrow` (decode.rs:3718-4058) for every sby of the frame

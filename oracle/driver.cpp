@@ -103,6 +103,9 @@ int r2o_filter_frame(const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t
     f.stride[0] = y_stride;
     f.stride[1] = uv_stride;
     f.mask.assign(side->masks, side->masks + side->n_sb256);
+    /* edge masks handed over as the decoder's create_db_mask calls: walk
+     * them as the decoder does */
+    if (side->db_masks) r2o_build_db_masks(side->db_masks, fp, f.mask.data(), side->n_sb256);
     f.lr_mask = side->lr;
     f.segmap = side->segmap;
     f.b4_stride = side->segmap_stride;

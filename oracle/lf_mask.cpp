@@ -214,6 +214,55 @@ static void create_db_mask(FilterMasks masks[2], const DbBlock &b, int bs, int b
     }
 }
 
+/* The decoder's walk over a frame's create_db_mask calls (decode.rs:7869-
+ * 7912, :12893-12928) in decode order: the left context (tx_lpf_y / _uv,
+ * indexed by the 4x4 row in the SB256 row) starts at 3 / 2 (decode.rs:207
+ * reset_context) for every tile column of every superblock row, the above
+ * context (indexed by the 4x4 column in the SB256 column) for every tile
+ * row; each call writes the masks of its SB256. */
+static void build_db_masks(const R2gDbMaskInput &in, const R2gFrameParams &fp, R2gAv2Filter *masks, int n_sb256) {
+    const int bw4 = ((fp.width + 7) >> 3) << 1, bh4 = ((fp.height + 7) >> 3) << 1;
+    const int sb256w = (bw4 + 63) >> 6;
+    for (int i = 0; i < n_sb256; i++) {
+        memset(masks[i].filter_y, 0, sizeof(masks[i].filter_y));
+        memset(masks[i].filter_uv, 0, sizeof(masks[i].filter_uv));
+    }
+    DbHeader h{in.sub_pu, in.tip_frame_mode, in.tip_subpel_filter, in.tip_refine_mv, {0}};
+    for (int i = 0; i < 8; i++) h.lossless[i] = fp.seg_lossless[i];
+    struct Ctx {
+        uint8_t y[64], uv[64];
+    };
+    std::vector<std::pair<long, Ctx>> lctx, actx;  // (key, context) created on first use
+    auto get = [](std::vector<std::pair<long, Ctx>> &v, long key) -> Ctx & {
+        for (auto &e : v)
+            if (e.first == key) return e.second;
+        Ctx c;
+        memset(c.y, 3, 64);
+        memset(c.uv, 2, 64);
+        v.push_back({key, c});
+        return v.back().second;
+    };
+    for (int i = 0; i < in.n_blocks; i++) {
+        const R2gDbBlock &r = in.blocks[i];
+        int tc = 0, tr = 0;
+        for (int t = 0; t < in.n_tile_cols; t++)
+            if (r.bx >= in.tile_col_start4[t]) tc = t;
+        for (int t = 0; t < in.n_tile_rows; t++)
+            if (r.by >= in.tile_row_start4[t]) tr = t;
+        Ctx &l = get(lctx, (long)tc * 4096 + (r.by >> 6));
+        Ctx &a = get(actx, (long)tr * 4096 + (r.bx >> 6));
+        DbBlock b{r.bs, (r.flags & R2G_DBB_INTRA) != 0, (r.flags & R2G_DBB_SKIP_TXFM) != 0, r.tx_part,
+                  (r.flags & R2G_DBB_TX_LL) != 0, r.seg_id, r.ref0, r.ref1, r.inter_mode,
+                  (r.flags & R2G_DBB_REFINE_MV) != 0, r.comp_type};
+        R2gAv2Filter &m = masks[(r.by >> 6) * sb256w + (r.bx >> 6)];
+        const bool chroma = (r.flags & R2G_DBB_CHROMA) != 0;
+        const int ss = chroma ? 1 : 0;
+        create_db_mask(chroma ? (FilterMasks *)m.filter_uv : (FilterMasks *)m.filter_y, b, r.bs, r.bx, r.by, bw4,
+                       bh4, I420, chroma, (chroma ? a.uv : a.y) + ((r.bx & 63) >> ss),
+                       (chroma ? l.uv : l.y) + ((r.by & 63) >> ss), h);
+    }
+}
+
 }  // namespace r2o
 
 /* ---- known-answer-test hooks (the reference's lf_mask.rs unit tests) ---- */
@@ -251,6 +300,10 @@ void r2o_create_db_mask(uint16_t *masks, const int *blk, int bs, int bx, int by,
     r2o::DbHeader h{hdr[0], hdr[1], hdr[2], hdr[3], {0}};
     for (int i = 0; i < 8; i++) h.lossless[i] = hdr[4 + i];
     r2o::create_db_mask((r2o::FilterMasks *)masks, b, bs, bx, by, iw, ih, layout, chroma != 0, a, l, h);
+}
+/* the frame's edge masks from its create_db_mask calls, walked in order */
+void r2o_build_db_masks(const R2gDbMaskInput *in, const R2gFrameParams *fp, R2gAv2Filter *masks, int n_sb256) {
+    r2o::build_db_masks(*in, *fp, masks, n_sb256);
 }
 /* lf_mask.rs:21-36 Av2Filter::default (cdef_idx -1, everything else 0) and
  * :45-51 Av2Restoration::default (all zero) */

@@ -106,4 +106,8 @@ void generate_scaling(int bitdepth, const uint8_t (*points)[2], int num, uint8_t
 
 }  // namespace r2o
 
+/* lf_mask.cpp: the decoder's walk over a frame's create_db_mask calls */
+extern "C" void r2o_build_db_masks(const R2gDbMaskInput *in, const R2gFrameParams *fp, R2gAv2Filter *masks,
+                                   int n_sb256);
+
 #endif

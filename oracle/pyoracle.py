@@ -53,6 +53,15 @@ def filter_frame(sf, inloop=None):
     return [p.astype(dt) for p in planes16]
 
 
+def build_db_masks(sf):
+    """The frame's edge masks from its block records (SynthFrame.use_db_blocks),
+    walked in decode order as the decoder's create_db_mask calls do; returns a
+    copy of sf.masks with filter_y / filter_uv rebuilt."""
+    masks = sf.masks.copy()
+    lib().r2o_build_db_masks(C.byref(sf.meta["db_input"]), C.byref(sf.fp), _p(masks), C.c_int(masks.shape[0]))
+    return masks
+
+
 def apply_grain(sf, planes):
     """Film grain on filtered planes; returns the display-copy planes."""
     src = [np.ascontiguousarray(p.astype(np.uint16)) for p in planes]

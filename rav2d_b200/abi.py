@@ -144,7 +144,51 @@ class SideInfo(C.Structure):
         ("segmap_stride", C.c_int32),
         ("segmap_uv", C.c_void_p),
         ("segmap_uv_stride", C.c_int32),
+        ("db_masks", C.c_void_p),
     ]
+
+
+# R2gDbBlock: one create_db_mask call (lf_mask.rs:399-503) of the decoder
+DB_BLOCK_DTYPE = np.dtype([
+    ("bx", "<u2"), ("by", "<u2"), ("bs", "u1"), ("flags", "u1"), ("tx_part", "u1"), ("seg_id", "u1"),
+    ("inter_mode", "u1"), ("comp_type", "u1"), ("ref0", "i1"), ("ref1", "i1"),
+])
+DBB_CHROMA, DBB_INTRA, DBB_SKIP_TXFM, DBB_TX_LL, DBB_REFINE_MV = 1, 2, 4, 8, 16
+
+
+class DbMaskInput(C.Structure):
+    """R2gDbMaskInput: the frame's create_db_mask calls, the header fields
+    subpu_flt_lvl reads (lf_mask.rs:367-397) and the tile starts that reset
+    the edge-level contexts (decode.rs:207)."""
+    _fields_ = [
+        ("blocks", C.c_void_p),
+        ("n_blocks", C.c_int32),
+        ("sub_pu", C.c_uint8),
+        ("tip_frame_mode", C.c_uint8),
+        ("tip_subpel_filter", C.c_uint8),
+        ("tip_refine_mv", C.c_uint8),
+        ("n_tile_cols", C.c_int32),
+        ("n_tile_rows", C.c_int32),
+        ("tile_col_start4", C.c_uint16 * 64),
+        ("tile_row_start4", C.c_uint16 * 64),
+    ]
+
+
+def db_mask_input(blocks, sub_pu=0, tip_frame_mode=0, tip_subpel_filter=0, tip_refine_mv=0,
+                  tile_cols=(0,), tile_rows=(0,)):
+    """Build an R2gDbMaskInput over a DB_BLOCK_DTYPE array (caller keeps it
+    alive); tile starts in luma 4x4 units."""
+    d = DbMaskInput()
+    d.blocks = blocks.ctypes.data if len(blocks) else None
+    d.n_blocks = len(blocks)
+    d.sub_pu, d.tip_frame_mode, d.tip_subpel_filter, d.tip_refine_mv = sub_pu, tip_frame_mode, \
+        tip_subpel_filter, tip_refine_mv
+    d.n_tile_cols, d.n_tile_rows = len(tile_cols), len(tile_rows)
+    for i, v in enumerate(tile_cols):
+        d.tile_col_start4[i] = v
+    for i, v in enumerate(tile_rows):
+        d.tile_row_start4[i] = v
+    return d
 
 
 class BatchItem(C.Structure):
@@ -225,6 +269,8 @@ STRUCT_SIZES = [
     ("R2gServeResult", C.sizeof(ServeResult)),
     ("R2gServeStats", C.sizeof(ServeStats)),
     ("R2gWienerParams", C.sizeof(WienerParams)),
+    ("R2gDbBlock", DB_BLOCK_DTYPE.itemsize),
+    ("R2gDbMaskInput", C.sizeof(DbMaskInput)),
 ]
 
 
@@ -242,9 +288,11 @@ def plane_geometry(width, height, bitdepth):
     return y_stride, uv_stride, ah, ah >> 1
 
 
-def side_info(masks, lr, segmap=None, segmap_stride=0, segmap_uv=None, segmap_uv_stride=0):
-    """Build an R2gSideInfo pointing at numpy arrays (caller keeps them alive)."""
+def side_info(masks, lr, segmap=None, segmap_stride=0, segmap_uv=None, segmap_uv_stride=0, db_masks=None):
+    """Build an R2gSideInfo pointing at numpy arrays (caller keeps them alive);
+    `db_masks` is an optional DbMaskInput (kept alive by the caller too)."""
     s = SideInfo()
+    s.db_masks = C.addressof(db_masks) if db_masks is not None else None
     s.masks = masks.ctypes.data
     s.lr = lr.ctypes.data
     s.n_sb256 = int(masks.shape[0])

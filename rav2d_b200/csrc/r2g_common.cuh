@@ -33,6 +33,10 @@ struct DevTables {
     const int16_t *GDF_BIAS;                // [36][3]
     const int8_t *GDF_INTRA_ERROR;          // [24576]
     const int8_t *GDF_INTER_ERROR;          // [30000]
+    const uint8_t *BLOCK_DIMENSIONS;        // [31][4]
+    const uint8_t *TXFM_DIMENSIONS;         // [25][8]
+    const uint8_t *MAX_TXFM_SIZE_FOR_BS;    // [31][4]
+    const int8_t *TX_PART_TBL;              // [31][8]
 };
 // Fills `t` with this device's table addresses (the current device).
 cudaError_t r2g_get_tables(DevTables *t);

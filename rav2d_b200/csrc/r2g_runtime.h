@@ -53,6 +53,7 @@ struct R2gCtx {
     // kernels, then the fault word (bounded waits that ran out)
     StageSched *sched = nullptr;
     unsigned *fault = nullptr;
+    unsigned *bad_blocks = nullptr;  // block records the mask builder skipped
 };
 // bytes of the context's device control block
 #define R2G_CTL_BYTES 256
@@ -82,7 +83,20 @@ struct R2gFrame {
     // (context stream), last download (down stream) of this frame
     cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_down = nullptr;
     bool pend_up = false, pend_comp = false, pend_down = false;
+    // device-built deblock masks (R2gSideInfo.db_masks): block records and
+    // level maps on the device, a pinned staging copy of the records, and
+    // the events that fork the build onto the side stream and join it back
+    void *dbm_dev = nullptr, *dbm_host = nullptr;
+    size_t dbm_bytes = 0, dbm_host_bytes = 0;
+    cudaEvent_t ev_dbm[2] = {nullptr, nullptr};
 };
+
+// Device mask build (dbmask.cu): zero the frame's filter_y / filter_uv and
+// build them from the block records; returns the kernels launched.
+int r2g_launch_db_masks(const R2gDbMaskInput &in, const R2gDbBlock *dev_blocks, R2gAv2Filter *dev_masks,
+                        int n_sb256, int sb256w, int bw4, int bh4, uint8_t *dev_levels, const uint8_t lossless[8],
+                        const DevTables &tab, unsigned *bad, cudaStream_t s);
+size_t r2g_db_levels_bytes(int bw4, int bh4);
 
 int r2g_dev_alloc(R2gCtx *ctx, void **p, size_t bytes);
 void r2g_dev_free(R2gCtx *ctx, void *p, size_t bytes);

@@ -9,6 +9,7 @@
 // A disabled stage aliases its output to its input, as the reference simply
 // skips it.
 #include <chrono>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -69,7 +70,8 @@ extern "C" int r2g_struct_sizes(int32_t *sizes, int n) {
                          (int32_t)sizeof(R2gFilmGrainData), (int32_t)sizeof(R2gSideInfo),
                          (int32_t)sizeof(R2gBatchItem), (int32_t)sizeof(R2gServeConfig),
                          (int32_t)sizeof(R2gServeRequest), (int32_t)sizeof(R2gServeResult),
-                         (int32_t)sizeof(R2gServeStats), (int32_t)sizeof(R2gWienerParams)};
+                         (int32_t)sizeof(R2gServeStats), (int32_t)sizeof(R2gWienerParams),
+                         (int32_t)sizeof(R2gDbBlock), (int32_t)sizeof(R2gDbMaskInput)};
     int m = (int)(sizeof(v) / sizeof(v[0]));
     for (int i = 0; i < n && i < m; i++) sizes[i] = v[i];
     return m;
@@ -104,6 +106,7 @@ extern "C" int r2g_ctx_create(int device, int64_t mem_budget, R2gCtx **out) {
     }
     ctx->sched = (StageSched *)ctl;
     ctx->fault = (unsigned *)((char *)ctl + 128);
+    ctx->bad_blocks = (unsigned *)((char *)ctl + 132);
     *out = ctx;
     return R2G_OK;
 }
@@ -232,6 +235,10 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     if (f->side_host) cudaFreeHost(f->side_host);
     if (f->seg_host) cudaFreeHost(f->seg_host);
     if (f->side_done) cudaEventDestroy(f->side_done);
+    r2g_dev_free(ctx, f->dbm_dev, f->dbm_bytes);
+    if (f->dbm_host) cudaFreeHost(f->dbm_host);
+    for (cudaEvent_t e : f->ev_dbm)
+        if (e) cudaEventDestroy(e);
     delete f;
     return R2G_OK;
 }
@@ -380,11 +387,17 @@ extern "C" int r2g_sync(R2gCtx *ctx) {
     for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
         if (st) CK(cudaStreamSynchronize(st));
     // a stage kernel whose bounded wait ran out left its work incomplete
-    uint32_t faults = 0;
-    CK(cudaMemcpy(&faults, ctx->fault, sizeof(faults), cudaMemcpyDeviceToHost));
-    if (faults) {
-        set_err(ctx, "%s", (std::to_string(faults) + " device-side waits ran out; the filtered output is incomplete").c_str());
+    uint32_t faults[2] = {0, 0};
+    CK(cudaMemcpy(faults, ctx->fault, sizeof(faults), cudaMemcpyDeviceToHost));
+    if (faults[0]) {
+        set_err(ctx, "%s", (std::to_string(faults[0]) + " device-side waits ran out; the filtered output is incomplete").c_str());
         return R2G_E_DEVICE;
+    }
+    // a block record the reference could not have produced was skipped
+    if (faults[1]) {
+        CK(cudaMemset(ctx->bad_blocks, 0, sizeof(unsigned)));  // reported once
+        set_err(ctx, "%s", (std::to_string(faults[1]) + " deblock block records were invalid and skipped").c_str());
+        return R2G_E_INVALID;
     }
     return R2G_OK;
 }
@@ -435,8 +448,86 @@ int r2g_validate(R2gCtx *ctx, const R2gFrame *f, const R2gFrameParams *fp, const
         set_err(ctx, "restoration unit size out of range");
         return R2G_E_INVALID;
     }
+    if (const R2gDbMaskInput *m = side->db_masks) {
+        const int bw4 = ((f->w + 7) >> 3) << 1, bh4 = ((f->h + 7) >> 3) << 1;
+        if (m->n_blocks < 0 || (m->n_blocks > 0 && !m->blocks) || m->n_tile_cols < 1 || m->n_tile_cols > 64 ||
+            m->n_tile_rows < 1 || m->n_tile_rows > 64 || bw4 > 2048 || bh4 > 2048) {
+            set_err(ctx, "invalid deblock block records");
+            return R2G_E_INVALID;
+        }
+        for (int i = 0; i < m->n_tile_cols; i++)
+            if (m->tile_col_start4[i] >= bw4 || (i && m->tile_col_start4[i] <= m->tile_col_start4[i - 1])) {
+                set_err(ctx, "tile column starts out of order or outside the frame");
+                return R2G_E_INVALID;
+            }
+        for (int i = 0; i < m->n_tile_rows; i++)
+            if (m->tile_row_start4[i] >= bh4 || (i && m->tile_row_start4[i] <= m->tile_row_start4[i - 1])) {
+                set_err(ctx, "tile row starts out of order or outside the frame");
+                return R2G_E_INVALID;
+            }
+    }
     // segmentation enabled without a map is accepted: the kernels read
     // segment 0 for every block when the map pointer is NULL
+    return R2G_OK;
+}
+
+// Stage the frame's block records and build its deblock masks on the device
+// (r2g_launch_db_masks) after the side-info copies on `cs`: records go
+// straight from page-locked caller memory in copy-overlap mode, else through
+// the frame's pinned staging copy.  The build runs on the side stream,
+// forked from and joined back to `cs` by events, so a stage kernel launched
+// with programmatic serialisation after it never overlaps the build.
+static int stage_db_masks(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gDbMaskInput &m,
+                          const DevFrame &d, cudaStream_t cs) {
+    const size_t rb = (size_t)m.n_blocks * sizeof(R2gDbBlock);
+    const size_t lb = r2g_db_levels_bytes(d.bw4, d.bh4);
+    const size_t need = ((rb + 255) & ~(size_t)255) + lb;
+    if (f->dbm_bytes < need) {
+        r2g_dev_free(ctx, f->dbm_dev, f->dbm_bytes);
+        f->dbm_dev = nullptr;
+        f->dbm_bytes = 0;
+        int rc = r2g_dev_alloc(ctx, &f->dbm_dev, need);
+        if (rc != R2G_OK) return rc;
+        f->dbm_bytes = need;
+    }
+    bool direct = false;
+    if (ctx->overlap && rb) {
+        cudaPointerAttributes am;
+        direct = cudaPointerGetAttributes(&am, m.blocks) == cudaSuccess && am.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+    }
+    if (rb && !direct && f->dbm_host_bytes < rb) {
+        if (f->dbm_host) cudaFreeHost(f->dbm_host);
+        f->dbm_host = nullptr;
+        f->dbm_host_bytes = 0;
+        if (cudaMallocHost(&f->dbm_host, rb) != cudaSuccess) {
+            cudaGetLastError();
+            set_err(ctx, "pinned allocation failed");
+            return R2G_E_OOM;
+        }
+        f->dbm_host_bytes = rb;
+    }
+    if (rb) {
+        const void *src = m.blocks;
+        if (!direct) {
+            memcpy(f->dbm_host, m.blocks, rb);
+            src = f->dbm_host;
+        }
+        CK(cudaMemcpyAsync(f->dbm_dev, src, rb, cudaMemcpyHostToDevice, cs));
+    }
+    for (cudaEvent_t &e : f->ev_dbm)
+        if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CK(cudaEventRecord(f->ev_dbm[0], cs));
+    CK(cudaStreamWaitEvent(ctx->side_stream, f->ev_dbm[0], 0));
+    uint8_t lossless[8];
+    for (int i = 0; i < 8; i++) lossless[i] = fp->seg_lossless[i];
+    ctx->launches += r2g_launch_db_masks(m, (const R2gDbBlock *)f->dbm_dev, (R2gAv2Filter *)f->side_dev, f->n_sb256,
+                                         d.sb256w, d.bw4, d.bh4,
+                                         (uint8_t *)f->dbm_dev + ((rb + 255) & ~(size_t)255), lossless, ctx->tab,
+                                         ctx->bad_blocks, ctx->side_stream);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(f->ev_dbm[1], ctx->side_stream));
+    CK(cudaStreamWaitEvent(cs, f->ev_dbm[1], 0));
     return R2G_OK;
 }
 
@@ -527,7 +618,23 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
                 memcpy(dst.f, src.ns_filter[0], sizeof(dst.f));
                 dst.pad = 0;
             }
-    if (direct) {
+    if (side->db_masks) {
+        // the edge masks are built on the device: upload the rest of each
+        // SB256 record only
+        const size_t head = offsetof(R2gAv2Filter, qidx), tail = sizeof(R2gAv2Filter) - head;
+        const char *src = (const char *)side->masks;
+        if (!direct) {
+            for (int i = 0; i < f->n_sb256; i++)
+                memcpy((char *)f->side_host + i * sizeof(R2gAv2Filter) + head, src + i * sizeof(R2gAv2Filter) + head,
+                       tail);
+            src = (const char *)f->side_host;
+        }
+        CK(cudaMemcpy2DAsync((char *)f->side_dev + head, sizeof(R2gAv2Filter), src + head, sizeof(R2gAv2Filter),
+                             tail, f->n_sb256, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpyAsync((char *)f->side_dev + mbytes, pk, lbytes, cudaMemcpyHostToDevice, cs));
+        int rc2 = stage_db_masks(ctx, f, fp, *side->db_masks, d, cs);
+        if (rc2 != R2G_OK) return rc2;
+    } else if (direct) {
         CK(cudaMemcpyAsync(f->side_dev, side->masks, mbytes, cudaMemcpyHostToDevice, cs));
         CK(cudaMemcpyAsync((char *)f->side_dev + mbytes, pk, lbytes, cudaMemcpyHostToDevice, cs));
     } else {
@@ -686,6 +793,19 @@ extern "C" int r2g_frame_run(R2gCtx *ctx, R2gFrame *f) {
     r2g_launch_pipeline(ctx, f->desc);
     CK(cudaGetLastError());
     return r2g_frame_after_compute(ctx, f);
+}
+
+extern "C" int r2g_frame_read_masks(R2gCtx *ctx, R2gFrame *f, R2gAv2Filter *out, int n) {
+    if (!ctx || !f || !out || n != f->n_sb256) return R2G_E_INVALID;
+    if (!f->staged) {
+        set_err(ctx, "frame has no staged side-info");
+        return R2G_E_INVALID;
+    }
+    CK(cudaSetDevice(ctx->device));
+    int rc = r2g_sync(ctx);
+    if (rc != R2G_OK) return rc;
+    CK(cudaMemcpy(out, f->side_dev, (size_t)n * sizeof(R2gAv2Filter), cudaMemcpyDeviceToHost));
+    return R2G_OK;
 }
 
 extern "C" int r2g_frame_filter(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSideInfo *side,

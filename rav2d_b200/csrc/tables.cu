@@ -29,5 +29,9 @@ cudaError_t r2g_get_tables(DevTables *t) {
     SYM(GDF_BIAS, GDF_BIAS);
     SYM(GDF_INTRA_ERROR, GDF_INTRA_ERROR);
     SYM(GDF_INTER_ERROR, GDF_INTER_ERROR);
+    SYM(BLOCK_DIMENSIONS, BLOCK_DIMENSIONS);
+    SYM(TXFM_DIMENSIONS, TXFM_DIMENSIONS);
+    SYM(MAX_TXFM_SIZE_FOR_BS, MAX_TXFM_SIZE_FOR_BS);
+    SYM(TX_PART_TBL, TX_PART_TBL);
     return cudaSuccess;
 }

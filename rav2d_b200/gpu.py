@@ -27,6 +27,7 @@ SYMBOLS = [
     "r2g_download_rows", "r2g_dsp_cdef_dir", "r2g_dsp_cdef_filter", "r2g_dsp_ccso_prep", "r2g_dsp_ccso_add",
     "r2g_dsp_gdf_add", "r2g_dsp_generate_grain", "r2g_dsp_ns_wiener_single_y", "r2g_dsp_ns_wiener_single_uv",
     "r2g_dsp_ns_wiener_multi", "r2g_dsp_pc_wiener", "r2g_dsp_gdf_prep", "r2g_ctx_device_faults",
+    "r2g_frame_read_masks",
 ]
 
 
@@ -63,6 +64,7 @@ def lib():
         L.r2g_frame_stage.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.FrameParams), C.POINTER(abi.SideInfo),
                                       C.c_uint32]
         L.r2g_frame_run.argtypes = [C.c_void_p, C.c_void_p]
+        L.r2g_frame_read_masks.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.r2g_ctx_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         L.r2g_ctx_profile.argtypes = [C.c_void_p, C.c_int]
         L.r2g_ctx_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
@@ -233,6 +235,13 @@ class Frame:
 
     def run(self):
         self.ctx.check(lib().r2g_frame_run(self.ctx.h, self.h))
+
+    def read_masks(self):
+        """The staged SB256 records as the stage kernels read them."""
+        n = ((self.width // 4 + 63) >> 6) * ((self.height // 4 + 63) >> 6)
+        out = np.zeros(n, abi.AV2_FILTER_DTYPE)
+        self.ctx.check(lib().r2g_frame_read_masks(self.ctx.h, self.h, _ptr(out), n))
+        return out
 
     def download_into(self, out, which=0):
         """Enqueue a download into preallocated (ideally pinned) planes."""

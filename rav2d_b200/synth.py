@@ -57,7 +57,19 @@ class SynthFrame:
         return self.fp.bitdepth
 
     def side(self):
-        return abi.side_info(self.masks, self.lr)
+        db = self.meta.get("db_input")
+        return abi.side_info(self.masks, self.lr, db_masks=db)
+
+    def use_db_blocks(self, blocks, hdr, garbage_rng=None):
+        """Hand the deblock masks over as block records (R2gSideInfo.db_masks);
+        with `garbage_rng` the given filter_y / filter_uv are overwritten with
+        noise, which the device build must ignore."""
+        self.meta["db_blocks"] = blocks
+        self.meta["db_hdr"] = hdr
+        self.meta["db_input"] = abi.db_mask_input(blocks, **hdr)
+        if garbage_rng is not None:
+            for k in ("filter_y", "filter_uv"):
+                self.masks[k] = garbage_rng.integers(0, 1 << 16, size=self.masks[k].shape).astype(np.uint16)
 
 
 def _plane(rng, w, h, rows, stride, bitdepth, pad_fill, bs=8):
@@ -173,6 +185,134 @@ def make_masks(rng, width, height, n_strengths, ccso_on=(1, 1, 1), gdf_p=0.5, no
         masks["lossless_mask_uv"] = (rng.random((n, 64, 4, 8)) < 0.05).astype(np.uint16).dot(
             (1 << np.arange(8)).astype(np.uint16)).astype(np.uint16)
     return masks
+
+
+def _c_table(name, dtype):
+    """A normative table from the generated csrc/av2_tables.h, as a flat array."""
+    import os
+    import re
+    txt = open(os.path.join(os.path.dirname(__file__), "csrc", "av2_tables.h")).read()
+    m = re.search(r"R2G_TABLE\(\w+, " + name + r"\)((?:\[\d+\])+) = \{([^}]*)\}", txt)
+    dims = [int(d) for d in re.findall(r"\d+", m.group(1))]
+    return np.array([int(v) for v in m.group(2).replace("\n", " ").split(",") if v.strip()], dtype).reshape(dims)
+
+
+_BLOCK_TABLES = {}
+
+
+def _block_tables():
+    if not _BLOCK_TABLES:
+        bd = _c_table("BLOCK_DIMENSIONS", np.int32)
+        _BLOCK_TABLES["bs_of"] = {(int(w), int(h)): i for i, (w, h, _, _) in enumerate(bd)}
+        _BLOCK_TABLES["tx_part"] = _c_table("TX_PART_TBL", np.int32)
+    return _BLOCK_TABLES
+
+
+def make_db_blocks(rng, width, height, *, seg_ids=1, tile_cols=(0,), tile_rows=(0,), tip_p=0.04, sub8_p=0.3,
+                   intra_p=0.35, skip_p=0.4):
+    """The create_db_mask calls of a random partition of the frame, in
+    decode order (tiles in raster order, SB256s in raster order inside a
+    tile, each partition tree depth first): a luma record per coded block and
+    a chroma record per 4:2:0 chroma block (for a split 8x8, after its last
+    luma block, at the 8x8's origin with BS_8X8, as decode.rs places cbx /
+    cby / cbs).  Square nodes split where half of them lies outside the
+    frame, as the partition syntax forces.  Returns (records, header dict
+    for abi.db_mask_input)."""
+    t = _block_tables()
+    bs_of, txp = t["bs_of"], t["tx_part"]
+    bw4, bh4 = ((width + 7) >> 3) << 1, ((height + 7) >> 3) << 1
+    recs = []
+
+    def rec(x, y, w, h, chroma, bs=None, ref0=None):
+        bs = bs_of[(w, h)] if bs is None else bs
+        intra = rng.random() < intra_p
+        flags = (abi.DBB_CHROMA if chroma else 0) | (abi.DBB_INTRA if intra else 0)
+        if not intra and rng.random() < skip_p:
+            flags |= abi.DBB_SKIP_TXFM
+        if rng.random() < 0.5:
+            flags |= abi.DBB_TX_LL
+        if rng.random() < 0.5:
+            flags |= abi.DBB_REFINE_MV
+        parts = np.nonzero(txp[bs] >= 0)[0]
+        r0 = ref0 if ref0 is not None else (7 if rng.random() < 0.1 else int(rng.integers(0, 7)))
+        r1 = -1 if rng.random() < 0.5 else int(rng.integers(0, 7))
+        recs.append((x, y, bs, flags, int(rng.choice(parts)) if len(parts) else 0, int(rng.integers(0, seg_ids)),
+                     int(rng.integers(0, 31)), int(rng.integers(0, 4)), r0, r1))
+
+    def leaf(x, y, w, h):
+        rec(x, y, w, h, False)
+        rec(x, y, w, h, True)
+
+    def node(x, y, w, h):
+        if x >= bw4 or y >= bh4:
+            return
+        if w == 2 and h == 2:  # 8x8: whole, or 4x4 / 4x8 / 8x4 luma blocks sharing one chroma block
+            if rng.random() < sub8_p:
+                kind = int(rng.integers(0, 3))
+                subs = {0: [(0, 0, 1, 1), (1, 0, 1, 1), (0, 1, 1, 1), (1, 1, 1, 1)],
+                        1: [(0, 0, 1, 2), (1, 0, 1, 2)], 2: [(0, 0, 2, 1), (0, 1, 2, 1)]}[kind]
+                for dx, dy, sw, sh in subs:
+                    if x + dx < bw4 and y + dy < bh4:
+                        rec(x + dx, y + dy, sw, sh, False)
+                rec(x, y, 2, 2, True)
+            else:
+                leaf(x, y, 2, 2)
+            return
+        if w == h:
+            has_rows, has_cols = y + h // 2 < bh4, x + w // 2 < bw4
+            if has_rows and has_cols:
+                pn = {64: 0.05, 32: 0.15, 16: 0.3, 8: 0.45, 4: 0.55}[w]
+                kind = int(rng.choice(4, p=[pn, 0.6 * (1 - pn), 0.2 * (1 - pn), 0.2 * (1 - pn)]))
+            elif has_cols:
+                kind = 1 if rng.random() < 0.5 else 2
+            elif has_rows:
+                kind = 1 if rng.random() < 0.5 else 3
+            else:
+                kind = 1
+            if kind == 0:
+                leaf(x, y, w, h)
+            elif kind == 1:
+                for dy in (0, h // 2):
+                    for dx in (0, w // 2):
+                        node(x + dx, y + dy, w // 2, h // 2)
+            elif kind == 2:  # horizontal halves
+                for dy in (0, h // 2):
+                    rect(x, y + dy, w, h // 2)
+            else:
+                for dx in (0, w // 2):
+                    rect(x + dx, y, w // 2, h)
+            return
+        rect(x, y, w, h)
+
+    def rect(x, y, w, h):
+        if x >= bw4 or y >= bh4:
+            return
+        if min(w, h) >= 4 and rng.random() < 0.3:  # halve the long side again
+            if w > h:
+                for dx in (0, w // 2):
+                    rect(x + dx, y, w // 2, h)
+            else:
+                for dy in (0, h // 2):
+                    rect(x, y + dy, w, h // 2)
+            return
+        leaf(x, y, w, h)
+
+    rows = list(tile_rows) + [bh4]
+    cols = list(tile_cols) + [bw4]
+    for tr in range(len(tile_rows)):
+        for tc in range(len(tile_cols)):
+            for sy in range(rows[tr], rows[tr + 1], 64):
+                for sx in range(cols[tc], cols[tc + 1], 64):
+                    if rng.random() < tip_p:  # a TIP superblock: one 256x256 block, chroma co-located
+                        rec(sx, sy, 64, 64, False, ref0=7)
+                        rec(sx, sy, 64, 64, True, ref0=7)
+                    else:
+                        node(sx, sy, 64, 64)
+    blocks = np.array(recs, abi.DB_BLOCK_DTYPE) if recs else np.zeros(0, abi.DB_BLOCK_DTYPE)
+    hdr = {"sub_pu": int(rng.random() < 0.7), "tip_frame_mode": int(rng.integers(0, 3)),
+           "tip_subpel_filter": int(rng.integers(0, 4)), "tip_refine_mv": int(rng.integers(0, 2)),
+           "tile_cols": tuple(tile_cols), "tile_rows": tuple(tile_rows)}
+    return blocks, hdr
 
 
 def _taps(rng, ranges, shape=()):
