@@ -18,7 +18,7 @@
 //   pass 1 (one thread per record): write the level the block leaves in the
 //          left context for each of its rows at its right-most 4x4 column,
 //          and the level it leaves in the above context for each column at
-//          its bottom 4x4 row, into frame-sized byte maps;
+//          its bottom 4x4 row, into frame-sized u16 maps;
 //   pass 2 (one thread per record): resolve the outer edges against the
 //          neighbour's cell in those maps (or the reset value at a tile
 //          start) and OR every edge bit into the SB256's masks with 32-bit
@@ -26,9 +26,14 @@
 //          edges reads the mask before OR-ing; only this block sets bits on
 //          its own rows at its interior positions, so the old value that
 //          atomicOr returns gives the same new bits as the sequential walk.
+// A 1:2:1 transform split (H5 / V5) whose parts do not reach the block's
+// far side (a lossless 4x4 transform in a taller block) leaves some rows /
+// columns of the context untouched: their cells hold 0x8000 | the block's
+// first column / row, and a reader steps over such blocks to the value
+// further left / up, as the walk carries it through.
 // Records that the reference could not have produced (out-of-range fields,
-// a block crossing its SB256, a transform split that does not tile the
-// block) are skipped and counted in the context's bad-record word.
+// a block crossing its SB256, a transform size the tables do not give) are
+// skipped and counted in the context's bad-record word.
 #include "r2g_common.cuh"
 
 namespace {
@@ -46,7 +51,7 @@ struct MaskArgs {
     R2gAv2Filter *masks;  // the frame's SB256 records (filter_y / filter_uv zeroed)
     int sb256w;
     int bw4, bh4;         // luma 4x4 units (the reference's fi.bw / fi.bh)
-    uint8_t *lv[4];       // left / above maps: luma (bh4 x bw4), chroma (bh4/2 x bw4/2)
+    uint16_t *lv[4];      // left / above maps: luma (bh4 x bw4), chroma (bh4/2 x bw4/2)
     int sub_pu, tip_frame_mode, tip_subpel_filter, tip_refine_mv;
     uint8_t lossless[8];
     uint32_t col_start[64], row_start[64];  // tile starts, bit per luma 4x4 column / row
@@ -123,10 +128,6 @@ R2G_D Geo geometry(const MaskArgs &a, const R2gDbBlock &b) {
         g.vlim = iclip_(g.subpu_l2 - g.ssv, 0, 3 - ci);
         g.twl4c = imin_(g.hlim, t[2]);
         g.thl4c = imin_(g.vlim, t[3]);
-        // an H5 / V5 split (1:2:1) must tile the block, as it does for every
-        // block size that has one
-        if (g.tx_part == TXP_H5 && g.h4 > 4 * g.th4) return g;
-        if (g.tx_part == TXP_V5 && g.w4 > 4 * g.tw4) return g;
         g.sub_twl = imin_(g.subpu_l2, t[2]);
         g.sub_thl = imin_(g.subpu_l2, t[3]);
     } else {
@@ -141,18 +142,46 @@ R2G_D Geo geometry(const MaskArgs &a, const R2gDbBlock &b) {
     return g;
 }
 
+constexpr int UNTOUCHED = -1;
+
 // The level this block's call(s) of mask_outer_edge_l write for row y (and
-// leave in the left context); mask_edges_part, lf_mask.rs:154-268.
+// leave in the left context), or UNTOUCHED; mask_edges_part,
+// lf_mask.rs:154-268.
 R2G_D int level_l(const Geo &g, int y) {
     if (!g.txb) return g.lvl_l;
-    if (g.tx_part == TXP_H5 && y >= g.th4 && y < 3 * g.th4) return imin_(g.twl4c + 1, g.hlim);
+    if (g.tx_part == TXP_H5) {
+        if (y >= g.th4 && y < 3 * g.th4) return imin_(g.twl4c + 1, g.hlim);
+        if (y >= 4 * g.th4) return UNTOUCHED;
+    }
     return g.twl4c;
 }
 // The same for column x and mask_outer_edge_t.
 R2G_D int level_t(const Geo &g, int x) {
     if (!g.txb) return g.lvl_t;
-    if (g.tx_part == TXP_V5 && x >= g.tw4 && x < 3 * g.tw4) return imin_(g.thl4c + 1, g.vlim);
+    if (g.tx_part == TXP_V5) {
+        if (x >= g.tw4 && x < 3 * g.tw4) return imin_(g.thl4c + 1, g.vlim);
+        if (x >= 4 * g.tw4) return UNTOUCHED;
+    }
     return g.thl4c;
+}
+
+// The context value a block starting at `pos` (column for the left context,
+// row for the above one) reads: the neighbour's cell at pos - 1 along
+// `step`, stepping over blocks that left it untouched, or the reset value
+// at a tile start.  `starts` is the tile-start bitmap along that axis (in
+// luma 4x4 units, `sh` the plane's subsampling).
+R2G_D int context_at(const uint16_t *map, size_t cell, int step, int pos, const uint32_t *starts, int sh, int reset) {
+    for (int guard = 0; guard < 4096; guard++) {
+        const int lp = pos << sh;
+        if ((starts[lp >> 5] >> (lp & 31)) & 1) return reset;
+        const uint16_t v = map[cell - step];
+        if (!(v & 0x8000)) return v;
+        const int start = v & 0x7fff;  // the untouched block's first column / row
+        if (start >= pos) return reset;   // only a stale cell (an incomplete record set) gets here
+        cell -= (size_t)(pos - start) * step;
+        pos = start;
+    }
+    return reset;
 }
 
 R2G_D uint64_t ones_shl(int n, int shift) { return (~0ull >> (64 - n)) << shift; }
@@ -181,9 +210,15 @@ __global__ void __launch_bounds__(128) db_levels_kernel(const __grid_constant__ 
     const Geo g = geometry(a, b);
     if (!g.ok) return;
     const int pw = a.bw4 >> g.ssh;  // map pitch
-    uint8_t *L = a.lv[g.chroma ? 2 : 0], *T = a.lv[g.chroma ? 3 : 1];
-    for (int y = 0; y < g.h4; y++) L[(size_t)(g.Y + y) * pw + g.X + g.w4 - 1] = (uint8_t)level_l(g, y);
-    for (int x = 0; x < g.w4; x++) T[(size_t)(g.Y + g.h4 - 1) * pw + g.X + x] = (uint8_t)level_t(g, x);
+    uint16_t *L = a.lv[g.chroma ? 2 : 0], *T = a.lv[g.chroma ? 3 : 1];
+    for (int y = 0; y < g.h4; y++) {
+        const int l = level_l(g, y);
+        L[(size_t)(g.Y + y) * pw + g.X + g.w4 - 1] = (uint16_t)(l == UNTOUCHED ? 0x8000 | g.X : l);
+    }
+    for (int x = 0; x < g.w4; x++) {
+        const int l = level_t(g, x);
+        T[(size_t)(g.Y + g.h4 - 1) * pw + g.X + x] = (uint16_t)(l == UNTOUCHED ? 0x8000 | g.Y : l);
+    }
 }
 
 __global__ void __launch_bounds__(128) db_masks_kernel(const __grid_constant__ MaskArgs a) {
@@ -199,20 +234,18 @@ __global__ void __launch_bounds__(128) db_masks_kernel(const __grid_constant__ M
     R2gAv2Filter &f = a.masks[g.sb];
     uint16_t(*m)[64][5][4] = g.chroma ? f.filter_uv : f.filter_y;
     const int pw = a.bw4 >> g.ssh, ci = g.chroma;
-    const uint8_t *L = a.lv[ci ? 2 : 0], *T = a.lv[ci ? 3 : 1];
+    const uint16_t *L = a.lv[ci ? 2 : 0], *T = a.lv[ci ? 3 : 1];
     const int reset = 3 - ci;
-    // tile starts (tile starts are superblock-aligned, so the chroma column
-    // X starts a tile when luma column 2X does)
-    const int lx = g.X << g.ssh, ly = g.Y << g.ssv;
-    const bool left_reset = (a.col_start[lx >> 5] >> (lx & 31)) & 1;
-    const bool top_reset = (a.row_start[ly >> 5] >> (ly & 31)) & 1;
 
-    // ---- outer edges against the neighbours' context levels ----
+    // ---- outer edges against the neighbours' context levels (tile starts
+    // are superblock-aligned, so chroma column X starts a tile when luma
+    // column 2X does; levels read from the maps are 0..3) ----
     uint64_t byl[4] = {0, 0, 0, 0};
     for (int y = 0; y < g.h4; y++) {
         const int own = level_l(g, y);
-        const int nb = left_reset ? reset : L[(size_t)(g.Y + y) * pw + g.X - 1];
-        byl[imin_(own, nb)] |= 1ull << (g.by4 + y);
+        if (own == UNTOUCHED) continue;
+        const int nb = context_at(L, (size_t)(g.Y + y) * pw + g.X, 1, g.X, a.col_start, g.ssh, reset);
+        byl[imin_(own, nb) & 3] |= 1ull << (g.by4 + y);
     }
 #pragma unroll
     for (int l = 0; l < 4; l++)
@@ -220,8 +253,9 @@ __global__ void __launch_bounds__(128) db_masks_kernel(const __grid_constant__ M
     uint64_t bxl[4] = {0, 0, 0, 0};
     for (int x = 0; x < g.w4; x++) {
         const int own = level_t(g, x);
-        const int nb = top_reset ? reset : T[(size_t)(g.Y - 1) * pw + g.X + x];
-        bxl[imin_(own, nb)] |= 1ull << (g.bx4 + x);
+        if (own == UNTOUCHED) continue;
+        const int nb = context_at(T, (size_t)g.Y * pw + g.X + x, pw, g.Y, a.row_start, g.ssv, reset);
+        bxl[imin_(own, nb) & 3] |= 1ull << (g.bx4 + x);
     }
 #pragma unroll
     for (int l = 0; l < 4; l++)
@@ -281,7 +315,7 @@ __global__ void __launch_bounds__(128) db_masks_kernel(const __grid_constant__ M
 // Zero the frame's filter_y / filter_uv, then the two passes; returns the
 // number of kernels launched.
 int r2g_launch_db_masks(const R2gDbMaskInput &in, const R2gDbBlock *dev_blocks, R2gAv2Filter *dev_masks,
-                        int n_sb256, int sb256w, int bw4, int bh4, uint8_t *dev_levels, const uint8_t lossless[8],
+                        int n_sb256, int sb256w, int bw4, int bh4, void *dev_levels, const uint8_t lossless[8],
                         const DevTables &tab, unsigned *bad, cudaStream_t s) {
     cudaMemset2DAsync(dev_masks, sizeof(R2gAv2Filter), 0, sizeof(dev_masks->filter_y) + sizeof(dev_masks->filter_uv),
                       n_sb256, s);
@@ -295,10 +329,11 @@ int r2g_launch_db_masks(const R2gDbMaskInput &in, const R2gDbBlock *dev_blocks, 
     a.bw4 = bw4;
     a.bh4 = bh4;
     const size_t ly = (size_t)bw4 * bh4, lc = ly / 4;
-    a.lv[0] = dev_levels;
-    a.lv[1] = dev_levels + ly;
-    a.lv[2] = dev_levels + 2 * ly;
-    a.lv[3] = dev_levels + 2 * ly + lc;
+    uint16_t *lv = static_cast<uint16_t *>(dev_levels);
+    a.lv[0] = lv;
+    a.lv[1] = lv + ly;
+    a.lv[2] = lv + 2 * ly;
+    a.lv[3] = lv + 2 * ly + lc;
     a.sub_pu = in.sub_pu;
     a.tip_frame_mode = in.tip_frame_mode;
     a.tip_subpel_filter = in.tip_subpel_filter;
@@ -319,4 +354,4 @@ int r2g_launch_db_masks(const R2gDbMaskInput &in, const R2gDbBlock *dev_blocks, 
 }
 
 // Bytes of the level maps r2g_launch_db_masks needs for a frame.
-size_t r2g_db_levels_bytes(int bw4, int bh4) { return (size_t)bw4 * bh4 * 5 / 2; }
+size_t r2g_db_levels_bytes(int bw4, int bh4) { return (size_t)bw4 * bh4 * 5; }

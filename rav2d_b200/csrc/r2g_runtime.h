@@ -94,7 +94,7 @@ struct R2gFrame {
 // Device mask build (dbmask.cu): zero the frame's filter_y / filter_uv and
 // build them from the block records; returns the kernels launched.
 int r2g_launch_db_masks(const R2gDbMaskInput &in, const R2gDbBlock *dev_blocks, R2gAv2Filter *dev_masks,
-                        int n_sb256, int sb256w, int bw4, int bh4, uint8_t *dev_levels, const uint8_t lossless[8],
+                        int n_sb256, int sb256w, int bw4, int bh4, void *dev_levels, const uint8_t lossless[8],
                         const DevTables &tab, unsigned *bad, cudaStream_t s);
 size_t r2g_db_levels_bytes(int bw4, int bh4);
 
