@@ -157,6 +157,13 @@ typedef struct R2gFrameParams {
     uint8_t frame_type;
     uint8_t n_ref_frames;
     uint8_t absrefdist[7];
+    /* TileInfo rows (headers.rs:325-337), read by init_start_of_tile_row
+     * (decode.rs:99-120) for the loop-restoration stripes: tile_rows and
+     * row_start_sb in superblock units (tile_rows + 1 entries).  tile_rows
+     * 0 is taken as one tile row. */
+    uint8_t tile_rows;
+    uint8_t _pad1;
+    uint16_t tile_row_start_sb[65];
 } R2gFrameParams;
 
 /* Mirrors `FilmGrainData` (headers.rs:509-525). */

@@ -114,9 +114,18 @@ int r2o_filter_frame(const R2gFrameParams *fp, const R2gSideInfo *side, uint32_t
     init_wiener(f);
     f.restore_planes = compute_restore_planes(fp);
     f.gdf_ref_dst_idx = compute_gdf_ref_dst_idx(fp);
-    /* decode.rs:82-100 init_start_of_tile_row with one tile row */
+    /* decode.rs:99-120 init_start_of_tile_row: (tile row << 1) | 1 on a
+     * tile row's first superblock row, tile row << 1 on the others */
     f.start_of_tile_row.assign(f.sbh, 0);
-    f.start_of_tile_row[0] = 1;
+    {
+        int rows = fp->tile_rows ? fp->tile_rows : 1;
+        int sby = 0;
+        for (int tr = 0; tr < rows && sby < f.sbh; tr++) {
+            f.start_of_tile_row[sby++] = (uint8_t)((tr << 1) | 1);
+            int end = fp->tile_rows ? imin(fp->tile_row_start_sb[tr + 1], f.sbh) : f.sbh;
+            while (sby < end) f.start_of_tile_row[sby++] = (uint8_t)(tr << 1);
+        }
+    }
     f.cdef_line_toggle = 0;
     for (int sby = 0; sby < f.sbh; sby++) filter_sbrow(f, sby, inloop);
     return 0;

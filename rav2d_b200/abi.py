@@ -112,6 +112,9 @@ class FrameParams(C.Structure):
         ("frame_type", C.c_uint8),
         ("n_ref_frames", C.c_uint8),
         ("absrefdist", C.c_uint8 * 7),
+        ("tile_rows", C.c_uint8),
+        ("_pad1", C.c_uint8),
+        ("tile_row_start_sb", C.c_uint16 * 65),
     ]
 
 

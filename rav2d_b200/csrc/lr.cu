@@ -39,7 +39,8 @@
 
 namespace {
 
-enum { LR_HAVE_LEFT = 1, LR_HAVE_RIGHT = 2, LR_HAVE_TOP = 4, LR_HAVE_BOTTOM = 8 };
+enum { LR_HAVE_LEFT = 1, LR_HAVE_RIGHT = 2, LR_HAVE_TOP = 4, LR_HAVE_BOTTOM = 8, LR_HAVE_TOP_INTEGRATED = 16,
+       LR_HAVE_BOTTOM_INTEGRATED = 32 };
 enum { W_NONE = 0, W_NS_SINGLE = 1, W_NS_MULTI = 2, W_PC = 3 };
 
 constexpr int NCW = 8;           // consumer warps
@@ -71,6 +72,7 @@ __constant__ int16_t c_mode_offsets[4] = {-547, -21565, -573, -680};
 
 struct UnitGeom {
     int plane, x0, uw, y0, sh, edges, valid;
+    int l45;  // top-integrated luma stripe: the deblocked row behind saved rows 4 and 5
     int sb256x, sb64x_idx;
     const LrUnitPacked *unit;
 };
@@ -85,40 +87,68 @@ R2G_D int get_qval(int qstep, int tskip, int i, int b8) {
     return 255 * (c_mode_offsets[i] + qval);
 }
 
+R2G_D bool tile_row_first(const DevFrame &f, int sby) {
+    return sby > 0 && sby < 128 && ((f.tr_first[sby >> 5] >> (sby & 31)) & 1);
+}
+
 // Stripe geometry and unit selection, following lr_sbrow_apply /
-// lr_sbrow_plane / lr_stripe for one tile row (sb128 = 0).  A superblock
-// row's LR call covers [y_call, row_h); its first stripe is 56 (luma) rows
-// high on superblock row 0 and 64 otherwise, so a call holds one stripe, or
-// two when the frame height is a multiple of 64 and this is the last
-// superblock row.
-R2G_D void unit_geom(const DevFrame &f, int plane, int sby, int sub, int ux, UnitGeom &g) {
+// lr_sbrow_plane / lr_stripe (sb128 = 0).  A superblock row's LR call
+// covers [y_call, row_h); its first stripe is 56 (luma) rows high on the
+// first superblock row of a tile row and 64 otherwise, so a call holds one
+// stripe, or two when the frame height is a multiple of 64 and this is the
+// last superblock row (mode 1 is that second stripe).  On the first
+// superblock row of a later tile row the call is split
+// (looprestoration.rs:2424-2548): mode 2 is the 8-row stripe above the tile
+// row's top edge, which reads the rows below it in place
+// (LR_HAVE_BOTTOM_INTEGRATED), and the call's first stripe starts at the
+// edge and reads four saved deblocked rows above it (LR_HAVE_TOP_INTEGRATED).
+R2G_D void unit_geom(const DevFrame &f, int plane, int sby, int mode, int ux, UnitGeom &g) {
     const int chroma = plane != 0;
     const int ss = chroma;  // 4:2:0: ss_hor = ss_ver = 1 for chroma
     const int W = chroma ? f.cw : f.w, H = chroma ? f.ch : f.h;
     const int not_last = sby + 1 < f.sbh;
     const int next_row_y = (sby + 1) << (6 - ss);
-    const int row_h = imin_(next_row_y - (8 >> ss) * not_last, H);
-    const int y_call = (sby << (6 - ss)) - ((8 * (sby != 0)) >> ss);
-    const int sh0 = imin_((sby == 0 ? 56 : 64) >> ss, row_h - y_call);
-    int y0 = y_call, sh = sh0;
-    if (sub) {
-        y0 = y_call + sh0;
-        sh = imin_(64 >> ss, row_h - y0);
+    const int trf = tile_row_first(f, sby);
+    const int first = sby == 0 || trf;  // FirstSbInTileRow other than None
+    int row_h = imin_(next_row_y - (8 >> ss) * not_last, H);
+    const int y_call = (sby << (6 - ss)) - (first ? 0 : (8 >> ss));
+    int y0, sh, edges;
+    if (mode == 2) {
+        // the 8 rows above the tile row's top edge (FirstSbInTileRow::Top)
+        y0 = y_call - (8 >> ss);
+        row_h = y_call;
+        sh = row_h - y0;
+        edges = LR_HAVE_TOP | LR_HAVE_BOTTOM_INTEGRATED;
+    } else {
+        const int sh0 = imin_((first ? 56 : 64) >> ss, row_h - y_call);
+        y0 = y_call;
+        sh = sh0;
+        edges = y0 > 0 ? LR_HAVE_TOP : 0;
+        if (trf && mode == 0) edges |= LR_HAVE_TOP_INTEGRATED;
+        if (mode == 1) {
+            y0 = y_call + sh0;
+            sh = imin_(64 >> ss, row_h - y0);
+            edges = LR_HAVE_TOP;
+        }
     }
     g.plane = plane;
     g.y0 = y0;
     g.sh = sh;
     g.x0 = ux * 64;
     g.uw = imin_(64, W - g.x0);
-    g.edges = (y0 > 0 ? LR_HAVE_TOP : 0) | (ux > 0 ? LR_HAVE_LEFT : 0) | (g.x0 + 64 < W ? LR_HAVE_RIGHT : 0) |
+    g.edges = edges | (ux > 0 ? LR_HAVE_LEFT : 0) | (g.x0 + 64 < W ? LR_HAVE_RIGHT : 0) |
               ((not_last || y0 + sh != row_h) ? LR_HAVE_BOTTOM : 0);
+    // saved deblocked rows 4 and 5 of a top-integrated luma stripe: the
+    // superblock row's own backup (copy_db / backup_db, deblock.rs:2192-2264)
+    // when it saved a stripe boundary, else the previous one left in place
+    g.l45 = (y0 + 56 <= f.h - 1) ? y0 + 54 : y0 - 10;
     g.sb256x = (g.x0 << ss) >> 8;
     g.sb64x_idx = ((g.x0 << ss) >> 6) & 3;
     // unit selection (looprestoration.rs:2295-2331) from the call's first
-    // row; only sby 0 is the first superblock row of the (single) tile row
+    // row, 8 (luma) rows lower on a tile row's first superblock row
     const int unit_size = 1 << f.fp.restoration_unit_size[chroma];
     const int half = unit_size >> 1;
-    int row_y = y_call + ((8 >> ss) * (sby == 0));
+    const int row_y = (mode == 2 ? y0 : y_call) + ((8 >> ss) * (first || mode == 2));
     int aligned = row_y & ~(unit_size - 1);
     if (aligned != 0 && aligned + half > H) aligned -= unit_size;
     aligned <<= ss;
@@ -139,6 +169,23 @@ R2G_D void unit_geom(const DevFrame &f, int plane, int sby, int sub, int ux, Uni
 // Source row of window row r (stripe-relative) and whether it is deblocked.
 R2G_D void row_src(const UnitGeom &g, int r, int &row, bool &from_d) {
     if (r >= 0 && r < g.sh) {
+        row = g.y0 + r;
+        from_d = false;
+    } else if (r < 0 && (g.edges & LR_HAVE_TOP_INTEGRATED)) {
+        // the saved deblocked rows 0.. of the line store (the previous stripe
+        // boundary's four rows, then the superblock row's own): luma window
+        // rows -6 .. -1 hold saved rows 0 .. 5 as gdf_prep reads them (the
+        // Wiener filters read rows 0 .. 3 as -4 .. -1, see filter_luma);
+        // chroma rows -2, -1 hold saved rows 0, 1
+        from_d = true;
+        if (g.plane) {
+            row = g.y0 - 6 + (r + 2);
+        } else {
+            const int k = r + 6;
+            row = k < 4 ? g.y0 - 10 + k : g.l45 + (k - 4);
+        }
+    } else if (r >= g.sh && (g.edges & LR_HAVE_BOTTOM_INTEGRATED)) {
+        // the rows below, read in place: not yet restored
         row = g.y0 + r;
         from_d = false;
     } else if (r < 0) {
@@ -207,6 +254,11 @@ struct LrSmem {
             uint32_t lwin[CH2 * CW2];  // downsampled luma window, same pairing
         } ch;
     } u;
+    // a top-integrated luma item's rows -4 .. 8 as the Wiener filters and the
+    // classification read them (saved rows 0 .. 3 above the stripe; the
+    // window holds gdf_prep's saved rows 0 .. 5 there), same layout as wp
+    // (rows -6, -5 unused)
+    uint32_t wtop[15 * LW];
     uint16_t gcell[17 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
     uint8_t classes[8][16];
     // consumer-side copies of the item's row data (the slot is released
@@ -234,11 +286,14 @@ R2G_D int uhi(uint32_t v) { return (int)(v >> 16); }
 // Per-frame item index b -> geometry (luma items first: stripe slot, row
 // part, unit; then U, then V: stripe slot, row part, unit).  Slots
 // 0 .. sbh-1 are the superblock rows' first stripes; slot sbh is the second
-// stripe only the last superblock row can have.  False: an empty item.
+// stripe only the last superblock row can have; slots sbh+1 .. sbh+n_tr are
+// the 8-row stripes above the tile rows after the first.  False: an empty
+// item.
 R2G_D bool item_geom(const DevFrame &f, int b, UnitGeom &g, int &ro, int &nr) {
     const int nux_l = (f.w + 63) >> 6, nux_c = (f.cw + 63) >> 6;
     const int nparts = 64 / f.lr_rows;
-    const int n_luma = (f.sbh + 1) * nparts * nux_l;
+    const int nslots = f.sbh + 1 + f.n_tr;
+    const int n_luma = nslots * nparts * nux_l;
     int plane, ux, part, slot;
     if (b < n_luma) {
         plane = 0;
@@ -248,7 +303,7 @@ R2G_D bool item_geom(const DevFrame &f, int b, UnitGeom &g, int &ro, int &nr) {
         slot = b / nparts;
     } else {
         b -= n_luma;
-        const int per = (f.sbh + 1) * 2 * nux_c;
+        const int per = nslots * 2 * nux_c;
         plane = 1 + b / per;
         b %= per;
         ux = b % nux_c;
@@ -256,8 +311,12 @@ R2G_D bool item_geom(const DevFrame &f, int b, UnitGeom &g, int &ro, int &nr) {
         part = b & 1;
         slot = b >> 1;
     }
-    const int sub = slot >= f.sbh;
-    unit_geom(f, plane, sub ? f.sbh - 1 : slot, sub, ux, g);
+    if (slot > f.sbh)
+        unit_geom(f, plane, f.tr_sby[slot - f.sbh - 1], 2, ux, g);
+    else if (slot == f.sbh)
+        unit_geom(f, plane, f.sbh - 1, 1, ux, g);
+    else
+        unit_geom(f, plane, slot, 0, ux, g);
     const int rows = plane ? CROWS : f.lr_rows;
     ro = part * rows;
     nr = imin_(rows, g.sh - ro);
@@ -317,13 +376,19 @@ R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int 
         }
         const int lce = imin_(2 * g.x0 + 128 + RG::XO, (int)ls);
         const uint32_t lbytes = (uint32_t)((lce - lcs) * bps);
+        const bool topi = g.edges & LR_HAVE_TOP_INTEGRATED, boti = g.edges & LR_HAVE_BOTTOM_INTEGRATED;
         for (int q = lane; q < 2 * wrows; q += 32) {
             int rr = ro + (q >> 1) - 2;
             if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
-            if (!(g.edges & LR_HAVE_BOTTOM) && rr >= g.sh) rr = g.sh - 1;
+            if (!(g.edges & LR_HAVE_BOTTOM) && !boti && rr >= g.sh) rr = g.sh - 1;
             const char *src;
             int ra, rb;
-            if (rr == -2) {
+            if ((rr < 0 && topi) || (rr >= g.sh && boti)) {
+                // integrated edges read the luma rows in place (pre-LR)
+                src = Cy;
+                ra = 2 * (g.y0 + rr);
+                rb = ra + 1;
+            } else if (rr == -2) {
                 src = Dy;
                 ra = rb = 2 * g.y0 - 2;
             } else if (rr == -1) {
@@ -372,7 +437,10 @@ R2G_D int produce_item(const DevFrame &f, int fi, int b, LrSmem &sm, int k, int 
         else if (wt == R2G_RESTORE_PC_WIENER)
             wkind = W_PC;
     }
-    const int inc = ((g.edges & LR_HAVE_TOP) && g.y0 + 8 < ((f.bh4 * 4) >> chroma)) ? 8 : 0;
+    const int inc = ((g.edges & (LR_HAVE_TOP | LR_HAVE_TOP_INTEGRATED | LR_HAVE_BOTTOM_INTEGRATED)) == LR_HAVE_TOP &&
+                     g.y0 + 8 < ((f.bh4 * 4) >> chroma))
+                        ? 8
+                        : 0;
     const int sb256_idx = f.sb256w * (((g.y0 << chroma) + inc) >> 8) + g.sb256x;
     const int nsb = f.sb256w * f.sb256h;
     const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && sb256_idx < nsb &&
@@ -755,10 +823,11 @@ R2G_D void gdf_pair(const DevFrame &f, const LrSmem &sm, const uint32_t *wc, int
 // Filters one staged luma item (everything after the window is built).
 template <typename P>
 R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, int ro, int nr, int uw, int kind,
-                       bool gdf, int c0, int tid) {
+                       bool gdf, int c0, bool topi, int tid) {
     const int warp = tid >> 5, lane = tid & 31;
     const R2gFrameParams &fp = f.fp;
     const int16_t *W16 = reinterpret_cast<const int16_t *>(sm.u.wp);  // scalar sample i at W16[2 * i]
+    const int16_t *WT16 = reinterpret_cast<const int16_t *>(sm.wtop);
     const int bh4 = nr >> 2, bw4 = uw >> 2, sbh4 = sh >> 2;
     const int b8 = f.bitdepth - 8;
     // ---- phase 1: GDF gradient cells (compute_gradient_row :114-193) and
@@ -804,7 +873,7 @@ R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, in
             for (int dy = -1; dy <= 4; dy++)
 #pragma unroll
                 for (int dx = -1; dx <= 4; dx++) {
-                    const int16_t *w = &W16[2 * ((by * 4 + dy + 6) * LW + bx * 4 + dx + 6)];
+                    const int16_t *w = &(topi && by == 0 ? WT16 : W16)[2 * ((by * 4 + dy + 6) * LW + bx * 4 + dx + 6)];
                     constexpr int R = 2 * LW, C1 = 2;
                     const int m2 = 2 * w[0];
                     const int vert = w[-R] - m2 + w[R];
@@ -852,6 +921,7 @@ R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, in
     if (x1 >= uw) return;
     for (int y = warp; y < nr; y += NCW) {
         const uint32_t *wc = &sm.u.wp[(y + 6) * LW + x1 + 6];
+        const uint32_t *wf = topi && y < 4 ? &sm.wtop[(y + 6) * LW + x1 + 6] : wc;  // the Wiener taps' rows
         const uint32_t mm = wc[0];
         int v0 = ulo(mm), v1 = uhi(mm);
         const bool ll = (sm.llm[(ro + y) >> 2] >> (x1 >> 2)) & 1;
@@ -867,7 +937,7 @@ R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, in
 #pragma unroll
                     for (int k = 0; k < 12; k++) {
                         const int o = TapsY::pc[k][0] * LW + TapsY::pc[k][1];
-                        const uint32_t t = wc[o] + wc[-o];  // both halves < 2^11: no carry
+                        const uint32_t t = wf[o] + wf[-o];  // both halves < 2^11: no carry
                         const int fk = flt[k];
                         s0 += ulo(t) * fk;
                         s1 += uhi(t) * fk;
@@ -888,7 +958,7 @@ R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, in
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
                         const int o = TapsY::ns[k][0] * LW + TapsY::ns[k][1];
-                        const uint32_t t = wc[o] + wc[-o];
+                        const uint32_t t = wf[o] + wf[-o];
                         const int fk = flt[k];
                         s0 += ulo(t) * fk;
                         s1 += uhi(t) * fk;
@@ -986,8 +1056,18 @@ R2G_D void consume_item(const DevFrame &f, LrSmem &sm, int s, int tid) {
     if ((tid & 31) == 0) mbar_arrive(&sm.empty[s]);
     bar_sync_n(NCT);
     if (tid == 0 && staged) commit_tables(f, fi, sm, staged);
+    // a top-integrated luma item: the Wiener filters' rows -4 .. -1 are the
+    // saved rows 0 .. 3, which the window holds as rows -6 .. -3
+    const bool topi = plane == 0 && ro == 0 && (edges & LR_HAVE_TOP_INTEGRATED) && kind != W_NONE;
+    if (topi) {
+        for (int i = 2 * LW + tid; i < 15 * LW; i += NCT) {
+            const int r = i / LW - 6;
+            sm.wtop[i] = sm.u.wp[i + (r < 0 ? -2 * LW : 0)];
+        }
+        bar_sync_n(NCT);
+    }
     if (plane == 0)
-        filter_luma<P>(f, sm, x0, y0, sh, ro, nr, uw, kind, gdf, c0, tid);
+        filter_luma<P>(f, sm, x0, y0, sh, ro, nr, uw, kind, gdf, c0, topi, tid);
     else
         filter_chroma<P>(f, sm, plane, x0, y0, ro, nr, uw, c0, c1, tid);
 }
@@ -1320,8 +1400,9 @@ void r2g_batch_launch_lr(const BatchArgs &a, int grid, cudaStream_t s) {
 }
 int r2g_batch_occupancy_lr() { return lr_info().occ[2]; }
 int r2g_lr_items(const DevFrame &f) {
+    const int nslots = f.sbh + 1 + f.n_tr;
     if (!f.lr_on) return 0;
-    return (f.sbh + 1) * (64 / f.lr_rows) * ((f.w + 63) >> 6) + 2 * (f.sbh + 1) * 2 * ((f.cw + 63) >> 6);
+    return nslots * (64 / f.lr_rows) * ((f.w + 63) >> 6) + 2 * nslots * 2 * ((f.cw + 63) >> 6);
 }
 
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {

@@ -79,6 +79,12 @@ struct DevFrame {
     // tile shape of the loop-restoration work items: luma rows per item (32,
     // or 16 for four lighter items per stripe); set by the batch autotuner
     int lr_rows;
+    // tile rows (loop restoration only): bit sby of tr_first is set when
+    // superblock row sby > 0 starts a tile row; tr_sby lists those rows, one
+    // extra 8-row stripe each (decode.rs:99-120, looprestoration.rs:2401-2548)
+    uint32_t tr_first[4];
+    int n_tr;
+    int16_t tr_sby[64];
     // per-stage work counters of the persistent kernels (per-frame launches;
     // the batched path keeps its own) and the context's device fault word
     // (bounded waits that ran out)

@@ -427,6 +427,19 @@ int r2g_validate(R2gCtx *ctx, const R2gFrame *f, const R2gFrameParams *fp, const
         set_err(ctx, "only 4:2:0 with 64x64 superblocks is supported");
         return R2G_E_INVALID;
     }
+    if (fp->tile_rows > 64) {
+        set_err(ctx, "more than 64 tile rows");
+        return R2G_E_INVALID;
+    }
+    for (int i = 1; i < fp->tile_rows; i++)
+        if (fp->tile_row_start_sb[i] <= fp->tile_row_start_sb[i - 1]) {
+            set_err(ctx, "tile row starts are not increasing");
+            return R2G_E_INVALID;
+        }
+    if (fp->tile_rows > 1 && ((fp->height + 63) >> 6) > 128) {
+        set_err(ctx, "tile rows are supported up to 128 superblock rows");
+        return R2G_E_INVALID;
+    }
     if (side->n_sb256 != f->n_sb256) {
         set_err(ctx, "side-info count does not match the frame size");
         return R2G_E_INVALID;
@@ -569,6 +582,18 @@ int r2g_prepare(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, const R2gSid
                        ((fp->restoration[2].restoration_type != R2G_RESTORE_NONE) << 2);
     d.lr_on = d.restore_planes != 0 && (inloop & (R2G_INLOOP_WIENER | R2G_INLOOP_GDF));
     d.lr_rows = 32;
+    // tile rows: init_start_of_tile_row (decode.rs:99-120) over sbh rows
+    d.n_tr = 0;
+    if (fp->tile_rows > 1)
+        for (int tr = 0, sby = 0; tr < fp->tile_rows && sby < d.sbh; tr++) {
+            if (sby > 0) {
+                d.tr_first[sby >> 5] |= 1u << (sby & 31);
+                d.tr_sby[d.n_tr++] = (int16_t)sby;
+            }
+            sby++;
+            const int end = imin_(fp->tile_row_start_sb[tr + 1], d.sbh);
+            while (sby < end) sby++;
+        }
     d.base_q = 0;
     d.wiener_idx = 0;
     d.ns_ci = -1;

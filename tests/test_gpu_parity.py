@@ -123,3 +123,34 @@ def test_parity_film_grain_variants(ctx, oracle):
                 g.uv_luma_mult[pl - 1] = int(rng.integers(-128, 128))
                 g.uv_offset[pl - 1] = int(rng.integers(-256, 256))
         _run(ctx, oracle, sf, grain=True)
+
+
+def _tile_rows(sf, starts_sb):
+    import ctypes as C
+
+    fp = abi.FrameParams()
+    C.memmove(C.byref(fp), C.byref(sf.fp), C.sizeof(fp))
+    fp.tile_rows = len(starts_sb) - 1
+    for i, v in enumerate(starts_sb):
+        fp.tile_row_start_sb[i] = v
+    sf.fp = fp
+    return sf
+
+
+TILE_ROW_CASES = [
+    # (w, h, bitdepth, tile row starts in superblock rows, seed)
+    (256, 320, 8, [0, 2, 5], 61),
+    (256, 320, 10, [0, 1, 3, 5], 62),
+    (640, 384, 10, [0, 3, 5, 6], 63),     # the last tile row is the last superblock row (two stripes)
+    (1920, 1080, 8, [0, 5, 11, 16, 17], 64),  # a tile row of one short superblock row at the bottom
+    (1920, 1080, 10, [0, 6, 12, 17], 65),
+]
+
+
+@pytest.mark.parametrize("w,h,bd,starts,seed", TILE_ROW_CASES)
+def test_parity_tile_rows(ctx, oracle, w, h, bd, starts, seed):
+    """Loop restoration over several tile rows: the split superblock row at
+    each tile row's top (looprestoration.rs:2401-2548) with its integrated
+    stripe edges, NS / PC / multi-class Wiener and GDF units."""
+    sf = _tile_rows(synth.make_frame(w, h, bd, seed, ns_multi=3 if bd == 10 else 0), starts)
+    _run(ctx, oracle, sf)
