@@ -15,9 +15,9 @@
  *
  * Sample storage: 8-bit frames are uint8_t samples, 10-bit frames uint16_t.
  * Strides are in BYTES, as in the reference's Picture (picture.rs:79-97).
- * Supported layout: 4:2:0, sb128 = 0, one tile row, width and height
- * multiples of 8 (every workload the library is specified for); anything else
- * is rejected with R2G_E_INVALID rather than filtered differently.
+ * Supported layout: 4:2:0, sb128 = 0, width and height multiples of 8, any
+ * tile grid (several tile rows up to 128 superblock rows); anything else is
+ * rejected with R2G_E_INVALID rather than filtered differently.
  *
  * Threading: a context is used by one host thread at a time. Calls enqueue
  * work on the context's streams and return; r2g_wait / r2g_sync block.
