@@ -367,6 +367,30 @@ int r2g_download_rows(R2gCtx *ctx, R2gFrame *f, int which, int row0, int nrows, 
  * block, both with the block's stride; `left` holds [h][2] samples (columns
  * -2, -1); edges: 1 left, 2 right, 4 top, 8 bottom available (CDEF_HAVE_*,
  * cdef.rs:6-9). */
+/* DeblockDSPContext.deblock_sb (dsp.rs:86-89): deblock_{h,v}_sb64{y,uv}_bd
+ * (deblock.rs:303-548), one 64-long edge of 16 four-line segments.  `dst`
+ * is the first positive-side sample of line 0; vert != 0: a vertical edge
+ * (lines run down the rows, the h variants), else horizontal.  vmask[4]:
+ * edge-class bits per segment (class 3 only for luma), ll_mask[0] / [1]:
+ * lossless negative / positive sides, q_thr[16] / side_thr[16] per segment,
+ * `edge` clamps the negative side to 6 (luma) / 2 (chroma) samples. */
+int r2g_dsp_deblock_sb64(void *dst, int64_t stride, const uint16_t *vmask, const uint16_t *ll_mask,
+                         const uint16_t *q_thr, const uint16_t *side_thr, int edge, int luma, int vert,
+                         int bitdepth);
+/* FilmGrainDSPContext.fgy_32x32xn / fguv_32x32xn (dsp.rs:9-16):
+ * filmgrain.rs:248-407 / :409-598 on one row band (bh rows, pw samples) of
+ * the caller's planes: dst = src + noise, `in_seed` the frame's grain seed,
+ * `row_num` the band index, `scaling` the plane's (1 << bitdepth)-entry LUT,
+ * `grain_lut` its [73][82] template; for chroma `luma_row` / `luma_stride`
+ * are the band's luma rows, uv 0 = U / 1 = V, sx / sy the subsampling.
+ * Samples above the bit depth's range are rejected (R2G_E_INVALID). */
+int r2g_dsp_fgy_32x32xn(void *dst, const void *src, int64_t stride, const R2gFilmGrainData *data,
+                        uint32_t in_seed, int pw, const uint8_t *scaling, const int16_t *grain_lut, int bh,
+                        int row_num, int bitdepth);
+int r2g_dsp_fguv_32x32xn(void *dst, const void *src, int64_t stride, const R2gFilmGrainData *data,
+                         uint32_t in_seed, int pw, const uint8_t *scaling, const int16_t *grain_lut, int bh,
+                         int row_num, const void *luma_row, int64_t luma_stride, int uv, int is_id, int sx,
+                         int sy, int bitdepth);
 /* CdefDSPContext.dir: cdef_find_dir_bd (cdef.rs:134-216) on the 8x8 block at
  * img; returns the direction 0..7 (or < 0 on error), *var its variance. */
 int r2g_dsp_cdef_dir(const void *img, int64_t stride, uint32_t *var, int bitdepth);

@@ -611,3 +611,31 @@ int r2g_launch_deblock(const DevFrame &f, cudaStream_t s) {
         r2g_launch_pdl(deblock_tile_kernel<uint8_t>, grid, dim3(256), s, f);
     return 1;
 }
+
+// ---------------------------------------------------------------- DSP slot
+// DeblockDSPContext.deblock_sb[dir][plane] (dsp.rs:86-89): one call of
+// deblock_{h,v}_sb64{y,uv}_bd (deblock.rs:303-548) on a staged strip: `strip`
+// holds the 16 samples across the edge (-8 .. 7) for every line along it
+// (line-major: strip[line * 16 + 8 + j]), one thread per 4-line segment
+// whose bit is set in the class masks.
+namespace {
+__global__ void dsp_deblock_sb64_kernel(int16_t *strip, uint32_t vm0, uint32_t vm1, uint32_t vm2, uint32_t vm3,
+                                        uint32_t ll_pos, uint32_t ll_neg, const uint16_t *thr, int edge, int luma,
+                                        int bdmax) {
+    const int seg = threadIdx.x;
+    const uint32_t y = 1u << seg;
+    const uint32_t vm = vm0 | vm1 | vm2 | (luma ? vm3 : 0);
+    if (seg >= 16 || !(vm & y)) return;
+    const int idx = luma ? ((vm3 & y) ? 3 : (vm2 & y) ? 2 : ((vm1 & y) != 0)) : ((vm2 & y) ? 2 : ((vm1 & y) != 0));
+    const int mwp = luma ? c_max_width_y[idx] : c_max_width_uv[idx];
+    const int mwn = edge ? imin_(luma ? 6 : 2, mwp) : mwp;
+    filter_edge(strip + seg * 4 * 16 + 8, 16, 1, thr[seg], thr[16 + seg], mwp, mwn, (ll_pos & y) != 0,
+                (ll_neg & y) != 0, bdmax);
+}
+}  // namespace
+
+void r2g_dsp_launch_deblock_sb64(int16_t *strip, const uint16_t vmask[4], const uint16_t ll_mask[2],
+                                 const uint16_t *thr, int edge, int luma, int bitdepth, cudaStream_t s) {
+    dsp_deblock_sb64_kernel<<<1, 16, 0, s>>>(strip, vmask[0], vmask[1], vmask[2], vmask[3], ll_mask[1], ll_mask[0],
+                                             thr, edge, luma, (1 << bitdepth) - 1);
+}

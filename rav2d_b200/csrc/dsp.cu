@@ -26,6 +26,8 @@ namespace {
 struct DspDevice {
     bool ready = false;
     char *buf = nullptr;
+    char *big = nullptr;  // grows for the row-band slots (film grain)
+    size_t big_bytes = 0;
     cudaStream_t st = nullptr;  // non-blocking: no implicit sync with the legacy stream
     DevTables tab{};
 };
@@ -93,12 +95,153 @@ void store_block(P *dst, int64_t stride, const std::vector<uint16_t> &v, int w, 
 
 bool ok_bd(int bd) { return bd == 8 || bd == 10; }
 
+int finish(const DspDevice *d, int rc);
+
+// (called with g_dsp_mu held)
+int big_scratch(DspDevice *d, size_t bytes) {
+    if (d->big_bytes >= bytes) return R2G_OK;
+    if (d->big) cudaFree(d->big);
+    d->big = nullptr;
+    d->big_bytes = 0;
+    if (cudaMalloc((void **)&d->big, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return R2G_E_OOM;
+    }
+    d->big_bytes = bytes;
+    return R2G_OK;
+}
+
+// rows x w samples of a plane (u8 or u16) as u16, or false if one exceeds
+// the bit depth's range (the scaling LUT has 1 << bitdepth entries)
+bool stage_rows(std::vector<uint16_t> &v, const void *src, int64_t stride, int w, int rows, int bitdepth) {
+    v.resize((size_t)w * rows);
+    const int bdmax = (1 << bitdepth) - 1;
+    for (int y = 0; y < rows; y++)
+        for (int x = 0; x < w; x++) {
+            const int s = bitdepth > 8 ? ((const uint16_t *)src)[y * stride + x] : ((const uint8_t *)src)[y * stride + x];
+            if (s > bdmax) return false;
+            v[(size_t)y * w + x] = (uint16_t)s;
+        }
+    return true;
+}
+
+// One row band of film grain (fgy_32x32xn / fguv_32x32xn): stage, run, and
+// write the band back.
+int fg_band(void *dst, const void *src, int64_t stride, const R2gFilmGrainData *data, uint32_t in_seed, int pw,
+            const uint8_t *scaling, const int16_t *grain_lut, int bh, int row_num, const void *luma_row,
+            int64_t luma_stride, int uv, int is_id, int sx, int sy, int bitdepth) {
+    if (!dst || !src || !data || !scaling || !grain_lut || !ok_bd(bitdepth) || pw <= 0 || bh <= 0 || row_num < 0 ||
+        in_seed > 0xffff || data->block_size < 0 || data->block_size > 1 || data->scaling_shift < 8 ||
+        data->scaling_shift > 11 || bh > ((16 << data->block_size) >> sy) || sx < 0 || sx > 1 || sy < 0 || sy > 1 ||
+        uv < 0 || uv > 1 || pw > r2g_dsp_fg_band_max_width(data->block_size, sx) || (luma_row == nullptr) != (uv < 0))
+        return R2G_E_INVALID;
+    std::vector<uint16_t> s16, l16;
+    if (!stage_rows(s16, src, stride, pw, bh, bitdepth)) return R2G_E_INVALID;
+    const int lw = pw << sx, lh = bh << sy;
+    if (luma_row && !stage_rows(l16, luma_row, luma_stride, lw, lh, bitdepth)) return R2G_E_INVALID;
+    std::lock_guard<std::mutex> lk(g_dsp_mu);
+    DspDevice *d;
+    int rc = dsp_device(&d);
+    if (rc != R2G_OK) return rc;
+    const size_t plane = s16.size() * 2, lbytes = l16.size() * 2, lut_bytes = 73 * 82 * 2, sc = (size_t)1 << bitdepth;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    if ((rc = big_scratch(d, 2 * al(plane) + al(lbytes) + al(lut_bytes) + al(sc))) != R2G_OK) return rc;
+    uint16_t *dsrc = (uint16_t *)d->big, *ddst = (uint16_t *)(d->big + al(plane));
+    uint16_t *dl = (uint16_t *)(d->big + 2 * al(plane));
+    int16_t *dlut = (int16_t *)(d->big + 2 * al(plane) + al(lbytes));
+    uint8_t *dsc = (uint8_t *)(d->big + 2 * al(plane) + al(lbytes) + al(lut_bytes));
+    if (cudaMemcpyAsync(dsrc, s16.data(), plane, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        (lbytes && cudaMemcpyAsync(dl, l16.data(), lbytes, cudaMemcpyHostToDevice, d->st) != cudaSuccess) ||
+        cudaMemcpyAsync(dlut, grain_lut, lut_bytes, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(dsc, scaling, sc, cudaMemcpyHostToDevice, d->st) != cudaSuccess)
+        return R2G_E_DEVICE;
+    r2g_dsp_launch_fg_band(ddst, dsrc, pw, luma_row ? dl : nullptr, lw, *data, in_seed, pw, dsc, dlut, bh, row_num,
+                           uv < 0 ? 0 : uv, is_id, sx, sy, bitdepth, d->st);
+    if (cudaMemcpyAsync(s16.data(), ddst, plane, cudaMemcpyDeviceToHost, d->st) != cudaSuccess) return R2G_E_DEVICE;
+    if ((rc = finish(d, R2G_OK)) != R2G_OK) return rc;
+    if (bitdepth > 8)
+        store_block((uint16_t *)dst, stride, s16, pw, bh);
+    else
+        store_block((uint8_t *)dst, stride, s16, pw, bh);
+    return R2G_OK;
+}
+
 int finish(const DspDevice *d, int rc) {
     if (rc != R2G_OK) return rc;
     return cudaStreamSynchronize(d->st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? R2G_OK : R2G_E_DEVICE;
 }
 
 }  // namespace
+
+// DeblockDSPContext.deblock_sb[vert ? 0 : 1][luma ? 0 : 1]: deblock_{h,v}_
+// sb64{y,uv}_bd (deblock.rs:303-548).  `dst` is the first positive-side
+// sample of line 0 (the reference's dst + dst_off); with `vert` the edge is
+// vertical and its lines run down the rows, else horizontal along the
+// columns.  The lines of every segment up to the highest class bit, and the
+// samples across the edge the filters can reach (8 per side for luma, 6 for
+// chroma), are staged, filtered and written back.
+extern "C" int r2g_dsp_deblock_sb64(void *dst, int64_t stride, const uint16_t *vmask, const uint16_t *ll_mask,
+                                    const uint16_t *q_thr, const uint16_t *side_thr, int edge, int luma, int vert,
+                                    int bitdepth) {
+    if (!dst || !vmask || !ll_mask || !q_thr || !side_thr || stride <= 0 || !ok_bd(bitdepth)) return R2G_E_INVALID;
+    const uint32_t vm = (uint32_t)vmask[0] | vmask[1] | vmask[2] | (luma ? vmask[3] : 0);
+    if (!vm) return R2G_OK;
+    const int nseg = 32 - __builtin_clz(vm), nlines = 4 * nseg;
+    const int reach = luma ? 8 : 6;
+    const int64_t along = vert ? stride : 1, across = vert ? 1 : stride;
+    std::lock_guard<std::mutex> lk(g_dsp_mu);
+    DspDevice *d;
+    int rc = dsp_device(&d);
+    if (rc != R2G_OK) return rc;
+    std::vector<int16_t> strip((size_t)nlines * 16, 0);
+    for (int l = 0; l < nlines; l++)
+        for (int j = -reach; j < reach; j++) {
+            const int64_t o = l * along + j * across;
+            strip[(size_t)l * 16 + 8 + j] = (int16_t)(bitdepth > 8 ? ((const uint16_t *)dst)[o] : ((const uint8_t *)dst)[o]);
+        }
+    uint16_t thr[32];
+    for (int i = 0; i < 16; i++) {
+        thr[i] = i < nseg ? q_thr[i] : 0;
+        thr[16 + i] = i < nseg ? side_thr[i] : 0;
+    }
+    int16_t *dstrip = (int16_t *)d->buf;
+    uint16_t *dthr = (uint16_t *)(d->buf + 4096);
+    if (cudaMemcpyAsync(dstrip, strip.data(), strip.size() * 2, cudaMemcpyHostToDevice, d->st) != cudaSuccess ||
+        cudaMemcpyAsync(dthr, thr, sizeof(thr), cudaMemcpyHostToDevice, d->st) != cudaSuccess)
+        return R2G_E_DEVICE;
+    r2g_dsp_launch_deblock_sb64(dstrip, vmask, ll_mask, dthr, edge != 0, luma != 0, bitdepth, d->st);
+    if (cudaMemcpyAsync(strip.data(), dstrip, strip.size() * 2, cudaMemcpyDeviceToHost, d->st) != cudaSuccess)
+        return R2G_E_DEVICE;
+    rc = finish(d, R2G_OK);
+    if (rc != R2G_OK) return rc;
+    for (int l = 0; l < nlines; l++)
+        for (int j = -reach; j < reach; j++) {
+            const int64_t o = l * along + j * across;
+            const int16_t v = strip[(size_t)l * 16 + 8 + j];
+            if (bitdepth > 8)
+                ((uint16_t *)dst)[o] = (uint16_t)v;
+            else
+                ((uint8_t *)dst)[o] = (uint8_t)v;
+        }
+    return R2G_OK;
+}
+
+// FilmGrainDSPContext.fgy_32x32xn (filmgrain.rs:248-407) and fguv_32x32xn
+// (:409-598) on one row band of the caller's planes.
+extern "C" int r2g_dsp_fgy_32x32xn(void *dst, const void *src, int64_t stride, const R2gFilmGrainData *data,
+                                   uint32_t in_seed, int pw, const uint8_t *scaling, const int16_t *grain_lut, int bh,
+                                   int row_num, int bitdepth) {
+    return fg_band(dst, src, stride, data, in_seed, pw, scaling, grain_lut, bh, row_num, nullptr, 0, -1, 0, 0, 0,
+                   bitdepth);
+}
+extern "C" int r2g_dsp_fguv_32x32xn(void *dst, const void *src, int64_t stride, const R2gFilmGrainData *data,
+                                    uint32_t in_seed, int pw, const uint8_t *scaling, const int16_t *grain_lut, int bh,
+                                    int row_num, const void *luma_row, int64_t luma_stride, int uv, int is_id, int sx,
+                                    int sy, int bitdepth) {
+    if (uv < 0 || !luma_row) return R2G_E_INVALID;
+    return fg_band(dst, src, stride, data, in_seed, pw, scaling, grain_lut, bh, row_num, luma_row, luma_stride, uv,
+                   is_id, sx, sy, bitdepth);
+}
 
 extern "C" int r2g_dsp_cdef_dir(const void *img, int64_t stride, uint32_t *var, int bitdepth) {
     if (!img || !var || !ok_bd(bitdepth)) return R2G_E_INVALID;

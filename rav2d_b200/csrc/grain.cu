@@ -890,3 +890,109 @@ void r2g_dsp_launch_grain_template(const GrainParams &gp, const DevTables &tab, 
     init_lfsr_pow(dev);
     grain_template_kernel<<<1, 256, 0, s>>>(gp, tab, lut, scaling);
 }
+
+// ---------------------------------------------------------------- DSP slots
+// FilmGrainDSPContext.fgy_32x32xn / fguv_32x32xn[] (dsp.rs:9-16): one row
+// band of blocks, as filmgrain.rs:248-407 (luma) and :409-598 (chroma) apply
+// it: the per-block template offsets are drawn in order along the band by one
+// thread into shared memory (seeds of this band and, with overlap, of the
+// band above), then every sample takes its grain (blended across the block's
+// top / left overlap) and noise from the staged template and scaling LUT.
+// Planes are staged as u16 (`pitch` samples per row); `luma` holds the
+// band's luma rows for chroma (NULL for luma).
+namespace {
+constexpr int FG_MAX_BLOCKS = 512;
+__global__ void dsp_fg_band_kernel(uint16_t *dst, const uint16_t *src, int pitch, const uint16_t *luma, int lpitch,
+                                   const R2gFilmGrainData data, uint32_t in_seed, int pw, const uint8_t *scaling,
+                                   const int16_t *lut, int bh, int row_num, int uv, int is_id, int sx, int sy,
+                                   int bitdepth) {
+    __shared__ int8_t offs[FG_MAX_BLOCKS][2][2];  // [block][row of seeds][y, x]
+    const int rows = 1 + (data.overlap_flag && row_num > 0);
+    const int bs = 16 << data.block_size, bsx = bs >> sx;
+    const int nb = (pw + bsx - 1) / bsx;
+    if (threadIdx.x == 0) {
+        uint32_t seed[2] = {0, 0};
+        for (int i = 0; i < rows; i++) {
+            seed[i] = in_seed;
+            seed[i] ^= (uint32_t)((((row_num - i) * 37 + 178) & 0xff)) << 8;
+            seed[i] ^= (uint32_t)(((row_num - i) * 173 + 105) & 0xff);
+        }
+        for (int b = 0; b < nb; b++)
+            for (int i = 0; i < 2; i++)
+                for (int n = 0; n < 2; n++) {
+                    int v = 0;
+                    if (i < rows) {
+                        seed[i] = lfsr_step(seed[i]);
+                        v = (int)(((uint32_t)(3 - data.block_size) * ((seed[i] >> 7) & 0x1ff)) >> 6);
+                        for (int k = 0; k < 3; k++) seed[i] = lfsr_step(seed[i]);
+                    }
+                    offs[b][i][n] = (int8_t)v;
+                }
+    }
+    __syncthreads();
+    const int b8 = bitdepth - 8;
+    const int grain_ctr = 128 << b8, grain_min = -grain_ctr, grain_max = grain_ctr - 1;
+    int min_value = 0, max_value = (1 << bitdepth) - 1;
+    if (data.clip_to_restricted_range) {
+        min_value = 16 << b8;
+        max_value = (luma && !is_id ? 240 : 235) << b8;
+    }
+    // blending weights: w[x] for the 2-wide overlap (27, 17 / 17, 27), or one
+    // column / row when subsampled (23, 22)
+    auto wgt = [](int sub, int i, int k) -> int {
+        return sub ? (k == 0 ? 23 : 22) : ((i == 0) == (k == 0) ? 27 : 17);
+    };
+    // sample_lut (filmgrain.rs:231-246): block column `prev` (the previous
+    // block) and seed row `above`
+    auto grain_at = [&](int b, int prev, int above, int x, int y) -> int {
+        const int ob = prev ? b - 1 : b;
+        const int offx = 3 + (2 >> sx) * (3 + offs[ob][above][1]);
+        const int offy = 3 + (2 >> sy) * (3 + offs[ob][above][0]);
+        return lut[(offy + y + (bs >> sy) * above) * GW + offx + x + bsx * prev];
+    };
+    for (int i = threadIdx.x; i < pw * bh; i += blockDim.x) {
+        const int y = i / pw, X = i - y * pw, b = X / bsx, x = X - b * bsx;
+        const int bw = imin_(bsx, pw - b * bsx);
+        const int ystart = (data.overlap_flag && row_num > 0) ? imin_(2 >> sy, bh) : 0;
+        const int xstart = (data.overlap_flag && b > 0) ? imin_(2 >> sx, bw) : 0;
+        int g = grain_at(b, 0, 0, x, y);
+        if (x < xstart) {
+            const int old = grain_at(b, 1, 0, x, y);
+            g = iclip_(round2(old * wgt(sx, x, 0) + g * wgt(sx, x, 1), 5), grain_min, grain_max);
+        }
+        if (y < ystart) {
+            int top = grain_at(b, 0, 1, x, y);
+            if (x < xstart) {
+                const int old = grain_at(b, 1, 1, x, y);
+                top = iclip_(round2(old * wgt(sx, x, 0) + top * wgt(sx, x, 1), 5), grain_min, grain_max);
+            }
+            g = iclip_(round2(top * wgt(sy, y, 0) + g * wgt(sy, y, 1), 5), grain_min, grain_max);
+        }
+        const int sv = src[y * pitch + X];
+        int val = sv;
+        if (luma) {
+            const int lx = X << sx, ly = y << sy;
+            const int l0 = luma[ly * lpitch + lx];
+            const int avg = sx ? (l0 + luma[ly * lpitch + lx + 1] + 1) >> 1 : l0;
+            if (!data.chroma_scaling_from_luma) {
+                const int combined = avg * data.uv_luma_mult[uv] + sv * data.uv_mult[uv];
+                val = iclip_((combined >> 6) + data.uv_offset[uv] * (1 << b8), 0, (1 << bitdepth) - 1);
+            } else {
+                val = avg;
+            }
+        }
+        const int noise = round2(scaling[val] * g, data.scaling_shift);
+        dst[y * pitch + X] = (uint16_t)iclip_(sv + noise, min_value, max_value);
+    }
+}
+}  // namespace
+
+int r2g_dsp_fg_band_max_width(int block_size, int sx) { return FG_MAX_BLOCKS * ((16 << block_size) >> sx); }
+
+void r2g_dsp_launch_fg_band(uint16_t *dst, const uint16_t *src, int pitch, const uint16_t *luma, int lpitch,
+                            const R2gFilmGrainData &data, uint32_t in_seed, int pw, const uint8_t *scaling,
+                            const int16_t *lut, int bh, int row_num, int uv, int is_id, int sx, int sy, int bitdepth,
+                            cudaStream_t s) {
+    dsp_fg_band_kernel<<<1, 256, 0, s>>>(dst, src, pitch, luma, lpitch, data, in_seed, pw, scaling, lut, bh, row_num,
+                                         uv, is_id, sx, sy, bitdepth);
+}

@@ -170,6 +170,13 @@ struct GrainDev;  // grain.cu
 void r2g_dsp_launch_cdef_filter(const uint16_t *tile, int w, int h, int edges, int pri, int sec, int dir, int damping,
                                 int bitdepth, const DevTables &tab, uint16_t *out, cudaStream_t s);
 void r2g_dsp_launch_cdef_dir(const uint16_t *blk, int bitdepth, uint32_t *out, cudaStream_t s);
+int r2g_dsp_fg_band_max_width(int block_size, int sx);
+void r2g_dsp_launch_fg_band(uint16_t *dst, const uint16_t *src, int pitch, const uint16_t *luma, int lpitch,
+                            const R2gFilmGrainData &data, uint32_t in_seed, int pw, const uint8_t *scaling,
+                            const int16_t *lut, int bh, int row_num, int uv, int is_id, int sx, int sy, int bitdepth,
+                            cudaStream_t s);
+void r2g_dsp_launch_deblock_sb64(int16_t *strip, const uint16_t vmask[4], const uint16_t ll_mask[2],
+                                 const uint16_t *thr, int edge, int luma, int bitdepth, cudaStream_t s);
 void r2g_dsp_launch_ccso_prep(const uint16_t *tile, int w, int h, int ss_hor, int ss_ver, int edges, int max_band_log2,
                               int ext, int quant_step, int edge_clf, int bo_only, int bitdepth, uint8_t *out,
                               cudaStream_t s);

@@ -27,7 +27,7 @@ SYMBOLS = [
     "r2g_download_rows", "r2g_dsp_cdef_dir", "r2g_dsp_cdef_filter", "r2g_dsp_ccso_prep", "r2g_dsp_ccso_add",
     "r2g_dsp_gdf_add", "r2g_dsp_generate_grain", "r2g_dsp_ns_wiener_single_y", "r2g_dsp_ns_wiener_single_uv",
     "r2g_dsp_ns_wiener_multi", "r2g_dsp_pc_wiener", "r2g_dsp_gdf_prep", "r2g_ctx_device_faults",
-    "r2g_frame_read_masks",
+    "r2g_frame_read_masks", "r2g_dsp_deblock_sb64", "r2g_dsp_fgy_32x32xn", "r2g_dsp_fguv_32x32xn",
 ]
 
 
@@ -96,6 +96,10 @@ def lib():
                   "r2g_dsp_pc_wiener"):
             getattr(L, n).argtypes = [vp, i64, vp, vp, vp, ci, ci, wp, ci, vp, ci]
         L.r2g_dsp_gdf_prep.argtypes = [vp, i64, vp, i64, vp, vp, vp] + [ci] * 6
+        L.r2g_dsp_deblock_sb64.argtypes = [vp, i64, vp, vp, vp, vp] + [ci] * 4
+        fgp = C.POINTER(abi.FilmGrainData)
+        L.r2g_dsp_fgy_32x32xn.argtypes = [vp, vp, i64, fgp, C.c_uint32, ci, vp, vp, ci, ci, ci]
+        L.r2g_dsp_fguv_32x32xn.argtypes = [vp, vp, i64, fgp, C.c_uint32, ci, vp, vp, ci, ci, vp, i64] + [ci] * 5
         L.r2g_y4m_header.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
         L.r2g_download_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.c_int64]

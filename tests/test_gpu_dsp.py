@@ -298,3 +298,94 @@ def test_lr_slots_reject_bad_arguments(L):
     e = np.zeros(64, np.int8)
     assert L.r2g_dsp_gdf_prep(p(e), 8, p(buf), 64, None, None, None, 8, 4, 0, 0, 0, 8) == abi.R2G_E_INVALID
     assert L.r2g_dsp_gdf_prep(p(e), 8, p(buf), 64, None, None, None, 8, 8, 6, 0, 0, 8) == abi.R2G_E_INVALID
+
+
+# ---- DeblockDSPContext.deblock_sb and FilmGrainDSPContext.fgy / fguv ----
+@pytest.mark.parametrize("bd", [8, 10])
+@pytest.mark.parametrize("luma", [1, 0])
+@pytest.mark.parametrize("vert", [1, 0])
+def test_deblock_sb64_slot(L, oracle, bd, luma, vert):
+    """deblock_{h,v}_sb64{y,uv}_bd (deblock.rs:303-548) on one 64-long edge:
+    random class / lossless bits, thresholds and the `edge` clamp; a plane
+    with a step across the edge so the filters engage."""
+    rng = np.random.default_rng(1000 * bd + 10 * luma + vert)
+    lib = oracle.lib()
+    for it in range(24):
+        plane = _plane(rng, bd, rows=80, cols=80)
+        step = rng.integers(-(1 << bd) // 8, (1 << bd) // 8 + 1)
+        if vert:
+            plane[:, 40:] = np.clip(plane[:, 40:].astype(np.int64) + step, 0, (1 << bd) - 1)
+        else:
+            plane[40:, :] = np.clip(plane[40:, :].astype(np.int64) + step, 0, (1 << bd) - 1)
+        off = (8 * 80 + 40) if vert else (40 * 80 + 8)
+        vmask = (rng.integers(0, 1 << 16, 4) * (rng.random(4) < 0.6)).astype(np.uint16)
+        if not luma:
+            vmask[3] = 0
+        ll = (rng.integers(0, 1 << 16, 2) * (rng.random(2) < 0.3)).astype(np.uint16)
+        q = rng.integers(0, 1 << (bd - 2), 16).astype(np.uint16)
+        sthr = rng.integers(0, 1 << bd, 16).astype(np.uint16)
+        edge = int(it & 1)
+        want = plane.copy()
+        lib.r2o_deblock_sb64(p(want), C.c_int64(off), C.c_int64(80), p(vmask), p(ll), p(q), p(sthr), edge, luma,
+                             vert, bd)
+        got = _st(plane, bd)
+        assert L.r2g_dsp_deblock_sb64(_ptr(got, off), 80, p(vmask), p(ll), p(q), p(sthr), edge, luma, vert, bd) == 0
+        assert np.array_equal(got.astype(np.uint16), want), it
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+@pytest.mark.parametrize("chroma", [0, 1])
+def test_film_grain_band_slots(L, oracle, bd, chroma):
+    """fgy_32x32xn / fguv_32x32xn (filmgrain.rs:248-598) on one row band:
+    band 0 and later bands (vertical overlap), with and without overlap,
+    restricted range, chroma from luma or with its own multipliers."""
+    lib = oracle.lib()
+    lib.r2o_fgy_32x32xn.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p,
+                                    C.c_void_p, C.c_int, C.c_int, C.c_int]
+    lib.r2o_fguv_32x32xn.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p,
+                                     C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64] + [C.c_int] * 5
+    rng = np.random.default_rng(77 + bd + 3 * chroma)
+    for it in range(12):
+        fgd, seed = synth.make_film_grain(rng)
+        fgd.overlap_flag = int(it % 3 != 2)
+        fgd.chroma_scaling_from_luma = int(it % 2)
+        fgd.uv_mult[0], fgd.uv_mult[1] = (int(v) for v in rng.integers(-128, 128, 2))
+        fgd.uv_luma_mult[0], fgd.uv_luma_mult[1] = (int(v) for v in rng.integers(-128, 128, 2))
+        fgd.uv_offset[0], fgd.uv_offset[1] = (int(v) for v in rng.integers(-256, 256, 2))
+        lut = rng.integers(-(128 << (bd - 8)), 128 << (bd - 8), (73, 82)).astype(np.int16)
+        scaling = rng.integers(0, 256, 1 << bd).astype(np.uint8)
+        row_num = int(it % 4)
+        sx = sy = chroma
+        pw = int(rng.integers(1, 9)) * (32 >> sx) - int(rng.integers(0, 5))
+        bh = (32 >> sy) - int(rng.integers(0, 3))
+        stride = pw + 7
+        src = rng.integers(0, 1 << bd, (bh, stride)).astype(np.uint16)
+        luma = rng.integers(0, 1 << bd, (bh << sy, (stride << sx) + 2)).astype(np.uint16)
+        want = np.zeros_like(src)
+        got = _st(np.zeros_like(src), bd)
+        if chroma:
+            uv, is_id = int(it & 1), int((it >> 1) & 1)
+            lib.r2o_fguv_32x32xn(p(want), p(src), stride, C.byref(fgd), seed, pw, p(scaling), p(lut), bh, row_num,
+                                 p(luma), luma.shape[1], uv, is_id, sx, sy, bd)
+            rc = L.r2g_dsp_fguv_32x32xn(p(got), p(_st(src, bd)), stride, C.byref(fgd), seed, pw, p(scaling), p(lut),
+                                        bh, row_num, p(_st(luma, bd)), luma.shape[1], uv, is_id, sx, sy, bd)
+        else:
+            lib.r2o_fgy_32x32xn(p(want), p(src), stride, C.byref(fgd), seed, pw, p(scaling), p(lut), bh, row_num, bd)
+            rc = L.r2g_dsp_fgy_32x32xn(p(got), p(_st(src, bd)), stride, C.byref(fgd), seed, pw, p(scaling), p(lut),
+                                       bh, row_num, bd)
+        assert rc == 0
+        assert np.array_equal(got[:, :pw].astype(np.uint16), want[:, :pw]), it
+
+
+def test_band_slots_reject_bad_arguments(L):
+    fgd, seed = synth.make_film_grain(np.random.default_rng(5))
+    src = np.full((32, 64), 2000, np.uint16)
+    dst = np.zeros_like(src)
+    lut = np.zeros((73, 82), np.int16)
+    sc = np.zeros(1024, np.uint8)
+    assert L.r2g_dsp_fgy_32x32xn(p(dst), p(src), 64, C.byref(fgd), seed, 64, p(sc), p(lut), 32, 0, 10) != 0  # > 1023
+    src[:] = 600
+    assert L.r2g_dsp_fgy_32x32xn(p(dst), p(src), 64, C.byref(fgd), seed, 64, p(sc), p(lut), 40, 0, 10) != 0  # bh
+    assert L.r2g_dsp_fgy_32x32xn(p(dst), p(src), 64, C.byref(fgd), 1 << 16, 64, p(sc), p(lut), 32, 0, 10) != 0
+    vm = np.zeros(4, np.uint16)
+    assert L.r2g_dsp_deblock_sb64(None, 64, p(vm), p(vm), p(vm), p(vm), 0, 1, 1, 10) != 0
