@@ -255,9 +255,17 @@ struct DeblockSmem {
     DbSide side;
 };
 
+// Appends to a list with one shared atomic per group of converged lanes
+// pushing to the same list (the lists' order does not matter: the edges of
+// one direction are independent).
 R2G_D void push_edge(DeblockSmem &sm, int list, EdgeDesc d) {
     EdgeDesc *dst = list == 0 ? sm.vl : list == 1 ? sm.vc : list == 2 ? sm.hl : sm.hc;
-    dst[atomicAdd(&sm.n[list], 1)] = d;
+    const unsigned peers = __match_any_sync(__activemask(), list);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&sm.n[list], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    dst[base + __popc(peers & ((1u << lane) - 1))] = d;
 }
 
 R2G_D uint32_t pack_geo(int x, int y, int mwp, int mwn, bool pos_ll, bool neg_ll) {
