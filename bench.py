@@ -44,10 +44,16 @@ MPIX = W_ * H_ / 1e6
 # scaling index (+2 B).  The deblock kernel runs both edge directions in one
 # pass over the frame, so its minimum is one read and one write.
 BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film_grain": 8.0}
-# dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload,
-# from one `ncu --set full` capture of each kernel (the outputs were still in
-# L2 when the capture ended, so the write term was 0)
-NCU_TRAFFIC = {"deblock": 6609664, "cdef_ccso": 6291200, "loop_restoration": 6850048}
+# From one `ncu --set full` capture of each kernel on this workload (one
+# launch each, `python -m rav2d_b200.profile --frames 24 --runs 2`): DRAM
+# bytes read + written per launch (the outputs were still in L2 when the
+# capture ended, so the write term was 0) and warp instructions per launch.
+NCU_CAPTURE = {
+    "commit": "ae38c6c",
+    "traffic": {"deblock": 6618112, "cdef_ccso": 6295808, "loop_restoration": 6849280},
+    "warp_inst": {"deblock": 9712384, "cdef_ccso": 26207300, "loop_restoration": 27162128},
+}
+SMS = 148
 
 
 def log(*a):
@@ -650,6 +656,8 @@ def main():
     dom_ms, dom_n = prof[dom]
     avg_launch_s = dom_ms / dom_n / 1e3
     achieved = BYTES_PER_PX[dom] * W_ * H_ / avg_launch_s / 1e9
+    stages_us = {k: round(v[0] / max(1, res["nprof"]) * 1e3, 2) for k, v in prof.items() if v[1]}
+    sm_mhz = (res["clocks"] or {}).get("sm_mhz")
     peak, peak_kind = peaks()
     cpu_v, cpu_n, cpu_dt = cpu_baseline(seconds=args.cpu_seconds, threads=1)
     ncores = os.cpu_count() or 1
@@ -668,11 +676,21 @@ def main():
                 "host_masks": {"value": round(res["e2e_full_rate"], 2), "h2d_bytes_per_step": res["h2d_full"],
                                "path": "the same, with the edge masks built on the host and uploaded"}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": NCU_TRAFFIC.get(dom),
-                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum, one launch",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": NCU_CAPTURE["traffic"].get(dom),
+                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum, one launch, from a capture "
+                                       "of commit " + NCU_CAPTURE["commit"],
                      "bytes_per_launch": int(BYTES_PER_PX[dom] * W_ * H_),
                      "avg_launch_us": round(avg_launch_s * 1e6, 2)},
-        "stages_us_per_frame": {k: round(v[0] / max(1, res["nprof"]) * 1e3, 2) for k, v in prof.items() if v[1]},
+        "stages_us_per_frame": stages_us,
+        # the bound that limits these stages: integer issue, warp
+        # instructions / (SMs x 4 schedulers x median SM clock x stage time)
+        "issue_roofline": {
+            k: {"warp_inst": NCU_CAPTURE["warp_inst"][k], "stage_us": stages_us[k],
+                "frac": round(NCU_CAPTURE["warp_inst"][k] / (SMS * 4 * sm_mhz * 1e6 * stages_us[k] * 1e-6), 3)}
+            for k in NCU_CAPTURE["warp_inst"] if k in stages_us and sm_mhz},
+        "issue_roofline_source": "warp instructions per launch from a one-kernel ncu capture of commit "
+                                 + NCU_CAPTURE["commit"] + "; stage times and SM clock from this run",
         "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpix/s", "cores": 1, "kind": "port",
                          "sample": f"{cpu_n} whole 1080p 10-bit frames through the oracle (C++ restatement of the "
                                    f"reference scalar Rust filter path) on 1 host core in {cpu_dt:.1f} s"},
