@@ -230,8 +230,10 @@ R2G_D void pad_chunk(const uint32_t (&v)[4], bool row_out, int x0, int w, uint32
 }
 
 // One 64x32 region (superblock column sbx, region row rr) of the frame; the
-// work of one CTA, shared by the per-frame and the batched kernels.
-template <typename P>
+// work of one CTA, shared by the per-frame and the batched kernels.  LB:
+// staging chunks whose loads a thread issues before their stores (more
+// loads in flight, more registers).
+template <typename P, int LB>
 R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
     const int gx0 = sbx * 64, gy0 = rr * RH;
     const int cx0 = gx0 >> 1, cy0 = gy0 >> 1;
@@ -311,41 +313,59 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
     // the deblocked planes come from the previous kernel on the stream:
     // wait for it before staging (everything above reads side-info only)
     pdl_wait();
-    // ---- stage the region and its halo, one 8-sample chunk per thread ----
-    for (int i = tid; i < NCHUNK; i += blockDim.x) {
-        uint32_t v[4], pv[4];
+    // ---- stage the region and its halo, one 8-sample chunk per thread and
+    // step; every step's loads are issued before any of its stores ----
+    for (int base = tid; base < NCHUNK; base += LB * 256) {
+    uint32_t v[LB][4];
+#pragma unroll
+    for (int k = 0; k < LB; k++) {
+        const int i = base + 256 * k;
+        if (i >= NCHUNK) break;
+        if (i < TH * TCH) {
+            const int r = i / TCH, kk = i - r * TCH;
+            load_chunk(Dy + iclip_(gy0 - 2 + r, 0, f.h - 1) * ys, gx0 - XO + 8 * kk, f.w, v[k]);
+        } else {
+            const int j = i - TH * TCH, pl = j / (CH * CCH), j2 = j - pl * (CH * CCH);
+            const int r = j2 / CCH, kk = j2 - r * CCH;
+            load_chunk((pl ? Dv : Du) + iclip_(cy0 - 2 + r, 0, f.ch - 1) * uvs, cx0 - XO + 8 * kk, f.cw, v[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < LB; k++) {
+        const int i = base + 256 * k;
+        if (i >= NCHUNK) break;
+        uint32_t pv[4];
         uint32_t *dt, *dp;
         int yy = -1, bc = 0;
         if (i < TH * TCH) {
-            const int r = i / TCH, k = i - r * TCH;
-            const int ry = gy0 - 2 + r, x0 = gx0 - XO + 8 * k;
-            load_chunk(Dy + iclip_(ry, 0, f.h - 1) * ys, x0, f.w, v);
-            pad_chunk(v, ry < 0 || ry >= f.h, x0, f.w, pv);
-            dt = reinterpret_cast<uint32_t *>(&sm.ty[r][8 * k]);
-            dp = reinterpret_cast<uint32_t *>(&sm.pty[r][8 * k]);
-            if (r >= 2 && r < RH + 2 && k >= 1 && k <= 8) {
+            const int r = i / TCH, kk = i - r * TCH;
+            const int ry = gy0 - 2 + r;
+            pad_chunk(v[k], ry < 0 || ry >= f.h, gx0 - XO + 8 * kk, f.w, pv);
+            dt = reinterpret_cast<uint32_t *>(&sm.ty[r][8 * kk]);
+            dp = reinterpret_cast<uint32_t *>(&sm.pty[r][8 * kk]);
+            if (r >= 2 && r < RH + 2 && kk >= 1 && kk <= 8) {
                 yy = r - 2;
-                bc = k - 1;
+                bc = kk - 1;
             }
         } else {
             const int j = i - TH * TCH, pl = j / (CH * CCH), j2 = j - pl * (CH * CCH);
-            const int r = j2 / CCH, k = j2 - r * CCH;
-            const int ry = cy0 - 2 + r, x0 = cx0 - XO + 8 * k;
-            load_chunk((pl ? Dv : Du) + iclip_(ry, 0, f.ch - 1) * uvs, x0, f.cw, v);
-            pad_chunk(v, ry < 0 || ry >= f.ch, x0, f.cw, pv);
-            dt = reinterpret_cast<uint32_t *>(&sm.tc[pl][r][8 * k]);
-            dp = reinterpret_cast<uint32_t *>(&sm.ptc[pl][r][8 * k]);
+            const int r = j2 / CCH, kk = j2 - r * CCH;
+            const int ry = cy0 - 2 + r;
+            pad_chunk(v[k], ry < 0 || ry >= f.ch, cx0 - XO + 8 * kk, f.cw, pv);
+            dt = reinterpret_cast<uint32_t *>(&sm.tc[pl][r][8 * kk]);
+            dp = reinterpret_cast<uint32_t *>(&sm.ptc[pl][r][8 * kk]);
         }
-        *reinterpret_cast<uint4 *>(dt) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4 *>(dt) = make_uint4(v[k][0], v[k][1], v[k][2], v[k][3]);
         *reinterpret_cast<uint4 *>(dp) = make_uint4(pv[0], pv[1], pv[2], pv[3]);
         if (yy >= 0) {
             uint32_t *d = reinterpret_cast<uint32_t *>(&sm.blk[(yy >> 3) * 8 + bc][(yy & 7) * 8]);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int lo = (int)((v[q] & 0xffffu) >> bd8) - 128, hi = (int)((v[q] >> 16) >> bd8) - 128;
+                const int lo = (int)((v[k][q] & 0xffffu) >> bd8) - 128, hi = (int)((v[k][q] >> 16) >> bd8) - 128;
                 d[q] = ((uint32_t)lo & 0xffffu) | ((uint32_t)hi << 16);
             }
         }
+    }
     }
 
     __syncthreads();
@@ -508,7 +528,7 @@ template <typename P>
 __global__ void __launch_bounds__(256, 7) cdef_ccso_kernel(const DevFrame f) {
     pdl_trigger();
     __shared__ CdefSmem sm;
-    cdef_region<P>(f, sm, blockIdx.x, blockIdx.y);
+    cdef_region<P, (NCHUNK + 255) / 256>(f, sm, blockIdx.x, blockIdx.y);
 }
 
 // Persistent kernel over a cross-frame work list: item = frame << 22 |
@@ -522,9 +542,9 @@ __global__ void __launch_bounds__(256, 6) cdef_batch_kernel(BatchArgs a) {
         const DevFrame &f = a.frames[it >> 22];
         const int b = it & 0x3fffff, sb64w = (f.w + 63) >> 6;
         if (f.bitdepth > 8)
-            cdef_region<uint16_t>(f, sm, b % sb64w, b / sb64w);
+            cdef_region<uint16_t, 1>(f, sm, b % sb64w, b / sb64w);
         else
-            cdef_region<uint8_t>(f, sm, b % sb64w, b / sb64w);
+            cdef_region<uint8_t, 1>(f, sm, b % sb64w, b / sb64w);
         __syncthreads();
     }
 }

@@ -482,34 +482,56 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
     const int64_t ys = f.stride[0], uvs = f.stride[1];
     if (tid < 4) sm.n[tid] = 0;
     __syncthreads();  // list counters reset before any thread appends
-    // ---- stage R (samples outside the frame read 0; no valid edge uses them)
-    for (int i = tid; i < LT * (LT / 4); i += nt) {
-        int r = i / (LT / 4), c4 = (i % (LT / 4)) * 4;
-        int gy = lsy + r, gx = lsx + c4;
-        int v[4] = {0, 0, 0, 0};
-        if (gy >= 0 && gy < f.h) {
-            if (gx >= 0 && gx + 3 < f.w)
-                Vec4<P>::unpack(*reinterpret_cast<const typename Vec4<P>::T *>(Ry + gy * ys + gx), v);
-            else
-                for (int k = 0; k < 4; k++)
-                    if (gx + k >= 0 && gx + k < f.w) v[k] = Ry[gy * ys + gx + k];
+    // ---- stage R (samples outside the frame read 0; no valid edge uses them):
+    // runs of 4 samples, eight loads in flight per thread before their stores
+    {
+        typedef typename Vec4<P>::T T;
+        constexpr int NLY = LT * (LT / 4), NST = NLY + 2 * CT * (CT / 4), B = 8;
+        for (int base = tid; base < NST; base += B * nt) {
+            T v[B];
+#pragma unroll
+            for (int k = 0; k < B; k++) {
+                const int i = base + k * nt;
+                int vv[4] = {0, 0, 0, 0};
+                v[k] = Vec4<P>::pack(vv);
+                if (i >= NST) continue;
+                const P *src;
+                int gy, gx, H, W;
+                int64_t st;
+                if (i < NLY) {
+                    const int r = i / (LT / 4), c4 = (i % (LT / 4)) * 4;
+                    gy = lsy + r, gx = lsx + c4, H = f.h, W = f.w, st = ys, src = Ry;
+                } else {
+                    const int j = i - NLY, pl = j / (CT * (CT / 4)), jj = j % (CT * (CT / 4));
+                    const int r = jj / (CT / 4), c4 = (jj % (CT / 4)) * 4;
+                    gy = csy + r, gx = csx + c4, H = f.ch, W = f.cw, st = uvs, src = plane_ptr<const P>(f.R[1 + pl]);
+                }
+                if (gy < 0 || gy >= H) continue;
+                if (gx >= 0 && gx + 3 < W) {
+                    v[k] = __ldg(reinterpret_cast<const T *>(src + gy * st + gx));
+                } else {
+                    for (int q = 0; q < 4; q++)
+                        if (gx + q >= 0 && gx + q < W) vv[q] = src[gy * st + gx + q];
+                    v[k] = Vec4<P>::pack(vv);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < B; k++) {
+                const int i = base + k * nt;
+                if (i >= NST) continue;
+                int16_t *dst;
+                if (i < NLY) {
+                    dst = &sm.y[(i / (LT / 4)) * LP + (i % (LT / 4)) * 4];
+                } else {
+                    const int j = i - NLY, pl = j / (CT * (CT / 4)), jj = j % (CT * (CT / 4));
+                    dst = &sm.uv[pl][(jj / (CT / 4)) * CP + (jj % (CT / 4)) * 4];
+                }
+                int o[4];
+                Vec4<P>::unpack(v[k], o);
+#pragma unroll
+                for (int q = 0; q < 4; q++) dst[q] = (int16_t)o[q];
+            }
         }
-        for (int k = 0; k < 4; k++) sm.y[r * LP + c4 + k] = (int16_t)v[k];
-    }
-    for (int i = tid; i < 2 * CT * (CT / 4); i += nt) {
-        int pl = i / (CT * (CT / 4)), j = i % (CT * (CT / 4));
-        int r = j / (CT / 4), c4 = (j % (CT / 4)) * 4;
-        int gy = csy + r, gx = csx + c4;
-        const P *Rc = plane_ptr<const P>(f.R[1 + pl]);
-        int v[4] = {0, 0, 0, 0};
-        if (gy >= 0 && gy < f.ch) {
-            if (gx >= 0 && gx + 3 < f.cw)
-                Vec4<P>::unpack(*reinterpret_cast<const typename Vec4<P>::T *>(Rc + gy * uvs + gx), v);
-            else
-                for (int k = 0; k < 4; k++)
-                    if (gx + k >= 0 && gx + k < f.cw) v[k] = Rc[gy * uvs + gx + k];
-        }
-        for (int k = 0; k < 4; k++) sm.uv[pl][r * CP + c4 + k] = (int16_t)v[k];
     }
     // the tile's side-info (its loads are in flight together with the
     // sample loads above); stage_side ends with a barrier
