@@ -252,7 +252,8 @@ def test_wiener_uv_slot(L, oracle, bd, ds):
         sp.filter = f.ctypes.data
         sp.luma, sp.luma_top, sp.luma_bottom = (gluma.ctypes.data + k * gluma.itemsize for k in (lo, lto, lbo))
         sp.stride, sp.ss_ver, sp.ss_hor, sp.ds_flt = LS, 1, 1, ds
-        rc = L.r2g_dsp_ns_wiener_single_uv(_ptr(got, o), S, p(_st(left, bd)), _ptr(got, o - 2 * S),
+        gleft = _st(left, bd)  # kept alive across the call
+        rc = L.r2g_dsp_ns_wiener_single_uv(_ptr(got, o), S, p(gleft), _ptr(got, o - 2 * S),
                                            _ptr(got, o + h * S), w, h, C.byref(prm), edges, p(ll), bd)
         assert rc == 0
         assert np.array_equal(got.astype(np.uint16), ref), (w, h, edges)
@@ -276,7 +277,8 @@ def test_gdf_prep_slot(L, oracle, bd):
                                   C.c_int64(o - 2 * S), p(plane), C.c_int64(o + h * S), w, h, rd, qp, edges, bd)
         got = np.full((h, w), 99, np.int8)
         g = _st(plane, bd).ravel()
-        rc = L.r2g_dsp_gdf_prep(p(got), w, _ptr(g, o), S, p(_st(left, bd)), _ptr(g, o - 2 * S), _ptr(g, o + h * S),
+        gleft = _st(left, bd)  # kept alive across the call
+        rc = L.r2g_dsp_gdf_prep(p(got), w, _ptr(g, o), S, p(gleft), _ptr(g, o - 2 * S), _ptr(g, o + h * S),
                                 w, h, rd, qp, edges, bd)
         assert rc == 0
         assert np.array_equal(got, want), (w, h, edges, rd, qp)
@@ -363,15 +365,16 @@ def test_film_grain_band_slots(L, oracle, bd, chroma):
         luma = rng.integers(0, 1 << bd, (bh << sy, (stride << sx) + 2)).astype(np.uint16)
         want = np.zeros_like(src)
         got = _st(np.zeros_like(src), bd)
+        gsrc, gluma = _st(src, bd), _st(luma, bd)  # kept alive across the calls
         if chroma:
             uv, is_id = int(it & 1), int((it >> 1) & 1)
             lib.r2o_fguv_32x32xn(p(want), p(src), stride, C.byref(fgd), seed, pw, p(scaling), p(lut), bh, row_num,
                                  p(luma), luma.shape[1], uv, is_id, sx, sy, bd)
-            rc = L.r2g_dsp_fguv_32x32xn(p(got), p(_st(src, bd)), stride, C.byref(fgd), seed, pw, p(scaling), p(lut),
-                                        bh, row_num, p(_st(luma, bd)), luma.shape[1], uv, is_id, sx, sy, bd)
+            rc = L.r2g_dsp_fguv_32x32xn(p(got), p(gsrc), stride, C.byref(fgd), seed, pw, p(scaling), p(lut),
+                                        bh, row_num, p(gluma), luma.shape[1], uv, is_id, sx, sy, bd)
         else:
             lib.r2o_fgy_32x32xn(p(want), p(src), stride, C.byref(fgd), seed, pw, p(scaling), p(lut), bh, row_num, bd)
-            rc = L.r2g_dsp_fgy_32x32xn(p(got), p(_st(src, bd)), stride, C.byref(fgd), seed, pw, p(scaling), p(lut),
+            rc = L.r2g_dsp_fgy_32x32xn(p(got), p(gsrc), stride, C.byref(fgd), seed, pw, p(scaling), p(lut),
                                        bh, row_num, bd)
         assert rc == 0
         assert np.array_equal(got[:, :pw].astype(np.uint16), want[:, :pw]), it
