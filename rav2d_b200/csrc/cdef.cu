@@ -528,7 +528,7 @@ template <typename P>
 __global__ void __launch_bounds__(256, 7) cdef_ccso_kernel(const DevFrame f) {
     pdl_trigger();
     __shared__ CdefSmem sm;
-    cdef_region<P, (NCHUNK + 255) / 256>(f, sm, blockIdx.x, blockIdx.y);
+    cdef_region<P, 1>(f, sm, blockIdx.x, blockIdx.y);
 }
 
 // Persistent kernel over a cross-frame work list: item = frame << 22 |

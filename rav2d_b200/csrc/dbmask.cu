@@ -15,11 +15,11 @@
 // block that covers a row left of a block B is decoded before B, left to
 // right, so the value B reads is the one its left neighbour on that row
 // left; likewise above.  The device form is two passes over the records:
-//   pass 1 (one thread per record): write the level the block leaves in the
+//   pass 1 (one warp per record): write the level the block leaves in the
 //          left context for each of its rows at its right-most 4x4 column,
 //          and the level it leaves in the above context for each column at
 //          its bottom 4x4 row, into frame-sized u16 maps;
-//   pass 2 (one thread per record): resolve the outer edges against the
+//   pass 2 (one warp per record): resolve the outer edges against the
 //          neighbour's cell in those maps (or the reset value at a tile
 //          start) and OR every edge bit into the SB256's masks with 32-bit
 //          atomics.  Inner and sub-PU edges need no context.  mask_subpu_
@@ -203,93 +203,101 @@ R2G_D uint64_t or_along(uint16_t (*m)[5][4], int pos, int lvl, uint64_t bits) {
     return old;
 }
 
+// One warp per record in both passes: its lanes take the block's rows,
+// columns or edge positions, so large blocks cost no more than small ones.
 __global__ void __launch_bounds__(128) db_levels_kernel(const __grid_constant__ MaskArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i >= a.n) return;
     const R2gDbBlock b = a.blk[i];
     const Geo g = geometry(a, b);
     if (!g.ok) return;
     const int pw = a.bw4 >> g.ssh;  // map pitch
     uint16_t *L = a.lv[g.chroma ? 2 : 0], *T = a.lv[g.chroma ? 3 : 1];
-    for (int y = 0; y < g.h4; y++) {
+    for (int y = lane; y < g.h4; y += 32) {
         const int l = level_l(g, y);
         L[(size_t)(g.Y + y) * pw + g.X + g.w4 - 1] = (uint16_t)(l == UNTOUCHED ? 0x8000 | g.X : l);
     }
-    for (int x = 0; x < g.w4; x++) {
+    for (int x = lane; x < g.w4; x += 32) {
         const int l = level_t(g, x);
         T[(size_t)(g.Y + g.h4 - 1) * pw + g.X + x] = (uint16_t)(l == UNTOUCHED ? 0x8000 | g.Y : l);
     }
 }
 
+// The four per-level bit sets of one outer edge, gathered by ballots (lane =
+// row or column of the block), then ORed in by lanes 0..3.
+R2G_D void outer_edge(uint16_t (*m)[5][4], int pos, int start, int n, int lane, bool left, const Geo &g,
+                      const MaskArgs &a, const uint16_t *map, int pw, int reset) {
+    uint64_t bits[4] = {0, 0, 0, 0};
+    for (int j0 = 0; j0 < n; j0 += 32) {
+        const int j = j0 + lane;
+        int lvl = -1;
+        if (j < n) {
+            const int own = left ? level_l(g, j) : level_t(g, j);
+            if (own != UNTOUCHED) {
+                const int nb = left ? context_at(map, (size_t)(g.Y + j) * pw + g.X, 1, g.X, a.col_start, g.ssh, reset)
+                                    : context_at(map, (size_t)g.Y * pw + g.X + j, pw, g.Y, a.row_start, g.ssv, reset);
+                lvl = imin_(own, nb) & 3;
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < 4; l++) bits[l] |= (uint64_t)__ballot_sync(0xffffffffu, lvl == l) << (start + j0);
+    }
+    const uint64_t mine = lane == 0 ? bits[0] : lane == 1 ? bits[1] : lane == 2 ? bits[2] : bits[3];
+    if (lane < 4 && mine) or_along(m, pos, lane, mine);
+}
+
 __global__ void __launch_bounds__(128) db_masks_kernel(const __grid_constant__ MaskArgs a) {
     pdl_wait();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i >= a.n) return;
     const R2gDbBlock b = a.blk[i];
     const Geo g = geometry(a, b);
     if (!g.ok) {
-        atomicAdd(a.bad, 1u);
+        if (lane == 0) atomicAdd(a.bad, 1u);
         return;
     }
     R2gAv2Filter &f = a.masks[g.sb];
     uint16_t(*m)[64][5][4] = g.chroma ? f.filter_uv : f.filter_y;
     const int pw = a.bw4 >> g.ssh, ci = g.chroma;
-    const uint16_t *L = a.lv[ci ? 2 : 0], *T = a.lv[ci ? 3 : 1];
     const int reset = 3 - ci;
 
     // ---- outer edges against the neighbours' context levels (tile starts
     // are superblock-aligned, so chroma column X starts a tile when luma
     // column 2X does; levels read from the maps are 0..3) ----
-    uint64_t byl[4] = {0, 0, 0, 0};
-    for (int y = 0; y < g.h4; y++) {
-        const int own = level_l(g, y);
-        if (own == UNTOUCHED) continue;
-        const int nb = context_at(L, (size_t)(g.Y + y) * pw + g.X, 1, g.X, a.col_start, g.ssh, reset);
-        byl[imin_(own, nb) & 3] |= 1ull << (g.by4 + y);
-    }
-#pragma unroll
-    for (int l = 0; l < 4; l++)
-        if (byl[l]) or_along(m[0], g.bx4, l, byl[l]);
-    uint64_t bxl[4] = {0, 0, 0, 0};
-    for (int x = 0; x < g.w4; x++) {
-        const int own = level_t(g, x);
-        if (own == UNTOUCHED) continue;
-        const int nb = context_at(T, (size_t)g.Y * pw + g.X + x, pw, g.Y, a.row_start, g.ssv, reset);
-        bxl[imin_(own, nb) & 3] |= 1ull << (g.bx4 + x);
-    }
-#pragma unroll
-    for (int l = 0; l < 4; l++)
-        if (bxl[l]) or_along(m[1], g.by4, l, bxl[l]);
+    outer_edge(m[0], g.bx4, g.by4, g.h4, lane, true, g, a, a.lv[ci ? 2 : 0], pw, reset);
+    outer_edge(m[1], g.by4, g.bx4, g.w4, lane, false, g, a, a.lv[ci ? 3 : 1], pw, reset);
 
-    // ---- inner transform edges (mask_edges_part) ----
+    // ---- inner transform edges (mask_edges_part): a lane per position ----
     if (g.txb) {
         const uint64_t rows = ones_shl(g.h4, g.by4), cols = ones_shl(g.w4, g.bx4);
+        const int tw = g.tw4, th = g.th4;
         if (g.tx_part < TXP_H5) {
-            if (g.w4 > g.tw4)
-                for (int x = g.tw4; x < g.w4; x += g.tw4) or_along(m[0], g.bx4 + x, g.twl4c, rows);
-            if (g.h4 > g.th4)
-                for (int y = g.th4; y < g.h4; y += g.th4) or_along(m[1], g.by4 + y, g.thl4c, cols);
+            for (int x = tw * (1 + lane); x < g.w4; x += 32 * tw) or_along(m[0], g.bx4 + x, g.twl4c, rows);
+            for (int y = th * (1 + lane); y < g.h4; y += 32 * th) or_along(m[1], g.by4 + y, g.thl4c, cols);
         } else if (g.tx_part == TXP_H5) {
-            for (int y = g.th4; y < g.h4; y += 2 * g.th4) or_along(m[1], g.by4 + y, g.thl4c, cols);
-            const uint64_t v = rows & ~ones_shl(2 * g.th4, g.by4 + g.th4);
+            for (int y = th + 2 * th * lane; y < g.h4; y += 64 * th) or_along(m[1], g.by4 + y, g.thl4c, cols);
+            const uint64_t v = rows & ~ones_shl(2 * th, g.by4 + th);
             if (v)
-                for (int x = g.tw4; x < g.w4; x += g.tw4) or_along(m[0], g.bx4 + x, g.twl4c, v);
+                for (int x = tw * (1 + lane); x < g.w4; x += 32 * tw) or_along(m[0], g.bx4 + x, g.twl4c, v);
         } else {
-            for (int x = g.tw4; x < g.w4; x += 2 * g.tw4) or_along(m[0], g.bx4 + x, g.twl4c, rows);
-            const uint64_t h = cols & ~ones_shl(2 * g.tw4, g.bx4 + g.tw4);
+            for (int x = tw + 2 * tw * lane; x < g.w4; x += 64 * tw) or_along(m[0], g.bx4 + x, g.twl4c, rows);
+            const uint64_t h = cols & ~ones_shl(2 * tw, g.bx4 + tw);
             if (h)
-                for (int y = g.th4; y < g.h4; y += g.th4) or_along(m[1], g.by4 + y, g.thl4c, h);
+                for (int y = th * (1 + lane); y < g.h4; y += 32 * th) or_along(m[1], g.by4 + y, g.thl4c, h);
         }
     }
+    // the sub-PU step reads what the inner edges wrote (other lanes' atomics)
+    __syncwarp();
 
-    // ---- sub-PU edges (create_db_mask's tail, mask_subpu_edges) ----
+    // ---- sub-PU edges (create_db_mask's tail, mask_subpu_edges): a lane
+    // per position ----
     if (g.subpu_l2 != 3) {
         const int ds = (a.tip_frame_mode != 2) * 15;
         const int hl = g.sub_twl - (g.ssh && g.sub_twl), vl = g.sub_thl - (g.ssv && g.sub_thl);
         const int hsz = (1 << g.subpu_l2) >> g.ssh, vsz = (1 << g.subpu_l2) >> g.ssv;
         if (hsz) {
             const uint64_t parts = ones_shl(g.h4, g.by4);
-            for (int x = hsz; x < g.w4; x += hsz) {
+            for (int x = hsz * (1 + lane); x < g.w4; x += 32 * hsz) {
                 const uint64_t old = or_along(m[0], g.bx4 + x, hl, parts);
                 if (x & ds) {
                     const uint64_t nb = parts & ~old;
@@ -299,7 +307,7 @@ __global__ void __launch_bounds__(128) db_masks_kernel(const __grid_constant__ M
         }
         if (vsz) {
             const uint64_t parts = ones_shl(g.w4, g.bx4);
-            for (int y = vsz; y < g.h4; y += vsz) {
+            for (int y = vsz * (1 + lane); y < g.h4; y += 32 * vsz) {
                 const uint64_t old = or_along(m[1], g.by4 + y, vl, parts);
                 if (y & ds) {
                     const uint64_t nb = parts & ~old;
@@ -347,7 +355,7 @@ int r2g_launch_db_masks(const R2gDbMaskInput &in, const R2gDbBlock *dev_blocks, 
     a.row_start[0] |= 1u;
     a.tab = tab;
     a.bad = bad;
-    const int grid = (in.n_blocks + 127) / 128;
+    const int grid = (in.n_blocks + 3) / 4;  // four warps (records) per CTA
     db_levels_kernel<<<grid, 128, 0, s>>>(a);
     r2g_launch_pdl(db_masks_kernel, dim3(grid), dim3(128), s, a);
     return 2;

@@ -133,7 +133,8 @@ int fg_band(void *dst, const void *src, int64_t stride, const R2gFilmGrainData *
     if (!dst || !src || !data || !scaling || !grain_lut || !ok_bd(bitdepth) || pw <= 0 || bh <= 0 || row_num < 0 ||
         in_seed > 0xffff || data->block_size < 0 || data->block_size > 1 || data->scaling_shift < 8 ||
         data->scaling_shift > 11 || bh > ((16 << data->block_size) >> sy) || sx < 0 || sx > 1 || sy < 0 || sy > 1 ||
-        uv < 0 || uv > 1 || pw > r2g_dsp_fg_band_max_width(data->block_size, sx) || (luma_row == nullptr) != (uv < 0))
+        (luma_row && uv > 1) || pw > r2g_dsp_fg_band_max_width(data->block_size, sx) ||
+        (luma_row == nullptr) != (uv < 0))
         return R2G_E_INVALID;
     std::vector<uint16_t> s16, l16;
     if (!stage_rows(s16, src, stride, pw, bh, bitdepth)) return R2G_E_INVALID;

@@ -590,11 +590,10 @@ R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
     StageSched *sched = src.sched();
     int k = 0;  // items published
     bool waited = false, ok = true;
-    auto next_pos = [&]() {
-        int nx = 0;
-        if (lane == 0) nx = (int)(gridDim.x + atomicAdd(&sched->next, 1u));
-        return __shfl_sync(0xffffffffu, nx, 0);
-    };
+    // a position fetch: the atomic is issued here and its result read (which
+    // waits for it) only after the current item is published
+    auto fetch = [&]() -> unsigned { return lane == 0 ? atomicAdd(&sched->next, 1u) : 0u; };
+    auto landed = [&](unsigned raw) { return (int)(gridDim.x + __shfl_sync(0xffffffffu, raw, 0)); };
     ItemRegs cur, nxt;
     bool have = blockIdx.x < n;
     if (have) {
@@ -602,15 +601,15 @@ R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
         src.item(blockIdx.x, fi, b);
         item_issue(src.frame(fi), fi, b, lane, cur);
     }
-    int w_next = have ? next_pos() : n;
+    int w_next = have ? landed(fetch()) : n;
     while (have) {
         const bool have_n = w_next < n;
-        int w_after = n;
+        unsigned raw_after = 0;
         if (have_n) {
             int fi, b;
             src.item(w_next, fi, b);
             item_issue(src.frame(fi), fi, b, lane, nxt);
-            w_after = next_pos();
+            raw_after = fetch();
         }
         if (cur.ok) {
             const DevFrame &f = src.frame(cur.fi);
@@ -624,7 +623,7 @@ R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
         }
         cur = nxt;
         have = have_n;
-        w_next = w_after;
+        w_next = have_n ? landed(raw_after) : n;
     }
     if (!waited) pdl_wait();
     if (ok) {
