@@ -416,113 +416,78 @@ R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int 
     return total;
 }
 
-// One work item as the producer holds it between the two halves of its
-// work: the geometry, and the side-info words each lane loaded for it (in
-// flight until item_finish reads them).
-struct ItemRegs {
-    UnitGeom g;
-    int b, fi, ro, nr;
-    bool ok;
-    int sb256_idx, inc;
-    uint32_t utype, gdfv;
-    uint32_t ll0, ll1, nsk;
-    int tap;
-};
-
-// First half: geometry, and every side-info load the item may need issued
-// at once (unit type, GDF flag, lossless and no-skip rows, unit taps), so a
-// single round trip covers them and it overlaps the previous item's copies.
-R2G_D void item_issue(const DevFrame &f, int fi, int b, int lane, ItemRegs &it) {
-    it.b = b;
-    it.fi = fi;
-    it.ok = item_geom(f, b, it.g, it.ro, it.nr);
-    it.utype = it.gdfv = it.ll0 = it.ll1 = it.nsk = 0;
-    it.tap = 0;
-    if (!it.ok) return;
-    const UnitGeom &g = it.g;
-    const int plane = g.plane, chroma = plane != 0;
-    it.inc = ((g.edges & (LR_HAVE_TOP | LR_HAVE_TOP_INTEGRATED | LR_HAVE_BOTTOM_INTEGRATED)) == LR_HAVE_TOP &&
-              g.y0 + 8 < ((f.bh4 * 4) >> chroma))
-                 ? 8
-                 : 0;
-    it.sb256_idx = f.sb256w * (((g.y0 << chroma) + it.inc) >> 8) + g.sb256x;
-    const int nsb = f.sb256w * f.sb256h;
-    if (g.valid) {
-        it.utype = g.unit->type;
-        if (lane < 18) it.tap = g.unit->f[lane];
-    }
-    if (plane == 0 && it.sb256_idx < nsb) it.gdfv = f.masks[it.sb256_idx].gdf[(((g.y0 + it.inc) >> 4) & 12) + g.sb64x_idx];
-    // lossless rows (looprestoration.rs:2037-2075)
-    if (lane < 17) {
-        const int ll_rows = imax_(g.sh >> 2, 1) + 1;
-        if (lane < ll_rows && it.sb256_idx < nsb) {
-            const R2gAv2Filter &m = f.masks[it.sb256_idx];
-            const int y4 = ((g.y0 << chroma) & 255) >> 2;
-            if (plane == 0) {
-                const int yy = y4 + lane;
-                if (yy < 64) it.ll0 = m.lossless_mask_y[yy][g.sb64x_idx];
-            } else {
-                const int init_y = g.y0 >> 2, end_y = (g.y0 + g.sh) >> 2;
-                const int sy = (y4 >> 1) + lane;
-                if (init_y + lane < end_y && sy < 64) {
-                    it.ll0 = m.lossless_mask_uv[sy][g.sb64x_idx] | 0x10000u;  // bit 16: row present
-                    if (g.sb64x_idx + 1 < 4) it.ll1 = m.lossless_mask_uv[sy][g.sb64x_idx + 1];
-                }
-            }
-        }
-    }
-    // multi-class no-skip rows (looprestoration.rs:1922-1944)
-    if (lane < 18) {
-        const int by = (g.y0 >> 2) + lane;
-        if (by < ((g.y0 + g.sh) >> 2)) {
-            const int sidx = f.sb256w * (by >> 6) + g.sb256x;
-            if (sidx < nsb) it.nsk = f.masks[sidx].lr_noskip_mask[by & 63][g.sb64x_idx] | 0x10000u;
-        }
-    }
-}
-
-// Second half: publishes the item into slot k & 1 (after the slot's release
-// when it was used before) and issues its row copies.  Returns 1 when
-// published, -1 when a wait ran out.
+// Produces one work item into slot k & 1, after waiting for the slot's
+// release when it was used before.  Returns 0 for an empty item (nothing
+// published), 1 when published, -1 when a wait ran out.
 template <typename P>
-R2G_D int item_publish(const DevFrame &f, const ItemRegs &it, LrSmem &sm, int k, int lane, bool &waited) {
-    const UnitGeom &g = it.g;
-    const int plane = g.plane, chroma = plane != 0, ro = it.ro, nr = it.nr;
+R2G_D int produce_item(const DevFrame &f, int fi, int b, LrSmem &sm, int k, int lane, bool &waited) {
+    UnitGeom g;
+    int ro, nr;
+    if (!item_geom(f, b, g, ro, nr)) return 0;
+    const int plane = g.plane, chroma = plane != 0;
     const R2gFrameParams &fp = f.fp;
     // ---- kernel selection (looprestoration.rs:1880-1920) ----
     int wkind = W_NONE;
     const bool plane_on = (f.restore_planes >> plane) & 1;
     if (plane_on && g.valid) {
-        const int wt = (f.inloop & R2G_INLOOP_WIENER) ? (int)it.utype : 0;
+        const int wt = (f.inloop & R2G_INLOOP_WIENER) ? g.unit->type : 0;
         const R2gRestorationPlane &pd = fp.restoration[plane];
         if (wt == R2G_RESTORE_NS_WIENER)
             wkind = (pd.frame_filters_on && pd.num_classes != 1) ? W_NS_MULTI : W_NS_SINGLE;
         else if (wt == R2G_RESTORE_PC_WIENER)
             wkind = W_PC;
     }
+    const int inc = ((g.edges & (LR_HAVE_TOP | LR_HAVE_TOP_INTEGRATED | LR_HAVE_BOTTOM_INTEGRATED)) == LR_HAVE_TOP &&
+                     g.y0 + 8 < ((f.bh4 * 4) >> chroma))
+                        ? 8
+                        : 0;
+    const int sb256_idx = f.sb256w * (((g.y0 << chroma) + inc) >> 8) + g.sb256x;
     const int nsb = f.sb256w * f.sb256h;
-    const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && it.sb256_idx < nsb &&
-                        it.gdfv != 0;
+    const bool gdf_on = plane_on && g.valid && plane == 0 && (f.inloop & R2G_INLOOP_GDF) && sb256_idx < nsb &&
+                        f.masks[sb256_idx].gdf[(((g.y0 + inc) >> 4) & 12) + g.sb64x_idx] != 0;
     const bool copy = wkind == W_NONE && !gdf_on;
+    // ---- per-lane side-info: lossless rows (looprestoration.rs:2037-2075),
+    // multi-class no-skip rows (:1922-1944), single-class taps ----
     uint16_t llm = 0, nsk = 0;
     int tap = 0;
     if (!copy) {
-        if (plane == 0)
-            llm = (uint16_t)it.ll0;
-        else if (it.ll0 >> 16)
-            llm = (uint16_t)((it.ll0 & 0xff) | ((it.ll1 & 0xff) << 8));
-        if ((wkind == W_NS_MULTI || wkind == W_PC) && (it.nsk >> 16)) {
-            uint16_t v = (uint16_t)it.nsk;
-            if (!(g.edges & LR_HAVE_RIGHT) && (g.uw & 63) != 0) {
-                const int sh = ((g.uw >> 2) & 15) - 1;
-                const uint16_t eb = (uint16_t)(v >> sh);
-                v = (uint16_t)(v | (uint16_t)(eb << (sh + 1)));
+        if (lane < 17) {
+            const int ll_rows = imax_(g.sh >> 2, 1) + 1;
+            if (lane < ll_rows && sb256_idx < nsb) {
+                const R2gAv2Filter &m = f.masks[sb256_idx];
+                const int y4 = ((g.y0 << chroma) & 255) >> 2;
+                if (plane == 0) {
+                    const int yy = y4 + lane;
+                    if (yy < 64) llm = m.lossless_mask_y[yy][g.sb64x_idx];
+                } else {
+                    const int init_y = g.y0 >> 2, end_y = (g.y0 + g.sh) >> 2;
+                    const int sy = (y4 >> 1) + lane;
+                    if (init_y + lane < end_y && sy < 64) {
+                        const uint16_t lo = m.lossless_mask_uv[sy][g.sb64x_idx];
+                        const uint16_t hi = g.sb64x_idx + 1 < 4 ? m.lossless_mask_uv[sy][g.sb64x_idx + 1] : 0;
+                        llm = (uint16_t)((lo & 0xff) | ((hi & 0xff) << 8));
+                    }
+                }
             }
-            nsk = v;
+        }
+        if ((wkind == W_NS_MULTI || wkind == W_PC) && lane < 18) {
+            const int by = (g.y0 >> 2) + lane;
+            if (by < ((g.y0 + g.sh) >> 2)) {
+                const int sidx = f.sb256w * (by >> 6) + g.sb256x;
+                if (sidx < nsb) {
+                    uint16_t v = f.masks[sidx].lr_noskip_mask[by & 63][g.sb64x_idx];
+                    if (!(g.edges & LR_HAVE_RIGHT) && (g.uw & 63) != 0) {
+                        const int s = ((g.uw >> 2) & 15) - 1;
+                        const uint16_t eb = (uint16_t)(v >> s);
+                        v = (uint16_t)(v | (uint16_t)(eb << (s + 1)));
+                    }
+                    nsk = v;
+                }
+            }
         }
         if (wkind == W_NS_SINGLE && lane < 18) {
             const R2gRestorationPlane &pd = fp.restoration[plane];
-            tap = pd.frame_filters_on ? pd.filter[0][lane] : it.tap;
+            tap = pd.frame_filters_on ? pd.filter[0][lane] : g.unit->f[lane];
         }
     }
     // single-class FIR constants: s = m * c0 + sum (a + b) f [- l * c1 + sum l' f]
@@ -541,8 +506,8 @@ R2G_D int item_publish(const DevFrame &f, const ItemRegs &it, LrSmem &sm, int k,
     if (k >= 2 && !mbar_wait(&sm.empty[s], ((k >> 1) - 1) & 1)) return -1;
     LrDesc &d = sm.desc[s];
     if (lane == 0) {
-        d.b = it.b;
-        d.fi = it.fi;
+        d.b = b;
+        d.fi = fi;
         d.plane = plane;
         d.x0 = g.x0;
         d.y0 = g.y0;
@@ -581,49 +546,32 @@ R2G_D bool is_hbd(const DevFrame &f) {
 }
 
 // The producer warp: work-list positions blockIdx.x, then
-// gridDim.x + atomicAdd(next), until the list is exhausted, as a two-stage
-// pipeline: while item j is published and its copies issued, item j + 1's
-// side-info loads are in flight and the position after it is being fetched.
+// gridDim.x + atomicAdd(next), until the list is exhausted.
 template <int HB, typename Src>
 R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
     const int n = src.count();
     StageSched *sched = src.sched();
     int k = 0;  // items published
+    int w = blockIdx.x;
     bool waited = false, ok = true;
-    // a position fetch: the atomic is issued here and its result read (which
-    // waits for it) only after the current item is published
-    auto fetch = [&]() -> unsigned { return lane == 0 ? atomicAdd(&sched->next, 1u) : 0u; };
-    auto landed = [&](unsigned raw) { return (int)(gridDim.x + __shfl_sync(0xffffffffu, raw, 0)); };
-    ItemRegs cur, nxt;
-    bool have = blockIdx.x < n;
-    if (have) {
+    while (w < n) {
         int fi, b;
-        src.item(blockIdx.x, fi, b);
-        item_issue(src.frame(fi), fi, b, lane, cur);
-    }
-    int w_next = have ? landed(fetch()) : n;
-    while (have) {
-        const bool have_n = w_next < n;
-        unsigned raw_after = 0;
-        if (have_n) {
-            int fi, b;
-            src.item(w_next, fi, b);
-            item_issue(src.frame(fi), fi, b, lane, nxt);
-            raw_after = fetch();
+        src.item(w, fi, b);
+        const DevFrame &f = src.frame(fi);
+        const int rc = is_hbd<HB>(f) ? produce_item<uint16_t>(f, fi, b, sm, k, lane, waited)
+                                     : produce_item<uint8_t>(f, fi, b, sm, k, lane, waited);
+        if (rc < 0) {
+            ok = false;
+            break;
         }
-        if (cur.ok) {
-            const DevFrame &f = src.frame(cur.fi);
-            const int rc = is_hbd<HB>(f) ? item_publish<uint16_t>(f, cur, sm, k, lane, waited)
-                                         : item_publish<uint8_t>(f, cur, sm, k, lane, waited);
-            if (rc < 0) {
-                ok = false;
-                break;
-            }
-            k += rc;
+        k += rc;
+        if (!waited) {
+            pdl_wait();
+            waited = true;
         }
-        cur = nxt;
-        have = have_n;
-        w_next = have_n ? landed(raw_after) : n;
+        int nx = 0;
+        if (lane == 0) nx = (int)(gridDim.x + atomicAdd(&sched->next, 1u));
+        w = __shfl_sync(0xffffffffu, nx, 0);
     }
     if (!waited) pdl_wait();
     if (ok) {

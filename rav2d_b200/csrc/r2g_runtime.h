@@ -54,6 +54,9 @@ struct R2gCtx {
     StageSched *sched = nullptr;
     unsigned *fault = nullptr;
     unsigned *bad_blocks = nullptr;  // block records the mask builder skipped
+    // set while r2g_frame_stage stages on the upload stream: the device mask
+    // build is then joined by the frame's kernels, not by the upload stream
+    bool defer_mask_join = false;
 };
 // bytes of the context's device control block
 #define R2G_CTL_BYTES 256
@@ -89,6 +92,7 @@ struct R2gFrame {
     void *dbm_dev = nullptr, *dbm_host = nullptr;
     size_t dbm_bytes = 0, dbm_host_bytes = 0;
     cudaEvent_t ev_dbm[2] = {nullptr, nullptr};
+    bool pend_dbm = false;  // the kernels must wait for ev_dbm[1]
 };
 
 // Device mask build (dbmask.cu): zero the frame's filter_y / filter_uv and

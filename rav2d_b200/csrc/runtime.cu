@@ -302,6 +302,7 @@ static int upload_done(R2gCtx *ctx, R2gFrame *f) {
 }
 
 int r2g_frame_before_compute(R2gCtx *ctx, R2gFrame *f) {
+    if (f->pend_dbm) CK(cudaStreamWaitEvent(ctx->stream, f->ev_dbm[1], 0));
     if (!ctx->overlap || !f->ev_up) return R2G_OK;
     // the kernels read this frame's uploads and overwrite planes a pending
     // download may still read
@@ -520,6 +521,9 @@ static int stage_db_masks(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, co
         }
         f->dbm_host_bytes = rb;
     }
+    // a deferred build of this frame's previous staging still reads the
+    // records and writes the masks: order this staging after it
+    if (f->pend_dbm) CK(cudaStreamWaitEvent(cs, f->ev_dbm[1], 0));
     if (rb) {
         const void *src = m.blocks;
         if (!direct) {
@@ -540,7 +544,14 @@ static int stage_db_masks(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *fp, co
                                          ctx->bad_blocks, ctx->side_stream);
     CK(cudaGetLastError());
     CK(cudaEventRecord(f->ev_dbm[1], ctx->side_stream));
-    CK(cudaStreamWaitEvent(cs, f->ev_dbm[1], 0));
+    if (ctx->defer_mask_join && cs != ctx->stream) {
+        // the upload stream goes on with the next copies; the frame's
+        // kernels wait for the build (r2g_frame_before_compute)
+        f->pend_dbm = true;
+    } else {
+        CK(cudaStreamWaitEvent(cs, f->ev_dbm[1], 0));
+        f->pend_dbm = false;
+    }
     return R2G_OK;
 }
 
@@ -800,7 +811,11 @@ extern "C" int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *f
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st;
     int rc = upload_stream(ctx, f, &st);
-    if (rc == R2G_OK) rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, st);
+    if (rc == R2G_OK) {
+        ctx->defer_mask_join = true;
+        rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, st);
+        ctx->defer_mask_join = false;
+    }
     if (rc != R2G_OK) return rc;
     f->staged = true;
     return upload_done(ctx, f);
