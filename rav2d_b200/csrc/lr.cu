@@ -338,6 +338,7 @@ R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int 
     if (copy) {
         // unfiltered unit: its output rows only, from the unit origin
         const uint32_t bytes = (uint32_t)((g.uw * bps + 15) & ~15);
+        if (!issue) return lane == 0 ? (uint32_t)nr * bytes : 0u;
         for (int r = lane; r < nr; r += 32) {
             if (issue)
                 bulk_g2s(raw + r * RG::RB, Cp + ((int64_t)(g.y0 + ro + r) * stride + g.x0) * bps, bytes, bar);
@@ -355,6 +356,18 @@ R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int 
     const uint32_t bytes = (uint32_t)((ce - cs) * bps);
     const int halo = plane ? 2 : 6;
     const int wrows = nr + 2 * halo;
+    if (!issue) {
+        // every row copy of the item has the same length: the byte count
+        // the slot's barrier expects, without walking the rows
+        uint32_t t = (uint32_t)wrows * bytes;
+        if (plane && kind == W_NS_SINGLE) {
+            int lcs = 2 * g.x0 - RG::XO;
+            if (lcs < 0) lcs = 0;
+            const int lce = imin_(2 * g.x0 + 128 + RG::XO, (int)f.stride[0]);
+            t += (uint32_t)(2 * wrows) * (uint32_t)((lce - lcs) * bps);
+        }
+        return lane == 0 ? t : 0u;
+    }
     for (int r = lane; r < wrows; r += 32) {
         int row;
         bool from_d;
@@ -568,6 +581,18 @@ R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
         if (!waited) {
             pdl_wait();
             waited = true;
+        }
+        // near the end of the list take the next item only once the
+        // consumers are on the last one published (one item queued rather
+        // than two), so the CTAs run out of work closer together
+        if (k >= 1) {
+            unsigned taken = 0;
+            if (lane == 0) taken = *reinterpret_cast<volatile unsigned *>(&sched->next);
+            taken = __shfl_sync(0xffffffffu, taken, 0);
+            if ((int)(3 * gridDim.x + taken) >= n && !mbar_wait(&sm.empty[(k - 1) & 1], ((k - 1) >> 1) & 1)) {
+                ok = false;
+                break;
+            }
         }
         int nx = 0;
         if (lane == 0) nx = (int)(gridDim.x + atomicAdd(&sched->next, 1u));
