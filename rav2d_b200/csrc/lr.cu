@@ -22,9 +22,8 @@
 //     counter), decodes their geometry, unit kind, lossless and no-skip rows
 //     from the side-info, and stages every source row of the item's window
 //     (C or D by the rule above; the unit's width plus a 16-byte margin on
-//     each side) into one of two shared-memory slots with 16-byte
-//     asynchronous copies (cp.async) spread over its lanes, completing on
-//     the slot's "full" mbarrier;
+//     each side) into one of two shared-memory slots, one bulk copy
+//     (cp.async.bulk) per row completing on the slot's "full" mbarrier;
 //   * eight consumer warps take the slots in turn: they turn the raw rows
 //     into the filter window (edge replication at the frame's left / right
 //     border; each position holds its sample and the right neighbour as a
@@ -325,27 +324,27 @@ R2G_D bool item_geom(const DevFrame &f, int b, UnitGeom &g, int &ro, int &nr) {
 }
 
 // ---------------------------------------------------------------- producer
-// Issues the copies of one item's raw rows as 16-byte asynchronous copies
-// (cp.async) spread over the warp's lanes: each lane takes one 16-byte
-// chunk of each of a group of rows (every row of an item has the same
-// length, a multiple of 16 bytes starting 16-byte aligned).  One copy
-// request per row through the bulk-copy unit measured 2.4 us per item at
-// 1080p, the issue-limited part of the producer.
+// Issues (issue = true) or only sizes the bulk copies of one item's raw
+// rows, spread over the warp's lanes; returns this lane's bytes.
 template <typename P>
-R2G_D void item_copies(const DevFrame &f, const UnitGeom &g, int plane, int ro, int nr, int kind, bool copy,
-                       unsigned char *raw, int lane) {
+R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int ro, int nr, int kind, bool copy,
+                           unsigned char *raw, uint64_t *bar, int lane, bool issue) {
     typedef RawGeom<P> RG;
     constexpr int bps = (int)sizeof(P);
     const int64_t stride = f.stride[plane != 0];
     const char *Cp = (const char *)f.C[plane];
     const char *Dp = (const char *)f.D[plane];
+    uint32_t total = 0;
     if (copy) {
         // unfiltered unit: its output rows only, from the unit origin
-        const int cpr = (g.uw * bps + 15) >> 4, rpi = 32 / cpr, lr = lane / cpr, lq = lane - lr * cpr;
-        if (lr < rpi)
-            for (int r = lr; r < nr; r += rpi)
-                cp_async16(raw + r * RG::RB + 16 * lq, Cp + ((int64_t)(g.y0 + ro + r) * stride + g.x0) * bps + 16 * lq);
-        return;
+        const uint32_t bytes = (uint32_t)((g.uw * bps + 15) & ~15);
+        if (!issue) return lane == 0 ? (uint32_t)nr * bytes : 0u;
+        for (int r = lane; r < nr; r += 32) {
+            if (issue)
+                bulk_g2s(raw + r * RG::RB, Cp + ((int64_t)(g.y0 + ro + r) * stride + g.x0) * bps, bytes, bar);
+            total += bytes;
+        }
+        return total;
     }
     // window columns [x0 - XO, x0 + 64 + XO), clipped to the plane row
     int cs = g.x0 - RG::XO, doff = 0;
@@ -354,18 +353,27 @@ R2G_D void item_copies(const DevFrame &f, const UnitGeom &g, int plane, int ro, 
         cs = 0;
     }
     const int ce = imin_(g.x0 + 64 + RG::XO, (int)stride);
+    const uint32_t bytes = (uint32_t)((ce - cs) * bps);
     const int halo = plane ? 2 : 6;
     const int wrows = nr + 2 * halo;
-    {
-        const int cpr = ((ce - cs) * bps) >> 4, rpi = 32 / cpr, lr = lane / cpr, lq = lane - lr * cpr;
-        if (lr < rpi)
-            for (int r = lr; r < wrows; r += rpi) {
-                int row;
-                bool from_d;
-                row_src(g, ro + r - halo, row, from_d);
-                cp_async16(raw + r * RG::RB + doff + 16 * lq,
-                           (from_d ? Dp : Cp) + ((int64_t)row * stride + cs) * bps + 16 * lq);
-            }
+    if (!issue) {
+        // every row copy of the item has the same length: the byte count
+        // the slot's barrier expects, without walking the rows
+        uint32_t t = (uint32_t)wrows * bytes;
+        if (plane && kind == W_NS_SINGLE) {
+            int lcs = 2 * g.x0 - RG::XO;
+            if (lcs < 0) lcs = 0;
+            const int lce = imin_(2 * g.x0 + 128 + RG::XO, (int)f.stride[0]);
+            t += (uint32_t)(2 * wrows) * (uint32_t)((lce - lcs) * bps);
+        }
+        return lane == 0 ? t : 0u;
+    }
+    for (int r = lane; r < wrows; r += 32) {
+        int row;
+        bool from_d;
+        row_src(g, ro + r - halo, row, from_d);
+        if (issue) bulk_g2s(raw + r * RG::RB + doff, (from_d ? Dp : Cp) + ((int64_t)row * stride + cs) * bps, bytes, bar);
+        total += bytes;
     }
     if (plane && kind == W_NS_SINGLE) {
         // CfL luma rows (backup_row_luma with ns_wiener_single_uv's row
@@ -380,44 +388,45 @@ R2G_D void item_copies(const DevFrame &f, const UnitGeom &g, int plane, int ro, 
             lcs = 0;
         }
         const int lce = imin_(2 * g.x0 + 128 + RG::XO, (int)ls);
-        const int cpr = ((lce - lcs) * bps) >> 4, rpi = 32 / cpr, lr = lane / cpr, lq = lane - lr * cpr;
+        const uint32_t lbytes = (uint32_t)((lce - lcs) * bps);
         const bool topi = g.edges & LR_HAVE_TOP_INTEGRATED, boti = g.edges & LR_HAVE_BOTTOM_INTEGRATED;
-        if (lr < rpi)
-            for (int q = lr; q < 2 * wrows; q += rpi) {
-                int rr = ro + (q >> 1) - 2;
-                if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
-                if (!(g.edges & LR_HAVE_BOTTOM) && !boti && rr >= g.sh) rr = g.sh - 1;
-                const char *src;
-                int ra, rb;
-                if ((rr < 0 && topi) || (rr >= g.sh && boti)) {
-                    // integrated edges read the luma rows in place (pre-LR)
-                    src = Cy;
-                    ra = 2 * (g.y0 + rr);
-                    rb = ra + 1;
-                } else if (rr == -2) {
-                    src = Dy;
-                    ra = rb = 2 * g.y0 - 2;
-                } else if (rr == -1) {
-                    src = Dy;
-                    ra = 2 * g.y0 - 2;
-                    rb = 2 * g.y0 - 1;
-                } else if (rr == g.sh) {
-                    src = Dy;
-                    ra = 2 * (g.y0 + g.sh);
-                    rb = ra + 1;
-                } else if (rr == g.sh + 1) {
-                    src = Dy;
-                    ra = rb = 2 * (g.y0 + g.sh) + 1;
-                } else {
-                    src = Cy;
-                    ra = 2 * (g.y0 + rr);
-                    rb = ra + 1;
-                }
-                const int lrow = (q & 1) ? rb : ra;
-                cp_async16(raw + RG::LOFF + q * RG::LRB + ldoff + 16 * lq,
-                           src + ((int64_t)lrow * ls + lcs) * bps + 16 * lq);
+        for (int q = lane; q < 2 * wrows; q += 32) {
+            int rr = ro + (q >> 1) - 2;
+            if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
+            if (!(g.edges & LR_HAVE_BOTTOM) && !boti && rr >= g.sh) rr = g.sh - 1;
+            const char *src;
+            int ra, rb;
+            if ((rr < 0 && topi) || (rr >= g.sh && boti)) {
+                // integrated edges read the luma rows in place (pre-LR)
+                src = Cy;
+                ra = 2 * (g.y0 + rr);
+                rb = ra + 1;
+            } else if (rr == -2) {
+                src = Dy;
+                ra = rb = 2 * g.y0 - 2;
+            } else if (rr == -1) {
+                src = Dy;
+                ra = 2 * g.y0 - 2;
+                rb = 2 * g.y0 - 1;
+            } else if (rr == g.sh) {
+                src = Dy;
+                ra = 2 * (g.y0 + g.sh);
+                rb = ra + 1;
+            } else if (rr == g.sh + 1) {
+                src = Dy;
+                ra = rb = 2 * (g.y0 + g.sh) + 1;
+            } else {
+                src = Cy;
+                ra = 2 * (g.y0 + rr);
+                rb = ra + 1;
             }
+            const int lrow = (q & 1) ? rb : ra;
+            if (issue)
+                bulk_g2s(raw + RG::LOFF + q * RG::LRB + ldoff, src + ((int64_t)lrow * ls + lcs) * bps, lbytes, bar);
+            total += lbytes;
+        }
     }
+    return total;
 }
 
 // Produces one work item into slot k & 1, after waiting for the slot's
@@ -531,14 +540,16 @@ R2G_D int produce_item(const DevFrame &f, int fi, int b, LrSmem &sm, int k, int 
         d.noskip[lane] = nsk;
         d.f[lane] = (int8_t)tap;
     }
-    // the copies (the consumers' reads of this slot are ordered before them
-    // by the empty barrier); each lane's arrival on the slot's barrier
-    // follows the completion of its own copies, lane 0's plain arrival the
-    // descriptor written above
-    item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], lane);
-    cp_async_mbar_arrive(&sm.full[s]);
+    const uint32_t total =
+        __reduce_add_sync(0xffffffffu, item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane,
+                                                      false));
+    // the consumers' reads of this slot (ordered before by the empty
+    // barrier) precede the copies' writes
+    fence_proxy_async();
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.full[s]);
+    if (lane == 0) mbar_arrive_expect_tx(&sm.full[s], total);
+    __syncwarp();
+    item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane, true);
     return 1;
 }
 

@@ -258,16 +258,6 @@ R2G_D void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
 }
 // orders this thread's earlier shared-memory accesses before its later
 // asynchronous-proxy (bulk copy) accesses
-// 16-byte asynchronous global -> shared copy (both addresses 16-byte
-// aligned), cached in L2 only
-R2G_D void cp_async16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-// An arrival on `bar` once this thread's earlier cp.async copies have
-// completed (the barrier's pending count is raised by one now)
-R2G_D void cp_async_mbar_arrive(uint64_t *bar) {
-    asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
-}
 R2G_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 // barrier among the first `n` threads (the consumer warps) on named barrier
 // 1; returns whether `pred` was true in any of them
