@@ -22,12 +22,8 @@
 //     counter), decodes their geometry, unit kind, lossless and no-skip rows
 //     from the side-info, and stages every source row of the item's window
 //     (C or D by the rule above; the unit's width plus a 16-byte margin on
-//     each side) into one of two shared-memory slots: the run of in-place
-//     rows as 8-row tensor boxes (cp.async.bulk.tensor, one request per 8
-//     rows), each distinct deblocked row as one bulk copy, repeated rows as
-//     entries of a row map; all complete on the slot's "full" mbarrier (the
-//     batched kernel, without tensor maps, copies every row with one bulk
-//     copy);
+//     each side) into one of two shared-memory slots, one bulk copy
+//     (cp.async.bulk) per row completing on the slot's "full" mbarrier;
 //   * eight consumer warps take the slots in turn: they turn the raw rows
 //     into the filter window (edge replication at the frame's left / right
 //     border; each position holds its sample and the right neighbour as a
@@ -36,10 +32,7 @@
 //     FIR, GDF add, one 2-sample store).
 // So the producer loads items k+1 and k+2 while the consumers filter item
 // k, and a frame's GDF / PC-Wiener tables are staged once per CTA.
-#include <cuda.h>
-
 #include <atomic>
-#include <mutex>
 #include <type_traits>
 
 #include "r2g_common.cuh"
@@ -56,14 +49,7 @@ constexpr int LR_NT = NCT + 32;  // plus the producer warp
 constexpr int CROWS = 16;        // chroma rows per work item
 constexpr int LW = 76, LH = 44;  // luma window: columns -6 .. 69, rows -6 .. nr + 5 (nr <= 32)
 constexpr int CW2 = 68, CH2 = 20;  // chroma windows: columns -2 .. 65, rows -2 .. 17
-constexpr int RAW_BYTES = 17152;   // one staging slot (largest item: 10-bit chroma with its CfL luma)
-// Raw-row layout of a slot when rows arrive as 8-row tensor boxes: the
-// item's run of consecutive in-place rows starts at raw row RUN_L (luma) /
-// RUN_C (chroma) / RUN_CFL (CfL luma rows), the rows before it hold the
-// distinct deblocked / saved rows; every raw row used sits 128-byte aligned
-// in groups of 8 (a box's destination) and a box's overrun rows land after
-// the run, unused.
-constexpr int BOXR = 8, RUN_L = 8, RUN_C = 4, RUN_CFL = 4, CRAW = 28;
+constexpr int RAW_BYTES = 14720;   // one staging slot (largest item: 10-bit chroma with its CfL luma)
 
 // Raw staging rows start 16 bytes left of the unit origin (every copy is
 // 16-byte aligned) and hold the unit's 64 samples plus 16 bytes on each
@@ -74,15 +60,9 @@ struct RawGeom {
     static constexpr int XO = 16 / (int)sizeof(P);                // margin in samples
     static constexpr int RB = (64 + 2 * XO) * (int)sizeof(P);    // bytes per raw row
     static constexpr int LRB = (128 + 2 * XO) * (int)sizeof(P);  // bytes per raw CfL luma row
-    static constexpr int LOFF = CRAW * RB;                        // offset of the CfL luma rows
-    static constexpr int BW = 64 + 2 * XO;                        // window row width in samples
-    static constexpr int LBW = 128 + 2 * XO;                      // CfL luma row width in samples
+    static constexpr int LOFF = CH2 * RB;                         // offset of the CfL luma rows
 };
-static_assert((RUN_L + 48) * RawGeom<uint16_t>::RB <= RAW_BYTES, "luma window slot");
-static_assert(RUN_C + 24 <= CRAW, "chroma rows");
-static_assert(RawGeom<uint16_t>::LOFF + (RUN_CFL + 40) * RawGeom<uint16_t>::LRB <= RAW_BYTES, "CfL rows");
-static_assert(RAW_BYTES % 128 == 0 && RawGeom<uint16_t>::LOFF % 128 == 0 && RawGeom<uint8_t>::LOFF % 128 == 0,
-              "128-byte aligned boxes");
+static_assert(LH * RawGeom<uint16_t>::RB <= RAW_BYTES, "luma window slot");
 static_assert(RawGeom<uint16_t>::LOFF + 2 * CH2 * RawGeom<uint16_t>::LRB <= RAW_BYTES, "chroma slot");
 static_assert(RawGeom<uint8_t>::LOFF + 2 * CH2 * RawGeom<uint8_t>::LRB <= RAW_BYTES, "chroma slot");
 
@@ -258,15 +238,12 @@ struct LrDesc {
     int8_t f[20];         // single-class NS-Wiener taps (the unit's or the frame's)
     uint16_t llm[18];     // lossless 4x4 bits per 4 rows of the stripe
     uint16_t noskip[18];  // no-skip 4x4 bits per 4 rows of the stripe (multi-class)
-    uint8_t rmap[48];     // raw row of each window row (output row of an unfiltered unit)
-    uint8_t cmap[40];     // raw CfL row of each CfL luma row
-    int xoff;             // bytes from a raw row's start to the unit origin of an unfiltered unit
 };
 
 struct LrSmem {
     uint64_t full[2], empty[2];
     LrDesc desc[2];
-    alignas(128) unsigned char raw[2][RAW_BYTES];
+    alignas(16) unsigned char raw[2][RAW_BYTES];
     union {
         // luma: every window position holds its sample and the right
         // neighbour as a 16x2 pair (low half = the sample), so a pixel pair
@@ -452,170 +429,11 @@ R2G_D uint32_t item_copies(const DevFrame &f, const UnitGeom &g, int plane, int 
     return total;
 }
 
-// Tensor maps of the frame's in-place planes (C) for the per-frame kernel:
-// luma window rows (64 + 2 XO samples wide), chroma window rows, CfL luma
-// rows (128 + 2 XO); all boxes 8 rows high.
-struct LrMaps {
-    CUtensorMap y, c[2], ycfl;
-};
-
-// The raw rows of one item with 8-row tensor boxes for its run of
-// consecutive in-place rows and a single-row bulk copy per distinct
-// deblocked row; replicated rows are not copied but mapped (d.rmap /
-// d.cmap) onto the row they repeat.  With issue = false it fills the maps
-// and returns this lane's share of the bytes the slot's barrier expects;
-// with issue = true it issues the copies.  Warp-uniform.
-template <typename P>
-R2G_D uint32_t item_copies_tma(const DevFrame &f, const LrMaps &mp, const UnitGeom &g, int plane, int ro, int nr,
-                               int kind, bool copy, LrDesc &d, unsigned char *raw, uint64_t *bar, int lane,
-                               bool issue) {
-    typedef RawGeom<P> RG;
-    constexpr int bps = (int)sizeof(P);
-    const int64_t stride = f.stride[plane != 0];
-    const char *Dp = (const char *)f.D[plane];
-    uint32_t total = 0;
-    const int halo = plane ? 2 : 6;
-    const int wrows = copy ? nr : nr + 2 * halo;
-    int run_lo = 0, run_hi = nr, A = 0;
-    if (!copy) {
-        run_lo = imax_(0, halo - ro);
-        run_hi = (g.edges & LR_HAVE_BOTTOM_INTEGRATED) ? wrows : imin_(wrows, halo - ro + g.sh);
-        A = plane ? RUN_C : RUN_L;
-    }
-    const int ybase = g.y0 + ro - (copy ? 0 : halo);  // in-place source row of window row 0
-    const int nbox = (run_hi - run_lo + BOXR - 1) / BOXR;
-    if (lane < nbox) {
-        if (issue)
-            tma_load_2d(raw + (A + BOXR * lane) * RG::RB, plane ? (const void *)&mp.c[plane - 1] : (const void *)&mp.y,
-                        g.x0 - RG::XO, ybase + run_lo + BOXR * lane, bar);
-        else
-            total += (uint32_t)(RG::BW * bps * BOXR);
-    }
-    if (!issue)
-        for (int r = run_lo + lane; r < run_hi; r += 32) d.rmap[r] = (uint8_t)(A + r - run_lo);
-    if (!copy) {
-        // window columns [x0 - XO, x0 + 64 + XO) of a deblocked row, clipped
-        int cs = g.x0 - RG::XO, doff = 0;
-        if (cs < 0) {
-            doff = -cs * bps;
-            cs = 0;
-        }
-        const int ce = imin_(g.x0 + 64 + RG::XO, (int)stride);
-        const uint32_t bytes = (uint32_t)((ce - cs) * bps);
-        const int nother = run_lo + (wrows - run_hi);
-        const bool mine = lane < nother;
-        int row = 0, r = 0;
-        bool from_d = false;
-        if (mine) {
-            r = lane < run_lo ? lane : run_hi + (lane - run_lo);
-            row_src(g, ro + r - halo, row, from_d);
-        }
-        const bool dm = mine && from_d;
-        const unsigned peers = __match_any_sync(0xffffffffu, dm ? row : -1 - lane);
-        const int leader = __ffs(peers) - 1;
-        const unsigned leads = __ballot_sync(0xffffffffu, dm && leader == lane);
-        const int slot = __popc(leads & ((1u << leader) - 1));
-        if (mine) {
-            if (from_d) {
-                if (!issue) d.rmap[r] = (uint8_t)imin_(slot, A - 1);
-                if (lane == leader) {
-                    if (issue)
-                        bulk_g2s(raw + slot * RG::RB + doff, Dp + ((int64_t)row * stride + cs) * bps, bytes, bar);
-                    else
-                        total += bytes;
-                }
-            } else if (!issue) {
-                // a row of the run, repeated (kept inside the slot's rows)
-                d.rmap[r] = (uint8_t)iclip_(A + (row - ybase) - run_lo, A, (plane ? CRAW : RUN_L + 48) - 1);
-            }
-        }
-    }
-    if (plane && kind == W_NS_SINGLE) {
-        // CfL luma rows (backup_row_luma with ns_wiener_single_uv's row
-        // selection, looprestoration.rs:1207-1350): two luma rows per window
-        // row; luma row q of the item is 2 * (y0 + ro - 2) + q in place
-        const int64_t ls = f.stride[0];
-        const char *Dy = (const char *)f.D[0];
-        const bool topi = g.edges & LR_HAVE_TOP_INTEGRATED, boti = g.edges & LR_HAVE_BOTTOM_INTEGRATED;
-        const int nq = 2 * wrows;
-        const int q_lo = topi ? 0 : imax_(0, 2 * (2 - ro));
-        const int q_hi = boti ? nq : imin_(nq, 2 * (2 - ro + g.sh));
-        const int lbase = 2 * (g.y0 + ro - 2);
-        const int nboxl = (q_hi - q_lo + BOXR - 1) / BOXR;
-        if (lane < nboxl) {
-            if (issue)
-                tma_load_2d(raw + RG::LOFF + (RUN_CFL + BOXR * lane) * RG::LRB, &mp.ycfl, 2 * g.x0 - RG::XO,
-                            lbase + q_lo + BOXR * lane, bar);
-            else
-                total += (uint32_t)(RG::LBW * bps * BOXR);
-        }
-        if (!issue)
-            for (int q = q_lo + lane; q < q_hi; q += 32) d.cmap[q] = (uint8_t)(RUN_CFL + q - q_lo);
-        int lcs = 2 * g.x0 - RG::XO, ldoff = 0;
-        if (lcs < 0) {
-            ldoff = -lcs * bps;
-            lcs = 0;
-        }
-        const int lce = imin_(2 * g.x0 + 128 + RG::XO, (int)ls);
-        const uint32_t lbytes = (uint32_t)((lce - lcs) * bps);
-        const int nother = q_lo + (nq - q_hi);
-        const bool mine = lane < nother;
-        int q = 0, lrow = 0;
-        bool from_d = false;
-        if (mine) {
-            q = lane < q_lo ? lane : q_hi + (lane - q_lo);
-            int rr = ro + (q >> 1) - 2;
-            if (!(g.edges & LR_HAVE_TOP) && rr < 0) rr = 0;
-            if (!(g.edges & LR_HAVE_BOTTOM) && !boti && rr >= g.sh) rr = g.sh - 1;
-            int ra, rb;
-            from_d = true;
-            if (rr == -2) {
-                ra = rb = 2 * g.y0 - 2;
-            } else if (rr == -1) {
-                ra = 2 * g.y0 - 2;
-                rb = 2 * g.y0 - 1;
-            } else if (rr == g.sh) {
-                ra = 2 * (g.y0 + g.sh);
-                rb = ra + 1;
-            } else if (rr == g.sh + 1) {
-                ra = rb = 2 * (g.y0 + g.sh) + 1;
-            } else {
-                from_d = false;
-                ra = 2 * (g.y0 + rr);
-                rb = ra + 1;
-            }
-            lrow = (q & 1) ? rb : ra;
-        }
-        const bool dm = mine && from_d;
-        const unsigned peers = __match_any_sync(0xffffffffu, dm ? lrow : -1 - lane);
-        const int leader = __ffs(peers) - 1;
-        const unsigned leads = __ballot_sync(0xffffffffu, dm && leader == lane);
-        const int slot = __popc(leads & ((1u << leader) - 1));
-        if (mine) {
-            if (from_d) {
-                if (!issue) d.cmap[q] = (uint8_t)imin_(slot, RUN_CFL - 1);
-                if (lane == leader) {
-                    if (issue)
-                        bulk_g2s(raw + RG::LOFF + slot * RG::LRB + ldoff, Dy + ((int64_t)lrow * ls + lcs) * bps, lbytes,
-                                 bar);
-                    else
-                        total += lbytes;
-                }
-            } else if (!issue) {
-                // an in-place row of the run, repeated (kept inside the slot's rows)
-                d.cmap[q] = (uint8_t)iclip_(RUN_CFL + (lrow - lbase) - q_lo, RUN_CFL, RUN_CFL + 39);
-            }
-        }
-    }
-    return total;
-}
-
 // Produces one work item into slot k & 1, after waiting for the slot's
 // release when it was used before.  Returns 0 for an empty item (nothing
 // published), 1 when published, -1 when a wait ran out.
 template <typename P>
-R2G_D int produce_item(const DevFrame &f, const LrMaps *mp, int fi, int b, LrSmem &sm, int k, int lane,
-                       bool &waited) {
+R2G_D int produce_item(const DevFrame &f, int fi, int b, LrSmem &sm, int k, int lane, bool &waited) {
     UnitGeom g;
     int ro, nr;
     if (!item_geom(f, b, g, ro, nr)) return 0;
@@ -722,28 +540,16 @@ R2G_D int produce_item(const DevFrame &f, const LrMaps *mp, int fi, int b, LrSme
         d.noskip[lane] = nsk;
         d.f[lane] = (int8_t)tap;
     }
-    // row maps and the bytes the slot's barrier expects
-    uint32_t mine;
-    if (mp) {
-        mine = item_copies_tma<P>(f, *mp, g, plane, ro, nr, wkind, copy, d, sm.raw[s], &sm.full[s], lane, false);
-        if (lane == 0) d.xoff = copy ? RawGeom<P>::XO * (int)sizeof(P) : 0;
-    } else {
-        for (int r = lane; r < 48; r += 32) d.rmap[r] = (uint8_t)r;
-        if (lane < 40) d.cmap[lane] = (uint8_t)lane;
-        if (lane == 0) d.xoff = 0;
-        mine = item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane, false);
-    }
-    const uint32_t total = __reduce_add_sync(0xffffffffu, mine);
+    const uint32_t total =
+        __reduce_add_sync(0xffffffffu, item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane,
+                                                      false));
     // the consumers' reads of this slot (ordered before by the empty
     // barrier) precede the copies' writes
     fence_proxy_async();
     __syncwarp();
     if (lane == 0) mbar_arrive_expect_tx(&sm.full[s], total);
     __syncwarp();
-    if (mp)
-        item_copies_tma<P>(f, *mp, g, plane, ro, nr, wkind, copy, d, sm.raw[s], &sm.full[s], lane, true);
-    else
-        item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane, true);
+    item_copies<P>(f, g, plane, ro, nr, wkind, copy, sm.raw[s], &sm.full[s], lane, true);
     return 1;
 }
 
@@ -765,8 +571,8 @@ R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
         int fi, b;
         src.item(w, fi, b);
         const DevFrame &f = src.frame(fi);
-        const int rc = is_hbd<HB>(f) ? produce_item<uint16_t>(f, src.maps(), fi, b, sm, k, lane, waited)
-                                     : produce_item<uint8_t>(f, src.maps(), fi, b, sm, k, lane, waited);
+        const int rc = is_hbd<HB>(f) ? produce_item<uint16_t>(f, fi, b, sm, k, lane, waited)
+                                     : produce_item<uint8_t>(f, fi, b, sm, k, lane, waited);
         if (rc < 0) {
             ok = false;
             break;
@@ -879,8 +685,7 @@ R2G_D int raw_at(const unsigned char *row, int x) {
 // Raw rows -> luma pair window (window column c holds source column c - 6),
 // replicating the frame's left / right edge samples.
 template <typename P>
-R2G_D void build_luma_window(LrSmem &sm, const unsigned char *raw, const uint8_t *rmap, int nr, int uw, int edges,
-                             int tid) {
+R2G_D void build_luma_window(LrSmem &sm, const unsigned char *raw, int nr, int uw, int edges, int tid) {
     typedef RawGeom<P> RG;
     const int wh = nr + 12;
     if ((edges & LR_HAVE_LEFT) && (edges & LR_HAVE_RIGHT)) {
@@ -888,7 +693,7 @@ R2G_D void build_luma_window(LrSmem &sm, const unsigned char *raw, const uint8_t
         // step, from raw samples 4q + 2 .. 4q + 6 (u16) / 4q + 10 .. 4q + 14 (u8)
         for (int i = tid; i < wh * 19; i += NCT) {
             const int r = i / 19, q = i - r * 19;
-            const unsigned char *row = raw + rmap[r] * RG::RB;
+            const unsigned char *row = raw + r * RG::RB;
             uint4 o;
             if (sizeof(P) == 2) {
                 const uint32_t w0 = *reinterpret_cast<const uint32_t *>(row + 8 * q + 4);
@@ -908,7 +713,7 @@ R2G_D void build_luma_window(LrSmem &sm, const unsigned char *raw, const uint8_t
         const int ww = uw + 12;
         for (int i = tid; i < wh * ww; i += NCT) {
             const int r = i / ww, c = i - r * ww;
-            const unsigned char *row = raw + rmap[r] * RG::RB;
+            const unsigned char *row = raw + r * RG::RB;
             const int a = raw_at<P>(row, col_clamp(c - 6, uw, edges) + RG::XO);
             const int b = raw_at<P>(row, col_clamp(c - 5, uw, edges) + RG::XO);
             sm.u.wp[r * LW + c] = (uint32_t)a | ((uint32_t)b << 16);
@@ -919,13 +724,13 @@ R2G_D void build_luma_window(LrSmem &sm, const unsigned char *raw, const uint8_t
 // Raw rows -> chroma pair window and (CfL) downsampled luma pair window
 // (window column j holds chroma column j - 2).
 template <typename P>
-R2G_D void build_chroma_windows(LrSmem &sm, const unsigned char *raw, const uint8_t *rmap, const uint8_t *cmap, int nr,
-                                int uw, int edges, bool cfl, int ds, int tid) {
+R2G_D void build_chroma_windows(LrSmem &sm, const unsigned char *raw, int nr, int uw, int edges, bool cfl, int ds,
+                                int tid) {
     typedef RawGeom<P> RG;
     const int wh = nr + 4, ww = uw + 4;
     for (int i = tid; i < wh * ww; i += NCT) {
         const int r = i / ww, j = i - r * ww;
-        const unsigned char *row = raw + rmap[r] * RG::RB;
+        const unsigned char *row = raw + r * RG::RB;
         const int a = raw_at<P>(row, col_clamp(j - 2, uw, edges) + RG::XO);
         const int b = raw_at<P>(row, col_clamp(j - 1, uw, edges) + RG::XO);
         sm.u.ch.win[r * CW2 + j] = (uint32_t)a | ((uint32_t)b << 16);
@@ -934,8 +739,8 @@ R2G_D void build_chroma_windows(LrSmem &sm, const unsigned char *raw, const uint
     const int lw = uw << 1;
     for (int i = tid; i < wh * ww; i += NCT) {
         const int r = i / ww, j = i - r * ww;
-        const unsigned char *ra = raw + RG::LOFF + cmap[2 * r] * RG::LRB;
-        const unsigned char *rb = raw + RG::LOFF + cmap[2 * r + 1] * RG::LRB;
+        const unsigned char *ra = raw + RG::LOFF + (2 * r) * RG::LRB;
+        const unsigned char *rb = ra + RG::LRB;
         int l[2];
 #pragma unroll
         for (int t = 0; t < 2; t++) {
@@ -956,8 +761,7 @@ R2G_D void build_chroma_windows(LrSmem &sm, const unsigned char *raw, const uint
 
 // An unfiltered unit: staged rows -> L, 16 bytes per store.
 template <typename P>
-R2G_D void copy_unit(const DevFrame &f, const unsigned char *raw, const uint8_t *rmap, int plane, int x0, int y, int nr,
-                     int uw, int tid) {
+R2G_D void copy_unit(const DevFrame &f, const unsigned char *raw, int plane, int x0, int y, int nr, int uw, int tid) {
     typedef RawGeom<P> RG;
     const int bytes = uw * (int)sizeof(P);
     const int nch = (bytes + 15) >> 4;
@@ -965,7 +769,7 @@ R2G_D void copy_unit(const DevFrame &f, const unsigned char *raw, const uint8_t 
     char *L = (char *)f.L[plane] + (int64_t)y * stride + (int64_t)x0 * sizeof(P);
     for (int i = tid; i < nr * nch; i += NCT) {
         const int r = i / nch, q = i - r * nch;
-        const unsigned char *src = raw + rmap[r] * RG::RB + 16 * q;
+        const unsigned char *src = raw + r * RG::RB + 16 * q;
         char *dst = L + r * stride + 16 * q;
         const int left = bytes - 16 * q;
         if (left >= 16) {
@@ -1258,7 +1062,7 @@ R2G_D void consume_item(const DevFrame &f, LrSmem &sm, int s, int tid) {
     const bool gdf = d.gdf, copy = d.copy;
     const unsigned char *raw = sm.raw[s];
     if (copy) {
-        copy_unit<P>(f, raw + d.xoff, d.rmap, plane, x0, y0 + ro, nr, uw, tid);
+        copy_unit<P>(f, raw, plane, x0, y0 + ro, nr, uw, tid);
         __syncwarp();
         if ((tid & 31) == 0) mbar_arrive(&sm.empty[s]);
         return;
@@ -1270,10 +1074,9 @@ R2G_D void consume_item(const DevFrame &f, LrSmem &sm, int s, int tid) {
         sm.f[tid] = d.f[tid];
     }
     if (plane == 0)
-        build_luma_window<P>(sm, raw, d.rmap, nr, uw, edges, tid);
+        build_luma_window<P>(sm, raw, nr, uw, edges, tid);
     else
-        build_chroma_windows<P>(sm, raw, d.rmap, d.cmap, nr, uw, edges, kind == W_NS_SINGLE, f.fp.cfl_ds_filter_index,
-                                tid);
+        build_chroma_windows<P>(sm, raw, nr, uw, edges, kind == W_NS_SINGLE, f.fp.cfl_ds_filter_index, tid);
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(&sm.empty[s]);
     bar_sync_n(NCT);
@@ -1340,8 +1143,6 @@ R2G_D void lr_run(const Src &src, LrSmem &sm) {
 struct FrameSrc {
     const DevFrame *f;
     int n;
-    const LrMaps *m;
-    R2G_D const LrMaps *maps() const { return m; }
     R2G_D int count() const { return n; }
     R2G_D const DevFrame &frame(int) const { return *f; }
     R2G_D void item(int w, int &fi, int &b) const {
@@ -1364,7 +1165,6 @@ struct FrameSrc {
 };
 struct BatchSrc {
     const BatchArgs *a;
-    R2G_D const LrMaps *maps() const { return nullptr; }
     R2G_D int count() const { return a->count[2]; }
     R2G_D const DevFrame &frame(int fi) const { return a->frames[fi]; }
     R2G_D void item(int w, int &fi, int &b) const {
@@ -1378,12 +1178,11 @@ struct BatchSrc {
 };
 
 template <typename P>
-__global__ void __launch_bounds__(LR_NT, 3) lr_kernel(const __grid_constant__ DevFrame f, int n,
-                                                      const __grid_constant__ LrMaps maps, int tma) {
+__global__ void __launch_bounds__(LR_NT, 3) lr_kernel(const __grid_constant__ DevFrame f, int n) {
     pdl_trigger();
     extern __shared__ __align__(128) unsigned char lr_smem[];
     LrSmem &sm = *reinterpret_cast<LrSmem *>(lr_smem);
-    FrameSrc src{&f, n, tma ? &maps : nullptr};
+    FrameSrc src{&f, n};
     lr_run<sizeof(P) == 2 ? 1 : 0>(src, sm);
 }
 
@@ -1631,81 +1430,6 @@ int r2g_lr_items(const DevFrame &f) {
     return nslots * (64 / f.lr_rows) * ((f.w + 63) >> 6) + 2 * nslots * 2 * ((f.cw + 63) >> 6);
 }
 
-// ---- tensor maps of the in-place planes (host) ----
-namespace {
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-        cudaGetLastError();
-    });
-    return fn;
-}
-// A plane of `rows` rows of `w` samples, `stride` bytes apart, in boxes of
-// box_w x 8 samples (reads outside the plane fill zeros).
-bool encode_plane(CUtensorMap *m, const void *base, int bps, int64_t w, int64_t rows, int64_t stride, int box_w) {
-    EncodeTiledFn fn = encode_fn();
-    if (!fn || !base || (reinterpret_cast<uintptr_t>(base) & 15) || (stride & 15)) return false;
-    const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)rows}, strides[1] = {(cuuint64_t)stride};
-    const cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)BOXR}, es[2] = {1, 1};
-    return fn(m, bps == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
-              const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-// The frame's maps, cached by plane addresses and geometry.
-struct MapEntry {
-    const void *c[3];
-    int64_t stride0, stride1;
-    int h, bd;
-    LrMaps maps;
-    uint64_t used;
-};
-std::mutex g_map_mu;
-MapEntry g_maps[32];
-uint64_t g_map_clock = 0;
-bool lr_maps(const DevFrame &f, LrMaps &out) {
-    std::lock_guard<std::mutex> lk(g_map_mu);
-    MapEntry *lru = &g_maps[0];
-    for (MapEntry &e : g_maps) {
-        if (e.used && e.c[0] == f.C[0] && e.c[1] == f.C[1] && e.c[2] == f.C[2] && e.stride0 == f.stride[0] &&
-            e.stride1 == f.stride[1] && e.h == f.h && e.bd == f.bitdepth) {
-            e.used = ++g_map_clock;
-            out = e.maps;
-            return true;
-        }
-        if (e.used < lru->used) lru = &e;
-    }
-    const int bps = f.bitdepth > 8 ? 2 : 1, xo = 16 / bps;
-    const int64_t rows = (f.h + 127) & ~127;  // the frame allocator's rows (r2g_plane_geometry)
-    LrMaps m;
-    if (!encode_plane(&m.y, f.C[0], bps, f.stride[0], rows, f.stride[0] * bps, 64 + 2 * xo) ||
-        !encode_plane(&m.c[0], f.C[1], bps, f.stride[1], rows / 2, f.stride[1] * bps, 64 + 2 * xo) ||
-        !encode_plane(&m.c[1], f.C[2], bps, f.stride[1], rows / 2, f.stride[1] * bps, 64 + 2 * xo) ||
-        !encode_plane(&m.ycfl, f.C[0], bps, f.stride[0], rows, f.stride[0] * bps, 128 + 2 * xo))
-        return false;
-    lru->c[0] = f.C[0];
-    lru->c[1] = f.C[1];
-    lru->c[2] = f.C[2];
-    lru->stride0 = f.stride[0];
-    lru->stride1 = f.stride[1];
-    lru->h = f.h;
-    lru->bd = f.bitdepth;
-    lru->maps = m;
-    lru->used = ++g_map_clock;
-    out = m;
-    return true;
-}
-}  // namespace
-
 int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     if (!f.lr_on) return 0;
     const LrLaunchInfo &li = lr_info();
@@ -1713,19 +1437,10 @@ int r2g_launch_lr(const DevFrame &f, cudaStream_t s) {
     const int hbd = f.bitdepth > 8;
     int grid = li.sms * li.occ[hbd];
     if (grid > n) grid = n;
-    // in-place rows by tensor boxes when the maps can be made (R2G_LR_TMA=0:
-    // one bulk copy per row)
-    static const bool tma_on = [] {
-        const char *e = getenv("R2G_LR_TMA");
-        return !(e && e[0] == '0');
-    }();
-    LrMaps maps;
-    memset(&maps, 0, sizeof(maps));
-    const int tma = tma_on && lr_maps(f, maps);
     if (hbd)
-        r2g_launch_pdl_smem(lr_kernel<uint16_t>, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, f, n, maps, tma);
+        r2g_launch_pdl_smem(lr_kernel<uint16_t>, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, f, n);
     else
-        r2g_launch_pdl_smem(lr_kernel<uint8_t>, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, f, n, maps, tma);
+        r2g_launch_pdl_smem(lr_kernel<uint8_t>, dim3(grid), dim3(LR_NT), sizeof(LrSmem), s, f, n);
     return 1;
 }
 

@@ -258,16 +258,6 @@ R2G_D void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
 }
 // orders this thread's earlier shared-memory accesses before its later
 // asynchronous-proxy (bulk copy) accesses
-// 2-D tensor-map load of one box into shared memory (128-byte aligned)
-// completing on `bar`; the map lives in kernel-parameter memory; never
-// multicast
-R2G_D void tma_load_2d(void *dst, const void *map, int x, int y, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-        "[%4];\n" ::"r"(smem_addr(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
-        : "memory");
-}
 R2G_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 // barrier among the first `n` threads (the consumer warps) on named barrier
 // 1; returns whether `pred` was true in any of them
