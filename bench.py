@@ -49,9 +49,9 @@ BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film
 # bytes read + written per launch (the outputs were still in L2 when the
 # capture ended, so the write term was 0) and warp instructions per launch.
 NCU_CAPTURE = {
-    "commit": "ae38c6c",
-    "traffic": {"deblock": 6618112, "cdef_ccso": 6295808, "loop_restoration": 6849280},
-    "warp_inst": {"deblock": 9712384, "cdef_ccso": 26207300, "loop_restoration": 27162128},
+    "commit": "bf7f127",
+    "traffic": {"deblock": 6657792, "cdef_ccso": 6297088, "loop_restoration": 6851584},
+    "warp_inst": {"deblock": 11917547, "cdef_ccso": 26460317, "loop_restoration": 27333859},
 }
 SMS = 148
 
