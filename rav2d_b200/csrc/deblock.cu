@@ -211,6 +211,7 @@ struct Vec4<uint16_t> {
 };
 
 // Shared-memory tile geometry.
+constexpr int DB_NT = 256;  // threads per tile CTA
 constexpr int LT = 88;   // luma staged span: tile origin - 12 .. + 76
 constexpr int LO = 12;   // luma halo
 constexpr int LP = 90;   // luma row pitch (int16)
@@ -632,7 +633,7 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
 }
 
 template <typename P>
-__global__ void __launch_bounds__(256, 4) deblock_tile_kernel(const DevFrame f) {
+__global__ void __launch_bounds__(DB_NT, 4) deblock_tile_kernel(const DevFrame f) {
     pdl_trigger();
     __shared__ DeblockSmem sm;
     deblock_tile<P>(f, sm, blockIdx.x, blockIdx.y);
@@ -640,7 +641,7 @@ __global__ void __launch_bounds__(256, 4) deblock_tile_kernel(const DevFrame f) 
 
 // Persistent kernel over a cross-frame work list: item = frame << 22 | ty *
 // tiles_w + tx.
-__global__ void __launch_bounds__(256, 4) deblock_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(DB_NT, 4) deblock_batch_kernel(BatchArgs a) {
     pdl_trigger();
     __shared__ DeblockSmem sm;
     const int n = a.count[0];
@@ -659,11 +660,11 @@ __global__ void __launch_bounds__(256, 4) deblock_batch_kernel(BatchArgs a) {
 }  // namespace
 
 void r2g_batch_launch_deblock(const BatchArgs &a, int grid, cudaStream_t s) {
-    r2g_launch_pdl(deblock_batch_kernel, dim3(grid), dim3(256), s, a);
+    r2g_launch_pdl(deblock_batch_kernel, dim3(grid), dim3(DB_NT), s, a);
 }
 int r2g_batch_occupancy_deblock() {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, deblock_batch_kernel, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, deblock_batch_kernel, DB_NT, 0);
     return nb;
 }
 int r2g_deblock_items(const DevFrame &f) { return f.deblock_on ? ((f.w + 63) >> 6) * ((f.h + 63) >> 6) : 0; }
@@ -672,9 +673,9 @@ int r2g_launch_deblock(const DevFrame &f, cudaStream_t s) {
     if (!f.deblock_on) return 0;
     dim3 grid((f.w + 63) / 64, (f.h + 63) / 64);
     if (f.bitdepth > 8)
-        r2g_launch_pdl(deblock_tile_kernel<uint16_t>, grid, dim3(256), s, f);
+        r2g_launch_pdl(deblock_tile_kernel<uint16_t>, grid, dim3(DB_NT), s, f);
     else
-        r2g_launch_pdl(deblock_tile_kernel<uint8_t>, grid, dim3(256), s, f);
+        r2g_launch_pdl(deblock_tile_kernel<uint8_t>, grid, dim3(DB_NT), s, f);
     return 1;
 }
 
