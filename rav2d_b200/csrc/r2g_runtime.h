@@ -43,7 +43,11 @@ struct R2gCtx {
     // up_stream, downloads on down_stream, ordered by per-frame events
     bool overlap = false;
     cudaStream_t up_stream = nullptr, down_stream = nullptr;
-    cudaEvent_t fence_ev[2] = {nullptr, nullptr};
+    // side-info staging of r2g_frame_stage: its own stream, so its small
+    // copies (each bound by PCIe latency while downloads run) overlap the
+    // recon upload instead of queueing behind it
+    cudaStream_t side_up_stream = nullptr;
+    cudaEvent_t fence_ev[3] = {nullptr, nullptr, nullptr};
     int64_t launches = 0;
     bool profiling = false;
     std::vector<ProfRun> prof;
@@ -84,8 +88,8 @@ struct R2gFrame {
     size_t pack_bytes = 0;
     // copy-overlap ordering: last upload / staging (up stream), last kernels
     // (context stream), last download (down stream) of this frame
-    cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_down = nullptr;
-    bool pend_up = false, pend_comp = false, pend_down = false;
+    cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_down = nullptr, ev_side = nullptr;
+    bool pend_up = false, pend_comp = false, pend_down = false, pend_side = false;
     // device-built deblock masks (R2gSideInfo.db_masks): block records and
     // level maps on the device, a pinned staging copy of the records, and
     // the events that fork the build onto the side stream and join it back

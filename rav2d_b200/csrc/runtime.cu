@@ -129,7 +129,7 @@ extern "C" int r2g_ctx_destroy(R2gCtx *ctx) {
     r2g_grain_ctx_free(ctx);
     r2g_batch_free(ctx);
     r2g_ctx_profile(ctx, 0);
-    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
+    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream, ctx->side_up_stream})
         if (st) {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
@@ -223,9 +223,9 @@ extern "C" int r2g_frame_free(R2gCtx *ctx, R2gFrame *f) {
     if (!ctx || !f) return R2G_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
+    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream, ctx->side_up_stream})
         if (st) cudaStreamSynchronize(st);
-    for (cudaEvent_t e : {f->ev_up, f->ev_comp, f->ev_down})
+    for (cudaEvent_t e : {f->ev_up, f->ev_comp, f->ev_down, f->ev_side})
         if (e) cudaEventDestroy(e);
     for (int i = 0; i < 5; i++) r2g_dev_free(ctx, f->buf[i], f->buf_bytes);
     r2g_dev_free(ctx, f->side_dev, f->side_bytes);
@@ -266,17 +266,24 @@ int r2g_copy_planes(R2gCtx *ctx, const R2gFrame *f, int buf, const void *y, int6
             set_err(ctx, "host stride smaller than the plane width");
             return R2G_E_INVALID;
         }
-        if (upload)
+        if (hstride == wbytes && dstride == wbytes) {
+            // rows back to back on both sides: one linear copy
+            if (upload)
+                CK(cudaMemcpyAsync(p[i], hs[i], (size_t)(wbytes * rows), cudaMemcpyHostToDevice, st));
+            else
+                CK(cudaMemcpyAsync((void *)hs[i], p[i], (size_t)(wbytes * rows), cudaMemcpyDeviceToHost, st));
+        } else if (upload) {
             CK(cudaMemcpy2DAsync(p[i], dstride, hs[i], hstride, wbytes, rows, cudaMemcpyHostToDevice, st));
-        else
+        } else {
             CK(cudaMemcpy2DAsync((void *)hs[i], hstride, p[i], dstride, wbytes, rows, cudaMemcpyDeviceToHost, st));
+        }
     }
     return R2G_OK;
 }
 
 // ---- copy overlap: per-frame ordering across the three streams
 static int ensure_events(R2gCtx *ctx, R2gFrame *f) {
-    for (cudaEvent_t *e : {&f->ev_up, &f->ev_comp, &f->ev_down})
+    for (cudaEvent_t *e : {&f->ev_up, &f->ev_comp, &f->ev_down, &f->ev_side})
         if (!*e) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return R2G_OK;
 }
@@ -307,6 +314,7 @@ int r2g_frame_before_compute(R2gCtx *ctx, R2gFrame *f) {
     // the kernels read this frame's uploads and overwrite planes a pending
     // download may still read
     if (f->pend_up) CK(cudaStreamWaitEvent(ctx->stream, f->ev_up, 0));
+    if (f->pend_side) CK(cudaStreamWaitEvent(ctx->stream, f->ev_side, 0));
     if (f->pend_down) CK(cudaStreamWaitEvent(ctx->stream, f->ev_down, 0));
     return R2G_OK;
 }
@@ -326,6 +334,7 @@ extern "C" int r2g_ctx_overlap_copies(R2gCtx *ctx, int enable) {
     if (enable && !ctx->up_stream) {
         CK(cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&ctx->down_stream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&ctx->side_up_stream, cudaStreamNonBlocking));
         for (cudaEvent_t &e : ctx->fence_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     if (!enable && ctx->up_stream) {
@@ -344,8 +353,8 @@ extern "C" int r2g_ctx_fence(R2gCtx *ctx) {
     CK(cudaSetDevice(ctx->device));
     CK(cudaEventRecord(ctx->fence_ev[0], ctx->up_stream));
     CK(cudaEventRecord(ctx->fence_ev[1], ctx->down_stream));
-    CK(cudaStreamWaitEvent(ctx->stream, ctx->fence_ev[0], 0));
-    CK(cudaStreamWaitEvent(ctx->stream, ctx->fence_ev[1], 0));
+    CK(cudaEventRecord(ctx->fence_ev[2], ctx->side_up_stream));
+    for (cudaEvent_t e : ctx->fence_ev) CK(cudaStreamWaitEvent(ctx->stream, e, 0));
     return R2G_OK;
 }
 
@@ -809,16 +818,25 @@ extern "C" int r2g_frame_stage(R2gCtx *ctx, R2gFrame *f, const R2gFrameParams *f
                                uint32_t inloop_mask) {
     if (!ctx || !f) return R2G_E_INVALID;
     CK(cudaSetDevice(ctx->device));
-    cudaStream_t st;
-    int rc = upload_stream(ctx, f, &st);
-    if (rc == R2G_OK) {
-        ctx->defer_mask_join = true;
-        rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, st);
-        ctx->defer_mask_join = false;
+    cudaStream_t st = ctx->stream;
+    if (ctx->overlap) {
+        // the side-info copies go on their own stream (the kernels of this
+        // frame's previous run may still read what they overwrite)
+        int rc = ensure_events(ctx, f);
+        if (rc != R2G_OK) return rc;
+        if (f->pend_comp) CK(cudaStreamWaitEvent(ctx->side_up_stream, f->ev_comp, 0));
+        st = ctx->side_up_stream;
     }
+    ctx->defer_mask_join = true;
+    int rc = r2g_prepare(ctx, f, fp, side, inloop_mask, f->desc, st);
+    ctx->defer_mask_join = false;
     if (rc != R2G_OK) return rc;
     f->staged = true;
-    return upload_done(ctx, f);
+    if (ctx->overlap) {
+        CK(cudaEventRecord(f->ev_side, ctx->side_up_stream));
+        f->pend_side = true;
+    }
+    return R2G_OK;
 }
 
 extern "C" int r2g_frame_run(R2gCtx *ctx, R2gFrame *f) {
