@@ -289,27 +289,22 @@ R2G_D void stage_side(const DevFrame &f, DbSide &sd, int tx, int ty, int tid, in
     const bool segs = f.segmap != nullptr, segsc = f.segmap_uv != nullptr;
     const int total = NV + NH + NVCW + NHCW + NLY + NLC + NQ + (segs ? NSY : 0) + (segsc ? NSC : 0);
     __shared__ uint16_t q64[9];
-    // item i -> its source word (NULL: 0) and destination in shared memory
-    auto item = [&](int i, const void *&src, void *&dst, bool &byte) {
+    for (int i = tid; i < total; i += nt) {
         int j = i;
-        src = nullptr;
-        byte = false;
         if (j < NV) {
             const int c = j / 15, s = (j / 5) % 3, k = j % 5;
             const int x4 = X0 - 1 + c, g = gy0 + s;
             const R2gAv2Filter *m = (x4 >= 0 && x4 < bw4 && g >= 0 && 16 * g < bh4) ? mask_at(g >> 2, x4 >> 6) : nullptr;
-            if (m) src = &m->filter_y[0][x4 & 63][k][g & 3];
-            dst = &sd.vy[c][s][k];
-            return;
+            sd.vy[c][s][k] = m ? m->filter_y[0][x4 & 63][k][g & 3] : 0;
+            continue;
         }
         j -= NV;
         if (j < NH) {
             const int r = j / 5, k = j % 5;
             const int y4 = Y0 - 1 + r;
             const R2gAv2Filter *m = (y4 >= 0 && y4 < bh4 && X0 < bw4) ? mask_at(y4 >> 6, X0 >> 6) : nullptr;
-            if (m) src = &m->filter_y[1][y4 & 63][k][(X0 >> 4) & 3];
-            dst = &sd.hy[r][k];
-            return;
+            sd.hy[r][k] = m ? m->filter_y[1][y4 & 63][k][(X0 >> 4) & 3] : 0;
+            continue;
         }
         j -= NH;
         if (j < NVCW) {
@@ -317,83 +312,52 @@ R2G_D void stage_side(const DevFrame &f, DbSide &sd, int tx, int ty, int tid, in
             const int cx4 = CX0 + c, g = gc0 + s;
             const R2gAv2Filter *m =
                 (cx4 < cbw4 && g >= 0 && 16 * g < cbh4) ? mask_at(g >> 1, cx4 >> 5) : nullptr;
-            if (m) src = &m->filter_uv[0][cx4 & 31][k][g & 1];
-            dst = &sd.vc[c][s][k];
-            return;
+            sd.vc[c][s][k] = m ? m->filter_uv[0][cx4 & 31][k][g & 1] : 0;
+            continue;
         }
         j -= NVCW;
         if (j < NHCW) {
             const int r = j / 5, k = j % 5;
             const int cy4 = CY0 + r;
             const R2gAv2Filter *m = (cy4 < cbh4 && CX0 < cbw4) ? mask_at(cy4 >> 5, CX0 >> 5) : nullptr;
-            if (m) src = &m->filter_uv[1][cy4 & 31][k][(CX0 & 31) >> 4];
-            dst = &sd.hc[r][k];
-            return;
+            sd.hc[r][k] = m ? m->filter_uv[1][cy4 & 31][k][(CX0 & 31) >> 4] : 0;
+            continue;
         }
         j -= NHCW;
         if (j < NLY) {
             const int r = j / 3, g = X0 / 16 - 1 + j % 3, y4 = Y0 - 4 + r;
             const R2gAv2Filter *m = (y4 >= 0 && y4 < bh4 && g >= 0 && 16 * g < bw4) ? mask_at(y4 >> 6, g >> 2) : nullptr;
-            if (m) src = &m->lossless_mask_y[y4 & 63][g & 3];
-            dst = &sd.lly[r][j % 3];
-            return;
+            sd.lly[r][j % 3] = m ? m->lossless_mask_y[y4 & 63][g & 3] : 0;
+            continue;
         }
         j -= NLY;
         if (j < NLC) {
             const int r = j / 3, g = tx - 1 + j % 3, cy4 = CY0 - 3 + r;
             const R2gAv2Filter *m =
                 (cy4 >= 0 && cy4 < cbh4 && g >= 0 && 8 * g < cbw4) ? mask_at(cy4 >> 5, g >> 2) : nullptr;
-            if (m) src = &m->lossless_mask_uv[cy4 & 31][g & 3];
-            dst = &sd.llc[r][j % 3];
-            return;
+            sd.llc[r][j % 3] = m ? m->lossless_mask_uv[cy4 & 31][g & 3] : 0;
+            continue;
         }
         j -= NLC;
         if (j < NQ) {
             const int bx = tx - 1 + j % 3, by = ty - 1 + j / 3;
             const R2gAv2Filter *m = (bx >= 0 && by >= 0 && 16 * bx < bw4 && 16 * by < bh4) ? mask_at(by >> 2, bx >> 2)
                                                                                           : nullptr;
-            if (m) src = &m->qidx[(bx & 3) + ((by & 3) << 2)];
-            dst = &q64[j];
-            return;
+            q64[j] = m ? m->qidx[(bx & 3) + ((by & 3) << 2)] : 0;
+            continue;
         }
         j -= NQ;
-        byte = true;
         if (segs && j < NSY) {
             const int r = j / 20, c = j % 20, y4 = Y0 - 4 + r, x4 = X0 - 2 + c;
-            if (x4 >= 0 && y4 >= 0 && x4 < bw4 && y4 < bh4) src = &f.segmap[(int64_t)y4 * f.segmap_stride + x4];
-            dst = &sd.segy[r][c];
-            return;
+            sd.segy[r][c] =
+                (x4 >= 0 && y4 >= 0 && x4 < bw4 && y4 < bh4) ? f.segmap[(int64_t)y4 * f.segmap_stride + x4] : 0;
+            continue;
         }
         if (segs) j -= NSY;
         const int r = j / 10, c = j % 10, cy4 = CY0 - 3 + r, cx4 = CX0 - 1 + c;
-        if (cx4 >= 0 && cy4 >= 0 && cx4 < cbw4 && cy4 < cbh4)
-            src = &f.segmap_uv[(int64_t)cy4 * f.segmap_uv_stride + cx4];
-        dst = &sd.segc[r][c];
-    };
-    // four loads in flight per thread before their stores
-    constexpr int B = 4;
-    for (int base = tid; base < total; base += B * nt) {
-        void *dst[B];
-        uint32_t v[B];
-        bool byte[B];
-#pragma unroll
-        for (int k = 0; k < B; k++) {
-            const int i = base + k * nt;
-            v[k] = 0;
-            dst[k] = nullptr;
-            if (i >= total) continue;
-            const void *src;
-            item(i, src, dst[k], byte[k]);
-            if (src) v[k] = byte[k] ? *static_cast<const uint8_t *>(src) : *static_cast<const uint16_t *>(src);
-        }
-#pragma unroll
-        for (int k = 0; k < B; k++) {
-            if (!dst[k]) continue;
-            if (byte[k])
-                *static_cast<uint8_t *>(dst[k]) = (uint8_t)v[k];
-            else
-                *static_cast<uint16_t *>(dst[k]) = (uint16_t)v[k];
-        }
+        sd.segc[r][c] = (cx4 >= 0 && cy4 >= 0 && cx4 < cbw4 && cy4 < cbh4)
+                            ? f.segmap_uv[(int64_t)cy4 * f.segmap_uv_stride + cx4]
+                            : 0;
     }
     __syncthreads();
     // thresholds of every (kind, block, segment id < 8) the tile can use
@@ -519,56 +483,34 @@ R2G_D void deblock_tile(const DevFrame &f, DeblockSmem &sm, int tx, int ty) {
     const int64_t ys = f.stride[0], uvs = f.stride[1];
     if (tid < 4) sm.n[tid] = 0;
     __syncthreads();  // list counters reset before any thread appends
-    // ---- stage R (samples outside the frame read 0; no valid edge uses them):
-    // runs of 4 samples, eight loads in flight per thread before their stores
-    {
-        typedef typename Vec4<P>::T T;
-        constexpr int NLY = LT * (LT / 4), NST = NLY + 2 * CT * (CT / 4), B = 8;
-        for (int base = tid; base < NST; base += B * nt) {
-            T v[B];
-#pragma unroll
-            for (int k = 0; k < B; k++) {
-                const int i = base + k * nt;
-                int vv[4] = {0, 0, 0, 0};
-                v[k] = Vec4<P>::pack(vv);
-                if (i >= NST) continue;
-                const P *src;
-                int gy, gx, H, W;
-                int64_t st;
-                if (i < NLY) {
-                    const int r = i / (LT / 4), c4 = (i % (LT / 4)) * 4;
-                    gy = lsy + r, gx = lsx + c4, H = f.h, W = f.w, st = ys, src = Ry;
-                } else {
-                    const int j = i - NLY, pl = j / (CT * (CT / 4)), jj = j % (CT * (CT / 4));
-                    const int r = jj / (CT / 4), c4 = (jj % (CT / 4)) * 4;
-                    gy = csy + r, gx = csx + c4, H = f.ch, W = f.cw, st = uvs, src = plane_ptr<const P>(f.R[1 + pl]);
-                }
-                if (gy < 0 || gy >= H) continue;
-                if (gx >= 0 && gx + 3 < W) {
-                    v[k] = __ldg(reinterpret_cast<const T *>(src + gy * st + gx));
-                } else {
-                    for (int q = 0; q < 4; q++)
-                        if (gx + q >= 0 && gx + q < W) vv[q] = src[gy * st + gx + q];
-                    v[k] = Vec4<P>::pack(vv);
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < B; k++) {
-                const int i = base + k * nt;
-                if (i >= NST) continue;
-                int16_t *dst;
-                if (i < NLY) {
-                    dst = &sm.y[(i / (LT / 4)) * LP + (i % (LT / 4)) * 4];
-                } else {
-                    const int j = i - NLY, pl = j / (CT * (CT / 4)), jj = j % (CT * (CT / 4));
-                    dst = &sm.uv[pl][(jj / (CT / 4)) * CP + (jj % (CT / 4)) * 4];
-                }
-                int o[4];
-                Vec4<P>::unpack(v[k], o);
-#pragma unroll
-                for (int q = 0; q < 4; q++) dst[q] = (int16_t)o[q];
-            }
+    // ---- stage R (samples outside the frame read 0; no valid edge uses them)
+    for (int i = tid; i < LT * (LT / 4); i += nt) {
+        int r = i / (LT / 4), c4 = (i % (LT / 4)) * 4;
+        int gy = lsy + r, gx = lsx + c4;
+        int v[4] = {0, 0, 0, 0};
+        if (gy >= 0 && gy < f.h) {
+            if (gx >= 0 && gx + 3 < f.w)
+                Vec4<P>::unpack(*reinterpret_cast<const typename Vec4<P>::T *>(Ry + gy * ys + gx), v);
+            else
+                for (int k = 0; k < 4; k++)
+                    if (gx + k >= 0 && gx + k < f.w) v[k] = Ry[gy * ys + gx + k];
         }
+        for (int k = 0; k < 4; k++) sm.y[r * LP + c4 + k] = (int16_t)v[k];
+    }
+    for (int i = tid; i < 2 * CT * (CT / 4); i += nt) {
+        int pl = i / (CT * (CT / 4)), j = i % (CT * (CT / 4));
+        int r = j / (CT / 4), c4 = (j % (CT / 4)) * 4;
+        int gy = csy + r, gx = csx + c4;
+        const P *Rc = plane_ptr<const P>(f.R[1 + pl]);
+        int v[4] = {0, 0, 0, 0};
+        if (gy >= 0 && gy < f.ch) {
+            if (gx >= 0 && gx + 3 < f.cw)
+                Vec4<P>::unpack(*reinterpret_cast<const typename Vec4<P>::T *>(Rc + gy * uvs + gx), v);
+            else
+                for (int k = 0; k < 4; k++)
+                    if (gx + k >= 0 && gx + k < f.cw) v[k] = Rc[gy * uvs + gx + k];
+        }
+        for (int k = 0; k < 4; k++) sm.uv[pl][r * CP + c4 + k] = (int16_t)v[k];
     }
     // the tile's side-info (its loads are in flight together with the
     // sample loads above); stage_side ends with a barrier

@@ -582,14 +582,16 @@ R2G_D void lr_producer(const Src &src, LrSmem &sm, int lane) {
             pdl_wait();
             waited = true;
         }
-        // near the end of the list take the next item only once the
-        // consumers are on the last one published (one item queued rather
-        // than two), so the CTAs run out of work closer together
+        // near the end of the list (fewer than two items per CTA left) take
+        // the next item only once the consumers are on the last one
+        // published (one item queued rather than two), so the CTAs run out
+        // of work closer together; from three items per CTA on it made the
+        // kernel shorter alone but the frame's pipelined step longer
         if (k >= 1) {
             unsigned taken = 0;
             if (lane == 0) taken = *reinterpret_cast<volatile unsigned *>(&sched->next);
             taken = __shfl_sync(0xffffffffu, taken, 0);
-            if ((int)(3 * gridDim.x + taken) >= n && !mbar_wait(&sm.empty[(k - 1) & 1], ((k - 1) >> 1) & 1)) {
+            if ((int)(2 * gridDim.x + taken) >= n && !mbar_wait(&sm.empty[(k - 1) & 1], ((k - 1) >> 1) & 1)) {
                 ok = false;
                 break;
             }
