@@ -188,6 +188,11 @@ struct CdefSmem {
     BlockParams bp[NB];
     int toff_y[8][6], toff_c[8][6];  // tap offsets per direction (tile pitches)
     int s_ccso[3];
+    // per plane, the CCSO offset of every class index (ccso_add's lookup
+    // of the plane's packed filter_off nibble in CCSO_OFFSET), so the
+    // per-pixel lookup is one shared-memory byte instead of a
+    // lane-dependent read of the kernel parameters
+    int8_t ccso_off[3][256];
 };
 
 // Eight consecutive samples x0 .. x0+7 of one row as four int16 pairs (low
@@ -261,6 +266,13 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
     const R2gAv2Filter &m = f.masks[(by0 >> 6) * f.sb256w + sb256x];
     const R2gFrameParams &fp = f.fp;
     if (tid < 3) sm.s_ccso[tid] = f.ccso_on ? m.ccso[tid] : 0;
+    if (f.ccso_on)
+        for (int i = tid; i < 3 * 256; i += blockDim.x) {
+            const int pl = i >> 8, idx = i & 255, bi = idx >> 1;
+            const R2gCcsoPlane &c = fp.ccso[pl];
+            const int packed = bi < 64 ? c.filter_off[bi] : 0;
+            sm.ccso_off[pl][idx] = f.tab.CCSO_OFFSET[c.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))];
+        }
     const int cdef_idx = m.cdef_idx[((by0 & 0x30) >> 2) + (sbx & 3)];
     const int sidx = cdef_idx < 0 ? 0 : cdef_idx;
     const bool cdef_active = !(cdef_idx == -1 || !f.cdef_on ||
@@ -475,9 +487,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
                     idx = ((int)((ccso_score(t[coff] - px, cq, cp.edge_clf) << 5) |
                                  (ccso_score(t[-coff] - px, cq, cp.edge_clf) << 3)) |
                            band_) & 0xff;
-                const int bi = idx >> 1;
-                const int packed = bi < 64 ? cp.filter_off[bi] : 0;
-                v = clip_px_(v + f.tab.CCSO_OFFSET[cp.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], bdmax);
+                v = clip_px_(v + sm.ccso_off[0][idx], bdmax);
             }
             out[k] = v;
         }
@@ -515,9 +525,7 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
                                  (ccso_score(t[-o] - cl, q, cpc.edge_clf) << 3)) |
                            band_) & 0xff;
                 }
-                const int bi = idx >> 1;
-                const int packed = bi < 64 ? cpc.filter_off[bi] : 0;
-                v = clip_px_(v + f.tab.CCSO_OFFSET[cpc.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))], bdmax);
+                v = clip_px_(v + sm.ccso_off[1 + pl][idx], bdmax);
             }
         }
         Cp[cgy * uvs + cgx] = (P)v;
