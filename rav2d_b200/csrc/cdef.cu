@@ -193,6 +193,9 @@ struct CdefSmem {
     // per-pixel lookup is one shared-memory byte instead of a
     // lane-dependent read of the kernel parameters
     int8_t ccso_off[3][256];
+    // chroma CCSO parameters per plane (U, V): band shift, band-only flag,
+    // quantiser step, tap offset in the luma tile, edge classifier
+    int ccso_c[2][5];
 };
 
 // Eight consecutive samples x0 .. x0+7 of one row as four int16 pairs (low
@@ -273,6 +276,14 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
             const int packed = bi < 64 ? c.filter_off[bi] : 0;
             sm.ccso_off[pl][idx] = f.tab.CCSO_OFFSET[c.scale_idx * 8 + (7 & (packed >> (4 * (idx & 1))))];
         }
+    if (tid < 2) {
+        const R2gCcsoPlane &c = fp.ccso[1 + tid];
+        sm.ccso_c[tid][0] = f.bitdepth - c.max_band_log2;
+        sm.ccso_c[tid][1] = c.bo_only;
+        sm.ccso_c[tid][2] = f.tab.CCSO_QUANT_SZ[c.scale_idx * 4 + c.quant_idx];
+        sm.ccso_c[tid][3] = c_ccso_pos[c.ext_filter_support][0] * TW + c_ccso_pos[c.ext_filter_support][1];
+        sm.ccso_c[tid][4] = c.edge_clf;
+    }
     const int cdef_idx = m.cdef_idx[((by0 & 0x30) >> 2) + (sbx & 3)];
     const int sidx = cdef_idx < 0 ? 0 : cdef_idx;
     const bool cdef_active = !(cdef_idx == -1 || !f.cdef_on ||
@@ -507,22 +518,20 @@ R2G_D void cdef_region(const DevFrame &f, CdefSmem &sm, int sbx, int rr) {
             v = bitdepth == 8 ? (v & 0xff) : (v & 0xffff);
         }
         if (sm.s_ccso[1 + pl]) {
-            const R2gCcsoPlane &cpc = fp.ccso[1 + pl];
+            const int *cpc = sm.ccso_c[pl];
             const int by_idx = ((by0 + br * 2) & 0x3e) >> 1;
             const bool ll = f.any_lossless && ((m.lossless_mask_uv[by_idx][sb64x_idx] >> (cc >> 2)) & 1);
             if (!ll) {
                 // co-located luma of the chroma sample (ccso_prep, 4:2:0)
                 const int16_t *t = &sm.ty[2 + 2 * cr][XO + 2 * cc];
                 const int cl = t[0];
-                const int band_ = (int)((uint32_t)cl >> (bitdepth - cpc.max_band_log2));
+                const int band_ = (int)((uint32_t)cl >> cpc[0]);
                 int idx;
-                if (cpc.bo_only) {
+                if (cpc[1]) {
                     idx = band_ & 0xff;
                 } else {
-                    const int q = f.tab.CCSO_QUANT_SZ[cpc.scale_idx * 4 + cpc.quant_idx];
-                    const int o = c_ccso_pos[cpc.ext_filter_support][0] * TW + c_ccso_pos[cpc.ext_filter_support][1];
-                    idx = ((int)((ccso_score(t[o] - cl, q, cpc.edge_clf) << 5) |
-                                 (ccso_score(t[-o] - cl, q, cpc.edge_clf) << 3)) |
+                    const int q = cpc[2], o = cpc[3];
+                    idx = ((int)((ccso_score(t[o] - cl, q, cpc[4]) << 5) | (ccso_score(t[-o] - cl, q, cpc[4]) << 3)) |
                            band_) & 0xff;
                 }
                 v = clip_px_(v + sm.ccso_off[1 + pl][idx], bdmax);
