@@ -31,6 +31,7 @@
 #include "r2g_runtime.h"
 
 int r2g_grain_ready(int device);
+int r2g_grain_enqueue(R2gCtx *ctx, R2gFrame *f, const R2gFilmGrainData *fgd, uint32_t seed);
 
 namespace {
 
@@ -39,6 +40,10 @@ enum { N_BSTAGES = 4 };  // deblock, cdef, lr, grain apply
 // count; the hardware then hands items to SMs as CTAs finish) rather than a
 // persistent grid of CTAs-per-SM x SMs.
 constexpr int PER_ITEM = 255;
+// Frames of at least this many luma samples skip the batch's persistent
+// kernels and run through the per-frame pipeline (measured on a B200: 1080p
+// and 4K frames filter faster per frame, 720p and smaller faster batched).
+constexpr int64_t R2G_BATCH_DIRECT_PIX = 1500000;
 
 struct Layout {
     int max_frames = 0;
@@ -329,8 +334,15 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
     if (!b.cache_loaded) load_cache(b);
     if (r2g_grain_ready(ctx->device) != R2G_OK) return R2G_E_DEVICE;
 
-    // stage every frame; collect descriptors and grain parameters
-    std::vector<DevFrame> frames(n);
+    // stage every frame; collect descriptors and grain parameters of the
+    // frames the batch's persistent kernels take.  A frame of at least
+    // R2G_BATCH_DIRECT_PIX luma samples fills the GPU by itself: it runs
+    // through the per-frame pipeline instead (its stages overlap the next
+    // frame's by programmatic dependent launch, which a batch's stage
+    // barriers do not allow), before the batch on the same stream.
+    std::vector<DevFrame> frames;
+    frames.reserve(n);
+    std::vector<int> direct, batched;
     std::vector<GrainBatch> grains;
     int counts[8] = {0};
     bool any8 = false, any10 = false;
@@ -345,15 +357,20 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
             ctx->err = "batch item without side-info on a frame that was never staged";
             return R2G_E_INVALID;
         }
-        frames[i] = f->desc;
+        if (items[i].fgd && r2g_grain_validate(items[i].fgd, items[i].grain_seed) != R2G_OK) {
+            ctx->err = "film-grain parameters out of range";
+            return R2G_E_INVALID;
+        }
+        if ((int64_t)f->w * f->h >= R2G_BATCH_DIRECT_PIX) {
+            direct.push_back(i);
+            continue;
+        }
+        batched.push_back(i);
+        frames.push_back(f->desc);
         (f->bd > 8 ? any10 : any8) = true;
         counts[0] += r2g_deblock_items(f->desc);
         counts[1] += r2g_cdef_items(f->desc);
         if (items[i].fgd) {
-            if (r2g_grain_validate(items[i].fgd, items[i].grain_seed) != R2G_OK) {
-                ctx->err = "film-grain parameters out of range";
-                return R2G_E_INVALID;
-            }
             if (!f->grain_scratch) {
                 rc = r2g_dev_alloc(ctx, &f->grain_scratch, R2G_GRAIN_SCRATCH);
                 if (rc != R2G_OK) return rc;
@@ -361,7 +378,7 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
             GrainBatch g;
             memset(&g, 0, sizeof(g));
             r2g_grain_params(*items[i].fgd, items[i].grain_seed, f->bd, g);
-            g.frame = i;
+            g.frame = (int)frames.size() - 1;
             g.lut = (int16_t *)f->grain_scratch;
             g.scaling = (uint8_t *)f->grain_scratch + 3 * 73 * 82 * 2;
             counts[3] += r2g_grain_items(f->w, f->h, items[i].fgd->block_size);
@@ -370,6 +387,29 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
         }
     }
     counts[4] = (int)grains.size();
+    if (copy_stream && copy_stream != ctx->stream) {
+        // the kernels wait for this batch's side-info (and any recon uploads
+        // the caller enqueued before) on the copy stream
+        if (cudaEventRecord(b.copied, copy_stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ctx->stream, b.copied, 0) != cudaSuccess)
+            return R2G_E_DEVICE;
+    }
+    for (int i : direct) {
+        R2gFrame *f = items[i].frame;
+        rc = r2g_frame_before_compute(ctx, f);
+        if (rc != R2G_OK) return rc;
+        r2g_launch_pipeline(ctx, f->desc);
+        if (cudaGetLastError() != cudaSuccess) return R2G_E_DEVICE;
+        f->out_buf = f->desc.lr_on ? 3 : (f->desc.cdef_stage_on ? 2 : (f->desc.deblock_on ? 1 : 0));
+        if (items[i].fgd) {
+            rc = r2g_grain_enqueue(ctx, f, items[i].fgd, items[i].grain_seed);
+            if (rc != R2G_OK) return rc;
+        }
+        rc = r2g_frame_after_compute(ctx, f);
+        if (rc != R2G_OK) return rc;
+    }
+    if (batched.empty()) return R2G_OK;
+    const int nb = (int)batched.size();
     const int cls = any8 && any10 ? 2 : (any10 ? 1 : 0);
     // loop-restoration tile shape: the tuned one, else the default; while
     // the stage is still to be tuned, room for the largest item count
@@ -392,13 +432,13 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
     if (s.used && cudaEventSynchronize(s.done) != cudaSuccess) return R2G_E_DEVICE;
     int need[N_BSTAGES];
     for (int k = 0; k < N_BSTAGES; k++) need[k] = k == 2 && lr_cap > counts[2] ? lr_cap : counts[k];
-    bool fits = n <= s.L.max_frames;
+    bool fits = nb <= s.L.max_frames;
     for (int k = 0; k < N_BSTAGES; k++) fits = fits && need[k] <= s.L.max_items[k];
     if (!fits) {
         int want_items[N_BSTAGES];
         for (int k = 0; k < N_BSTAGES; k++)
             want_items[k] = need[k] > s.L.max_items[k] ? need[k] + need[k] / 2 + 64 : s.L.max_items[k];
-        Layout L = make_layout(n > s.L.max_frames ? n + n / 2 + 4 : s.L.max_frames, want_items);
+        Layout L = make_layout(nb > s.L.max_frames ? nb + nb / 2 + 4 : s.L.max_frames, want_items);
         if (s.host) cudaFreeHost(s.host);
         if (s.dev) r2g_dev_free(ctx, s.dev, s.L.bytes);
         s.host = nullptr;
@@ -416,14 +456,14 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
     // fill the staging blob
     memset(s.host, 0, 256);
     memcpy(s.host, counts, sizeof(counts));
-    memcpy(s.host + s.L.off_frames, frames.data(), sizeof(DevFrame) * n);
+    memcpy(s.host + s.L.off_frames, frames.data(), sizeof(DevFrame) * nb);
     if (!grains.empty()) memcpy(s.host + s.L.off_grain, grains.data(), sizeof(GrainBatch) * grains.size());
     {
         uint32_t *w0 = (uint32_t *)(s.host + s.L.off_work[0]);
         uint32_t *w1 = (uint32_t *)(s.host + s.L.off_work[1]);
         uint32_t *w2 = (uint32_t *)(s.host + s.L.off_work[2]);
         int c0 = 0, c1 = 0, c2 = 0;
-        for (int i = 0; i < n; i++) {
+        for (int i = 0; i < nb; i++) {
             uint32_t hi = (uint32_t)i << 22;
             for (int j = 0, e = r2g_deblock_items(frames[i]); j < e; j++) w0[c0++] = hi | j;
             for (int j = 0, e = r2g_cdef_items(frames[i]); j < e; j++) w1[c1++] = hi | j;
@@ -436,13 +476,6 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
             int e = r2g_grain_items(f.w, f.h, grains[gi].gp.d.block_size);
             for (int j = 0; j < e; j++) w3[c3++] = ((uint32_t)gi << 22) | j;
         }
-    }
-    if (copy_stream && copy_stream != ctx->stream) {
-        // the kernels wait for this batch's side-info (and any recon uploads
-        // the caller enqueued before) on the copy stream
-        if (cudaEventRecord(b.copied, copy_stream) != cudaSuccess ||
-            cudaStreamWaitEvent(ctx->stream, b.copied, 0) != cudaSuccess)
-            return R2G_E_DEVICE;
     }
     rc = copy_blob(ctx, s, counts);
     if (rc != R2G_OK) return rc;
@@ -469,19 +502,19 @@ int r2g_batch_enqueue(R2gCtx *ctx, const R2gBatchItem *items, int n, cudaStream_
         rc = build_graph(ctx, b, s, grids, tpl_grid);
         if (rc != R2G_OK) return rc;
     }
-    for (int i = 0; i < n; i++) {
+    for (int i : batched) {
         rc = r2g_frame_before_compute(ctx, items[i].frame);
         if (rc != R2G_OK) return rc;
     }
     if (cudaGraphLaunch(s.exec, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
-    for (int i = 0; i < n; i++) {
+    for (int i : batched) {
         rc = r2g_frame_after_compute(ctx, items[i].frame);
         if (rc != R2G_OK) return rc;
     }
     ctx->launches += 5;
     if (cudaEventRecord(s.done, ctx->stream) != cudaSuccess) return R2G_E_DEVICE;
     s.used = true;
-    for (int i = 0; i < n; i++) {
+    for (int i : batched) {
         R2gFrame *f = items[i].frame;
         f->out_buf = f->desc.lr_on ? 3 : (f->desc.cdef_stage_on ? 2 : (f->desc.deblock_on ? 1 : 0));
     }

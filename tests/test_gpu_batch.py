@@ -104,11 +104,15 @@ def test_batch_alone_equals_in_mix(ctx):
 def test_batch_grows_and_reports_grid(ctx):
     small = _frames([(64, 64, 8, "db", False)])
     _batch(ctx, small)
-    big = _frames([(1920, 1080, 10, "full", True)] * 2 + [(3840, 2160, 8, "full", True)])
+    # many small frames grow the batch's staging slots; the 1080p and 4K
+    # frames of the same call run through the per-frame pipeline
+    big = _frames([(1920, 1080, 10, "full", True)] * 2 + [(3840, 2160, 8, "full", True)] +
+                  [(640, 360, 10, "full", True)] * 24)
     got = _batch(ctx, big)
-    wf, wg = _per_frame(ctx, big[2], True)
-    _same(got[2][0], wf, big[2], "4K after growth (filter)")
-    _same(got[2][1], wg, big[2], "4K after growth (grain)")
+    for k in (2, 26):
+        wf, wg = _per_frame(ctx, big[k], True)
+        _same(got[k][0], wf, big[k], f"frame {k} after growth (filter)")
+        _same(got[k][1], wg, big[k], f"frame {k} after growth (grain)")
     sms, cfg = ctx.batch_config()
     assert sms > 0 and all(v >= 0 for v in cfg.values())  # 0: one CTA per work item
 
