@@ -486,7 +486,9 @@ typedef struct R2gBatchItem {
     uint32_t grain_seed;
 } R2gBatchItem;
 /* Enqueue the whole batch (at most 1023 distinct frames) as one persistent
- * launch per stage; returns a ticket for r2g_wait.  An item whose fp and side
+ * launch per stage; frames of at least 1.5 M luma samples (1080p and up),
+ * which fill the GPU alone, run through the per-frame pipeline first, on
+ * the same stream.  Returns a ticket for r2g_wait.  An item whose fp and side
  * are both NULL runs with the side-info of the frame's last r2g_frame_stage
  * (as r2g_frame_run does); its inloop_mask is then ignored.  Film grain is
  * applied per item when fgd is non-NULL (read it back with which = 1). */
