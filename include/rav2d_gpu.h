@@ -267,11 +267,12 @@ const char *r2g_last_error(R2gCtx *ctx);
  * (a cudaStream_t passed as void*; NULL restores the context's own stream). */
 int r2g_ctx_set_stream(R2gCtx *ctx, void *stream);
 /* Copy overlap (no counterpart in the reference, whose filters work on host
- * memory): when enabled, r2g_frame_upload_recon and r2g_frame_stage copy on
- * an upload stream and r2g_download on a download stream of the context,
- * each frame's copies and kernels ordered by events, so the transfers of one
- * frame overlap the kernels of another.  r2g_sync waits for all three
- * streams; r2g_ctx_fence makes the context stream wait for every copy issued
+ * memory): when enabled, r2g_frame_upload_recon copies on an upload
+ * stream, r2g_frame_stage on a second upload stream (its small side-info
+ * copies then overlap the recon upload instead of queueing behind it) and
+ * r2g_download on a download stream of the context, each frame's copies and
+ * kernels ordered by events, so the transfers of one frame overlap the
+ * kernels of another.  r2g_sync waits for all of these streams; r2g_ctx_fence makes the context stream wait for every copy issued
  * so far (an event recorded on it afterwards marks the end of all of them).
  * In this mode host buffers are read asynchronously: page-locked recon
  * planes, and side-info records that are page-locked (they are then copied

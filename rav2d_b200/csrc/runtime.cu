@@ -394,7 +394,7 @@ extern "C" int r2g_sync(R2gCtx *ctx) {
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->side_stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream})
+    for (cudaStream_t st : {ctx->up_stream, ctx->down_stream, ctx->side_up_stream})
         if (st) CK(cudaStreamSynchronize(st));
     // a stage kernel whose bounded wait ran out left its work incomplete
     uint32_t faults[2] = {0, 0};
