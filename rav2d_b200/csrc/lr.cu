@@ -893,23 +893,39 @@ R2G_D void filter_luma(const DevFrame &f, LrSmem &sm, int x0, int y0, int sh, in
                                      ? f.tab.PC_WIENER_SUB_CLASSIFY + f.wiener_idx * 256
                                      : f.tab.PC_WIENER_SUB_CLASSIFY_NS +
                                            (f.wiener_idx * 7 + (f.ns_ci >= 0 ? imin_(f.ns_ci, 6) : 0)) * 256;
-        for (int i = tid; i < bh4 * bw4; i += NCT) {
-            const int by = i / bw4, bx = i - by * bw4;
+        // two adjacent lanes per 4x4 block, each summing three of the six
+        // feature rows; the trip count is uniform over the consumers so
+        // the pair's partial sums combine with one shuffle
+        const int nblk = bh4 * bw4;
+        for (int base = 0; base < 2 * nblk; base += NCT) {
+            const int i = base + tid;
+            const bool act = i < 2 * nblk;
+            const int blk = act ? (i >> 1) : 0, half = i & 1;
+            const int by = blk / bw4, bx = blk - by * bw4;
             int fs0 = 0, fs1 = 0, fs2 = 0;
+            if (act) {
 #pragma unroll
-            for (int dy = -1; dy <= 4; dy++)
+                for (int t = 0; t < 3; t++) {
+                    const int dy = 3 * half - 1 + t;
 #pragma unroll
-                for (int dx = -1; dx <= 4; dx++) {
-                    const int16_t *w = &(topi && by == 0 ? WT16 : W16)[2 * ((by * 4 + dy + 6) * LW + bx * 4 + dx + 6)];
-                    constexpr int R = 2 * LW, C1 = 2;
-                    const int m2 = 2 * w[0];
-                    const int vert = w[-R] - m2 + w[R];
-                    const int anti = w[-R + C1] - m2 + w[R - C1];
-                    const int diag = w[-R - C1] - m2 + w[R + C1];
-                    fs0 += vert < 0 ? -vert : vert;
-                    fs1 += anti < 0 ? -anti : anti;
-                    fs2 += diag < 0 ? -diag : diag;
+                    for (int dx = -1; dx <= 4; dx++) {
+                        const int16_t *w =
+                            &(topi && by == 0 ? WT16 : W16)[2 * ((by * 4 + dy + 6) * LW + bx * 4 + dx + 6)];
+                        constexpr int R = 2 * LW, C1 = 2;
+                        const int m2 = 2 * w[0];
+                        const int vert = w[-R] - m2 + w[R];
+                        const int anti = w[-R + C1] - m2 + w[R - C1];
+                        const int diag = w[-R - C1] - m2 + w[R + C1];
+                        fs0 += vert < 0 ? -vert : vert;
+                        fs1 += anti < 0 ? -anti : anti;
+                        fs2 += diag < 0 ? -diag : diag;
+                    }
                 }
+            }
+            fs0 += __shfl_xor_sync(0xffffffffu, fs0, 1);
+            fs1 += __shfl_xor_sync(0xffffffffu, fs1, 1);
+            fs2 += __shfl_xor_sync(0xffffffffu, fs2, 1);
+            if (!act || half) continue;
             int s = 0;
             const int np[3] = {16, 4, 1};
 #pragma unroll
