@@ -259,7 +259,7 @@ struct LrSmem {
     // window holds gdf_prep's saved rows 0 .. 5 there), same layout as wp
     // (rows -6, -5 unused)
     uint32_t wtop[15 * LW];
-    uint16_t gcell[17 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
+    alignas(8) uint16_t gcell[17 * 33 * 4];  // GDF 2x2 gradient cells, 4 directions
     uint8_t classes[8][16];
     // consumer-side copies of the item's row data (the slot is released
     // before filtering)
@@ -794,11 +794,12 @@ R2G_D void gdf_pair(const DevFrame &f, const LrSmem &sm, const uint32_t *wc, int
     constexpr int up = sizeof(P) == 1 ? 2 : 0;  // the 10-bit internal domain
     const int ci = (uw >> 1) + 1;
     const int j = y >> 1, c = x1 >> 1;
-    int gsum[4];
-#pragma unroll
-    for (int d = 0; d < 4; d++)
-        gsum[d] = sm.gcell[(j * ci + c) * 4 + d] + sm.gcell[(j * ci + c + 1) * 4 + d] +
-                  sm.gcell[((j + 1) * ci + c) * 4 + d] + sm.gcell[((j + 1) * ci + c + 1) * 4 + d];
+    // the four cells' 16-bit direction sums add as 16x2 pairs without a
+    // carry between the halves: a cell holds at most 4 x 2046 per direction
+    const uint2 *gc = reinterpret_cast<const uint2 *>(sm.gcell);
+    const uint2 ca = gc[j * ci + c], cb = gc[j * ci + c + 1], cc = gc[(j + 1) * ci + c], cd = gc[(j + 1) * ci + c + 1];
+    const uint32_t s01 = ca.x + cb.x + cc.x + cd.x, s23 = ca.y + cb.y + cc.y + cd.y;
+    const int gsum[4] = {(int)(s01 & 0xffff), (int)(s01 >> 16), (int)(s23 & 0xffff), (int)(s23 >> 16)};
     const int cls = (gsum[0] <= gsum[1]) | ((gsum[2] <= gsum[3]) << 1);
     const int4 *wt = sm.s_w[cls];
     const uint2 *aa = sm.s_aa[cls];
