@@ -49,9 +49,9 @@ BYTES_PER_PX = {"deblock": 6.0, "cdef_ccso": 6.0, "loop_restoration": 8.0, "film
 # bytes read + written per launch (the outputs were still in L2 when the
 # capture ended, so the write term was 0) and warp instructions per launch.
 NCU_CAPTURE = {
-    "commit": "b61cfe5 (deblock, LR), 7a43533 (CDEF+CCSO)",
-    "traffic": {"deblock": 6619904, "cdef_ccso": 6298624, "loop_restoration": 6850304},
-    "warp_inst": {"deblock": 10063486, "cdef_ccso": 26085809, "loop_restoration": 27323495},
+    "commit": "b61cfe5 (deblock), 7a43533 (CDEF+CCSO), 2b0974d (LR)",
+    "traffic": {"deblock": 6619904, "cdef_ccso": 6298624, "loop_restoration": 6847232},
+    "warp_inst": {"deblock": 10063486, "cdef_ccso": 26085809, "loop_restoration": 26899014},
 }
 SMS = 148
 
